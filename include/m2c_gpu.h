@@ -1,0 +1,231 @@
+/*
+ * m2c_gpu.h — C ABI of the B200 (sm_100a) finite-volume step for M2C.
+ *
+ * The library replaces, on one structured subdomain, the explicit residual
+ * and Runge-Kutta update of the M2C reference:
+ *   SpaceOperator::ComputeResidual          (SpaceOperator.cpp:3351-3409)
+ *   SpaceOperator::ComputeTimeStepSize      (SpaceOperator.cpp:2202-2227)
+ *   TimeIntegratorRK2/RK3::AdvanceOneTimeStep (TimeIntegrator.cpp:291-428, 496-690)
+ *   ExactRiemannSolverBase::ComputeRiemannSolution (ExactRiemannSolverBase.cpp:59-342)
+ *   LevelSetOperator::ComputeResidual / Reinitialize, MultiPhaseOperator updates
+ * The reference reaches these through C++ virtual dispatch per face and per
+ * state; this boundary is field-level: one call advances a whole field.
+ *
+ * Conventions
+ *  - Every entry point returns m2cg_status (0 = OK). The first failure inside
+ *    a kernel is recorded (cell index, code) and readable with
+ *    m2cg_last_error(); kernels never trap.
+ *  - Host arrays use the reference's ghosted local-vector layout
+ *    (SpaceVariable3D::GetDataPointer, SpaceVariable.cpp:254-261): a box of
+ *    (nx+2)*(ny+2)*(nz+2) nodes, node (i,j,k) with i,j,k in [-1, n] stored at
+ *    ((k+1)*(ny+2) + (j+1))*(nx+2) + (i+1); V carries 5 doubles per node
+ *    (rho, u, v, w, p), ID and phi one double per node.
+ *  - Host buffers are borrowed only for the duration of a call.
+ *  - One context = one CUDA stream; calls are stream-ordered and a context is
+ *    not thread-safe. Different contexts may be used from different threads.
+ */
+#ifndef M2C_GPU_H
+#define M2C_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  M2CG_OK = 0,
+  M2CG_ERR_ARG = 1,          /* bad argument or unsupported option */
+  M2CG_ERR_CUDA = 2,         /* CUDA runtime error (message in m2cg_last_error) */
+  M2CG_ERR_STATE = 3,        /* non-physical state (VarFcnBase::CheckState fails) */
+  M2CG_ERR_RIEMANN = 4,      /* interface Riemann solver reported failures */
+  M2CG_ERR_REINIT = 5,       /* level-set reinitialisation did not converge */
+  M2CG_ERR_ITER_CAP = 6,     /* a device loop hit its iteration cap */
+  M2CG_ERR_NOMEM = 7,        /* device allocation failed */
+  M2CG_ERR_UNSUPPORTED = 8   /* option the GPU path does not implement */
+} m2cg_status;
+
+/* Boundary types: values of MeshData::BcType (IoData.h:266-267), plus
+ * PERIODIC, which the reference cannot express (extension). */
+enum {
+  M2CG_BC_NONE = 0, M2CG_BC_INLET = 1, M2CG_BC_OUTLET = 2, M2CG_BC_SLIPWALL = 3,
+  M2CG_BC_STICKWALL = 4, M2CG_BC_SYMMETRY = 5, M2CG_BC_PERIODIC = 100
+};
+
+/* Mesh and boundary conditions (MeshData, IoData.h:255-278; BcsData inlet/outlet).
+ * Cell centres/widths: uniform as MeshGenerator::ComputeMesh1DUniform
+ * (MeshGenerator.cpp:146-158) unless xc/dx (etc.) are given (length nx). */
+typedef struct {
+  int nx, ny, nz;
+  double x0, xmax, y0, ymax, z0, zmax;
+  const double *xc, *dx, *yc, *dy, *zc, *dz; /* optional non-uniform mesh, else NULL */
+  int bc[6];              /* x0, xmax, y0, ymax, z0, zmax */
+  double inlet[5];        /* primitive state at INLET ghosts */
+  double outlet[5];       /* primitive state at OUTLET ghosts */
+} m2cg_grid;
+
+/* Material (MaterialModelData, IoData.h:458-486): SG (VarFcnSG.h) or NASG
+ * (VarFcnNASG.h) with clipping bounds. */
+enum { M2CG_EOS_SG = 0, M2CG_EOS_NASG = 1 };
+typedef struct {
+  int eos;
+  double gamma;           /* specificHeatRatio */
+  double p_c;             /* SG pressureConstant / NASG pressureConstant */
+  double b;               /* NASG volumeConstant */
+  double q;               /* NASG energyConstant */
+  double rhomin, pmin, rhomax, pmax;
+  double failsafe_density;
+} m2cg_material;
+
+/* Numerical scheme (SchemeData, ReconstructionData, TsData, MultiPhaseData,
+ * ExactRiemannSolverData: IoData.h:544-795). Enum values are the reference's. */
+enum { M2CG_FLUX_ROE = 0, M2CG_FLUX_LLF = 1, M2CG_FLUX_HLLC = 2 };
+enum { M2CG_REC_CONSTANT = 0, M2CG_REC_LINEAR = 1 };
+enum { M2CG_LIM_NONE = 0, M2CG_LIM_GENMINMOD = 1, M2CG_LIM_VANALBADA = 2 };
+enum { M2CG_RECVAR_PRIMITIVE = 0, M2CG_RECVAR_CONSERVATIVE = 1,
+       M2CG_RECVAR_PRIM_CHAR = 2, M2CG_RECVAR_CONS_CHAR = 3 };
+enum { M2CG_PREC_FP64 = 0, M2CG_PREC_MIXED = 1 };
+enum { M2CG_MPFLUX_EXACT = 0, M2CG_MPFLUX_NUMERICAL = 1, M2CG_MPFLUX_LLF = 2 };
+
+typedef struct {
+  int flux;               /* SchemeData::flux */
+  double roe_delta;       /* SchemeData::delta (Harten entropy fix) */
+  int rec_type;           /* ReconstructionData::type */
+  int limiter;            /* ReconstructionData::limiter */
+  double minmod_coeff;    /* ReconstructionData::generalized_minmod_coeff */
+  int slope_near_interface; /* 0 ZERO, 1 NONZERO */
+  int rec_var;            /* ReconstructionData::varType */
+  int rk_order;           /* 1 (forward Euler), 2, 3 */
+  double cfl;             /* TsData::cfl */
+  int precision;          /* M2CG_PREC_FP64 or M2CG_PREC_MIXED */
+  /* MultiPhaseData */
+  int mp_flux;            /* EXACT / NUMERICAL / LLF */
+  int mp_recon;           /* CONSTANT / LINEAR */
+  int mp_phasechange_type;/* 0 RIEMANN_SOLUTION, 1 EXTRAPOLATION */
+  int mp_phasechange_dir; /* 0 ALL, 1 UPWIND */
+  int mp_apply_failsafe_density; /* 0 Off, 1 On */
+  /* ExactRiemannSolverData */
+  int riem_maxits_main, riem_maxits_bracket, riem_maxits_shock, riem_nsteps_rarefaction;
+  double riem_tol_main, riem_tol_shock, riem_tol_rarefaction;
+  double riem_min_pressure, riem_failure_threshold, riem_pressure_at_failure;
+} m2cg_scheme;
+
+/* One level set (LevelSetSchemeData, IoData.h:653-679; reinit
+ * LevelSetReinitializationData, IoData.h:628-651). Finite-difference
+ * UPWIND_CENTRAL_3 solver, full domain. */
+enum { M2CG_LSBC_NONE = 0, M2CG_LSBC_ZERO_NEUMANN = 1, M2CG_LSBC_LINEAR_EXTRAPOLATION = 2,
+       M2CG_LSBC_NON_NEGATIVE = 3 };
+typedef struct {
+  int material_id;        /* material in the phi<0 region */
+  int bc[6];
+  int reinit_frequency;   /* <=0: never */
+  int reinit_maxits;
+  double reinit_cfl;
+  double reinit_tol;
+  int reinit_first_layer; /* 0 FIXED (only FIXED is implemented) */
+} m2cg_levelset;
+
+/* Fill a scheme/material/level-set struct with the reference's defaults
+ * (IoData.cpp:860-871, 1049-1058, 1154-1160, 1205-1265, 1345-1357, 1400-1417,
+ * 1472-1503). */
+void m2cg_default_scheme(m2cg_scheme* s);
+void m2cg_default_material(m2cg_material* m);
+void m2cg_default_levelset(m2cg_levelset* l);
+
+typedef struct m2cg_ctx m2cg_ctx;
+
+/* Create a context on the current CUDA device. nls = 0 (one material) or 1.
+ * Replaces the setup in Main.cpp:106-379 for this path. */
+m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* scheme,
+                        const m2cg_material* mats, int nmat,
+                        const m2cg_levelset* ls, int nls, m2cg_ctx** out);
+m2cg_status m2cg_destroy(m2cg_ctx* ctx);
+
+/* Host <-> device state in the ghosted host layout above. ID and phi may be
+ * NULL (single material). Upload clips density/pressure and fills ghost
+ * nodes as SpaceOperator::SetInitialCondition does at its end
+ * (SpaceOperator.cpp:1088-1090), then sets ghost IDs from their images
+ * (MultiPhaseOperator::UpdateMaterialIDAtGhostNodes, MultiPhaseOperator.cpp:796-819). */
+m2cg_status m2cg_upload_state(m2cg_ctx* ctx, const double* V, const double* ID, const double* phi);
+m2cg_status m2cg_download_state(m2cg_ctx* ctx, double* V, double* ID, double* phi);
+
+/* dt = cfl * min over cells of dx/(|u|+c)  (SpaceOperator::ComputeTimeStepSize). */
+m2cg_status m2cg_compute_dt(m2cg_ctx* ctx, double* dt_out);
+
+/* R = -(1/vol) * sum of face fluxes for the current state, written to R in
+ * the ghosted host layout (interior nodes only are meaningful).
+ * (SpaceOperator::ComputeResidual, SpaceOperator.cpp:3351-3409.) */
+m2cg_status m2cg_compute_residual(m2cg_ctx* ctx, double* R_host);
+
+/* One full time step of size dt at time t_new (the reference passes the
+ * updated time), including level-set advance, material-ID update,
+ * reinitialisation and the post-step multiphase update
+ * (TimeIntegratorRK*::AdvanceOneTimeStep + UpdateSolutionAfterTimeStepping). */
+m2cg_status m2cg_advance(m2cg_ctx* ctx, double t_new, double dt, int time_step);
+
+/* Run nsteps steps with dt from the CFL condition each step, stopping at
+ * t_max (the last step is shortened as in Main.cpp:537-541). *t is updated. */
+m2cg_status m2cg_run(m2cg_ctx* ctx, int nsteps, double t_max, double* t, int* steps_done);
+
+/* Per-run counters, mirroring the reference's warnings and totals. */
+typedef struct {
+  long long steps;
+  long long cells_updated;       /* interior cells x steps */
+  long long riemann_calls;       /* interface Riemann problems solved */
+  long long riemann_iterations;  /* outer secant iterations, summed */
+  long long riemann_errors;      /* as counted at SpaceOperator.cpp:2818 */
+  long long clipped_cells;       /* ClipDensityAndPressure counts */
+  long long reinit_calls;
+  long long kernel_launches;
+} m2cg_counters;
+m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
+
+/* Text of the last error on this thread (never NULL). */
+const char* m2cg_last_error(void);
+
+/* ---------------------------------------------------------------------------
+ * Batched interface Riemann problems (ExactRiemannSolverBase::ComputeRiemannSolution,
+ * ExactRiemannSolverBase.cpp:59-342), FP64, one problem per thread.
+ * Inputs per problem: VL[5], VR[5] primitive states, idl/idr material ids,
+ * dir[3] unit normal. Outputs: Vs[5] state at xi=0, id, Vsm[5], Vsp[5]
+ * star states, iterations (outer secant iterations), err (0 OK).
+ * Host pointers; the call copies in and out.
+ * warm (optional, may be NULL): an initial star-pressure guess per problem;
+ * NaN entries mean "no guess".
+ * ------------------------------------------------------------------------- */
+m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_material* mats, int nmat,
+                               int n, const double* VL, const int* idl, const double* VR,
+                               const int* idr, const double* dir, const double* warm,
+                               double* Vs, int* id, double* Vsm, double* Vsp, int* iters, int* err);
+
+/* ---------------------------------------------------------------------------
+ * Batched 1D two-material shock tubes of uneven lengths, all advanced in one
+ * persistent launch per RK stage, captured in a CUDA graph.
+ * ------------------------------------------------------------------------- */
+typedef struct m2cg_batch m2cg_batch;
+typedef struct {
+  int cells_per_block;   /* cells handled by one CTA per work item; 0 = autotune */
+  int threads_per_block; /* 0 = autotune */
+  int use_graph;         /* capture the step loop in a CUDA graph */
+} m2cg_batch_tuning;
+
+/* ntubes tubes; tube t has len[t] cells on [0, 1] (cell width 1/len[t]),
+ * material mats[2t] on the left half and mats[2t+1] on the right half, left
+ * and right primitive states VL[5t..], VR[5t..], interface at x = 0.5 as the
+ * zero of phi = 0.5 - x. Boundary ghosts are OUTLET-type Dirichlet copies of
+ * the initial end states. */
+m2cg_status m2cg_batch_create(const m2cg_scheme* scheme, int ntubes, const int* len,
+                              const m2cg_material* mats, const double* VL, const double* VR,
+                              const m2cg_batch_tuning* tuning, m2cg_batch** out);
+/* Advance every tube by nsteps steps with a per-tube CFL dt. */
+m2cg_status m2cg_batch_run(m2cg_batch* b, int nsteps);
+/* Download tube states: V (5 doubles per cell, tubes concatenated), ID per cell. */
+m2cg_status m2cg_batch_download(m2cg_batch* b, double* V, int* ID, double* t_per_tube);
+m2cg_status m2cg_batch_get_tuning(const m2cg_batch* b, m2cg_batch_tuning* t);
+m2cg_status m2cg_batch_destroy(m2cg_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
