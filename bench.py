@@ -1,0 +1,310 @@
+"""Benchmark: cell-updates/s per RK step of the explicit finite-volume step.
+
+Workload (one GPU holds it): the 3D single-material periodic box, 256^3
+cells, ideal gas gamma 1.4, rho = 1 and p = 1/1.4 perturbed by 16 seeded
+Fourier modes (|k| in 1..8, 1%), solenoidal velocity with RMS Mach 0.3,
+generalized Roe flux with generalized minmod MUSCL (alpha 1), RK3, CFL 0.4.
+The headline runs the mixed path (FP32 reconstruction/flux, FP64 state);
+the FP64 path is timed on the same state and the L1 difference between the
+two is reported.
+
+A "step" is one full RK3 step (3 fused stage launches + the device clock).
+Inputs are larger than L2 (5 x 128 MiB per state array), so no explicit
+flush is needed between steps.
+
+Multi-GPU: the north-star path does not shard; --gpus N runs N independent
+replicas (one per GPU, "scaling": "weak"), value = all cells updated / max
+time over ranks.
+
+--impl reference: the reference's own CPU implementation (the unmodified
+sources built with single-rank shims under oracle/_ref), run on the host
+cores as independent processes, each advancing a bounded 64^3 sample of the
+same physics (symmetry walls instead of periodic: the reference has no
+periodic boundary) by one RK3 step per benchmark step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s per RK step (RK3, 256^3 periodic box, mixed FP32/FP64)"
+UNIT = "cell-updates/s"
+CPU_SAMPLE_N = 48
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=256)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+# --------------------------------------------------------------------------
+# CPU reference leg (also the cpu_baseline): independent processes
+# --------------------------------------------------------------------------
+def _cpu_worker(args):
+    n, steps, seed = args
+    sys.path.insert(0, ROOT)
+    from m2c_b200 import abi, cases
+    from oracle import ref
+    g, s, mats, V = cases.fourier_box(CPU_SAMPLE_N if n is None else n, seed=seed, bc=abi.BC_SYMMETRY)
+    c = ref.RefCase(g, s, mats)
+    c.set_state(V)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        c.run(1)
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def cpu_reference(steps, warmup, cores=None):
+    """Run the reference on `cores` processes; returns per-step wall times
+    (max over processes) and the cell count per step (all processes)."""
+    import multiprocessing as mp
+    cores = cores or min(os.cpu_count() or 1, 64)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(CPU_SAMPLE_N, warmup + steps, 100 + r) for r in range(cores)])
+    per_step = [max(r[w + warmup] for r in res) for w in range(steps)]
+    cells = cores * CPU_SAMPLE_N ** 3
+    return per_step, cells, cores
+
+
+# --------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# --------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) > 8:
+                for q, name in enumerate(names):
+                    if "Active" in r[5 + q] and "Not" not in r[5 + q]:
+                        reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per cell per stage launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return None
+    return None
+
+
+# --------------------------------------------------------------------------
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n = args.n
+    cells = n ** 3
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        per_step, ccells, cores = cpu_reference(args.steps, args.warmup)
+        tot = sum(per_step)
+        v = ccells * len(per_step) / tot
+        sample = f"{cores} processes x one {CPU_SAMPLE_N}^3 box (symmetry walls), 1 RK3 step each per benchmark step"
+        print(json.dumps({
+            "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * tot / len(per_step), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Fourier modes)",
+            "config": {"workload": f"periodic box {n}^3 RK3 Roe/minmod, sampled on CPU as {CPU_SAMPLE_N}^3 boxes",
+                       "flush": "inputs larger than L2"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    # CPU baseline first (spawned processes, before any GPU work), rank 0, N=1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            per_step, ccells, cores = cpu_reference(12, 1)
+            cpu = {"value": ccells * len(per_step) / sum(per_step), "unit": UNIT, "cores": cores,
+                   "kind": "reference",
+                   "sample": f"{cores} processes x one {CPU_SAMPLE_N}^3 box, 12 RK3 steps each (after 1 warm-up)"}
+        except Exception as e:  # the oracle build is missing on this host
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    import numpy as np
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    from m2c_b200 import abi, cases, gpu
+    gpu.set_device(local if world > 1 else 0)
+
+    g, s, mats, V = cases.fourier_box(n, precision=abi.PREC_MIXED, seed=2024 + rank)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    sol.time_steps(args.warmup)
+
+    clocks = Clocks(local if world > 1 else 0)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ms, launches = sol.time_steps(args.steps)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * cells * args.steps / (ms / 1000.0)
+
+    # roofline of the dominant kernel (the fused stage): algorithmic bytes
+    # 320 B/cell per RK3 step (8 FP64 5-vectors) over the 3 stage launches
+    prof_steps = 3
+    stage_ms, nlaunch, _ = sol.profile_stages(prof_steps)
+    avg_launch_ms = stage_ms / nlaunch
+    alg_bytes_per_launch = 320.0 * cells / 3.0
+    achieved = alg_bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9
+    peak, peak_kind = measured_peak()
+    tr = profiled_traffic()
+    traffic = tr["bytes_per_cell_per_launch"] * cells if tr else None
+
+    # FP64 path on the same state, and the L1 difference to it
+    fp64 = None
+    if rank == 0:
+        s64 = abi.scheme(**{f: getattr(s, f) for f, _ in abi.Scheme._fields_})
+        s64.precision = abi.PREC_FP64
+        sol64 = gpu.Solver(g, s64, mats)
+        sol64.upload(V)
+        sol64.time_steps(args.warmup)
+        ms64, _ = sol64.time_steps(args.steps)
+        # L1 after the same number of steps from the same initial state
+        a = gpu.Solver(g, s, mats)
+        a.upload(V)
+        b = gpu.Solver(g, s64, mats)
+        b.upload(V)
+        a.run(args.steps)
+        b.run(args.steps)
+        Va, _, _ = a.download()
+        Vb, _, _ = b.download()
+        ia, ib = Va[1:-1, 1:-1, 1:-1].reshape(-1, 5), Vb[1:-1, 1:-1, 1:-1].reshape(-1, 5)
+        l1 = (np.abs(ia - ib).sum(0) / np.abs(ib).sum(0)).tolist()
+        linf = (np.abs(ia - ib).max(0) / np.abs(ib).max(0)).tolist()
+        fp64 = {"value": cells * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
+                "mixed_speedup": ms64 / ms, "mixed_vs_fp64_rel_L1": dict(zip(["rho", "u", "v", "w", "p"], l1)),
+                "mixed_vs_fp64_rel_Linf": dict(zip(["rho", "u", "v", "w", "p"], linf)),
+                "after_steps": args.steps}
+        del a, b, sol64
+
+    # end to end through the public API: host state in pinned memory,
+    # upload + one step + download per step
+    e2e = None
+    if not args.no_e2e:
+        Vh = torch.empty(V.shape, dtype=torch.float64, pin_memory=True).numpy()
+        Vh[...] = V
+        Vo = torch.empty(V.shape, dtype=torch.float64, pin_memory=True).numpy()
+        ne = max(3, min(args.steps, 10))
+        sol.upload(Vh)
+        sol.run(1)
+        sol.download(out_V=Vo)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            sol.upload(Vh)
+            sol.run(1)
+            sol.download(out_V=Vo)
+        te = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": world * cells * ne / te, "unit": UNIT, "h2d_bytes_per_step": int(Vh.nbytes),
+               "d2h_bytes_per_step": int(Vo.nbytes), "steps": ne,
+               "note": "m2cg_upload_state + m2cg_run(1) + m2cg_download_state per step, ghosted AoS host state"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 flux / f64 state", "data": "synthetic (seeded Fourier modes)",
+            "config": {"workload": f"periodic box {n}^3, ideal gas, Roe + generalized minmod, RK3, CFL 0.4, mixed",
+                       "cells": cells, "flush": "inputs larger than L2 (no explicit flush)",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "m2c::stage_kernel<float,8>", "avg_launch_ms": avg_launch_ms,
+                         "alg_bytes_per_launch": alg_bytes_per_launch},
+            "clocks": clk,
+            "fp64": fp64,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+        }
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -135,6 +135,10 @@ void m2cg_default_levelset(m2cg_levelset* l);
 
 typedef struct m2cg_ctx m2cg_ctx;
 
+/* Make `device` the current CUDA device of the calling thread for contexts
+ * created afterwards (one process per GPU; no reference counterpart). */
+m2cg_status m2cg_set_device(int device);
+
 /* Create a context on the current CUDA device. nls = 0 (one material) or 1.
  * Replaces the setup in Main.cpp:106-379 for this path. */
 m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* scheme,
@@ -180,6 +184,23 @@ typedef struct {
   long long kernel_launches;
 } m2cg_counters;
 m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
+
+/* Run nsteps CFL-limited steps with the state resident in device memory and
+ * report their device time (CUDA events on the context's stream) and the
+ * number of kernels launched. Used by the benchmark; no reference counterpart
+ * (the reference times with clock(), Main.cpp:559). */
+m2cg_status m2cg_time_steps(m2cg_ctx* ctx, int nsteps, float* ms, long long* launches);
+
+/* Device time of the fused stage kernel alone over nsteps CFL steps (CUDA
+ * events around each stage launch): summed milliseconds, number of stage
+ * launches, and the whole-step milliseconds. Benchmark support; no
+ * reference counterpart. */
+m2cg_status m2cg_profile_stages(m2cg_ctx* ctx, int nsteps, float* stage_ms, int* stage_launches,
+                                float* step_ms);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work after the library's. */
+m2cg_status m2cg_get_stream(const m2cg_ctx* ctx, void** stream);
 
 /* Text of the last error on this thread (never NULL). */
 const char* m2cg_last_error(void);

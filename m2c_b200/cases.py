@@ -1,0 +1,137 @@
+"""Seeded synthetic workloads with the shapes, sizes and value distributions
+of the benchmark configurations (no dataset exists for this path; every
+field here is generated from a fixed seed).
+
+Host arrays use the reference's ghosted layout: V[(nz+2),(ny+2),(nx+2),5].
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+def empty_state(g):
+    return np.zeros(abi.ghosted_shape(g, 5))
+
+
+def sod(n=400, flux=abi.FLUX_HLLC, limiter=abi.LIM_VANALBADA, rk=2, cfl=0.5, precision=abi.PREC_FP64):
+    """Sod shock tube: gamma 1.4, [0,1], diaphragm at 0.5, left (1,0,1), right
+    (0.125,0,0.1); MUSCL + van Albada, HLLC, RK2, CFL 0.5, t_end 0.2.
+    Transmissive ends are Dirichlet INLET/OUTLET ghosts holding the initial
+    end states (identical while waves stay inside the tube)."""
+    g = abi.grid(n, 1, 1, bc=(abi.BC_INLET, abi.BC_OUTLET) + (abi.BC_SYMMETRY,) * 4,
+                 inlet=(1.0, 0.0, 0.0, 0.0, 1.0), outlet=(0.125, 0.0, 0.0, 0.0, 0.1))
+    s = abi.scheme(flux=flux, limiter=limiter, rk_order=rk, cfl=cfl, precision=precision)
+    mats = [abi.material(1.4, 0.0)]
+    V = empty_state(g)
+    x = abi.cell_centres(g)[0]
+    V[1:-1, 1:-1, 1:-1, 0] = np.where(x < 0.5, 1.0, 0.125)
+    V[1:-1, 1:-1, 1:-1, 4] = np.where(x < 0.5, 1.0, 0.1)
+    return g, s, mats, V
+
+
+def fourier_box(n, seed=2024, nmodes=16, kmax=8, amp=0.01, mach_rms=0.3, bc=abi.BC_PERIODIC,
+                flux=abi.FLUX_ROE, limiter=abi.LIM_GENMINMOD, minmod=1.0, rk=3, cfl=0.4, precision=abi.PREC_FP64,
+                shape=None):
+    """3D single-material box on [0,1)^3, ideal gas gamma 1.4: rho = 1 and
+    p = 1/1.4 (c = 1) each perturbed by `nmodes` seeded Fourier modes with
+    integer wave vectors 1 <= |k| <= kmax (units of 2 pi), relative amplitude
+    `amp`; velocity = sum of seeded solenoidal modes scaled to RMS |u| = mach_rms.
+    Roe flux (delta 0.2) with generalized minmod (alpha = 1), RK3, CFL 0.4."""
+    nx, ny, nz = shape if shape else (n, n, n)
+    g = abi.grid(nx, ny, nz, bc=(bc,) * 6)
+    s = abi.scheme(flux=flux, limiter=limiter, minmod_coeff=minmod, rk_order=rk, cfl=cfl, precision=precision)
+    mats = [abi.material(1.4, 0.0)]
+    rng = np.random.default_rng(seed)
+    xc, yc, zc = abi.cell_centres(g)
+    Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
+
+    def wavevectors(m):
+        out = []
+        while len(out) < m:
+            k = rng.integers(-kmax, kmax + 1, size=3)
+            if 1 <= np.linalg.norm(k) <= kmax:
+                out.append(k)
+        return out
+
+    def scalar_field():
+        f = np.zeros_like(X)
+        for k in wavevectors(nmodes):
+            ph = rng.uniform(0, 2 * np.pi)
+            f += np.cos(2 * np.pi * (k[0] * X + k[1] * Y + k[2] * Z) + ph)
+        return f / np.sqrt(nmodes / 2.0)
+
+    rho = 1.0 * (1.0 + amp * scalar_field())
+    p = (1.0 / 1.4) * (1.0 + amp * scalar_field())
+    u = np.zeros((3,) + X.shape)
+    for k in wavevectors(nmodes):
+        a = rng.normal(size=3)
+        b = np.cross(k, a)  # k x a is orthogonal to k: divergence-free mode
+        ph = rng.uniform(0, 2 * np.pi)
+        phase = np.cos(2 * np.pi * (k[0] * X + k[1] * Y + k[2] * Z) + ph)
+        for d in range(3):
+            u[d] += b[d] * phase
+    rms = np.sqrt(np.mean(np.sum(u * u, axis=0)))
+    u *= mach_rms / rms
+    V = empty_state(g)
+    V[1:-1, 1:-1, 1:-1, 0] = rho
+    V[1:-1, 1:-1, 1:-1, 1] = u[0]
+    V[1:-1, 1:-1, 1:-1, 2] = u[1]
+    V[1:-1, 1:-1, 1:-1, 3] = u[2]
+    V[1:-1, 1:-1, 1:-1, 4] = p
+    return g, s, mats, V
+
+
+def random_box(nx, ny, nz, seed=7, bc=(abi.BC_SYMMETRY,) * 6, flux=abi.FLUX_HLLC, limiter=abi.LIM_VANALBADA,
+               rk=3, cfl=0.5, precision=abi.PREC_FP64, water=False):
+    """Small box with smooth seeded fields plus a density/pressure jump: a
+    parity workload that exercises every limiter branch and both wave
+    directions. water=True uses the stiffened-gas water of the bubble case
+    (gamma 6.12, p_inf 3.43e8 Pa)."""
+    g = abi.grid(nx, ny, nz, bc=bc, inlet=(1.2, 0.3, 0.0, 0.0, 1.1), outlet=(0.9, 0.0, 0.0, 0.0, 0.8))
+    s = abi.scheme(flux=flux, limiter=limiter, rk_order=rk, cfl=cfl, precision=precision)
+    rng = np.random.default_rng(seed)
+    xc, yc, zc = abi.cell_centres(g)
+    Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
+    if water:
+        mats = [abi.material(6.12, 3.43e8)]
+        rho0, p0, u0 = 1000.0, 1.0e5, 50.0
+        if g.bc[0] == abi.BC_INLET:
+            g.inlet = (C.c_double * 5)(1100.0, 60.0, 0.0, 0.0, 2.0e8)
+            g.outlet = (C.c_double * 5)(1000.0, 0.0, 0.0, 0.0, 1.0e5)
+    else:
+        mats = [abi.material(1.4, 0.0)]
+        rho0, p0, u0 = 1.0, 1.0, 0.3
+    V = empty_state(g)
+    jump = np.where(X + 0.3 * Y + 0.2 * Z < 0.55, 1.0, 0.25)
+    smooth = lambda: 0.05 * np.sin(2 * np.pi * (rng.uniform(0.5, 2) * X + rng.uniform(0.5, 2) * Y +
+                                                rng.uniform(0.5, 2) * Z) + rng.uniform(0, 6.28))
+    V[1:-1, 1:-1, 1:-1, 0] = rho0 * (jump + smooth() + 0.1)
+    V[1:-1, 1:-1, 1:-1, 1] = u0 * (0.5 + smooth() * 10)
+    V[1:-1, 1:-1, 1:-1, 2] = u0 * (smooth() * 10 - 0.2)
+    V[1:-1, 1:-1, 1:-1, 3] = u0 * (smooth() * 10)
+    V[1:-1, 1:-1, 1:-1, 4] = p0 * (jump * (1.0 + smooth()) + 0.05)
+    if water:
+        V[1:-1, 1:-1, 1:-1, 4] = np.where(jump > 0.5, 1.0e9, 1.0e5) * (1.0 + smooth())
+    return g, s, mats, V
+
+
+def tile_periodic(g, V, reps):
+    """Copy of a periodic box tiled reps=(rx,ry,rz) times, with symmetry
+    ghosts: the reference (which has no periodic boundary) run on the tiled
+    copy reproduces the periodic evolution in the central tile for as many
+    steps as the wave of boundary influence needs to cross one tile
+    (2 cells per stage)."""
+    rx, ry, rz = reps
+    G = abi.grid(g.nx * rx, g.ny * ry, g.nz * rz, x=(0.0, (g.xmax - g.x0) * rx), y=(0.0, (g.ymax - g.y0) * ry),
+                 z=(0.0, (g.zmax - g.z0) * rz), bc=(abi.BC_SYMMETRY,) * 6)
+    inner = V[1:-1, 1:-1, 1:-1]
+    T = np.tile(inner, (rz, ry, rx, 1))
+    W = np.zeros((G.nz + 2, G.ny + 2, G.nx + 2, 5))
+    W[1:-1, 1:-1, 1:-1] = T
+    return G, W
+
+
+def interior(A):
+    return A[1:-1, 1:-1, 1:-1]

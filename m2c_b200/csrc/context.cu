@@ -1,0 +1,844 @@
+// Host side of the C ABI declared in include/m2c_gpu.h: context set-up
+// (mesh, limiter coefficients, EOS tables, device buffers), state transfer
+// between the reference's ghosted AoS host layout and the device SoA layout,
+// the device clock (dt from the CFL reduction, last step shortened to t_max),
+// and the RK step driver.
+//
+// Compiled with -fmad=false (the small kernels here feed the FP64 path).
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/m2c_gpu.h"
+#include "launch.h"
+#include "multiphase.h"
+
+using namespace m2c;
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error = "";
+
+static m2cg_status fail(m2cg_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return st;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t _e = (call);                                                                  \
+    if (_e != cudaSuccess)                                                                    \
+      return fail(M2CG_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e)); \
+  } while (0)
+
+extern "C" const char* m2cg_last_error(void) { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------------------
+// Defaults: IoData constructors of the reference.
+// ---------------------------------------------------------------------------
+extern "C" void m2cg_default_scheme(m2cg_scheme* s) {
+  memset(s, 0, sizeof *s);
+  s->flux = M2CG_FLUX_HLLC;            // SchemeData::SchemeData (IoData.cpp:1154-1160)
+  s->roe_delta = 0.2;
+  s->rec_type = M2CG_REC_LINEAR;       // ReconstructionData (IoData.cpp:1049-1058)
+  s->limiter = M2CG_LIM_NONE;
+  s->minmod_coeff = 1.2;
+  s->slope_near_interface = 1;
+  s->rec_var = M2CG_RECVAR_PRIMITIVE;
+  s->rk_order = 2;                     // TsData / ExplicitData (IoData.cpp:1472-1503)
+  s->cfl = 0.5;
+  s->precision = M2CG_PREC_FP64;
+  s->mp_flux = M2CG_MPFLUX_NUMERICAL;  // MultiPhaseData (IoData.cpp:1400-1417)
+  s->mp_recon = 0;
+  s->mp_phasechange_type = 0;
+  s->mp_phasechange_dir = 1;
+  s->mp_apply_failsafe_density = 1;
+  s->riem_maxits_main = 200;           // ExactRiemannSolverData (IoData.cpp:1345-1357)
+  s->riem_maxits_bracket = 100;
+  s->riem_maxits_shock = 200;
+  s->riem_nsteps_rarefaction = 200;
+  s->riem_tol_main = 1.0e-4;
+  s->riem_tol_shock = 1.0e-12;
+  s->riem_tol_rarefaction = 1.0e-8;
+  s->riem_min_pressure = -1.0e8;
+  s->riem_failure_threshold = 0.2;
+  s->riem_pressure_at_failure = 1.0e-8;
+}
+
+extern "C" void m2cg_default_material(m2cg_material* m) {
+  memset(m, 0, sizeof *m);             // MaterialModelData (IoData.cpp:860-871)
+  m->eos = M2CG_EOS_SG;
+  m->gamma = 1.4;
+  m->rhomin = 0.0;
+  m->pmin = -DBL_MAX;
+  m->rhomax = DBL_MAX;
+  m->pmax = DBL_MAX;
+  m->failsafe_density = 1.0e-10;
+}
+
+extern "C" void m2cg_default_levelset(m2cg_levelset* l) {
+  memset(l, 0, sizeof *l);             // LevelSetSchemeData (IoData.cpp:1245-1265)
+  l->material_id = 1;
+  for (int q = 0; q < 6; q++) l->bc[q] = M2CG_LSBC_ZERO_NEUMANN;
+  l->reinit_frequency = -1;            // LevelSetReinitializationData (IoData.cpp:1205-1213)
+  l->reinit_maxits = 30;
+  l->reinit_cfl = 0.8;
+  l->reinit_tol = 2.0e-4;
+  l->reinit_first_layer = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct m2cg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  m2cg_scheme scheme;
+  std::vector<m2cg_material> mats;
+  Grid3 g;
+  SchemeK sk;
+  int nx = 0, ny = 0, nz = 0;
+  long long px = 0, plane = 0, nalloc = 0;
+  // SoA state: V double-buffered (step state), U two stage buffers
+  double* V[2][5] = {};
+  double* U[2][5] = {};
+  int cur = 0;
+  uint8_t* id = nullptr;
+  // mesh
+  double *dx = nullptr, *dy = nullptr, *dz = nullptr;
+  double* lA[3] = {};
+  double* lB[3] = {};
+  int* lK[3] = {};
+  std::vector<double> hdx, hdy, hdz;
+  // device scratch: clock [t, dt, tmax, cfl], dtmin bits, flags, error
+  double* clock = nullptr;
+  unsigned long long* dtmin = nullptr;
+  int* clipflags = nullptr;  // [4]
+  DevError* err = nullptr;
+  // staging buffers for host transfers (ghosted AoS)
+  double* stage_buf = nullptr;
+  size_t stage_bytes = 0;
+  bool dtmin_valid = false;
+  m2cg_counters counters = {};
+  Multiphase* mp = nullptr;  // two-material machinery (nullptr for one material)
+  int zchunk = 32;
+  // optional per-stage event timing (benchmark roofline)
+  bool profile = false;
+  std::vector<cudaEvent_t> ev;  // pairs (before, after) per stage launch
+};
+
+static double* dalloc(size_t n, m2cg_status* st) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) {
+    *st = fail(M2CG_ERR_NOMEM, "cudaMalloc of %zu doubles failed", n);
+    return nullptr;
+  }
+  return (double*)p;
+}
+
+// Cell widths per axis: uniform as MeshGenerator::ComputeMesh1DUniform
+// (MeshGenerator.cpp:146-158) unless given.
+static void axis_mesh(int n, double a, double b, const double* wc, const double* w, std::vector<double>& dx) {
+  dx.assign(n, 0.0);
+  if (w) {
+    for (int i = 0; i < n; i++) dx[i] = w[i];
+  } else {
+    double h = (b - a) / n;
+    for (int i = 0; i < n; i++) dx[i] = h;
+  }
+  (void)wc;
+}
+
+// Limiter coefficients per axis index (Reconstructor::Setup, Reconstructor.cpp:53-99,
+// CalculateSlopeLimiterCoefficientK, 103-121). Ghost widths equal the
+// adjacent interior width (SpaceOperator::PopulateGhostBoundaryCoordinates,
+// SpaceOperator.cpp:218-300); periodic axes wrap.
+static bool axis_limiter(const std::vector<double>& dx, bool periodic, int limiter, std::vector<double>& A,
+                         std::vector<double>& B, std::vector<int>& K) {
+  int n = (int)dx.size();
+  A.resize(n);
+  B.resize(n);
+  K.resize(n);
+  for (int i = 0; i < n; i++) {
+    double dm = i > 0 ? dx[i - 1] : (periodic ? dx[n - 1] : dx[0]);
+    double dp = i < n - 1 ? dx[i + 1] : (periodic ? dx[0] : dx[n - 1]);
+    A[i] = (dm + dx[i]) / (dx[i] + dp);
+    B[i] = 2.0 * dx[i] / (dx[i] + dp);
+    K[i] = 0;
+    if (limiter == M2CG_LIM_VANALBADA) {
+      int k;
+      for (k = 2; k < 1000; k++) {
+        double rhs = 2.0 / (1.0 + pow((k - 1.0) / k, k - 1) / k) * std::min(A[i], 1.0);
+        if (B[i] <= rhs) break;
+      }
+      if (k >= 999) return false;
+      K[i] = k;
+    }
+  }
+  return true;
+}
+
+template <typename T>
+static void upload_vec(T** d, const std::vector<T>& h, cudaStream_t s, m2cg_status* st) {
+  if (cudaMalloc((void**)d, h.size() * sizeof(T)) != cudaSuccess) {
+    *st = fail(M2CG_ERR_NOMEM, "cudaMalloc failed");
+    return;
+  }
+  cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+static m2cg_status check_scheme(const m2cg_scheme* s, const m2cg_material* mats, int nmat) {
+  if (nmat < 1 || nmat > MAXMAT) return fail(M2CG_ERR_ARG, "nmat must be in [1,%d]", MAXMAT);
+  if (s->flux < 0 || s->flux > 2) return fail(M2CG_ERR_UNSUPPORTED, "flux %d not supported (ROE/LLF/HLLC)", s->flux);
+  if (s->rec_var != M2CG_RECVAR_PRIMITIVE)
+    return fail(M2CG_ERR_UNSUPPORTED, "only primitive-variable reconstruction is implemented on the GPU");
+  if (s->rk_order < 1 || s->rk_order > 3) return fail(M2CG_ERR_ARG, "rk_order must be 1, 2 or 3");
+  for (int m = 0; m < nmat; m++)
+    if (mats[m].eos != M2CG_EOS_SG && mats[m].eos != M2CG_EOS_NASG)
+      return fail(M2CG_ERR_UNSUPPORTED, "material %d: only stiffened gas and NASG are supported", m);
+  return M2CG_OK;
+}
+
+static MatParams to_params(const m2cg_material& m) {
+  MatParams p;
+  p.kind = m.eos;
+  p.gam = m.gamma;
+  p.pc = m.p_c;
+  p.b = m.b;
+  p.q = m.q;
+  p.rhomin = m.rhomin;
+  p.pmin = m.pmin;
+  p.rhomax = m.rhomax;
+  p.pmax = m.pmax;
+  p.failsafe_density = m.failsafe_density;
+  return p;
+}
+
+extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* scheme, const m2cg_material* mats,
+                                   int nmat, const m2cg_levelset* ls, int nls, m2cg_ctx** out) {
+  if (!grid || !scheme || !mats || !out) return fail(M2CG_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) return fail(M2CG_ERR_ARG, "grid sizes must be positive");
+  if (nls < 0 || nls > 1) return fail(M2CG_ERR_UNSUPPORTED, "at most one level set is supported");
+  for (int q = 0; q < 6; q++) {
+    int b = grid->bc[q];
+    if (b != M2CG_BC_INLET && b != M2CG_BC_OUTLET && b != M2CG_BC_SLIPWALL && b != M2CG_BC_STICKWALL &&
+        b != M2CG_BC_SYMMETRY && b != M2CG_BC_PERIODIC)
+      return fail(M2CG_ERR_UNSUPPORTED, "boundary %d: type %d not supported", q, b);
+  }
+  for (int a = 0; a < 3; a++)
+    if ((grid->bc[2 * a] == M2CG_BC_PERIODIC) != (grid->bc[2 * a + 1] == M2CG_BC_PERIODIC))
+      return fail(M2CG_ERR_ARG, "periodic boundaries must be set on both sides of an axis");
+  m2cg_status st = check_scheme(scheme, mats, nmat);
+  if (st) return st;
+  if (nls == 1 && nmat != 2) return fail(M2CG_ERR_UNSUPPORTED, "a level set needs exactly two materials");
+
+  m2cg_ctx* c = new m2cg_ctx;
+  cudaGetDevice(&c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(M2CG_ERR_CUDA, "cudaStreamCreate failed (no CUDA device?)");
+  }
+  c->scheme = *scheme;
+  c->mats.assign(mats, mats + nmat);
+  c->nx = grid->nx;
+  c->ny = grid->ny;
+  c->nz = grid->nz;
+  c->px = (grid->nx + 15) / 16 * 16;
+  c->plane = c->px * grid->ny;
+  c->nalloc = c->plane * grid->nz;
+  st = M2CG_OK;
+  for (int b = 0; b < 2; b++)
+    for (int p = 0; p < 5; p++) {
+      c->V[b][p] = dalloc(c->nalloc, &st);
+      c->U[b][p] = dalloc(c->nalloc, &st);
+    }
+  if (cudaMalloc((void**)&c->id, c->nalloc) != cudaSuccess) st = fail(M2CG_ERR_NOMEM, "cudaMalloc id failed");
+  if (!st) cudaMemsetAsync(c->id, 0, c->nalloc, c->stream);
+  axis_mesh(grid->nx, grid->x0, grid->xmax, grid->xc, grid->dx, c->hdx);
+  axis_mesh(grid->ny, grid->y0, grid->ymax, grid->yc, grid->dy, c->hdy);
+  axis_mesh(grid->nz, grid->z0, grid->zmax, grid->zc, grid->dz, c->hdz);
+  upload_vec(&c->dx, c->hdx, c->stream, &st);
+  upload_vec(&c->dy, c->hdy, c->stream, &st);
+  upload_vec(&c->dz, c->hdz, c->stream, &st);
+  const std::vector<double>* ax[3] = {&c->hdx, &c->hdy, &c->hdz};
+  for (int a = 0; a < 3; a++) {
+    std::vector<double> A, B;
+    std::vector<int> K;
+    if (!axis_limiter(*ax[a], grid->bc[2 * a] == M2CG_BC_PERIODIC, scheme->limiter, A, B, K)) {
+      st = fail(M2CG_ERR_ARG, "cannot set up the van Albada exponent on axis %d", a);
+      break;
+    }
+    upload_vec(&c->lA[a], A, c->stream, &st);
+    upload_vec(&c->lB[a], B, c->stream, &st);
+    upload_vec(&c->lK[a], K, c->stream, &st);
+  }
+  if (cudaMalloc((void**)&c->clock, 8 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&c->dtmin, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc((void**)&c->clipflags, 4 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&c->err, sizeof(DevError)) != cudaSuccess)
+    st = fail(M2CG_ERR_NOMEM, "cudaMalloc of scalars failed");
+  if (!st) {
+    cudaMemsetAsync(c->clock, 0, 8 * sizeof(double), c->stream);
+    cudaMemsetAsync(c->clipflags, 0, 4 * sizeof(int), c->stream);
+    cudaMemsetAsync(c->err, 0, sizeof(DevError), c->stream);
+  }
+  // kernel parameter blocks
+  Grid3& g = c->g;
+  g.nx = c->nx; g.ny = c->ny; g.nz = c->nz;
+  g.px = c->px; g.plane = c->plane;
+  for (int q = 0; q < 6; q++) g.bc[q] = grid->bc[q];
+  for (int p = 0; p < 5; p++) { g.inlet[p] = grid->inlet[p]; g.outlet[p] = grid->outlet[p]; }
+  g.dx = c->dx; g.dy = c->dy; g.dz = c->dz;
+  for (int a = 0; a < 3; a++) { g.lA[a] = c->lA[a]; g.lB[a] = c->lB[a]; g.lK[a] = c->lK[a]; }
+  SchemeK& sk = c->sk;
+  sk.flux = scheme->flux;
+  sk.limiter = scheme->limiter;
+  sk.rec_linear = scheme->rec_type == M2CG_REC_LINEAR;
+  sk.slope_zero_at_interface = scheme->slope_near_interface == 0;
+  sk.alpha = scheme->minmod_coeff;
+  sk.delta = scheme->roe_delta;
+  sk.nmat = nmat;
+  for (int m = 0; m < MAXMAT; m++) {
+    MatParams p = to_params(mats[m < nmat ? m : 0]);
+    sk.ed[m] = make_eos<double>(p);
+    sk.ef[m] = make_eos<float>(p);
+  }
+  size_t smem = scheme->precision == M2CG_PREC_MIXED ? stage_smem_mixed() : stage_smem_fp64();
+  int maxsm = 0;
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  if (!st && (size_t)maxsm < smem) st = fail(M2CG_ERR_CUDA, "stage kernel needs %zu B shared memory, device has %d", smem, maxsm);
+  if (!st && nls == 1) st = multiphase_create(c->stream, g, sk, *scheme, mats, nmat, *ls, &c->mp);
+  if (st) {
+    m2cg_destroy(c);
+    return st;
+  }
+  // z chunk: enough CTAs to fill 148 SMs at least twice, chunks of >= 8 planes
+  int tiles = ((c->nx + TX - 1) / TX) * ((c->ny + STAGE_TY - 1) / STAGE_TY);
+  int want_chunks = (2 * 148 + tiles - 1) / tiles;
+  int chunk = (c->nz + want_chunks - 1) / want_chunks;
+  if (chunk < 8) chunk = 8;
+  c->zchunk = chunk;
+  CK(cudaStreamSynchronize(c->stream));
+  *out = c;
+  return M2CG_OK;
+}
+
+extern "C" m2cg_status m2cg_destroy(m2cg_ctx* c) {
+  if (!c) return M2CG_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int b = 0; b < 2; b++)
+    for (int p = 0; p < 5; p++) {
+      cudaFree(c->V[b][p]);
+      cudaFree(c->U[b][p]);
+    }
+  cudaFree(c->id);
+  cudaFree(c->dx); cudaFree(c->dy); cudaFree(c->dz);
+  for (int a = 0; a < 3; a++) { cudaFree(c->lA[a]); cudaFree(c->lB[a]); cudaFree(c->lK[a]); }
+  cudaFree(c->clock); cudaFree(c->dtmin); cudaFree(c->clipflags); cudaFree(c->err);
+  cudaFree(c->stage_buf);
+  if (c->mp) multiphase_destroy(c->mp);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return M2CG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Small kernels
+// ---------------------------------------------------------------------------
+// Ghosted AoS (host layout) -> interior SoA, with clipping of the primitive
+// state (the end of SpaceOperator::SetInitialCondition clips, 1088).
+__global__ void k_unpack_state(const double* aos, int nx, int ny, int nz, long long px, long long plane, int dof,
+                               double* const* soa_ptrs_unused, double* s0, double* s1, double* s2, double* s3,
+                               double* s4) {
+  long long n = (long long)nx * ny * nz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % nx);
+    int j = (int)((q / nx) % ny);
+    int k = (int)(q / ((long long)nx * ny));
+    long long h = (((long long)(k + 1) * (ny + 2) + (j + 1)) * (nx + 2) + (i + 1)) * dof;
+    long long o = (long long)k * plane + (long long)j * px + i;
+    double* d[5] = {s0, s1, s2, s3, s4};
+    for (int p = 0; p < dof; p++) d[p][o] = aos[h + p];
+  }
+}
+
+__global__ void k_clip_state(Grid3 g, SchemeK sk, double* v0, double* v1, double* v2, double* v3, double* v4,
+                             const uint8_t* id, DevError* err) {
+  long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % g.nx);
+    int j = (int)((q / g.nx) % g.ny);
+    int k = (int)(q / ((long long)g.nx * g.ny));
+    long long o = (long long)k * g.plane + (long long)j * g.px + i;
+    double V[5] = {v0[o], v1[o], v2[o], v3[o], v4[o]};
+    const Eos<double>& e = sk.ed[id[o] < sk.nmat ? id[o] : 0];
+    e.clip(V);
+    if (e.bad(V)) report(err, ERR_STATE, (int)q, 0);
+    v0[o] = V[0]; v1[o] = V[1]; v2[o] = V[2]; v3[o] = V[3]; v4[o] = V[4];
+  }
+}
+
+__global__ void k_unpack_id(const double* aos, int nx, int ny, int nz, long long px, long long plane, uint8_t* id) {
+  long long n = (long long)nx * ny * nz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % nx);
+    int j = (int)((q / nx) % ny);
+    int k = (int)(q / ((long long)nx * ny));
+    long long h = ((long long)(k + 1) * (ny + 2) + (j + 1)) * (nx + 2) + (i + 1);
+    id[(long long)k * plane + (long long)j * px + i] = (uint8_t)aos[h];
+  }
+}
+
+// Interior SoA -> ghosted AoS with face ghosts filled by the boundary rule
+// (SpaceOperator::ApplyBoundaryConditions, 1667-1745). Edge/corner ghosts are
+// left at zero (the reference never populates them).
+__global__ void k_pack_state(Grid3 g, const double* s0, const double* s1, const double* s2, const double* s3,
+                             const double* s4, const uint8_t* id, double* aos, double* idaos) {
+  int gx = g.nx + 2, gy = g.ny + 2, gz = g.nz + 2;
+  long long n = (long long)gx * gy * gz;
+  const double* s[5] = {s0, s1, s2, s3, s4};
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % gx) - 1;
+    int j = (int)((q / gx) % gy) - 1;
+    int k = (int)(q / ((long long)gx * gy)) - 1;
+    int out[3] = {i < 0 ? 0 : i >= g.nx ? 1 : -1, j < 0 ? 0 : j >= g.ny ? 1 : -1, k < 0 ? 0 : k >= g.nz ? 1 : -1};
+    int nout = (out[0] >= 0) + (out[1] >= 0) + (out[2] >= 0);
+    double V[5] = {0, 0, 0, 0, 0};
+    double idv = 0.0;
+    if (nout <= 1) {
+      int ii = i < 0 ? 0 : i >= g.nx ? g.nx - 1 : i;
+      int jj = j < 0 ? 0 : j >= g.ny ? g.ny - 1 : j;
+      int kk = k < 0 ? 0 : k >= g.nz ? g.nz - 1 : k;
+      int axis = out[0] >= 0 ? 0 : out[1] >= 0 ? 1 : out[2] >= 0 ? 2 : -1;
+      if (axis >= 0 && g.bc[2 * axis] == BC_PERIODIC) {
+        int c3[3] = {i, j, k};
+        int n3[3] = {g.nx, g.ny, g.nz};
+        int w = (c3[axis] + n3[axis]) % n3[axis];
+        if (axis == 0) ii = w; else if (axis == 1) jj = w; else kk = w;
+        axis = -1;  // plain copy of the periodic image
+      }
+      long long o = (long long)kk * g.plane + (long long)jj * g.px + ii;
+      for (int p = 0; p < 5; p++) V[p] = s[p][o];
+      idv = id ? (double)id[o] : 0.0;
+      if (axis >= 0) {
+        int bc = g.bc[2 * axis + out[axis]];
+        if (bc == BC_INLET) for (int p = 0; p < 5; p++) V[p] = g.inlet[p];
+        else if (bc == BC_OUTLET) for (int p = 0; p < 5; p++) V[p] = g.outlet[p];
+        else if (bc == BC_STICKWALL) { V[1] = -V[1]; V[2] = -V[2]; V[3] = -V[3]; }
+        else V[axis + 1] = -V[axis + 1];
+      }
+    }
+    for (int p = 0; p < 5; p++) aos[q * 5 + p] = V[p];
+    if (idaos) idaos[q] = idv;
+  }
+}
+
+// CFL sweep (SpaceOperator::FindExtremeValuesOfFlowVariables, 2128-2198):
+// min over cells of min(dx/(|u|+c), dy/(|v|+c), dz/(|w|+c)).
+__global__ void k_cfl(Grid3 g, SchemeK sk, const double* v0, const double* v1, const double* v2, const double* v3,
+                      const double* v4, const uint8_t* id, unsigned long long* dtmin, DevError* err) {
+  long long n = (long long)g.nx * g.ny * g.nz;
+  double best = 1.0e300;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % g.nx);
+    int j = (int)((q / g.nx) % g.ny);
+    int k = (int)(q / ((long long)g.nx * g.ny));
+    long long o = (long long)k * g.plane + (long long)j * g.px + i;
+    const Eos<double>& e = sk.ed[id && id[o] < sk.nmat ? id[o] : 0];
+    double rho = v0[o], p = v4[o];
+    double c2 = e.c2(rho, e.energy(rho, p));
+    if (c2 < 0.0) report(err, ERR_SOUND, (int)q, 5);
+    double c = sqrt(c2);
+    double r = smin(g.dx[i] / (fabs(v1[o]) + c), smin(g.dy[j] / (fabs(v2[o]) + c), g.dz[k] / (fabs(v3[o]) + c)));
+    best = smin(best, r);
+  }
+  for (int o = 16; o > 0; o >>= 1) best = smin(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0 && best < 1.0e300) atomicMin(dtmin, (unsigned long long)__double_as_longlong(best));
+}
+
+__global__ void k_reset_dtmin(unsigned long long* dtmin) { *dtmin = 0x7ff0000000000000ull; }
+
+// Device clock: dt = cfl * min(dx/lambda) (SpaceOperator::ComputeTimeStepSize,
+// 2202-2227), shortened so the run ends at t_max (Main.cpp:537-541), t += dt.
+// clock = [t, dt, t_max, cfl].
+__global__ void k_clock_from_cfl(double* clock, unsigned long long* dtmin) {
+  double m = __longlong_as_double((long long)*dtmin);
+  double t = clock[0], tmax = clock[2], cfl = clock[3];
+  double dt = cfl * m;
+  if (t + dt > tmax) dt = tmax - t;
+  clock[1] = dt;
+  clock[0] = t + dt;
+  *dtmin = 0x7ff0000000000000ull;
+}
+
+__global__ void k_set_clock(double* clock, double t, double dt, double tmax, double cfl) {
+  clock[0] = t;
+  clock[1] = dt;
+  clock[2] = tmax;
+  clock[3] = cfl;
+}
+
+static int grid1d(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+static m2cg_status check_device_error(m2cg_ctx* c) {
+  DevError e;
+  CK(cudaMemcpyAsync(&e, c->err, sizeof e, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (e.code) {
+    cudaMemsetAsync(c->err, 0, sizeof(DevError), c->stream);
+    m2cg_status st = e.code == ERR_STATE || e.code == ERR_SOUND || e.code == ERR_HLLC ? M2CG_ERR_STATE
+                     : e.code == ERR_RIEMANN ? M2CG_ERR_RIEMANN
+                     : e.code == ERR_ITER_CAP ? M2CG_ERR_ITER_CAP : M2CG_ERR_STATE;
+    return fail(st, "device error code %d at cell %d (site %d)", e.code, e.cell, e.where);
+  }
+  return M2CG_OK;
+}
+
+static m2cg_status ensure_stage_buf(m2cg_ctx* c, size_t bytes) {
+  if (c->stage_bytes >= bytes) return M2CG_OK;
+  cudaFree(c->stage_buf);
+  c->stage_buf = nullptr;
+  c->stage_bytes = 0;
+  if (cudaMalloc((void**)&c->stage_buf, bytes) != cudaSuccess) return fail(M2CG_ERR_NOMEM, "staging alloc failed");
+  c->stage_bytes = bytes;
+  return M2CG_OK;
+}
+
+static m2cg_status compute_dtmin(m2cg_ctx* c) {
+  k_reset_dtmin<<<1, 1, 0, c->stream>>>(c->dtmin);
+  double** V = c->V[c->cur];
+  k_cfl<<<grid1d((long long)c->nx * c->ny * c->nz), 256, 0, c->stream>>>(c->g, c->sk, V[0], V[1], V[2], V[3], V[4],
+                                                                         c->id, c->dtmin, c->err);
+  c->counters.kernel_launches += 2;
+  CK(cudaGetLastError());
+  c->dtmin_valid = true;
+  return M2CG_OK;
+}
+
+extern "C" m2cg_status m2cg_upload_state(m2cg_ctx* c, const double* V, const double* ID, const double* phi) {
+  if (!c || !V) return fail(M2CG_ERR_ARG, "null argument");
+  size_t ng = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  m2cg_status st = ensure_stage_buf(c, ng * 5 * sizeof(double));
+  if (st) return st;
+  long long n = (long long)c->nx * c->ny * c->nz;
+  double** D = c->V[c->cur];
+  if (ID) {
+    CK(cudaMemcpyAsync(c->stage_buf, ID, ng * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k_unpack_id<<<grid1d(n), 256, 0, c->stream>>>(c->stage_buf, c->nx, c->ny, c->nz, c->px, c->plane, c->id);
+  }
+  CK(cudaMemcpyAsync(c->stage_buf, V, ng * 5 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  k_unpack_state<<<grid1d(n), 256, 0, c->stream>>>(c->stage_buf, c->nx, c->ny, c->nz, c->px, c->plane, 5, nullptr,
+                                                    D[0], D[1], D[2], D[3], D[4]);
+  k_clip_state<<<grid1d(n), 256, 0, c->stream>>>(c->g, c->sk, D[0], D[1], D[2], D[3], D[4], c->id, c->err);
+  c->counters.kernel_launches += ID ? 3 : 2;
+  CK(cudaGetLastError());
+  if (c->mp) {
+    st = multiphase_upload_phi(c->mp, c->stream, phi, c->stage_buf, c->id);
+    if (st) return st;
+  }
+  st = compute_dtmin(c);
+  if (st) return st;
+  return check_device_error(c);
+}
+
+extern "C" m2cg_status m2cg_download_state(m2cg_ctx* c, double* V, double* ID, double* phi) {
+  if (!c) return fail(M2CG_ERR_ARG, "null argument");
+  size_t ng = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  m2cg_status st = ensure_stage_buf(c, ng * 6 * sizeof(double));
+  if (st) return st;
+  double** D = c->V[c->cur];
+  k_pack_state<<<grid1d((long long)ng), 256, 0, c->stream>>>(c->g, D[0], D[1], D[2], D[3], D[4], c->id, c->stage_buf,
+                                                             c->stage_buf + ng * 5);
+  c->counters.kernel_launches += 1;
+  CK(cudaGetLastError());
+  if (V) CK(cudaMemcpyAsync(V, c->stage_buf, ng * 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (ID) CK(cudaMemcpyAsync(ID, c->stage_buf + ng * 5, ng * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (phi && c->mp) {
+    st = multiphase_download_phi(c->mp, c->stream, phi);
+    if (st) return st;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return M2CG_OK;
+}
+
+extern "C" m2cg_status m2cg_compute_dt(m2cg_ctx* c, double* dt_out) {
+  if (!c || !dt_out) return fail(M2CG_ERR_ARG, "null argument");
+  m2cg_status st = compute_dtmin(c);
+  if (st) return st;
+  unsigned long long bits;
+  CK(cudaMemcpyAsync(&bits, c->dtmin, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double m;
+  memcpy(&m, &bits, sizeof m);
+  *dt_out = c->scheme.cfl * m;
+  return check_device_error(c);
+}
+
+// RK coefficients of stage s (1-based) for order r: U_new = a_prev*U_s + a_un*U^n + (b*dt)*R
+// (TimeIntegrator.cpp:367-372, 588-593, 644-649).
+static void rk_coeffs(int r, int s, double& a_prev, double& a_un, double& b) {
+  a_prev = 0.0; a_un = 1.0; b = 1.0;
+  if (s == 1) return;
+  if (r == 2) { a_prev = 0.5; a_un = 0.5; b = 0.5; return; }
+  if (s == 2) { a_prev = 0.25; a_un = 0.75; b = 0.25; return; }
+  a_prev = 2.0 / 3.0; a_un = 1.0 / 3.0; b = 2.0 / 3.0;
+}
+
+static m2cg_status launch_stage(m2cg_ctx* c, StageArgs& a) {
+  dim3 grid((c->nx + TX - 1) / TX, (c->ny + STAGE_TY - 1) / STAGE_TY, (c->nz + c->zchunk - 1) / c->zchunk);
+  a.zchunk = c->zchunk;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c->profile) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c->stream);
+  }
+  cudaError_t e = c->scheme.precision == M2CG_PREC_MIXED ? launch_stage_mixed(a, grid, c->stream)
+                                                          : launch_stage_fp64(a, grid, c->stream);
+  if (c->profile) {
+    cudaEventRecord(e1, c->stream);
+    c->ev.push_back(e0);
+    c->ev.push_back(e1);
+  }
+  c->counters.kernel_launches += 1;
+  if (e != cudaSuccess) return fail(M2CG_ERR_CUDA, "stage launch: %s", cudaGetErrorString(e));
+  return M2CG_OK;
+}
+
+static void base_args(m2cg_ctx* c, StageArgs& a) {
+  memset(&a, 0, sizeof a);
+  a.g = c->g;
+  a.s = c->sk;
+  a.id = c->id;
+  a.clock = c->clock;
+  a.err = c->err;
+}
+
+// All RK stages of one step; dt is already in the device clock.
+static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
+  int r = c->scheme.rk_order;
+  double** Vn = c->V[c->cur];
+  double** Vo = c->V[1 - c->cur];
+  cudaMemsetAsync(c->clipflags, 0, 4 * sizeof(int), c->stream);
+  if (c->mp) {
+    m2cg_status st = multiphase_begin_step(c->mp, c->stream, Vn, c->id);
+    if (st) return st;
+  }
+  for (int s = 1; s <= r; s++) {
+    StageArgs a;
+    base_args(c, a);
+    a.stage = s;
+    a.final_stage = s == r;
+    rk_coeffs(r, s, a.a_prev, a.a_un, a.bdt_coef);
+    for (int p = 0; p < 5; p++) {
+      a.Vn[p] = Vn[p];
+      a.Us[p] = s == 1 ? nullptr : c->U[(s - 2) & 1][p];
+      a.Uo[p] = c->U[(s - 1) & 1][p];
+      a.Vo[p] = Vo[p];
+    }
+    a.us_clipped = s > 1 ? c->clipflags + (s - 2) : nullptr;
+    a.clipped_out = c->clipflags + (s - 1);
+    a.dtmin_bits = (a.final_stage && want_dtmin && !c->mp) ? c->dtmin : nullptr;
+    if (c->mp) {
+      m2cg_status st = multiphase_stage(c->mp, c->stream, a);
+      if (st) return st;
+    }
+    m2cg_status st = launch_stage(c, a);
+    if (st) return st;
+  }
+  c->cur = 1 - c->cur;
+  if (c->mp) {
+    m2cg_status st = multiphase_end_step(c->mp, c->stream, c->V[1 - c->cur], c->V[c->cur], c->id,
+                                         c->clock, c->err, &c->counters);
+    if (st) return st;
+    c->dtmin_valid = false;
+  } else {
+    c->dtmin_valid = want_dtmin;
+  }
+  c->counters.steps += 1;
+  c->counters.cells_updated += (long long)c->nx * c->ny * c->nz;
+  return M2CG_OK;
+}
+
+extern "C" m2cg_status m2cg_advance(m2cg_ctx* c, double t_new, double dt, int time_step) {
+  if (!c) return fail(M2CG_ERR_ARG, "null argument");
+  (void)time_step;
+  k_set_clock<<<1, 1, 0, c->stream>>>(c->clock, t_new, dt, 1.0e300, c->scheme.cfl);
+  k_reset_dtmin<<<1, 1, 0, c->stream>>>(c->dtmin);
+  c->counters.kernel_launches += 2;
+  if (c->mp) multiphase_set_step(c->mp, time_step);
+  m2cg_status st = rk_step(c, true);
+  if (st) return st;
+  return check_device_error(c);
+}
+
+// Steps with dt from the CFL condition; no host synchronisation per step
+// unless t_max is finite (then t is read back each step to stop exactly
+// where the reference's loop stops, Main.cpp:514).
+static m2cg_status run_steps(m2cg_ctx* c, int nsteps, double t_max, double t0, double* t, int* done, bool check) {
+  k_set_clock<<<1, 1, 0, c->stream>>>(c->clock, t0, 0.0, t_max, c->scheme.cfl);
+  c->counters.kernel_launches += 1;
+  int n = 0;
+  double tnow = t0;
+  bool finite = std::isfinite(t_max);
+  while (n < nsteps && (!finite || tnow < t_max)) {
+    if (!c->dtmin_valid) {
+      m2cg_status st = compute_dtmin(c);
+      if (st) return st;
+    }
+    k_clock_from_cfl<<<1, 1, 0, c->stream>>>(c->clock, c->dtmin);
+    c->counters.kernel_launches += 1;
+    if (c->mp) multiphase_set_step(c->mp, -1);
+    m2cg_status st = rk_step(c, true);
+    if (st) return st;
+    n++;
+    if (finite) {
+      CK(cudaMemcpyAsync(&tnow, c->clock, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+  }
+  if (!finite) {
+    CK(cudaMemcpyAsync(&tnow, c->clock, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (done) *done = n;
+  if (check) {
+    m2cg_status st = check_device_error(c);
+    if (st) return st;
+  }
+  if (t) *t = tnow;
+  return M2CG_OK;
+}
+
+extern "C" m2cg_status m2cg_run(m2cg_ctx* c, int nsteps, double t_max, double* t, int* steps_done) {
+  if (!c) return fail(M2CG_ERR_ARG, "null argument");
+  double t0 = t ? *t : 0.0;
+  return run_steps(c, nsteps, t_max, t0, t, steps_done, true);
+}
+
+extern "C" m2cg_status m2cg_compute_residual(m2cg_ctx* c, double* R_host) {
+  if (!c || !R_host) return fail(M2CG_ERR_ARG, "null argument");
+  StageArgs a;
+  base_args(c, a);
+  a.stage = 1;
+  a.final_stage = 0;
+  a.bdt_coef = 0.0;
+  double** Vn = c->V[c->cur];
+  for (int p = 0; p < 5; p++) {
+    a.Vn[p] = Vn[p];
+    a.Uo[p] = c->U[0][p];
+    a.Ro[p] = c->U[1][p];
+  }
+  if (c->mp) {
+    m2cg_status st = multiphase_begin_step(c->mp, c->stream, Vn, c->id);
+    if (st) return st;
+    st = multiphase_stage(c->mp, c->stream, a);
+    if (st) return st;
+  }
+  m2cg_status st = launch_stage(c, a);
+  if (st) return st;
+  // pack R (interior) into the ghosted AoS layout
+  size_t ng = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  st = ensure_stage_buf(c, ng * 6 * sizeof(double));
+  if (st) return st;
+  Grid3 gz = c->g;
+  for (int q = 0; q < 6; q++) gz.bc[q] = M2CG_BC_OUTLET;  // ghosts of R are not meaningful
+  for (int p = 0; p < 5; p++) { gz.outlet[p] = 0.0; gz.inlet[p] = 0.0; }
+  double** R = c->U[1];
+  k_pack_state<<<grid1d((long long)ng), 256, 0, c->stream>>>(gz, R[0], R[1], R[2], R[3], R[4], nullptr, c->stage_buf,
+                                                             nullptr);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(R_host, c->stage_buf, ng * 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_device_error(c);
+}
+
+extern "C" m2cg_status m2cg_get_counters(const m2cg_ctx* c, m2cg_counters* out) {
+  if (!c || !out) return fail(M2CG_ERR_ARG, "null argument");
+  *out = c->counters;
+  if (c->mp) multiphase_counters(c->mp, out);
+  return M2CG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Timing entry point used by the benchmark: nsteps CFL steps with the state
+// resident in HBM, bracketed by CUDA events on the context's stream.
+// ---------------------------------------------------------------------------
+extern "C" m2cg_status m2cg_time_steps(m2cg_ctx* c, int nsteps, float* ms_out, long long* launches_out) {
+  if (!c) return fail(M2CG_ERR_ARG, "null argument");
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  long long l0 = c->counters.kernel_launches;
+  CK(cudaEventRecord(e0, c->stream));
+  double t = 0.0;
+  int done = 0;
+  m2cg_status st = run_steps(c, nsteps, INFINITY, 0.0, &t, &done, false);
+  if (st) return st;
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ms_out) *ms_out = ms;
+  if (launches_out) *launches_out = c->counters.kernel_launches - l0;
+  return check_device_error(c);
+}
+
+// Stream of the context (cudaStream_t), for callers that time on it.
+extern "C" m2cg_status m2cg_get_stream(const m2cg_ctx* c, void** stream) {
+  if (!c || !stream) return fail(M2CG_ERR_ARG, "null argument");
+  *stream = (void*)c->stream;
+  return M2CG_OK;
+}
+
+// Per-launch device time of the fused stage kernel over nsteps CFL steps
+// (CUDA events around each launch on the context's stream): total stage
+// milliseconds, number of stage launches, and whole-step milliseconds.
+extern "C" m2cg_status m2cg_profile_stages(m2cg_ctx* c, int nsteps, float* stage_ms, int* stage_launches,
+                                           float* step_ms) {
+  if (!c) return fail(M2CG_ERR_ARG, "null argument");
+  c->profile = true;
+  c->ev.clear();
+  float total = 0.f;
+  m2cg_status st = m2cg_time_steps(c, nsteps, &total, nullptr);
+  c->profile = false;
+  if (st) return st;
+  float sum = 0.f;
+  for (size_t q = 0; q + 1 < c->ev.size(); q += 2) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[q], c->ev[q + 1]);
+    sum += ms;
+    cudaEventDestroy(c->ev[q]);
+    cudaEventDestroy(c->ev[q + 1]);
+  }
+  if (stage_ms) *stage_ms = sum;
+  if (stage_launches) *stage_launches = (int)(c->ev.size() / 2);
+  if (step_ms) *step_ms = total;
+  c->ev.clear();
+  return M2CG_OK;
+}
+
+// Select the CUDA device for contexts created afterwards on this thread.
+extern "C" m2cg_status m2cg_set_device(int device) {
+  CK(cudaSetDevice(device));
+  return M2CG_OK;
+}

@@ -1,0 +1,29 @@
+// Two-material machinery attached to a context: level set, material IDs,
+// interface exact Riemann problems and the post-step multiphase update.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/m2c_gpu.h"
+#include "stage.cuh"
+
+namespace m2c {
+struct Multiphase;
+}
+using m2c::Multiphase;
+
+m2cg_status multiphase_create(cudaStream_t s, const m2c::Grid3& g, const m2c::SchemeK& sk, const m2cg_scheme& scheme,
+                              const m2cg_material* mats, int nmat, const m2cg_levelset& ls, Multiphase** out);
+void multiphase_destroy(Multiphase* mp);
+m2cg_status multiphase_upload_phi(Multiphase* mp, cudaStream_t s, const double* phi_host, double* staging,
+                                  uint8_t* id);
+m2cg_status multiphase_download_phi(Multiphase* mp, cudaStream_t s, double* phi_host);
+void multiphase_set_step(Multiphase* mp, int time_step);
+// Called before the stages of a step (V^n, ID) and before each stage launch
+// (fills the interface fields of the stage arguments).
+m2cg_status multiphase_begin_step(Multiphase* mp, cudaStream_t s, double* const* Vn, const uint8_t* id);
+m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, m2c::StageArgs& a);
+// After the last stage: level-set update, ID update, reinitialisation,
+// state update of cells that changed material.
+m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* Vn, double* const* Vnew, uint8_t* id,
+                                const double* clock, m2c::DevError* err, m2cg_counters* counters);
+void multiphase_counters(const Multiphase* mp, m2cg_counters* out);

@@ -1,0 +1,162 @@
+"""Python handle on the CUDA library (libm2c_gpu.so) through its C ABI.
+
+The host-side mirror of the reference's interface for this path:
+``Solver`` plays the role of SpaceOperator + TimeIntegrator on one
+subdomain (SpaceOperator.h:103-140, TimeIntegrator.h:66-73) and exposes
+``compute_residual`` / ``compute_dt`` / ``advance`` / ``run`` with the
+reference's ghosted array layout. There is no CPU fallback: if the CUDA
+library cannot be loaded or no device is present, construction raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libm2c_gpu.so")
+
+_lib = None
+
+
+class M2CError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"m2cg status {status}: {msg}")
+        self.status = status
+
+
+class Counters(C.Structure):
+    _fields_ = [(n, C.c_longlong) for n in (
+        "steps", "cells_updated", "riemann_calls", "riemann_iterations", "riemann_errors",
+        "clipped_cells", "reinit_calls", "kernel_launches")]
+
+
+def lib():
+    """Load libm2c_gpu.so (fails loudly when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"CUDA library not built: {LIB_PATH} (run m2c_b200/build.py)")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+    L.m2cg_last_error.restype = C.c_char_p
+    L.m2cg_create.argtypes = [C.POINTER(abi.Grid), C.POINTER(abi.Scheme), C.POINTER(abi.Material), C.c_int,
+                              C.POINTER(abi.LevelSet), C.c_int, C.POINTER(vp)]
+    L.m2cg_destroy.argtypes = [vp]
+    L.m2cg_upload_state.argtypes = [vp, dp, dp, dp]
+    L.m2cg_download_state.argtypes = [vp, dp, dp, dp]
+    L.m2cg_compute_dt.argtypes = [vp, dp]
+    L.m2cg_compute_residual.argtypes = [vp, dp]
+    L.m2cg_advance.argtypes = [vp, C.c_double, C.c_double, C.c_int]
+    L.m2cg_run.argtypes = [vp, C.c_int, C.c_double, dp, ip]
+    L.m2cg_get_counters.argtypes = [vp, C.POINTER(Counters)]
+    L.m2cg_time_steps.argtypes = [vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_longlong)]
+    L.m2cg_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.m2cg_profile_stages.argtypes = [vp, C.c_int, C.POINTER(C.c_float), ip, C.POINTER(C.c_float)]
+    L.m2cg_set_device.argtypes = [C.c_int]
+    L.m2cg_set_device.restype = C.c_int
+    L.m2cg_default_scheme.argtypes = [C.POINTER(abi.Scheme)]
+    L.m2cg_default_material.argtypes = [C.POINTER(abi.Material)]
+    L.m2cg_default_levelset.argtypes = [C.POINTER(abi.LevelSet)]
+    for name in ("m2cg_create", "m2cg_destroy", "m2cg_upload_state", "m2cg_download_state", "m2cg_compute_dt",
+                 "m2cg_compute_residual", "m2cg_advance", "m2cg_run", "m2cg_get_counters", "m2cg_time_steps",
+                 "m2cg_get_stream", "m2cg_profile_stages"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def set_device(device):
+    check(lib().m2cg_set_device(device))
+
+
+def check(st):
+    if st != 0:
+        raise M2CError(st, lib().m2cg_last_error().decode())
+
+
+class Solver:
+    """One structured subdomain advanced on the GPU (FP64 or mixed precision)."""
+
+    def __init__(self, g, s, mats, ls=None):
+        L = lib()
+        self.g, self.s = g, s
+        self.nls = 0 if ls is None else 1
+        arr = (abi.Material * len(mats))(*mats)
+        h = C.c_void_p()
+        check(L.m2cg_create(C.byref(g), C.byref(s), arr, len(mats), C.byref(ls) if ls is not None else None,
+                            self.nls, C.byref(h)))
+        self.h = h
+        self.t = 0.0
+        self.step = 0
+
+    def upload(self, V, ID=None, phi=None):
+        V = np.ascontiguousarray(V, np.float64)
+        ID = None if ID is None else np.ascontiguousarray(ID, np.float64)
+        phi = None if phi is None else np.ascontiguousarray(phi, np.float64)
+        check(lib().m2cg_upload_state(self.h, abi.dptr(V), abi.dptr(ID), abi.dptr(phi)))
+
+    def download(self, out_V=None, out_ID=None, out_phi=None):
+        V = out_V if out_V is not None else np.empty(abi.ghosted_shape(self.g, 5))
+        ID = out_ID if out_ID is not None else np.empty(abi.ghosted_shape(self.g))
+        phi = out_phi if out_phi is not None else (np.empty(abi.ghosted_shape(self.g)) if self.nls else None)
+        check(lib().m2cg_download_state(self.h, abi.dptr(V), abi.dptr(ID), abi.dptr(phi)))
+        return V, ID, phi
+
+    def compute_dt(self):
+        dt = C.c_double()
+        check(lib().m2cg_compute_dt(self.h, C.byref(dt)))
+        return dt.value
+
+    def residual(self):
+        R = np.empty(abi.ghosted_shape(self.g, 5))
+        check(lib().m2cg_compute_residual(self.h, abi.dptr(R)))
+        return R
+
+    def advance(self, dt):
+        """One step of size dt (the reference passes the updated time t+dt)."""
+        self.t += dt
+        self.step += 1
+        check(lib().m2cg_advance(self.h, self.t, dt, self.step))
+
+    def run(self, nsteps, t_max=float("inf")):
+        t = C.c_double(self.t)
+        n = C.c_int()
+        check(lib().m2cg_run(self.h, nsteps, t_max, C.byref(t), C.byref(n)))
+        self.t = t.value
+        self.step += n.value
+        return n.value, self.t
+
+    def time_steps(self, nsteps):
+        ms = C.c_float()
+        launches = C.c_longlong()
+        check(lib().m2cg_time_steps(self.h, nsteps, C.byref(ms), C.byref(launches)))
+        return ms.value, launches.value
+
+    def profile_stages(self, nsteps):
+        ms, n, step = C.c_float(), C.c_int(), C.c_float()
+        check(lib().m2cg_profile_stages(self.h, nsteps, C.byref(ms), C.byref(n), C.byref(step)))
+        return ms.value, n.value, step.value
+
+    def counters(self):
+        c = Counters()
+        check(lib().m2cg_get_counters(self.h, C.byref(c)))
+        return {n: getattr(c, n) for n, _ in Counters._fields_}
+
+    def stream(self):
+        p = C.c_void_p()
+        check(lib().m2cg_get_stream(self.h, C.byref(p)))
+        return p.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().m2cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
