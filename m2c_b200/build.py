@@ -5,7 +5,8 @@ Translation units and their floating-point contract:
       -fmad=false : FP64 path, no FMA contraction (rounds like the reference's
                     x86-64 build)
   kernels_mixed.cu, mlp.cu
-      -fmad=true  : mixed path / learned warm start
+      -fmad=true  : mixed path / learned warm start (kernels_mixed.cu also
+                    --use_fast_math: FP32 division/sqrt approximate, FTZ)
 The library exports the C ABI of include/m2c_gpu.h (plain pointers and sizes).
 """
 import os
@@ -20,6 +21,9 @@ LIB = os.path.join(HERE, "libm2c_gpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                  "-I" + os.path.join(HERE, "..", "include")]
+# --use_fast_math changes only single-precision arithmetic (approximate
+# division/sqrt, flush to zero): the FP32 flux half of the mixed path.
+FAST_FP32 = {"kernels_mixed.cu"}
 NO_FMA = {"kernels_fp64.cu", "context.cu", "multiphase.cu", "riemann.cu", "levelset.cu", "batch.cu",
           "noalloc.cu"}
 
@@ -49,6 +53,8 @@ def build(verbose=False, jobs=8):
         if os.path.exists(obj) and os.path.getmtime(obj) > max(os.path.getmtime(src), hdr_mtime):
             continue
         flags = COMMON + (["-fmad=false"] if f in NO_FMA else ["-fmad=true"])
+        if f in FAST_FP32:
+            flags = flags + ["--use_fast_math"]
         cmd = [cc] + flags + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))

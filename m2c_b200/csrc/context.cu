@@ -121,6 +121,8 @@ struct m2cg_ctx {
   double* lA[3] = {};
   double* lB[3] = {};
   int* lK[3] = {};
+  double* lC[3] = {};
+  int ntx = 1, nty = 1, nitems = 1;
   std::vector<double> hdx, hdy, hdz;
   // device scratch: clock [t, dt, tmax, cfl], dtmin bits, flags, error
   double* clock = nullptr;
@@ -281,9 +283,12 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
       st = fail(M2CG_ERR_ARG, "cannot set up the van Albada exponent on axis %d", a);
       break;
     }
+    std::vector<double> Cm(A.size());
+    for (size_t q = 0; q < A.size(); q++) Cm[q] = B[q] / (A[q] + 1.0);  // Reconstructor.h:97
     upload_vec(&c->lA[a], A, c->stream, &st);
     upload_vec(&c->lB[a], B, c->stream, &st);
     upload_vec(&c->lK[a], K, c->stream, &st);
+    upload_vec(&c->lC[a], Cm, c->stream, &st);
   }
   if (cudaMalloc((void**)&c->clock, 8 * sizeof(double)) != cudaSuccess ||
       cudaMalloc((void**)&c->dtmin, sizeof(unsigned long long)) != cudaSuccess ||
@@ -302,7 +307,7 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   for (int q = 0; q < 6; q++) g.bc[q] = grid->bc[q];
   for (int p = 0; p < 5; p++) { g.inlet[p] = grid->inlet[p]; g.outlet[p] = grid->outlet[p]; }
   g.dx = c->dx; g.dy = c->dy; g.dz = c->dz;
-  for (int a = 0; a < 3; a++) { g.lA[a] = c->lA[a]; g.lB[a] = c->lB[a]; g.lK[a] = c->lK[a]; }
+  for (int a = 0; a < 3; a++) { g.lA[a] = c->lA[a]; g.lB[a] = c->lB[a]; g.lK[a] = c->lK[a]; g.lC[a] = c->lC[a]; }
   SchemeK& sk = c->sk;
   sk.flux = scheme->flux;
   sk.limiter = scheme->limiter;
@@ -316,7 +321,7 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
     sk.ed[m] = make_eos<double>(p);
     sk.ef[m] = make_eos<float>(p);
   }
-  size_t smem = scheme->precision == M2CG_PREC_MIXED ? stage_smem_mixed() : stage_smem_fp64();
+  size_t smem = scheme->precision == M2CG_PREC_MIXED ? stage_smem_mixed(nls == 1) : stage_smem_fp64(nls == 1);
   int maxsm = 0;
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   if (!st && (size_t)maxsm < smem) st = fail(M2CG_ERR_CUDA, "stage kernel needs %zu B shared memory, device has %d", smem, maxsm);
@@ -325,12 +330,28 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
     m2cg_destroy(c);
     return st;
   }
-  // z chunk: enough CTAs to fill 148 SMs at least twice, chunks of >= 8 planes
-  int tiles = ((c->nx + TX - 1) / TX) * ((c->ny + STAGE_TY - 1) / STAGE_TY);
-  int want_chunks = (2 * 148 + tiles - 1) / tiles;
-  int chunk = (c->nz + want_chunks - 1) / want_chunks;
-  if (chunk < 8) chunk = 8;
-  c->zchunk = chunk;
+  // Work items = (x,y) tiles x z-chunks, run by a persistent grid of
+  // resident CTAs. Pick the chunk length that minimises rounds x (chunk +
+  // pipeline prologue of ~2.5 planes).
+  c->ntx = (c->nx + TX - 1) / TX;
+  c->nty = (c->ny + STAGE_TY - 1) / STAGE_TY;
+  {
+    int resident = scheme->precision == M2CG_PREC_MIXED ? stage_resident_mixed(scheme->flux, nls == 1)
+                                                        : stage_resident_fp64(scheme->flux, nls == 1);
+    const int cand[] = {4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 256};
+    double best = 1e300;
+    int bestc = c->nz;
+    for (int ch : cand) {
+      if (ch > c->nz) ch = c->nz;
+      long long items = (long long)c->ntx * c->nty * ((c->nz + ch - 1) / ch);
+      long long rounds = (items + resident - 1) / resident;
+      double cost = rounds * (ch + 2.5);
+      if (cost < best - 1e-9) { best = cost; bestc = ch; }
+      if (ch == c->nz) break;
+    }
+    c->zchunk = bestc;
+    c->nitems = c->ntx * c->nty * ((c->nz + bestc - 1) / bestc);
+  }
   CK(cudaStreamSynchronize(c->stream));
   *out = c;
   return M2CG_OK;
@@ -346,7 +367,7 @@ extern "C" m2cg_status m2cg_destroy(m2cg_ctx* c) {
     }
   cudaFree(c->id);
   cudaFree(c->dx); cudaFree(c->dy); cudaFree(c->dz);
-  for (int a = 0; a < 3; a++) { cudaFree(c->lA[a]); cudaFree(c->lB[a]); cudaFree(c->lK[a]); }
+  for (int a = 0; a < 3; a++) { cudaFree(c->lA[a]); cudaFree(c->lB[a]); cudaFree(c->lK[a]); cudaFree(c->lC[a]); }
   cudaFree(c->clock); cudaFree(c->dtmin); cudaFree(c->clipflags); cudaFree(c->err);
   cudaFree(c->stage_buf);
   if (c->mp) multiphase_destroy(c->mp);
@@ -603,16 +624,19 @@ static void rk_coeffs(int r, int s, double& a_prev, double& a_un, double& b) {
 }
 
 static m2cg_status launch_stage(m2cg_ctx* c, StageArgs& a) {
-  dim3 grid((c->nx + TX - 1) / TX, (c->ny + STAGE_TY - 1) / STAGE_TY, (c->nz + c->zchunk - 1) / c->zchunk);
   a.zchunk = c->zchunk;
+  a.ntx = c->ntx;
+  a.nty = c->nty;
+  a.nitems = c->nitems;
+  int grid = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (c->profile) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, c->stream);
   }
-  cudaError_t e = c->scheme.precision == M2CG_PREC_MIXED ? launch_stage_mixed(a, grid, c->stream)
-                                                          : launch_stage_fp64(a, grid, c->stream);
+  cudaError_t e = c->scheme.precision == M2CG_PREC_MIXED ? launch_stage_mixed(a, c->stream, c->mp != nullptr, &grid)
+                                                          : launch_stage_fp64(a, c->stream, c->mp != nullptr, &grid);
   if (c->profile) {
     cudaEventRecord(e1, c->stream);
     c->ev.push_back(e0);

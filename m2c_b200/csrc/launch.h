@@ -1,7 +1,7 @@
-// Host-side launchers for the stage kernels, one per precision. The FP64
-// instantiation lives in a translation unit compiled without FMA
-// contraction (-fmad=false) so that its arithmetic rounds like the
-// reference's x86-64 build; the mixed instantiation keeps contraction on.
+// Host-side launchers for the stage kernels, one translation unit per
+// precision. The FP64 instantiations live in a unit compiled without FMA
+// contraction (-fmad=false) so that their arithmetic rounds like the
+// reference's x86-64 build; the mixed instantiations keep contraction on.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -9,11 +9,73 @@
 
 namespace m2c {
 
-// Shared-memory bytes and launch of one fused RK stage.
-size_t stage_smem_fp64();
-size_t stage_smem_mixed();
-cudaError_t launch_stage_fp64(const StageArgs& a, dim3 grid, cudaStream_t s);
-cudaError_t launch_stage_mixed(const StageArgs& a, dim3 grid, cudaStream_t s);
 constexpr int STAGE_TY = 8;
+
+size_t stage_smem_fp64(bool multi);
+size_t stage_smem_mixed(bool multi);
+// Launch one stage over a.nitems work items on a persistent grid of
+// min(nitems, SMs x resident CTAs per SM) CTAs. *grid_out reports the grid.
+cudaError_t launch_stage_fp64(const StageArgs& a, cudaStream_t s, bool multi, int* grid_out);
+cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s, bool multi, int* grid_out);
+// Resident CTAs on the whole device of the stage kernel for (flux, multi);
+// each precision's translation unit instantiates only its own kernels.
+int stage_resident_fp64(int flux, bool multi);
+int stage_resident_mixed(int flux, bool multi);
+
+template <typename T, int FLUX, bool MULTI>
+cudaError_t stage_occupancy(int* per_sm, int* nsm) {
+  auto k = stage_kernel<T, STAGE_TY, FLUX, MULTI>;
+  const size_t smem = sizeof(StageSmemAll<T, STAGE_TY, MULTI>);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  e = cudaDeviceGetAttribute(nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, TX * STAGE_TY, smem);
+  if (*per_sm < 1) *per_sm = 1;
+  return e;
+}
+
+template <typename T, int FLUX, bool MULTI>
+cudaError_t launch_stage_one(const StageArgs& a, cudaStream_t s, int* grid_out) {
+  auto k = stage_kernel<T, STAGE_TY, FLUX, MULTI>;
+  const size_t smem = sizeof(StageSmemAll<T, STAGE_TY, MULTI>);
+  int per_sm = 1, nsm = 148;
+  cudaError_t e = stage_occupancy<T, FLUX, MULTI>(&per_sm, &nsm);
+  if (e != cudaSuccess) return e;
+  int grid = a.nitems < per_sm * nsm ? a.nitems : per_sm * nsm;
+  if (grid_out) *grid_out = grid;
+  k<<<grid, dim3(TX, STAGE_TY), smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_stage_t(const StageArgs& a, cudaStream_t s, bool multi, int* g) {
+  switch (a.s.flux) {
+    case FLUX_ROE:
+      return multi ? launch_stage_one<T, FLUX_ROE, true>(a, s, g) : launch_stage_one<T, FLUX_ROE, false>(a, s, g);
+    case FLUX_LLF:
+      return multi ? launch_stage_one<T, FLUX_LLF, true>(a, s, g) : launch_stage_one<T, FLUX_LLF, false>(a, s, g);
+    default:
+      return multi ? launch_stage_one<T, FLUX_HLLC, true>(a, s, g) : launch_stage_one<T, FLUX_HLLC, false>(a, s, g);
+  }
+}
+
+template <typename T>
+int blocks_per_sm_t(int flux, bool multi) {
+  int per_sm = 1, nsm = 148;
+  switch (flux) {
+    case FLUX_ROE:
+      multi ? stage_occupancy<T, FLUX_ROE, true>(&per_sm, &nsm) : stage_occupancy<T, FLUX_ROE, false>(&per_sm, &nsm);
+      break;
+    case FLUX_LLF:
+      multi ? stage_occupancy<T, FLUX_LLF, true>(&per_sm, &nsm) : stage_occupancy<T, FLUX_LLF, false>(&per_sm, &nsm);
+      break;
+    default:
+      multi ? stage_occupancy<T, FLUX_HLLC, true>(&per_sm, &nsm) : stage_occupancy<T, FLUX_HLLC, false>(&per_sm, &nsm);
+  }
+  return per_sm * nsm;
+}
 
 }  // namespace m2c

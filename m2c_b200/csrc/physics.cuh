@@ -44,6 +44,11 @@ template <typename T> M2C_HD T smax(T a, T b) { return (a < b) ? b : a; }
 
 template <typename T> M2C_HD bool finite_(T x) { return isfinite(x); }
 
+// Component d of a 3-vector / of the velocity part of a state, by selects
+// (no dynamically indexed local arrays).
+template <typename T> M2C_HD T pick3(int d, T a, T b, T c) { return d == 0 ? a : (d == 1 ? b : c); }
+template <typename T> M2C_HD T vnorm(int d, const T* V) { return pick3(d, V[1], V[2], V[3]); }
+
 // Material parameters in arithmetic type T.
 template <typename T>
 struct Eos {
@@ -177,6 +182,24 @@ M2C_HD T lim_vanalbada(T A, T B, int k, T dq0, T dq1) {
   return B * (dq1 * p0 + dq0 * p1) / (p0 + A * p1);
 }
 
+// Generalized minmod with its coefficient C = B/(A+1) precomputed (the
+// reference evaluates B/(A+1.0) per call, Reconstructor.h:95-101; the value
+// is the same double).
+template <typename T>
+M2C_HD T lim_genminmod_c(T C, T alpha, T dq0, T dq1) {
+  if (dq0 < T(0) && dq1 < T(0)) return smax(alpha * dq0, smax(C * (dq0 + dq1), alpha * dq1));
+  if (dq0 > T(0) && dq1 > T(0)) return smin(alpha * dq0, smin(C * (dq0 + dq1), alpha * dq1));
+  return T(0);
+}
+
+// Slope with limiter; for the generalized minmod B carries C = B/(A+1).
+template <typename T>
+M2C_HD T limited_slope_c(int limiter, T A, T B, int k, T alpha, T dql, T dqr) {
+  if (limiter == LIM_GENMINMOD) return lim_genminmod_c(B, alpha, dql, dqr);
+  if (limiter == LIM_VANALBADA) return lim_vanalbada(A, B, k, dql, dqr);
+  return T(0.5) * (dql + dqr);
+}
+
 template <typename T>
 M2C_HD T limited_slope(int limiter, T A, T B, int k, T alpha, T dql, T dqr) {
   if (limiter == LIM_GENMINMOD) return lim_genminmod(A, B, alpha, dql, dqr);
@@ -190,12 +213,12 @@ M2C_HD T limited_slope(int limiter, T A, T B, int k, T alpha, T dql, T dqr) {
 template <typename T>
 M2C_HD void phys_flux(const Eos<T>& eos, int d, const T* V, T* F) {
   T H = eos.enthalpy(V);
-  T rvn = V[0] * V[d + 1];
+  T vn = vnorm(d, V);
+  T rvn = V[0] * vn;
   F[0] = rvn;
-  F[1] = rvn * V[1];
-  F[2] = rvn * V[2];
-  F[3] = rvn * V[3];
-  F[d + 1] = rvn * V[d + 1] + V[4];
+  F[1] = d == 0 ? rvn * V[1] + V[4] : rvn * V[1];
+  F[2] = d == 1 ? rvn * V[2] + V[4] : rvn * V[2];
+  F[3] = d == 2 ? rvn * V[3] + V[4] : rvn * V[3];
   F[4] = rvn * H;
 }
 
@@ -217,7 +240,7 @@ M2C_HD void roe_hat(const Eos<T>& eos, int d, const T* Vm, const T* Vp, RoeHat<T
   h.sp = sqrt(Vp[0]);
   T drho = Vp[0] - Vm[0];
   T dp = Vp[4] - Vm[4];
-  T dvel = Vp[d + 1] - Vm[d + 1];
+  T dvel = vnorm(d, Vp) - vnorm(d, Vm);
   T diff = dvel / (h.sm + h.sp);
   T p_over_rho_hat = roe_avg(h.sm, Vm[4] / Vm[0], h.sp, Vp[4] / Vp[0]) + T(0.5) * diff * diff;
   h.em = eos.energy(Vm[0], Vm[4]);
@@ -247,16 +270,15 @@ M2C_HD void roe_hat(const Eos<T>& eos, int d, const T* Vm, const T* Vp, RoeHat<T
 // HLLC star-region flux F* for one side (FluxFcnHLLC.h:159-195).
 template <typename T>
 M2C_HD void hllc_fstar(const Eos<T>& eos, int d, const T* V, T S, T Sstar, T* F) {
-  T velo = V[d + 1];
+  T velo = vnorm(d, V);
   T rhostar = V[0] * (S - velo) / (S - Sstar);
   T U[5];
   eos.p2c(V, U);
   T Us[5];
   Us[0] = T(1);
-  Us[1] = V[1];
-  Us[2] = V[2];
-  Us[3] = V[3];
-  Us[d + 1] = Sstar;
+  Us[1] = d == 0 ? Sstar : V[1];
+  Us[2] = d == 1 ? Sstar : V[2];
+  Us[3] = d == 2 ? Sstar : V[3];
   Us[4] = U[4] / V[0] + (Sstar - velo) * (Sstar + V[4] / (V[0] * (S - velo)));
   for (int i = 0; i < 5; i++) Us[i] = Us[i] * rhostar;
   phys_flux(eos, d, V, F);
@@ -274,15 +296,15 @@ M2C_HD int flux_hllc(const Eos<T>& eos, int d, const T* Vm, const T* Vp, T* F) {
   T cp = eos.c2(Vp[0], h.ep);
   if (cp < T(0)) return ERR_SOUND;
   cp = sqrt(cp);
-  T u_hat = roe_avg(h.sm, Vm[d + 1], h.sp, Vp[d + 1]);
-  T Sm = smin(Vm[d + 1] - cm, u_hat - h.c_hat);
-  T Sp = smax(Vp[d + 1] + cp, u_hat + h.c_hat);
+  T vm = vnorm(d, Vm), vp = vnorm(d, Vp);
+  T u_hat = roe_avg(h.sm, vm, h.sp, vp);
+  T Sm = smin(vm - cm, u_hat - h.c_hat);
+  T Sp = smax(vp + cp, u_hat + h.c_hat);
   if (T(0) <= Sm) {
     phys_flux(eos, d, Vm, F);
   } else if (T(0) >= Sp) {
     phys_flux(eos, d, Vp, F);
   } else {
-    T vm = Vm[d + 1], vp = Vp[d + 1];
     T Sstar = (Vp[4] - Vm[4] + Vm[0] * vm * (Sm - vm) - Vp[0] * vp * (Sp - vp)) /
               (Vm[0] * (Sm - vm) - Vp[0] * (Sp - vp));
     if (Sstar >= T(0))
@@ -296,57 +318,29 @@ M2C_HD int flux_hllc(const Eos<T>& eos, int d, const T* Vm, const T* Vp, T* F) {
 }
 
 // Generalized Roe flux with Harten's entropy fix (FluxFcnGenRoe.h:64-221).
+// The dissipation sum runs over eigenvectors in the outer loop; for every
+// flux component the terms are still subtracted in eigenvector order 1..5,
+// as the reference's inner loop does.
 template <typename T>
 M2C_HD int flux_roe(const Eos<T>& eos, int d, const T* Vm, const T* Vp, T delta, T* F) {
   RoeHat<T> h;
-  // The Roe path averages velocities and enthalpy before the sound speed.
   T sm0 = sqrt(Vm[0]), sp0 = sqrt(Vp[0]);
-  T u = roe_avg(sm0, Vm[1], sp0, Vp[1]);
-  T v = roe_avg(sm0, Vm[2], sp0, Vp[2]);
-  T w = roe_avg(sm0, Vm[3], sp0, Vp[3]);
-  T Hm = eos.enthalpy(Vm), Hp = eos.enthalpy(Vp);
-  T H = roe_avg(sm0, Hm, sp0, Hp);
+  T vel[3];
+  vel[0] = roe_avg(sm0, Vm[1], sp0, Vp[1]);
+  vel[1] = roe_avg(sm0, Vm[2], sp0, Vp[2]);
+  vel[2] = roe_avg(sm0, Vm[3], sp0, Vp[3]);
+  T H = roe_avg(sm0, eos.enthalpy(Vm), sp0, eos.enthalpy(Vp));
   roe_hat(eos, d, Vm, Vp, h);
-  T c = h.c_hat, c2 = h.c_hat2, rho = h.rho_hat;
-  T drho = Vp[0] - Vm[0], du = Vp[1] - Vm[1], dv = Vp[2] - Vm[2], dw = Vp[3] - Vm[3], dp = Vp[4] - Vm[4];
-  T vel2 = u * u + v * v + w * w;
-  T r2e = h.e_hat + T(0.5) * vel2 - h.dpdrho_hat / h.Gamma_hat;
-  T lam[5], a[5], r[5][5];
-  T dn, un;
-  if (d == 0) { un = u; dn = du; }
-  else if (d == 1) { un = v; dn = dv; }
-  else { un = w; dn = dw; }
+  const T c = h.c_hat, c2 = h.c_hat2, rho = h.rho_hat;
+  const T drho = Vp[0] - Vm[0], dp = Vp[4] - Vm[4];
+  const T du = Vp[1] - Vm[1], dv = Vp[2] - Vm[2], dw = Vp[3] - Vm[3];
+  const T un = pick3(d, vel[0], vel[1], vel[2]), dn = pick3(d, du, dv, dw);
+  const T vel2 = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
+  const T r2e = h.e_hat + T(0.5) * vel2 - h.dpdrho_hat / h.Gamma_hat;
+  T lam[5];
   lam[0] = un - c;
   lam[1] = lam[2] = lam[3] = un;
   lam[4] = un + c;
-  a[0] = (dp - rho * c * dn) / (T(2) * c2);
-  a[4] = (dp + rho * c * dn) / (T(2) * c2);
-  T acoustic_free = -dp / c2 + drho;
-  // eigenvectors: r1, r5 acoustic; the middle three follow FluxFcnBase.h:155-245
-  T vel[3] = {u, v, w};
-  for (int q = 0; q < 5; q++) { r[0][q] = T(0); r[4][q] = T(0); }
-  r[0][0] = T(1); r[4][0] = T(1);
-  for (int q = 0; q < 3; q++) { r[0][q + 1] = vel[q]; r[4][q + 1] = vel[q]; }
-  r[0][d + 1] = un - c;
-  r[4][d + 1] = un + c;
-  r[0][4] = H - un * c;
-  r[4][4] = H + un * c;
-  // middle vectors: index 1..3 in the order (x: r2 entropy, r3 v, r4 w),
-  // (y: r2 u, r3 entropy, r4 w), (z: r2 u, r3 v, r4 entropy)
-  for (int m = 1; m <= 3; m++) {
-    int comp = m - 1;  // which velocity component this vector carries (0 u, 1 v, 2 w)
-    for (int q = 0; q < 5; q++) r[m][q] = T(0);
-    if (comp == d) {  // entropy wave
-      r[m][0] = T(1);
-      r[m][1] = u; r[m][2] = v; r[m][3] = w;
-      r[m][4] = r2e;
-      a[m] = acoustic_free;
-    } else {          // shear wave in component comp
-      r[m][comp + 1] = T(1);
-      r[m][4] = vel[comp];
-      a[m] = rho * (comp == 0 ? du : comp == 1 ? dv : dw);
-    }
-  }
   // Harten's entropy fix: tol = delta * max(lam[0], |lam[1..4]|)
   T tol = lam[0];
   for (int i = 1; i < 5; i++)
@@ -354,13 +348,39 @@ M2C_HD int flux_roe(const Eos<T>& eos, int d, const T* Vm, const T* Vp, T delta,
   tol = tol * delta;
   for (int i = 0; i < 5; i++)
     if (fabs(lam[i]) < tol) lam[i] = (lam[i] * lam[i] + tol * tol) / (T(2) * tol);
-  T fm[5], fp[5];
+  T fm[5];
   phys_flux(eos, d, Vm, fm);
-  phys_flux(eos, d, Vp, fp);
-  for (int i = 0; i < 5; i++) {
-    T f = T(0.5) * (fm[i] + fp[i]);
-    for (int p = 0; p < 5; p++) f = f - T(0.5) * fabs(lam[p]) * a[p] * r[p][i];
-    F[i] = f;
+  phys_flux(eos, d, Vp, F);
+  for (int i = 0; i < 5; i++) F[i] = T(0.5) * (fm[i] + F[i]);
+  for (int p = 0; p < 5; p++) {
+    // eigenvector p and its wave strength (FluxFcnBase.h:155-245, FluxFcnGenRoe.h:125-163)
+    T a, r[5];
+    if (p == 0 || p == 4) {
+      a = p == 0 ? (dp - rho * c * dn) / (T(2) * c2) : (dp + rho * c * dn) / (T(2) * c2);
+      T unc = p == 0 ? un - c : un + c;
+      r[0] = T(1);
+      r[1] = d == 0 ? unc : vel[0];
+      r[2] = d == 1 ? unc : vel[1];
+      r[3] = d == 2 ? unc : vel[2];
+      r[4] = p == 0 ? H - un * c : H + un * c;
+    } else {
+      int comp = p - 1;  // the middle vectors carry u, v, w in turn
+      if (comp == d) {   // entropy wave
+        a = -dp / c2 + drho;
+        r[0] = T(1);
+        r[1] = vel[0]; r[2] = vel[1]; r[3] = vel[2];
+        r[4] = r2e;
+      } else {           // shear wave
+        a = rho * pick3(comp, du, dv, dw);
+        r[0] = T(0);
+        r[1] = comp == 0 ? T(1) : T(0);
+        r[2] = comp == 1 ? T(1) : T(0);
+        r[3] = comp == 2 ? T(1) : T(0);
+        r[4] = pick3(comp, vel[0], vel[1], vel[2]);
+      }
+    }
+    T coef = T(0.5) * fabs(lam[p]) * a;
+    for (int i = 0; i < 5; i++) F[i] = F[i] - coef * r[i];
   }
   return ERR_NONE;
 }
@@ -377,7 +397,7 @@ M2C_HD int flux_llf2(const Eos<T>& em, const Eos<T>& ep, int d, const T* Vm, con
   T c_p = ep.c2(Vp[0], e_p);
   if (c_p < T(0)) return ERR_SOUND;
   c_p = sqrt(c_p);
-  T a = smax(fabs(Vm[d + 1]) + c_m, fabs(Vp[d + 1]) + c_p);
+  T a = smax(fabs(vnorm(d, Vm)) + c_m, fabs(vnorm(d, Vp)) + c_p);
   T fm[5], fp[5], Um[5], Up[5];
   phys_flux(em, d, Vm, fm);
   phys_flux(ep, d, Vp, fp);

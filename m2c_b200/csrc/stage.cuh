@@ -17,17 +17,17 @@
 // they are rebuilt from interior cells by the boundary rule when loaded.
 //
 // Work decomposition: a CTA owns a 32 x TY column of cells and marches along
-// z through a chunk of planes, keeping a ring of 3 primitive planes
-// (with a 2-cell x/y halo) in shared memory. Each plane step:
+// z through a chunk of planes, keeping a ring of 3 primitive planes (with a
+// 2-cell x/y halo) in shared memory. Iteration m of the plane pipeline:
 //   (1) load plane m+2 (ghost rules applied on the fly),
-//   (2) slopes + revert mask for every cell of plane m+1 (x -1..32, y -1..TY),
-//   (3) x/y face fluxes of plane m and the z face m+1/2 (one flux per face),
-//   (4) residual + RK update of plane m; the z face m-1/2 is carried in
-//       registers from the previous step.
+//   (2) slopes + revert mask of every cell of plane m+1 (x -1..32, y -1..TY),
+//   (3) every face flux once: x/y faces of plane m and the z faces m+1/2,
+//   (4) residual + RK update of plane m (z faces m-1/2 and m+1/2 from the
+//       two-plane z-flux ring).
 // Face states follow Reconstructor.cpp: slope-limited primitive values, the
 // first face (in the order l,r,b,t,k,f) failing CheckState reverted to the
-// cell value, every face needing clipping reverted to the cell value, and
-// a remaining CheckState failure reported as an error.
+// cell value, every face needing clipping reverted to the cell value, and a
+// remaining CheckState failure reported as an error (never a trap).
 #pragma once
 #include "physics.cuh"
 
@@ -57,6 +57,7 @@ struct Grid3 {
   const double* lA[3];  // limiter coefficient A per axis index
   const double* lB[3];  // limiter coefficient B per axis index
   const int* lK[3];     // van Albada exponent per axis index
+  const double* lC[3];  // generalized minmod B/(A+1) per axis index
 };
 
 struct SchemeK {
@@ -67,6 +68,19 @@ struct SchemeK {
   Eos<float> ef[MAXMAT];   // the same in FP32 for the mixed path's flux half
 };
 
+// Interface faces of a two-material stage: for a cell, the star states of
+// the exact Riemann problems on its three low faces (x, y, z), found through
+// slot[cell] (written only where a low face separates two materials).
+struct IfaceView {
+  const int* slot;       // per cell; valid only where a low face is an interface
+  const double* Vsm;     // [slot][3 faces][5]: left star state  (Riemann side idl)
+  const double* Vsp;     // [slot][3 faces][5]: right star state (Riemann side idr)
+  const double* Vmid;    // [slot][3 faces][5]: state at xi = 0 (EXACT flux)
+  const int* midid;      // [slot][3 faces]
+  int mp_flux;           // 0 EXACT, 1 NUMERICAL, 2 LLF
+  int mp_recon;          // 0 CONSTANT (cell states), 1 LINEAR (face states)
+};
+
 struct StageArgs {
   Grid3 g;
   SchemeK s;
@@ -74,7 +88,7 @@ struct StageArgs {
   const double* Us[5];   // flux source of stages >= 2 (conserved, raw)
   double* Uo[5];         // stage output (conserved) for non-final stages
   double* Vo[5];         // final-stage output (primitive)
-  const uint8_t* id;     // material id per cell (nullptr: all 0)
+  const uint8_t* id;     // material id per cell
   int stage;             // 1-based
   int final_stage;
   double a_prev, a_un;   // U_new = a_prev*U_s + a_un*U^n (stages >= 2)
@@ -84,8 +98,10 @@ struct StageArgs {
   int* clipped_out;      // set if any cell of this stage's output was clipped
   unsigned long long* dtmin_bits;  // final stage: min dx/(|u|+c) as ordered bits
   DevError* err;
-  int zchunk;
+  int zchunk;            // planes per work item
+  int ntx, nty, nitems;  // tiles in x, y and work items (tiles x z-chunks)
   double* Ro[5];         // if set: write the residual R only (no RK update)
+  IfaceView iface;
 };
 
 __device__ __forceinline__ void report(DevError* e, int code, int cell, int where) {
@@ -99,84 +115,76 @@ template <typename T, int TY>
 struct StageSmem {
   static constexpr int RX = TX + 4, RY = TY + 4;   // loaded region: x -2..TX+1, y -2..TY+1
   static constexpr int MX = TX + 2, MY = TY + 2;   // mask region: x -1..TX, y -1..TY
+  static constexpr int NFX = (TX + 1) * TY;        // x faces of a plane
+  static constexpr int NFY = TX * (TY + 1);        // y faces of a plane
+  static constexpr int NFZ = TX * TY;              // z faces between two planes
   T v[3][5][RY][RX];
   T sig[2][3][5][MY][MX];
-  T fx[5][TY][TX + 1];
-  T fy[5][TY + 1][TX];
+  T fx[5][NFX];
+  T fy[5][NFY];
+  T fz[2][5][NFZ];
   uint8_t mask[2][MY][MX];
   uint8_t real[3][RY][RX];  // 1 = real (interior or periodic image), 0 = ghost / unused
   uint8_t ids[3][RY][RX];
+  double raw[5][RY * RX];     // next plane as loaded from HBM (V or U, FP64), in flight via cp.async
+  uint8_t rinfo[RY * RX];     // per loaded cell: bit0 real, bits1-2 ghost axis+1, bit3 ghost side
+  uint8_t rid[RY * RX];
   double red[TY * TX / 32];
 };
 
-// Resolve a possibly-outside index along one axis. Returns the interior index
-// to read; sets ghost side (-1 none, 0 low, 1 high) or far (outside by > 1).
-__device__ __forceinline__ int resolve_axis(int c, int n, int bclo, int bchi, int& side, bool& far) {
+// Two-material extra buffers: fluxes of the right-hand cell at interface faces.
+template <typename T, int TY, bool MULTI>
+struct IfaceSmem {
+  T fx2[5][(TX + 1) * TY];
+  T fy2[5][TX * (TY + 1)];
+  T fz2[2][5][TX * TY];
+};
+template <typename T, int TY>
+struct IfaceSmem<T, TY, false> {};
+
+template <typename T, int TY, bool MULTI>
+struct StageSmemAll {
+  StageSmem<T, TY> b;
+  IfaceSmem<T, TY, MULTI> x;
+};
+
+// Resolve a possibly-outside index along one axis (at most two cells out).
+// Returns the interior index to read; sets ghost side (-1 none, 0 low, 1 high)
+// or far (outside by more than one cell, not periodic).
+__device__ __forceinline__ int resolve_axis(int c, int n, bool periodic, int& side, bool& far) {
   side = -1;
   if (c >= 0 && c < n) return c;
-  int bc = c < 0 ? bclo : bchi;
-  if (bc == BC_PERIODIC) return ((c % n) + n) % n;
+  if (periodic) {
+    int w = c < 0 ? c + n : c - n;
+    if (w < 0) w += n;
+    if (w >= n) w -= n;
+    return w;
+  }
   if (c == -1) { side = 0; return 0; }
   if (c == n) { side = 1; return n - 1; }
   far = true;
   return c < 0 ? 0 : n - 1;
 }
 
-template <typename T> struct EosPick;
-template <> struct EosPick<double> {
-  __device__ static const Eos<double>& get(const SchemeK& s, int id) { return s.ed[id < s.nmat ? id : 0]; }
-};
-template <> struct EosPick<float> {
-  __device__ static const Eos<float>& get(const SchemeK& s, int id) { return s.ef[id < s.nmat ? id : 0]; }
-};
-template <typename T>
-__device__ __forceinline__ Eos<T> eos_of(const SchemeK& s, int id) {
-  return EosPick<T>::get(s, id);
+__device__ __forceinline__ int wrap_index(int c, int n) {
+  if (c < 0) c += n;
+  if (c >= n) c -= n;
+  if (c < 0) c += n;
+  if (c >= n) c -= n;
+  return c;
 }
 
-// Load one primitive state (FP64 on the way in, rounded to T for the flux
-// half) at global (i,j,k), applying ghost rules. Returns 1 if the cell is
-// real, 0 if it is a ghost/unused cell. For stage >= 2 the state comes from
-// U_s by C2P + clip (SpaceOperator::ConservativeToPrimitive + ClipDensityAndPressure).
-template <typename T>
-__device__ int load_cell(const StageArgs& a, int i, int j, int k, T* out, uint8_t& idout) {
-  const Grid3& g = a.g;
-  int sx, sy, sz;
-  bool far = false;
-  int ii = resolve_axis(i, g.nx, g.bc[0], g.bc[1], sx, far);
-  int jj = resolve_axis(j, g.ny, g.bc[2], g.bc[3], sy, far);
-  int kk = resolve_axis(k, g.nz, g.bc[4], g.bc[5], sz, far);
-  int nghost = (sx >= 0) + (sy >= 0) + (sz >= 0);
-  long long off = (long long)kk * g.plane + (long long)jj * g.px + ii;
-  uint8_t id = a.id ? a.id[off] : 0;
-  idout = id;
-  double V[5];
-  if (a.stage == 1) {
-    for (int p = 0; p < 5; p++) V[p] = a.Vn[p][off];
-  } else {
-    double U[5];
-    for (int p = 0; p < 5; p++) U[p] = a.Us[p][off];
-    Eos<double> e = eos_of<double>(a.s, id);
-    e.c2p(U, V);
-    e.clip(V);
-  }
-  int real = (nghost == 0 && !far) ? 1 : 0;
-  if (nghost == 1 && !far) {
-    int axis = sx >= 0 ? 0 : sy >= 0 ? 1 : 2;
-    int side = sx >= 0 ? sx : sy >= 0 ? sy : sz;
-    int bc = g.bc[2 * axis + side];
-    if (bc == BC_INLET) {
-      for (int p = 0; p < 5; p++) V[p] = g.inlet[p];
-    } else if (bc == BC_OUTLET) {
-      for (int p = 0; p < 5; p++) V[p] = g.outlet[p];
-    } else if (bc == BC_STICKWALL) {
-      V[1] = -V[1]; V[2] = -V[2]; V[3] = -V[3];
-    } else {  // SYMMETRY / SLIPWALL
-      V[axis + 1] = -V[axis + 1];
-    }
-  }
-  for (int p = 0; p < 5; p++) out[p] = T(V[p]);
-  return real;
+template <typename T> struct EosPick;
+template <> struct EosPick<double> {
+  __device__ static const Eos<double>& get(const SchemeK& s, int id) { return s.ed[id]; }
+};
+template <> struct EosPick<float> {
+  __device__ static const Eos<float>& get(const SchemeK& s, int id) { return s.ef[id]; }
+};
+
+template <typename T, bool MULTI>
+__device__ __forceinline__ const Eos<T>& eos_of(const SchemeK& s, int id) {
+  return EosPick<T>::get(s, MULTI ? (id < s.nmat ? id : 0) : 0);
 }
 
 // Reconstructed face states of one real cell and the revert mask
@@ -184,37 +192,28 @@ __device__ int load_cell(const StageArgs& a, int i, int j, int k, T* out, uint8_
 template <typename T>
 __device__ __forceinline__ int cell_faces(const Eos<T>& e, const T* v, const T* sx, const T* sy, const T* sz,
                                           uint8_t& mask) {
-  T f[6][5];
-  for (int p = 0; p < 5; p++) {
-    T hx = T(0.5) * sx[p], hy = T(0.5) * sy[p], hz = T(0.5) * sz[p];
-    f[0][p] = v[p] - hx; f[1][p] = v[p] + hx;
-    f[2][p] = v[p] - hy; f[3][p] = v[p] + hy;
-    f[4][p] = v[p] - hz; f[5][p] = v[p] + hz;
-  }
   uint8_t m = 0;
-  // Reconstructor.cpp:719-775: only the first non-physical face is reverted.
-  for (int q = 0; q < 6; q++)
-    if (e.bad(f[q])) { m |= uint8_t(1u << q); break; }
-  // SpaceOperator.cpp:3240-3273: faces needing clipping revert to the cell value.
-  for (int q = 0; q < 6; q++)
-    if (!(m & (1u << q)) && e.needs_clip(f[q])) m |= uint8_t(1u << q);
-  mask = m;
-  // SpaceOperator.cpp:3275-3277: any face still non-physical is fatal.
-  for (int q = 0; q < 6; q++)
-    if (!(m & (1u << q)) && e.bad(f[q])) return ERR_STATE;
-  return ERR_NONE;
-}
-
-// Final face value of a real cell: side 0 = minus face (v - s/2), 1 = plus face.
-template <typename T>
-__device__ __forceinline__ void face_value(const T* v, const T* s, bool reverted, int side, T* out) {
-  if (reverted) {
-    for (int p = 0; p < 5; p++) out[p] = v[p];
-  } else if (side == 0) {
-    for (int p = 0; p < 5; p++) out[p] = v[p] - T(0.5) * s[p];
-  } else {
-    for (int p = 0; p < 5; p++) out[p] = v[p] + T(0.5) * s[p];
+  bool chain_done = false;
+  int err = ERR_NONE;
+  // faces in the reference's order l, r, b, t, k, f
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const T* s = q < 2 ? sx : (q < 4 ? sy : sz);
+    T f[5];
+#pragma unroll
+    for (int p = 0; p < 5; p++) f[p] = (q & 1) ? v[p] + T(0.5) * s[p] : v[p] - T(0.5) * s[p];
+    const bool bad = e.bad(f);
+    bool reverted = false;
+    // Reconstructor.cpp:719-775: only the first non-physical face is reverted.
+    if (!chain_done && bad) { reverted = true; chain_done = true; }
+    // SpaceOperator.cpp:3240-3273: a face needing clipping reverts to the cell value.
+    if (!reverted && e.needs_clip(f)) reverted = true;
+    if (reverted) m |= uint8_t(1u << q);
+    // SpaceOperator.cpp:3275-3277: a face still non-physical is fatal.
+    else if (bad) err = ERR_STATE;
   }
+  mask = m;
+  return err;
 }
 
 // Boundary face state built from the interior neighbour's face state
@@ -224,83 +223,197 @@ template <typename T>
 __device__ __forceinline__ void ghost_face(int bc, int axis, const T* inner_face, const T* ghost_cell,
                                            const Eos<T>& e, T* out) {
   if (bc == BC_INLET || bc == BC_OUTLET) {
+#pragma unroll
     for (int p = 0; p < 5; p++) out[p] = ghost_cell[p];
   } else {
+#pragma unroll
     for (int p = 0; p < 5; p++) out[p] = inner_face[p];
     if (bc == BC_STICKWALL) {
       out[1] = -out[1]; out[2] = -out[2]; out[3] = -out[3];
     } else {
-      out[axis + 1] = -out[axis + 1];
+      if (axis == 0) out[1] = -out[1];
+      else if (axis == 1) out[2] = -out[2];
+      else out[3] = -out[3];
     }
   }
-  if (e.needs_clip(out))
+  if (e.needs_clip(out)) {
+#pragma unroll
     for (int p = 0; p < 5; p++) out[p] = ghost_cell[p];
+  }
 }
 
-template <typename T, int TY>
-__global__ void __launch_bounds__(TX * TY, 1) stage_kernel(const StageArgs a) {
+template <typename T, int FLUX>
+__device__ __forceinline__ int flux_of(const Eos<T>& e, int d, const T* VL, const T* VR, T delta, T* F) {
+  if (FLUX == FLUX_HLLC) return flux_hllc(e, d, VL, VR, F);
+  if (FLUX == FLUX_ROE) return flux_roe(e, d, VL, VR, delta, F);
+  return flux_llf2(e, e, d, VL, VR, F);
+}
+
+// Asynchronous 8-byte global -> shared copy (cp.async, L1-allocating) and
+// its completion wait; used to prefetch the next plane while the current one
+// is being computed.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <typename T> struct StageOcc { static constexpr int value = 1; };
+template <> struct StageOcc<float> { static constexpr int value = 2; };
+
+template <typename T, int TY, int FLUX, bool MULTI>
+__global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(const __grid_constant__ StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef StageSmem<T, TY> S;
-  S& sm = *reinterpret_cast<S*>(smem_raw);
+  typedef StageSmemAll<T, TY, MULTI> SA;
+  SA& all = *reinterpret_cast<SA*>(smem_raw);
+  S& sm = all.b;
   const Grid3& g = a.g;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int NT = TX * TY;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-  const int kb = blockIdx.z * a.zchunk;
-  const int ke = min(kb + a.zchunk, g.nz);
-  if (kb >= ke) return;
-  const bool zper = g.bc[4] == BC_PERIODIC;
+  constexpr int NT = TX * TY;
+  constexpr int NLOAD = S::RY * S::RX;
+  constexpr int LPT = (NLOAD + NT - 1) / NT;  // loaded cells per thread
+  const bool xper = g.bc[0] == BC_PERIODIC, yper = g.bc[2] == BC_PERIODIC, zper = g.bc[4] == BC_PERIODIC;
   const double dt = a.clock[1];
   const double bdt = a.bdt_coef * dt;
   const bool us_clip = (a.stage > 1) && a.us_clipped && *a.us_clipped;
   const T alpha = T(a.s.alpha), delta = T(a.s.delta);
   const int where = a.stage * 16;
+  const int limiter = a.s.limiter;
+  const bool rec_linear = a.s.rec_linear;
+  const bool slope_zero = MULTI && a.s.slope_zero_at_interface;
+  const double* const* src = a.stage == 1 ? a.Vn : a.Us;
+
+  int i0 = 0, j0 = 0;  // tile origin of the current work item
+  uint8_t idreg[LPT];
 
   auto slot3 = [](int p) { return ((p % 3) + 3) % 3; };
   auto plane_is_ghost = [&](int p) { return !zper && (p < 0 || p >= g.nz); };
 
-  // (1) load plane p into the ring
-  auto load_plane = [&](int p) {
-    int s = slot3(p);
-    for (int q = tid; q < S::RY * S::RX; q += NT) {
-      int ly = q / S::RX, lx = q % S::RX;
-      T v[5];
-      uint8_t id;
-      int real = load_cell<T>(a, i0 + lx - 2, j0 + ly - 2, p, v, id);
-      for (int c = 0; c < 5; c++) sm.v[s][c][ly][lx] = v[c];
-      sm.real[s][ly][lx] = (uint8_t)real;
+  // (1a) start fetching plane p: one cp.async per value into the staging
+  // buffer, ghost cells read from their image cell; cell kind kept in rinfo.
+  auto issue_plane = [&](int p) {
+    int sz;
+    bool farz = false;
+    const int kk = resolve_axis(p, g.nz, zper, sz, farz);
+#pragma unroll
+    for (int r = 0; r < LPT; r++) {
+      const int q = tid + r * NT;
+      if (q >= NLOAD) break;
+      const int ly = q / S::RX, lx = q - ly * S::RX;
+      int sx, sy;
+      bool far = farz;
+      const int ii = resolve_axis(i0 + lx - 2, g.nx, xper, sx, far);
+      const int jj = resolve_axis(j0 + ly - 2, g.ny, yper, sy, far);
+      const int nghost = (sx >= 0) + (sy >= 0) + (sz >= 0);
+      const long long off = (long long)kk * g.plane + (long long)jj * g.px + ii;
+#pragma unroll
+      for (int c = 0; c < 5; c++) cp_async8(&sm.raw[c][q], src[c] + off);
+      uint8_t info = 0;
+      if (nghost == 0 && !far) {
+        info = 1;
+      } else if (nghost == 1 && !far) {
+        const int axis = sx >= 0 ? 0 : (sy >= 0 ? 1 : 2);
+        const int side = sx >= 0 ? sx : (sy >= 0 ? sy : sz);
+        info = uint8_t(((axis + 1) << 1) | (side << 3));
+      }
+      sm.rinfo[q] = info;
+      if (MULTI) idreg[r] = a.id[off];
+    }
+    cp_async_commit();
+  };
+
+  // (1b) turn the fetched plane into primitive states in the ring: C2P + clip
+  // for stages >= 2 (SpaceOperator::ConservativeToPrimitive +
+  // ClipDensityAndPressure), the boundary rule for ghost cells
+  // (SpaceOperator::ApplyBoundaryConditions), rounding to T.
+  auto commit_plane = [&](int p) {
+    const int s = slot3(p);
+#pragma unroll
+    for (int r = 0; r < LPT; r++) {
+      const int q = tid + r * NT;
+      if (q >= NLOAD) break;
+      const int ly = q / S::RX, lx = q - ly * S::RX;
+      const uint8_t info = sm.rinfo[q];
+      const uint8_t id = MULTI ? idreg[r] : 0;
+      double V[5];
+      if (a.stage == 1) {
+#pragma unroll
+        for (int c = 0; c < 5; c++) V[c] = sm.raw[c][q];
+      } else {
+        double U[5];
+#pragma unroll
+        for (int c = 0; c < 5; c++) U[c] = sm.raw[c][q];
+        const Eos<double>& e = eos_of<double, MULTI>(a.s, id);
+        e.c2p(U, V);
+        e.clip(V);
+      }
+      const int gaxis = (info >> 1) & 3;
+      if (gaxis) {
+        const int axis = gaxis - 1, side = (info >> 3) & 1;
+        const int bc = g.bc[2 * axis + side];
+        if (bc == BC_INLET) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) V[c] = g.inlet[c];
+        } else if (bc == BC_OUTLET) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) V[c] = g.outlet[c];
+        } else if (bc == BC_STICKWALL) {
+          V[1] = -V[1]; V[2] = -V[2]; V[3] = -V[3];
+        } else {  // SYMMETRY / SLIPWALL: normal velocity flipped
+          if (axis == 0) V[1] = -V[1];
+          else if (axis == 1) V[2] = -V[2];
+          else V[3] = -V[3];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 5; c++) sm.v[s][c][ly][lx] = T(V[c]);
+      sm.real[s][ly][lx] = info & 1;
       sm.ids[s][ly][lx] = id;
     }
   };
 
-  // (2) slopes + mask for plane p (needs planes p-1, p, p+1 in the ring)
+  // (2) slopes + revert mask of plane p (needs planes p-1, p, p+1 in the ring)
   auto mask_plane = [&](int p) {
-    int sm1 = slot3(p - 1), s0 = slot3(p), sp1 = slot3(p + 1), ms = p & 1;
+    const int sm1 = slot3(p - 1), s0 = slot3(p), sp1 = slot3(p + 1), ms = p & 1;
+    const int ka = wrap_index(p, g.nz);
     for (int q = tid; q < S::MY * S::MX; q += NT) {
-      int my = q / S::MX, mx = q % S::MX;
-      int ly = my + 1, lx = mx + 1;  // position in the loaded region
-      if (!sm.real[s0][ly][lx]) { sm.mask[ms][my][mx] = 0; continue; }
-      int gi = i0 + mx - 1, gj = j0 + my - 1;
-      uint8_t id = sm.ids[s0][ly][lx];
-      Eos<T> e = eos_of<T>(a.s, id);
-      T v[5], sx[5], sy[5], sz[5];
-      int ia = ((gi % g.nx) + g.nx) % g.nx, ja = ((gj % g.ny) + g.ny) % g.ny, ka = ((p % g.nz) + g.nz) % g.nz;
-      T Ax = T(g.lA[0][ia]), Bx = T(g.lB[0][ia]), Ay = T(g.lA[1][ja]), By = T(g.lB[1][ja]);
-      T Az = T(g.lA[2][ka]), Bz = T(g.lB[2][ka]);
-      int Kx = g.lK[0][ia], Ky = g.lK[1][ja], Kz = g.lK[2][ka];
+      const int my = q / S::MX, mx = q - my * S::MX;
+      const int ly = my + 1, lx = mx + 1;  // position in the loaded region
+      if (!sm.real[s0][ly][lx]) {
+        sm.mask[ms][my][mx] = 0;
+        continue;
+      }
+      const int ia = wrap_index(i0 + mx - 1, g.nx), ja = wrap_index(j0 + my - 1, g.ny);
+      const uint8_t id = sm.ids[s0][ly][lx];
+      const Eos<T>& e = eos_of<T, MULTI>(a.s, id);
+      T Ax, Bx, Ay, By, Az, Bz;
+      int Kx = 0, Ky = 0, Kz = 0;
+      if (limiter == LIM_VANALBADA) {
+        Ax = T(g.lA[0][ia]); Bx = T(g.lB[0][ia]); Kx = g.lK[0][ia];
+        Ay = T(g.lA[1][ja]); By = T(g.lB[1][ja]); Ky = g.lK[1][ja];
+        Az = T(g.lA[2][ka]); Bz = T(g.lB[2][ka]); Kz = g.lK[2][ka];
+      } else {  // generalized minmod uses B/(A+1) only
+        Ax = T(0); Bx = T(g.lC[0][ia]);
+        Ay = T(0); By = T(g.lC[1][ja]);
+        Az = T(0); Bz = T(g.lC[2][ka]);
+      }
       bool zx = false, zy = false, zz = false;
-      if (a.s.slope_zero_at_interface && a.id) {
+      if (slope_zero) {
         zx = id != sm.ids[s0][ly][lx - 1] || id != sm.ids[s0][ly][lx + 1];
         zy = id != sm.ids[s0][ly - 1][lx] || id != sm.ids[s0][ly + 1][lx];
         zz = id != sm.ids[sm1][ly][lx] || id != sm.ids[sp1][ly][lx];
       }
+      T v[5], sx[5], sy[5], sz[5];
+#pragma unroll
       for (int c = 0; c < 5; c++) {
-        T vc = sm.v[s0][c][ly][lx];
+        const T vc = sm.v[s0][c][ly][lx];
         v[c] = vc;
-        if (a.s.rec_linear) {
-          sx[c] = limited_slope(a.s.limiter, Ax, Bx, Kx, alpha, vc - sm.v[s0][c][ly][lx - 1], sm.v[s0][c][ly][lx + 1] - vc);
-          sy[c] = limited_slope(a.s.limiter, Ay, By, Ky, alpha, vc - sm.v[s0][c][ly - 1][lx], sm.v[s0][c][ly + 1][lx] - vc);
-          sz[c] = limited_slope(a.s.limiter, Az, Bz, Kz, alpha, vc - sm.v[sm1][c][ly][lx], sm.v[sp1][c][ly][lx] - vc);
+        if (rec_linear) {
+          sx[c] = limited_slope_c(limiter, Ax, Bx, Kx, alpha, vc - sm.v[s0][c][ly][lx - 1], sm.v[s0][c][ly][lx + 1] - vc);
+          sy[c] = limited_slope_c(limiter, Ay, By, Ky, alpha, vc - sm.v[s0][c][ly - 1][lx], sm.v[s0][c][ly + 1][lx] - vc);
+          sz[c] = limited_slope_c(limiter, Az, Bz, Kz, alpha, vc - sm.v[sm1][c][ly][lx], sm.v[sp1][c][ly][lx] - vc);
           if (zx) sx[c] = T(0);
           if (zy) sy[c] = T(0);
           if (zz) sz[c] = T(0);
@@ -312,127 +425,207 @@ __global__ void __launch_bounds__(TX * TY, 1) stage_kernel(const StageArgs a) {
         sm.sig[ms][2][c][my][mx] = sz[c];
       }
       uint8_t m;
-      int err = cell_faces(e, v, sx, sy, sz, m);
+      const int err = cell_faces(e, v, sx, sy, sz, m);
       sm.mask[ms][my][mx] = m;
-      if (err) report(a.err, err, (int)((long long)p * g.ny * g.nx + (long long)gj * g.nx + gi), where + 1);
+      if (err) report(a.err, err, (int)(((long long)ka * g.ny + ja) * g.nx + ia), where + 1);
     }
   };
 
-  // Face state of a real cell at mask-region position (mx,my) in plane p,
-  // direction d, side (0 minus, 1 plus).
+  // Final face state of the real cell at mask-region (mx,my) of plane p:
+  // direction d, side 0 = minus face (v - s/2), 1 = plus face (v + s/2).
   auto cell_face = [&](int p, int mx, int my, int d, int side, T* out) {
-    int s0 = slot3(p), ms = p & 1;
-    T v[5], s[5];
+    const int s0 = slot3(p), ms = p & 1;
+    const bool rev = (sm.mask[ms][my][mx] >> (2 * d + side)) & 1u;
+#pragma unroll
     for (int c = 0; c < 5; c++) {
-      v[c] = sm.v[s0][c][my + 1][mx + 1];
-      s[c] = sm.sig[ms][d][c][my][mx];
+      const T v = sm.v[s0][c][my + 1][mx + 1];
+      const T s = sm.sig[ms][d][c][my][mx];
+      out[c] = rev ? v : (side ? v + T(0.5) * s : v - T(0.5) * s);
     }
-    bool rev = (sm.mask[ms][my][mx] >> (2 * d + side)) & 1u;
-    face_value(v, s, rev, side, out);
   };
 
-  // Flux across the face between mask-region cells L and R (R = L + e_d).
-  // pL/pR are the planes of L and R; real flags say whether each is a real cell.
-  auto face_flux = [&](int d, int pL, int mxL, int myL, int pR, int mxR, int myR, T* F) {
-    bool rL = sm.real[slot3(pL)][myL + 1][mxL + 1], rR = sm.real[slot3(pR)][myR + 1][mxR + 1];
-    T VL[5], VR[5];
-    uint8_t idL = sm.ids[slot3(pL)][myL + 1][mxL + 1], idR = sm.ids[slot3(pR)][myR + 1][mxR + 1];
-    int bcside;
-    if (rL) cell_face(pL, mxL, myL, d, 1, VL);
-    if (rR) cell_face(pR, mxR, myR, d, 0, VR);
+  // (3) flux across the face between mask-region cells L (plane pL) and
+  // R = L + e_d (plane pR). Writes the flux seen by the left cell (F) and,
+  // for two materials, the flux seen by the right cell (F2; they differ only
+  // at a material interface).
+  auto face_flux = [&](int d, int pL, int mxL, int myL, int pR, int mxR, int myR, T* F, T* F2) {
+    const int sL = slot3(pL), sR = slot3(pR);
+    const bool rL = sm.real[sL][myL + 1][mxL + 1], rR = sm.real[sR][myR + 1][mxR + 1];
     if (!rL && !rR) {
-      for (int c = 0; c < 5; c++) F[c] = T(0);
+#pragma unroll
+      for (int c = 0; c < 5; c++) { F[c] = T(0); F2[c] = T(0); }
       return;
     }
+    T VL[5], VR[5];
+    const uint8_t idL = sm.ids[sL][myL + 1][mxL + 1], idR = sm.ids[sR][myR + 1][mxR + 1];
+    if (rL) cell_face(pL, mxL, myL, d, 1, VL);
+    if (rR) cell_face(pR, mxR, myR, d, 0, VR);
     if (!rL) {  // low-side boundary face
-      bcside = 2 * d;
       T gc[5];
-      for (int c = 0; c < 5; c++) gc[c] = sm.v[slot3(pL)][c][myL + 1][mxL + 1];
-      ghost_face(g.bc[bcside], d, VR, gc, eos_of<T>(a.s, idL), VL);
+#pragma unroll
+      for (int c = 0; c < 5; c++) gc[c] = sm.v[sL][c][myL + 1][mxL + 1];
+      ghost_face(g.bc[2 * d], d, VR, gc, eos_of<T, MULTI>(a.s, idL), VL);
     }
     if (!rR) {  // high-side boundary face
-      bcside = 2 * d + 1;
       T gc[5];
-      for (int c = 0; c < 5; c++) gc[c] = sm.v[slot3(pR)][c][myR + 1][mxR + 1];
-      ghost_face(g.bc[bcside], d, VL, gc, eos_of<T>(a.s, idR), VR);
+#pragma unroll
+      for (int c = 0; c < 5; c++) gc[c] = sm.v[sR][c][myR + 1][mxR + 1];
+      ghost_face(g.bc[2 * d + 1], d, VL, gc, eos_of<T, MULTI>(a.s, idR), VR);
     }
-    // same material (single-material path): flux with the right cell's EOS,
-    // as the reference's face loop does (myid = id of the right cell).
-    uint8_t idf = rR ? idR : idL;
-    int err = num_flux(a.s.flux, eos_of<T>(a.s, idf), d, VL, VR, delta, F);
+    int err = ERR_NONE;
+    if (MULTI && idL != idR) {
+      // Material interface (SpaceOperator.cpp:2486-2542): two one-sided fluxes
+      // against the exact Riemann star states, or LLF across the interface.
+      const IfaceView& iv = a.iface;
+      T WL[5], WR[5];
+      if (iv.mp_recon == 0) {  // constant reconstruction: cell-centred states
+#pragma unroll
+        for (int c = 0; c < 5; c++) {
+          WL[c] = sm.v[sL][c][myL + 1][mxL + 1];
+          WR[c] = sm.v[sR][c][myR + 1][mxR + 1];
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 5; c++) { WL[c] = VL[c]; WR[c] = VR[c]; }
+      }
+      if (iv.mp_flux == 2) {
+        err = flux_llf2(eos_of<T, MULTI>(a.s, idL), eos_of<T, MULTI>(a.s, idR), d, WL, WR, F);
+#pragma unroll
+        for (int c = 0; c < 5; c++) F2[c] = F[c];
+      } else {
+        // the right cell's index carries the slot of its low faces
+        const int gi = wrap_index(i0 + mxR - 1, g.nx), gj = wrap_index(j0 + myR - 1, g.ny);
+        const int gk = wrap_index(pR, g.nz);
+        const int slot = iv.slot[(long long)gk * g.plane + (long long)gj * g.px + gi];
+        const long long base = ((long long)slot * 3 + d) * 5;
+        if (iv.mp_flux == 0) {  // Godunov flux of the state at xi = 0
+          T Vm[5];
+#pragma unroll
+          for (int c = 0; c < 5; c++) Vm[c] = T(iv.Vmid[base + c]);
+          phys_flux(eos_of<T, MULTI>(a.s, iv.midid[slot * 3 + d]), d, Vm, F);
+#pragma unroll
+          for (int c = 0; c < 5; c++) F2[c] = F[c];
+        } else {
+          T Sm[5], Sp[5];
+#pragma unroll
+          for (int c = 0; c < 5; c++) {
+            Sm[c] = T(iv.Vsm[base + c]);
+            Sp[c] = T(iv.Vsp[base + c]);
+          }
+          err = flux_of<T, FLUX>(eos_of<T, MULTI>(a.s, idL), d, WL, Sm, delta, F);
+          if (!err) err = flux_of<T, FLUX>(eos_of<T, MULTI>(a.s, idR), d, Sp, WR, delta, F2);
+        }
+      }
+    } else {
+      // same material: flux with the right cell's EOS, as the reference's
+      // face loop does (myid = id of the right cell)
+      err = flux_of<T, FLUX>(eos_of<T, MULTI>(a.s, rR ? idR : idL), d, VL, VR, delta, F);
+#pragma unroll
+      for (int c = 0; c < 5; c++) F2[c] = F[c];
+    }
     if (err) report(a.err, err, -1, where + 2);
   };
 
-  // ---- prologue ----
-  T Hprev[5];
-  if (!plane_is_ghost(kb - 1)) {
-    load_plane(kb - 2);
-    load_plane(kb - 1);
-    load_plane(kb);
-    __syncthreads();
-    mask_plane(kb - 1);
-    __syncthreads();
-    load_plane(kb + 1);
-    __syncthreads();
-    mask_plane(kb);
-    __syncthreads();
-  } else {
-    load_plane(kb - 1);
-    load_plane(kb);
-    load_plane(kb + 1);
-    __syncthreads();
-    mask_plane(kb);
-    __syncthreads();
-  }
-  face_flux(2, kb - 1, tx + 1, ty + 1, kb, tx + 1, ty + 1, Hprev);
-
-  const int gi = i0 + tx, gj = j0 + ty;
-  const bool own = gi < g.nx && gj < g.ny;
-  double dxi = 0, dyj = 0;
-  if (own) { dxi = g.dx[gi]; dyj = g.dy[gj]; }
-  double dtmin_local = 1.0e300;
-  int clipped_local = 0;
-
-  for (int m = kb; m < ke; m++) {
-    __syncthreads();
-    load_plane(m + 2);
-    __syncthreads();
-    if (!plane_is_ghost(m + 1)) mask_plane(m + 1);
-    __syncthreads();
-    // (3) faces of plane m
-    {
-      T F[5];
-      face_flux(0, m, tx, ty + 1, m, tx + 1, ty + 1, F);
-      for (int c = 0; c < 5; c++) sm.fx[c][ty][tx] = F[c];
-      if (tid < TY) {
-        face_flux(0, m, TX, tid + 1, m, TX + 1, tid + 1, F);
-        for (int c = 0; c < 5; c++) sm.fx[c][tid][TX] = F[c];
-      }
-      face_flux(1, m, tx + 1, ty, m, tx + 1, ty + 1, F);
-      for (int c = 0; c < 5; c++) sm.fy[c][ty][tx] = F[c];
-      if (tid < TX) {
-        face_flux(1, m, tid + 1, TY, m, tid + 1, TY + 1, F);
-        for (int c = 0; c < 5; c++) sm.fy[c][TY][tid] = F[c];
+  // All faces needed by plane m: x and y faces of plane m (if do_xy) and the
+  // z faces m+1/2, one work item per face.
+  auto faces = [&](int m, bool do_xy) {
+    const int nxy = do_xy ? S::NFX + S::NFY : 0;
+    const int nall = nxy + S::NFZ;
+    const int zs = (m + 1) & 1;
+    for (int q = tid; q < nall; q += NT) {
+      T F[5], F2[5];
+      if (q < S::NFX && do_xy) {              // x face left of (fxi, fyi)
+        const int fyi = q / (TX + 1), fxi = q - fyi * (TX + 1);
+        face_flux(0, m, fxi, fyi + 1, m, fxi + 1, fyi + 1, F, F2);
+#pragma unroll
+        for (int c = 0; c < 5; c++) sm.fx[c][q] = F[c];
+        if constexpr (MULTI) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) all.x.fx2[c][q] = F2[c];
+        }
+      } else if (q < nxy) {                   // y face below (fxi, fyi)
+        const int r = q - S::NFX;
+        const int fyi = r / TX, fxi = r - fyi * TX;
+        face_flux(1, m, fxi + 1, fyi, m, fxi + 1, fyi + 1, F, F2);
+#pragma unroll
+        for (int c = 0; c < 5; c++) sm.fy[c][r] = F[c];
+        if constexpr (MULTI) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) all.x.fy2[c][r] = F2[c];
+        }
+      } else {                                // z face m+1/2 of column (fxi, fyi)
+        const int r = q - nxy;
+        const int fyi = r / TX, fxi = r - fyi * TX;
+        face_flux(2, m, fxi + 1, fyi + 1, m + 1, fxi + 1, fyi + 1, F, F2);
+#pragma unroll
+        for (int c = 0; c < 5; c++) sm.fz[zs][c][r] = F[c];
+        if constexpr (MULTI) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) all.x.fz2[zs][c][r] = F2[c];
+        }
       }
     }
-    T Hnext[5];
-    face_flux(2, m, tx + 1, ty + 1, m + 1, tx + 1, ty + 1, Hnext);
+  };
+
+  double dtmin_local = 1.0e300;
+  int clipped_local = 0;
+  const int tiles = a.ntx * a.nty;
+
+  for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+    const int zc = item / tiles, t2 = item - zc * tiles;
+    const int tyi = t2 / a.ntx, txi = t2 - tyi * a.ntx;
+    i0 = txi * TX;
+    j0 = tyi * TY;
+    const int kb = zc * a.zchunk;
+    const int ke = min(kb + a.zchunk, g.nz);
+    const int gi = i0 + tx, gj = j0 + ty;
+    const bool own = gi < g.nx && gj < g.ny;
+    double dxi = 0, dyj = 0;
+    if (own) { dxi = g.dx[gi]; dyj = g.dy[gj]; }
+
+    // pipeline prologue: planes kb-2 and kb-1 committed, plane kb in flight
     __syncthreads();
-    // (4) residual + RK update
-    if (own) {
-      double dzk = g.dz[m];
-      double ax = dyj * dzk, ay = dxi * dzk, az = dxi * dyj;
-      double vol = dxi * dyj * dzk;
-      long long off = (long long)m * g.plane + (long long)gj * g.px + gi;
-      uint8_t id = a.id ? a.id[off] : 0;
-      Eos<double> e = eos_of<double>(a.s, id);
+    issue_plane(kb - 2);
+    cp_async_wait_all();
+    __syncthreads();
+    commit_plane(kb - 2);
+    __syncthreads();
+    issue_plane(kb - 1);
+    cp_async_wait_all();
+    __syncthreads();
+    commit_plane(kb - 1);
+    __syncthreads();
+    issue_plane(kb);
+    for (int m = kb - 2; m < ke; m++) {
+      cp_async_wait_all();
+      __syncthreads();
+      commit_plane(m + 2);
+      __syncthreads();
+      if (m + 3 <= ke + 1) issue_plane(m + 3);  // in flight during the work below
+      if (m + 1 >= kb - 1 && !plane_is_ghost(m + 1)) mask_plane(m + 1);
+      __syncthreads();
+      if (m >= kb - 1) faces(m, m >= kb);
+      __syncthreads();
+      if (m < kb || !own) continue;
+      // (4) residual + RK update of plane m
+      const double dzk = g.dz[m];
+      const double ax = dyj * dzk, ay = dxi * dzk, az = dxi * dyj;
+      const double vol = dxi * dyj * dzk;
+      // Vec5D::operator/= multiplies by the reciprocal (Vector5D.h:172-181)
+      const double inv_mvol = 1.0 / (-vol);
+      const long long off = (long long)m * g.plane + (long long)gj * g.px + gi;
+      const uint8_t id = MULTI ? a.id[off] : 0;
+      const Eos<double>& e = eos_of<double, MULTI>(a.s, id);
       double Un[5], Unew[5], Vn[5];
+#pragma unroll
       for (int c = 0; c < 5; c++) Vn[c] = a.Vn[c][off];
       e.p2c(Vn, Un);
       if (a.stage == 1) {
+#pragma unroll
         for (int c = 0; c < 5; c++) Unew[c] = Un[c];
       } else {
         double Us[5];
+#pragma unroll
         for (int c = 0; c < 5; c++) Us[c] = a.Us[c][off];
         if (us_clip) {
           double Vs[5];
@@ -440,41 +633,57 @@ __global__ void __launch_bounds__(TX * TY, 1) stage_kernel(const StageArgs a) {
           e.clip(Vs);
           e.p2c(Vs, Us);
         }
+#pragma unroll
         for (int c = 0; c < 5; c++) Unew[c] = a.a_prev * Us[c] + a.a_un * Un[c];
       }
+      const int fxl = ty * (TX + 1) + tx, fyl = ty * TX + tx, fzc = ty * TX + tx;
+      const int zl = m & 1, zr = (m + 1) & 1;
+#pragma unroll
       for (int c = 0; c < 5; c++) {
+        // low faces: the flux this cell sees as the right-hand cell
+        // (SpaceOperator.cpp:2555-2556, 2683-2684, 2810-2811)
+        double fl, gl, hl;
+        if constexpr (MULTI) {
+          fl = double(all.x.fx2[c][fxl]);
+          gl = double(all.x.fy2[c][fyl]);
+          hl = double(all.x.fz2[zl][c][fzc]);
+        } else {
+          fl = double(sm.fx[c][fxl]);
+          gl = double(sm.fy[c][fyl]);
+          hl = double(sm.fz[zl][c][fzc]);
+        }
         double f = 0.0;
-        f = f - double(sm.fx[c][ty][tx]) * ax;
-        f = f - double(sm.fy[c][ty][tx]) * ay;
-        f = f - double(Hprev[c]) * az;
-        f = f + double(sm.fx[c][ty][tx + 1]) * ax;
-        f = f + double(sm.fy[c][ty + 1][tx]) * ay;
-        f = f + double(Hnext[c]) * az;
-        double R = f / (-vol);
+        f = f - fl * ax;
+        f = f - gl * ay;
+        f = f - hl * az;
+        f = f + double(sm.fx[c][fxl + 1]) * ax;
+        f = f + double(sm.fy[c][fyl + TX]) * ay;
+        f = f + double(sm.fz[zr][c][fzc]) * az;
+        const double R = f * inv_mvol;
         if (a.Ro[0]) a.Ro[c][off] = R;
         Unew[c] = Unew[c] + bdt * R;
       }
-      if (!a.Ro[0]) {
+      if (a.Ro[0]) continue;
       double V[5];
       e.c2p(Unew, V);
-      bool clipped = e.clip(V);
+      const bool clipped = e.clip(V);
       clipped_local |= clipped ? 1 : 0;
-      if (e.bad(V)) report(a.err, ERR_STATE, (int)(off), where + 3);
+      if (e.bad(V)) report(a.err, ERR_STATE, (int)((long long)m * g.ny * g.nx + (long long)gj * g.nx + gi), where + 3);
       if (a.final_stage) {
+#pragma unroll
         for (int c = 0; c < 5; c++) a.Vo[c][off] = V[c];
-        double ee = e.energy(V[0], V[4]);
-        double c2 = e.c2(V[0], ee);
+        const double ee = e.energy(V[0], V[4]);
+        const double c2 = e.c2(V[0], ee);
         if (c2 < 0.0) report(a.err, ERR_SOUND, (int)off, where + 4);
-        double cs = sqrt(c2);
-        double lx = fabs(V[1]) + cs, ly = fabs(V[2]) + cs, lz = fabs(V[3]) + cs;
-        double r = smin(dxi / lx, smin(dyj / ly, dzk / lz));
+        const double cs = sqrt(c2);
+        const double lx = fabs(V[1]) + cs, ly = fabs(V[2]) + cs, lz = fabs(V[3]) + cs;
+        const double r = smin(dxi / lx, smin(dyj / ly, dzk / lz));
         dtmin_local = smin(dtmin_local, r);
       } else {
+#pragma unroll
         for (int c = 0; c < 5; c++) a.Uo[c][off] = Unew[c];
       }
-      }  // !Ro
     }
-    for (int c = 0; c < 5; c++) Hprev[c] = Hnext[c];
   }
 
   if (a.clipped_out && __syncthreads_or(clipped_local)) {
@@ -482,7 +691,9 @@ __global__ void __launch_bounds__(TX * TY, 1) stage_kernel(const StageArgs a) {
   }
   if (a.final_stage && a.dtmin_bits) {
     double v = dtmin_local;
+#pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();
     if (tx == 0) sm.red[ty] = v;
     __syncthreads();
     if (tid == 0) {
