@@ -135,3 +135,34 @@ def tile_periodic(g, V, reps):
 
 def interior(A):
     return A[1:-1, 1:-1, 1:-1]
+
+
+def stiffened_gas_pair(rng):
+    """One seeded stiffened-gas material: gamma in [1.2, 7], p_inf = 0 with
+    probability 1/4, else log-uniform in [1e6, 1e9] Pa."""
+    gam = rng.uniform(1.2, 7.0)
+    pinf = 0.0 if rng.uniform() < 0.25 else 10.0 ** rng.uniform(6.0, 9.0)
+    return abi.material(gam, pinf)
+
+
+def riemann_problems(n, seed=3, nmat_pairs=None):
+    """Seeded two-material interface Riemann problems with the state
+    distribution of the batched-tube workload: densities log-uniform in
+    1..1000 kg/m^3, pressures log-uniform in 1e4..1e9 Pa, velocities uniform
+    in +-200 m/s, material 0 on the left and 1 on the right, unit normal x.
+    Returns (materials, VL, idl, VR, idr, dirs)."""
+    rng = np.random.default_rng(seed)
+    mats = [stiffened_gas_pair(rng), stiffened_gas_pair(rng)]
+    VL = np.zeros((n, 5))
+    VR = np.zeros((n, 5))
+    for V in (VL, VR):
+        V[:, 0] = 10.0 ** rng.uniform(0.0, 3.0, n)
+        V[:, 1] = rng.uniform(-200.0, 200.0, n)
+        V[:, 2] = rng.uniform(-20.0, 20.0, n)
+        V[:, 3] = rng.uniform(-20.0, 20.0, n)
+        V[:, 4] = 10.0 ** rng.uniform(4.0, 9.0, n)
+    dirs = np.zeros((n, 3))
+    dirs[:, 0] = 1.0
+    idl = np.zeros(n, np.int32)
+    idr = np.ones(n, np.int32)
+    return mats, VL, idl, VR, idr, dirs

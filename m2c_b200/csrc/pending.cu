@@ -2,11 +2,6 @@
 // they report M2CG_ERR_UNSUPPORTED instead of computing anything.
 #include "../../include/m2c_gpu.h"
 
-extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme*, const m2cg_material*, int, int, const double*,
-                                          const int*, const double*, const int*, const double*, const double*,
-                                          double*, int*, double*, double*, int*, int*) {
-  return M2CG_ERR_UNSUPPORTED;
-}
 extern "C" m2cg_status m2cg_batch_create(const m2cg_scheme*, int, const int*, const m2cg_material*, const double*,
                                          const double*, const m2cg_batch_tuning*, m2cg_batch** out) {
   if (out) *out = nullptr;

@@ -55,6 +55,9 @@ def lib():
     L.m2cg_time_steps.argtypes = [vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_longlong)]
     L.m2cg_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.m2cg_profile_stages.argtypes = [vp, C.c_int, C.POINTER(C.c_float), ip, C.POINTER(C.c_float)]
+    L.m2cg_riemann_batch.argtypes = [C.POINTER(abi.Scheme), C.POINTER(abi.Material), C.c_int, C.c_int, dp, ip, dp,
+                                     ip, dp, dp, dp, ip, dp, dp, ip, ip]
+    L.m2cg_riemann_batch.restype = C.c_int
     L.m2cg_set_device.argtypes = [C.c_int]
     L.m2cg_set_device.restype = C.c_int
     L.m2cg_default_scheme.argtypes = [C.POINTER(abi.Scheme)]
@@ -66,6 +69,23 @@ def lib():
         getattr(L, name).restype = C.c_int
     _lib = L
     return L
+
+
+def riemann_batch(s, mats, VL, idl, VR, idr, dirs, warm=None):
+    """Exact two-material Riemann problems on the GPU
+    (ExactRiemannSolverBase::ComputeRiemannSolution, one problem per thread).
+    Returns Vs, id, Vsm, Vsp, iterations, err."""
+    n = len(idl)
+    VL, VR, dirs = (np.ascontiguousarray(a, np.float64) for a in (VL, VR, dirs))
+    idl, idr = np.ascontiguousarray(idl, np.int32), np.ascontiguousarray(idr, np.int32)
+    warm = None if warm is None else np.ascontiguousarray(warm, np.float64)
+    Vs, Vsm, Vsp = np.zeros((n, 5)), np.zeros((n, 5)), np.zeros((n, 5))
+    mid, it, err = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    arr = (abi.Material * len(mats))(*mats)
+    check(lib().m2cg_riemann_batch(C.byref(s), arr, len(mats), n, abi.dptr(VL), abi.iptr(idl), abi.dptr(VR),
+                                   abi.iptr(idr), abi.dptr(dirs), abi.dptr(warm), abi.dptr(Vs), abi.iptr(mid),
+                                   abi.dptr(Vsm), abi.dptr(Vsp), abi.iptr(it), abi.iptr(err)))
+    return Vs, mid, Vsm, Vsp, it, err
 
 
 def set_device(device):
