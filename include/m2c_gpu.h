@@ -182,6 +182,7 @@ typedef struct {
   long long clipped_cells;       /* ClipDensityAndPressure counts */
   long long reinit_calls;
   long long kernel_launches;
+  long long unresolved_cells;    /* cells that changed material with no usable star state */
 } m2cg_counters;
 m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
 

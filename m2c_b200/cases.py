@@ -166,3 +166,81 @@ def riemann_problems(n, seed=3, nmat_pairs=None):
     idl = np.zeros(n, np.int32)
     idr = np.ones(n, np.int32)
     return mats, VL, idl, VR, idr, dirs
+
+
+WATER = dict(gamma=6.12, p_c=3.43e8)
+AIR = dict(gamma=1.4, p_c=0.0)
+
+
+def post_shock_sg(rho0, p0, p1, gamma, p_c):
+    """State behind a right-moving shock of pressure p1 entering still
+    stiffened gas (rho0, p0): the Rankine-Hugoniot root of
+    e(rho1,p1) - e(rho0,p0) + (p0+p1)/2 (1/rho1 - 1/rho0) = 0 in closed form,
+    and u1 = sqrt((p1-p0)(1/rho0 - 1/rho1))."""
+    a = (gamma + 1.0) * (p1 + p_c) + (gamma - 1.0) * (p0 + p_c)
+    b = (gamma - 1.0) * (p1 + p_c) + (gamma + 1.0) * (p0 + p_c)
+    rho1 = rho0 * a / b
+    u1 = np.sqrt((p1 - p0) * (1.0 / rho0 - 1.0 / rho1))
+    return rho1, u1
+
+
+def bubble_case(n, nbubbles=1, seed=5, rk=3, cfl=0.4, precision=abi.PREC_FP64, reinit_frequency=10,
+                radius=2.0e-3, radii=(0.5e-3, 1.5e-3), shape=None):
+    """Shock-induced collapse of air bubble(s) in water in a 2 cm cube:
+    water is stiffened gas (gamma 6.12, p_inf 3.43e8 Pa, rho 1000, p 1e5),
+    air is gamma 1.4 (rho 1.2, p 1e5); a planar shock from the post-shock
+    water state at p = 1e9 Pa occupies x < 5 mm; INLET (post-shock) at x0,
+    OUTLET (ambient water) at xmax, SYMMETRY on y and z; HLLC + van Albada,
+    exact interface Riemann problems, FD3 level set with reinitialisation
+    every `reinit_frequency` steps, RK3, CFL 0.4. nbubbles = 1: one bubble of
+    radius 2 mm at the centre; otherwise seeded non-overlapping bubbles with
+    radii uniform in `radii`, at least two cells apart, fully inside.
+    The level set is the signed distance to the nearest bubble surface
+    (material 1, air, where phi < 0)."""
+    L = 0.02
+    nx, ny, nz = shape if shape else (n, n, n)
+    rho1, u1 = post_shock_sg(1000.0, 1.0e5, 1.0e9, **WATER)
+    post = (rho1, u1, 0.0, 0.0, 1.0e9)
+    g = abi.grid(nx, ny, nz, x=(0.0, L), y=(0.0, L), z=(0.0, L),
+                 bc=(abi.BC_INLET, abi.BC_OUTLET) + (abi.BC_SYMMETRY,) * 4,
+                 inlet=post, outlet=(1000.0, 0.0, 0.0, 0.0, 1.0e5))
+    s = abi.scheme(flux=abi.FLUX_HLLC, limiter=abi.LIM_VANALBADA, rk_order=rk, cfl=cfl, precision=precision)
+    mats = [abi.material(**WATER), abi.material(**AIR)]
+    ls = abi.levelset(material_id=1, reinit_frequency=reinit_frequency)
+    xc, yc, zc = abi.cell_centres(g)
+    Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
+    h = L / nx
+    if nbubbles == 1:
+        centres = [(L / 2, L / 2, L / 2)]
+        rads = [radius]
+    else:
+        rng = np.random.default_rng(seed)
+        centres, rads = [], []
+        tries = 0
+        while len(centres) < nbubbles and tries < 100000:
+            tries += 1
+            r = rng.uniform(*radii)
+            c = rng.uniform(0.0075 + r + 2 * h, L - r - 2 * h, size=3)  # downstream of the shock front
+            c[1] = rng.uniform(r + 2 * h, L - r - 2 * h)
+            c[2] = rng.uniform(r + 2 * h, L - r - 2 * h)
+            if all(np.linalg.norm(c - np.array(c2)) >= r + r2 + 2 * h for c2, r2 in zip(centres, rads)):
+                centres.append(tuple(c))
+                rads.append(r)
+    phi = np.full(X.shape, np.inf)
+    for c, r in zip(centres, rads):
+        phi = np.minimum(phi, np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - r)
+    V = empty_state(g)
+    ID = np.zeros(abi.ghosted_shape(g))
+    PHI = np.zeros(abi.ghosted_shape(g))
+    inner = np.s_[1:-1, 1:-1, 1:-1]
+    shocked = X < 0.005
+    V[inner + (0,)] = np.where(shocked, rho1, 1000.0)
+    V[inner + (1,)] = np.where(shocked, u1, 0.0)
+    V[inner + (4,)] = np.where(shocked, 1.0e9, 1.0e5)
+    air = phi < 0
+    V[inner + (0,)] = np.where(air, 1.2, V[inner + (0,)])
+    V[inner + (1,)] = np.where(air, 0.0, V[inner + (1,)])
+    V[inner + (4,)] = np.where(air, 1.0e5, V[inner + (4,)])
+    ID[inner] = np.where(air, 1.0, 0.0)
+    PHI[inner] = phi
+    return g, s, mats, ls, V, ID, PHI

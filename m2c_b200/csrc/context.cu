@@ -123,7 +123,7 @@ struct m2cg_ctx {
   int* lK[3] = {};
   double* lC[3] = {};
   int ntx = 1, nty = 1, nitems = 1;
-  std::vector<double> hdx, hdy, hdz;
+  std::vector<double> hdx, hdy, hdz, hxc, hyc, hzc;
   // device scratch: clock [t, dt, tmax, cfl], dtmin bits, flags, error
   double* clock = nullptr;
   unsigned long long* dtmin = nullptr;
@@ -150,17 +150,17 @@ static double* dalloc(size_t n, m2cg_status* st) {
   return (double*)p;
 }
 
-// Cell widths per axis: uniform as MeshGenerator::ComputeMesh1DUniform
-// (MeshGenerator.cpp:146-158) unless given.
-static void axis_mesh(int n, double a, double b, const double* wc, const double* w, std::vector<double>& dx) {
+// Cell centres and widths per axis: uniform as MeshGenerator::ComputeMesh1DUniform
+// (MeshGenerator.cpp:146-158: x_i = x0 + h/2 + i h) unless given.
+static void axis_mesh(int n, double a, double b, const double* wc, const double* w, std::vector<double>& xc,
+                      std::vector<double>& dx) {
   dx.assign(n, 0.0);
-  if (w) {
-    for (int i = 0; i < n; i++) dx[i] = w[i];
-  } else {
-    double h = (b - a) / n;
-    for (int i = 0; i < n; i++) dx[i] = h;
+  xc.assign(n, 0.0);
+  double h = (b - a) / n;
+  for (int i = 0; i < n; i++) {
+    dx[i] = w ? w[i] : h;
+    xc[i] = wc ? wc[i] : a + 0.5 * h + i * h;
   }
-  (void)wc;
 }
 
 // Limiter coefficients per axis index (Reconstructor::Setup, Reconstructor.cpp:53-99,
@@ -269,9 +269,9 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
     }
   if (cudaMalloc((void**)&c->id, c->nalloc) != cudaSuccess) st = fail(M2CG_ERR_NOMEM, "cudaMalloc id failed");
   if (!st) cudaMemsetAsync(c->id, 0, c->nalloc, c->stream);
-  axis_mesh(grid->nx, grid->x0, grid->xmax, grid->xc, grid->dx, c->hdx);
-  axis_mesh(grid->ny, grid->y0, grid->ymax, grid->yc, grid->dy, c->hdy);
-  axis_mesh(grid->nz, grid->z0, grid->zmax, grid->zc, grid->dz, c->hdz);
+  axis_mesh(grid->nx, grid->x0, grid->xmax, grid->xc, grid->dx, c->hxc, c->hdx);
+  axis_mesh(grid->ny, grid->y0, grid->ymax, grid->yc, grid->dy, c->hyc, c->hdy);
+  axis_mesh(grid->nz, grid->z0, grid->zmax, grid->zc, grid->dz, c->hzc, c->hdz);
   upload_vec(&c->dx, c->hdx, c->stream, &st);
   upload_vec(&c->dy, c->hdy, c->stream, &st);
   upload_vec(&c->dz, c->hdz, c->stream, &st);
@@ -325,7 +325,11 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   int maxsm = 0;
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   if (!st && (size_t)maxsm < smem) st = fail(M2CG_ERR_CUDA, "stage kernel needs %zu B shared memory, device has %d", smem, maxsm);
-  if (!st && nls == 1) st = multiphase_create(c->stream, g, sk, *scheme, mats, nmat, *ls, &c->mp);
+  if (!st && nls == 1) {
+    const double* xc[3] = {c->hxc.data(), c->hyc.data(), c->hzc.data()};
+    const double* dxs[3] = {c->hdx.data(), c->hdy.data(), c->hdz.data()};
+    st = multiphase_create(c->stream, g, sk, *scheme, mats, nmat, *ls, xc, dxs, &c->mp);
+  }
   if (st) {
     m2cg_destroy(c);
     return st;

@@ -1,0 +1,47 @@
+// Level-set transport on the GPU: finite-difference UPWIND_CENTRAL_3 residual
+// (LevelSetOperator::ComputeResidualFDM_FullDomain, LevelSetOperator.cpp:1066-1140,
+// GradientCalculatorFD3.cpp:54-470), boundary rules
+// (LevelSetOperator::ApplyBoundaryConditions, 934-1034) and reinitialisation
+// (LevelSetReinitializer::ReinitializeFullDomain).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/m2c_gpu.h"
+#include "stage.cuh"
+
+namespace m2c {
+
+// Per-axis geometry of the level-set operator, on the device.
+struct LsGeom {
+  const double* xg[3];   // coordinates incl. one ghost per side: index c+1 for c in [-1, n]
+  const double* cl[3];   // left-biased FD3 coefficients [n][4] (third order where i > 0)
+  const double* cr[3];   // right-biased FD3 coefficients [n][4] (third order where i < n-1)
+  const double* cr1y;    // right-biased first-order y coefficients [ny][4] (see levelset.cu)
+  int bc[6];             // LevelSetSchemeData::BcType per side
+  double* base;          // single allocation holding the arrays above
+};
+
+// xc/dx: host cell centres and widths per axis (length n of that axis).
+m2cg_status levelset_geom_create(cudaStream_t s, const Grid3& g, const m2cg_levelset& ls, const double* const* xc,
+                                 const double* const* dx, LsGeom* out);
+void levelset_geom_destroy(LsGeom* geo);
+void levelset_unpack(cudaStream_t s, const Grid3& g, const double* aos, double* phi);
+void levelset_pack(cudaStream_t s, const Grid3& g, const LsGeom& geo, const double* phi, double* aos);
+// One level-set RK stage: out = a_prev*in + a_un*phi_n + (bdt_coef*dt)*R(in, V_stage)
+// (stage 1: out = phi_n + dt*R).
+m2cg_status levelset_stage(cudaStream_t s, const Grid3& g, const SchemeK& sk, const LsGeom& geo, const StageArgs& a,
+                           const double* in, const double* phin, double* out);
+m2cg_status reinit_alloc(long long ncell, double** buf);
+m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& geo, const m2cg_levelset& ls,
+                                  double* phi, double* buf, DevError* err);
+
+}  // namespace m2c
+
+using m2c::LsGeom;
+using m2c::levelset_geom_create;
+using m2c::levelset_geom_destroy;
+using m2c::levelset_unpack;
+using m2c::levelset_pack;
+using m2c::levelset_stage;
+using m2c::reinit_alloc;
+using m2c::levelset_reinitialize;

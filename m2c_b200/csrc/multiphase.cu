@@ -1,25 +1,654 @@
-// Two-material machinery (placeholder until the level-set path lands).
+// Two-material machinery of the time step on the GPU: one level set,
+// material IDs, the exact Riemann problems at material interfaces and the
+// post-step state update of cells that changed material.
+//
+// Per step (TimeIntegratorRK2/RK3::AdvanceOneTimeStep + UpdateSolutionAfterTimeStepping,
+// TimeIntegrator.cpp:291-797):
+//   begin: Phi_tmp = Phi, IDn = ID; interface faces (ID differs across a
+//          face) are collected once, since IDs are fixed during the stages.
+//   stage s: exact Riemann problem on every interface face with the stage's
+//          cell states (SpaceOperator.cpp:2486-2542, MultiPhase recon CONSTANT);
+//          stage 1 keeps its star states as the "riemann_solutions" of the
+//          reference (RiemannSolutions.h); level-set RK stage with the stage's
+//          velocity (LevelSetOperator::ComputeResidualFDM_FullDomain, 1066-1140);
+//          the fused N-S stage kernel consumes the star states.
+//   end:   material ID from the sign change of phi
+//          (MultiPhaseOperator::UpdateMaterialIDByLevelSet, 127-332), optional
+//          reinitialisation, and the state update of cells whose ID changed
+//          from the stored star states with upwind weights
+//          (UpdateStateVariablesByRiemannSolutions / LocalUpdateByRiemannSolutions,
+//          857-1027), processed in the reference's (k, j, i) order because
+//          each update reads neighbours already updated in the same pass.
+//
+// Compiled with -fmad=false (FP64 path).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "levelset.h"
 #include "multiphase.h"
+#include "riemann_batch.h"
 
 namespace m2c {
+
+// Threads running Riemann problems at once (each owns an integration-path
+// scratch region of 2 x RIEMANN_PATH_CAP x 3 doubles).
+constexpr int IFACE_RIEMANN_THREADS = 148 * 4 * 128;
+
 struct Multiphase {
-  int dummy;
+  Grid3 g;
+  SchemeK sk;
+  m2cg_scheme scheme;
+  m2cg_levelset ls;
+  RiemannParams rp;
+  Eos<double>* d_eos = nullptr;  // material table on the device
+  long long ncell = 0;           // allocated cells (plane * nz)
+  // level set buffers (interior, SoA single component, same indexing as V)
+  double* phiN = nullptr;  // phi^n / phi^{n+1}
+  double* phiA = nullptr;  // stage 1 output
+  double* phiB = nullptr;  // stage 2 output (RK3)
+  double* phiT = nullptr;  // phi at the start of the step (Phi_tmp)
+  LsGeom lsg;
+  uint8_t* idn = nullptr;  // ID at the start of the step
+  // interface faces
+  int* slot = nullptr;     // per cell: slot of its low faces (valid where flagged)
+  int* faces = nullptr;    // [cap_faces][3]: cell offset, slot, direction
+  int* counts = nullptr;   // [0] slots, [1] faces, [2] overflow, [3] riemann errors, [4] iterations (low), [5] calls
+  long long cap_slots = 0, cap_faces = 0;
+  double* Vsm = nullptr;   // [slot][3][5] current stage
+  double* Vsp = nullptr;
+  double* Vmid = nullptr;
+  int* midid = nullptr;    // [slot][3]
+  double* rsVsm = nullptr; // stage-1 copies (the reference's riemann_solutions)
+  double* rsVsp = nullptr;
+  uint8_t* rsValid = nullptr;  // [slot][3]
+  double* scratch = nullptr;   // Riemann integration paths
+  // changed cells (ordered)
+  int* changed = nullptr;      // [ncell] ordered list of linear offsets
+  int* blockcnt = nullptr;     // per-block counts for the ordered compaction
+  int* nchanged = nullptr;     // [0] changed, [1] unresolved
+  int nblocks_scan = 0;
+  int time_step = 0;
+  int stage = 0;
+  // host-side counters
+  long long riemann_calls = 0, riemann_iterations = 0, riemann_errors = 0, unresolved = 0, reinit_calls = 0;
+  double* reinit_buf = nullptr;  // reinitialisation work arrays
 };
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cell_coords(const Grid3& g, long long q, int& i, int& j, int& k) {
+  i = (int)(q % g.nx);
+  j = (int)((q / g.nx) % g.ny);
+  k = (int)(q / ((long long)g.nx * g.ny));
+}
+
+__device__ __forceinline__ long long offset_of(const Grid3& g, int i, int j, int k) {
+  return (long long)k * g.plane + (long long)j * g.px + i;
+}
+
+// Neighbour across the low face in direction d; false if it is a (non-periodic) ghost.
+__device__ __forceinline__ bool low_neighbour(const Grid3& g, int i, int j, int k, int d, int& ni, int& nj, int& nk) {
+  ni = i; nj = j; nk = k;
+  int* c = d == 0 ? &ni : (d == 1 ? &nj : &nk);
+  const int n = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+  *c -= 1;
+  if (*c < 0) {
+    if (g.bc[2 * d] != BC_PERIODIC) return false;
+    *c += n;
+  }
+  return true;
+}
+
+// Collect interface faces: every low face whose two cells carry different IDs.
+__global__ void k_detect_iface(Grid3 g, const uint8_t* id, int* slot, int* faces, int* counts, long long cap_slots,
+                               long long cap_faces) {
+  long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(g, q, i, j, k);
+    const long long off = offset_of(g, i, j, k);
+    const uint8_t me = id[off];
+    int mask = 0;
+    for (int d = 0; d < 3; d++) {
+      int ni, nj, nk;
+      if (!low_neighbour(g, i, j, k, d, ni, nj, nk)) continue;
+      if (id[offset_of(g, ni, nj, nk)] != me) mask |= 1 << d;
+    }
+    if (!mask) continue;
+    int s = atomicAdd(&counts[0], 1);
+    if (s >= cap_slots) {
+      atomicOr(&counts[2], 1);
+      continue;
+    }
+    slot[off] = s;
+    for (int d = 0; d < 3; d++) {
+      if (!(mask & (1 << d))) continue;
+      int f = atomicAdd(&counts[1], 1);
+      if (f >= cap_faces) {
+        atomicOr(&counts[2], 1);
+        continue;
+      }
+      faces[3 * f] = (int)q;  // linear interior index of the right cell
+      faces[3 * f + 1] = s;
+      faces[3 * f + 2] = d;
+    }
+  }
+}
+
+// Primitive state of a cell at this stage: V^n (stage 1) or clip(C2P(U_s)).
+__device__ __forceinline__ void stage_state(const StageArgs& a, const Eos<double>* eos, long long off, uint8_t id,
+                                            double* V) {
+  if (a.stage == 1) {
+    for (int c = 0; c < 5; c++) V[c] = a.Vn[c][off];
+  } else {
+    double U[5];
+    for (int c = 0; c < 5; c++) U[c] = a.Us[c][off];
+    eos[id].c2p(U, V);
+    eos[id].clip(V);
+  }
+}
+
+struct IfaceRiemannArgs {
+  StageArgs st;           // the stage's state pointers (Vn, Us, stage)
+  const Eos<double>* eos;
+  RiemannParams P;
+  const int* faces;
+  int* counts;
+  long long cap_faces;
+  double* Vsm;
+  double* Vsp;
+  double* Vmid;
+  int* midid;
+  double* rsVsm;          // stage 1: also written here
+  double* rsVsp;
+  uint8_t* rsValid;
+  double* scratch;
+  DevError* err;
+};
+
+// One exact Riemann problem per interface face (SpaceOperator.cpp:2499-2523):
+// MESH normal, cell-centred states (constant reconstruction at the interface),
+// star states clipped with each side's EOS, stage-1 results kept.
+__global__ void k_iface_riemann(IfaceRiemannArgs a) {
+  const Grid3& g = a.st.g;
+  long long nf = a.counts[1];
+  if (nf > a.cap_faces) nf = a.cap_faces;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  RiemannSolver rs;
+  rs.P = a.P;
+  rs.eos = a.eos;
+  rs.path1.pt = a.scratch + tid * 2 * 3 * RIEMANN_PATH_CAP;
+  rs.path1.cap = RIEMANN_PATH_CAP;
+  rs.path3.pt = rs.path1.pt + 3 * RIEMANN_PATH_CAP;
+  rs.path3.cap = RIEMANN_PATH_CAP;
+  for (long long f = tid; f < nf; f += nthreads) {
+    const int q = a.faces[3 * f], s = a.faces[3 * f + 1], d = a.faces[3 * f + 2];
+    int i, j, k;
+    cell_coords(g, q, i, j, k);
+    int ni, nj, nk;
+    low_neighbour(g, i, j, k, d, ni, nj, nk);
+    const long long offR = offset_of(g, i, j, k), offL = offset_of(g, ni, nj, nk);
+    const uint8_t idR = a.st.id[offR], idL = a.st.id[offL];
+    double VL[5], VR[5];
+    stage_state(a.st, a.eos, offL, idL, VL);
+    stage_state(a.st, a.eos, offR, idR, VR);
+    double dir[3] = {d == 0 ? 1.0 : 0.0, d == 1 ? 1.0 : 0.0, d == 2 ? 1.0 : 0.0};
+    double Vs[5], Vsm[5], Vsp[5];
+    int mid = 0;
+    bool bad = false;
+    int r = rs.solve(dir, VL, idL, VR, idR, Vs, mid, Vsm, Vsp, NAN, bad);
+    a.eos[idL].clip(Vsm);
+    a.eos[idR].clip(Vsp);
+    const long long b = ((long long)s * 3 + d) * 5;
+    for (int c = 0; c < 5; c++) {
+      a.Vsm[b + c] = Vsm[c];
+      a.Vsp[b + c] = Vsp[c];
+      a.Vmid[b + c] = Vs[c];
+    }
+    a.midid[s * 3 + d] = mid;
+    if (a.rsVsm) {
+      for (int c = 0; c < 5; c++) {
+        a.rsVsm[b + c] = Vsm[c];
+        a.rsVsp[b + c] = Vsp[c];
+      }
+      a.rsValid[s * 3 + d] = (r == RIEM_OK) ? 1 : 0;
+    }
+    if (r != RIEM_OK) atomicAdd(&a.counts[3], 1);
+    if (r & RIEM_PATH_OVERFLOW) report(a.err, ERR_ITER_CAP, q, 7);
+    if (bad) report(a.err, ERR_STATE, q, 8);
+    atomicAdd(&a.counts[4], rs.iterations);
+    atomicAdd(&a.counts[5], 1);
+  }
+}
+
+// Material ID from the sign change of phi (MultiPhaseOperator.cpp:150-202):
+// with one level set and two materials a swept cell becomes the level set's
+// material where phi < 0 and material 0 otherwise.
+__global__ void k_update_id(Grid3 g, const double* phi, const double* phi0, uint8_t* id, int ls_mat) {
+  long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(g, q, i, j, k);
+    const long long off = offset_of(g, i, j, k);
+    const double p = phi[off], p0 = phi0[off];
+    if (p * p0 > 0.0) continue;
+    id[off] = p < 0 ? (uint8_t)ls_mat : (uint8_t)0;
+  }
+}
+
+// Ordered compaction of cells whose ID changed: per-block counts, then
+// exclusive offsets, then in-block ordered writes (linear index order is the
+// reference's k, j, i loop order).
+__global__ void k_count_changed(Grid3 g, const uint8_t* id, const uint8_t* idn, int* blockcnt, long long per_block) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  long long n = (long long)g.nx * g.ny * g.nz;
+  long long b0 = blockIdx.x * per_block, b1 = min(n, b0 + per_block);
+  int local = 0;
+  for (long long q = b0 + threadIdx.x; q < b1; q += blockDim.x) {
+    int i, j, k;
+    cell_coords(g, q, i, j, k);
+    long long off = offset_of(g, i, j, k);
+    local += id[off] != idn[off];
+  }
+  atomicAdd(&cnt, local);
+  __syncthreads();
+  if (threadIdx.x == 0) blockcnt[blockIdx.x] = cnt;
+}
+
+__global__ void k_scan_blocks(int* blockcnt, int nb, int* total) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int s = 0;
+    for (int b = 0; b < nb; b++) {
+      int c = blockcnt[b];
+      blockcnt[b] = s;
+      s += c;
+    }
+    *total = s;
+  }
+}
+
+__global__ void k_write_changed(Grid3 g, const uint8_t* id, const uint8_t* idn, const int* blockoff, long long per_block,
+                                int* list) {
+  __shared__ int warp_sums[32];
+  long long n = (long long)g.nx * g.ny * g.nz;
+  long long b0 = blockIdx.x * per_block, b1 = min(n, b0 + per_block);
+  int base = blockoff[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (long long c0 = b0; c0 < b1; c0 += blockDim.x) {
+    long long q = c0 + threadIdx.x;
+    int flag = 0;
+    if (q < b1) {
+      int i, j, k;
+      cell_coords(g, q, i, j, k);
+      long long off = offset_of(g, i, j, k);
+      flag = id[off] != idn[off];
+    }
+    unsigned bal = __ballot_sync(0xffffffffu, flag);
+    int wpre = __popc(bal & ((1u << lane) - 1));
+    if (lane == 0) warp_sums[warp] = __popc(bal);
+    __syncthreads();
+    int before = 0, tot = 0;
+    for (int w = 0; w < nwarps; w++) {
+      if (w < warp) before += warp_sums[w];
+      tot += warp_sums[w];
+    }
+    if (flag) list[base + before + wpre] = (int)q;
+    base += tot;
+    __syncthreads();
+  }
+}
+
+struct StateUpdateArgs {
+  Grid3 g;
+  const Eos<double>* eos;
+  double* V[5];
+  const uint8_t* id;
+  const uint8_t* idn;
+  const int* slot;
+  const double* rsVsm;
+  const double* rsVsp;
+  const uint8_t* rsValid;
+  const int* changed;
+  int* nchanged;        // [0] count, [1] unresolved (out)
+  int* unresolved;      // list (reuses the tail of `changed`)
+  DevError* err;
+};
+
+// Star state stored on one face of cell (i,j,k): side 0 = its low face
+// ("left/bottom/back": Vsm of the slot of this cell), side 1 = its high
+// face ("right/top/front": Vsp of the slot of the neighbour above).
+__device__ bool stored_state(const StateUpdateArgs& a, int i, int j, int k, int d, int side, double* S, int& sid) {
+  const Grid3& g = a.g;
+  int ci = i, cj = j, ck = k;
+  if (side == 1) {
+    int* c = d == 0 ? &ci : (d == 1 ? &cj : &ck);
+    const int n = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+    *c += 1;
+    if (*c >= n) {
+      if (g.bc[2 * d + 1] != BC_PERIODIC) return false;
+      *c -= n;
+    }
+  }
+  int ni, nj, nk;
+  if (!low_neighbour(g, ci, cj, ck, d, ni, nj, nk)) return false;
+  const long long offc = offset_of(g, ci, cj, ck), offn = offset_of(g, ni, nj, nk);
+  if (a.idn[offc] == a.idn[offn]) return false;  // not an interface face this step
+  const int s = a.slot[offc];
+  if (!a.rsValid[s * 3 + d]) return false;       // Riemann solve reported an error: not stored
+  const double* src = side == 0 ? a.rsVsm : a.rsVsp;
+  for (int c = 0; c < 5; c++) S[c] = src[((long long)s * 3 + d) * 5 + c];
+  sid = side == 0 ? a.idn[offn] : a.idn[offc];
+  return true;
+}
+
+// LocalUpdateByRiemannSolutions (MultiPhaseOperator.cpp:916-1027)
+__device__ int local_update(const StateUpdateArgs& a, int i, int j, int k, int myid, double* v, bool upwind) {
+  const Grid3& g = a.g;
+  int counter = 0;
+  double weight = 0, sum_weight = 0;
+  // faces in the reference's order: left, right, bottom, top, back, front
+  for (int q = 0; q < 6; q++) {
+    const int d = q >> 1, side = q & 1;
+    double S[5];
+    int sid;
+    if (!stored_state(a, i, j, k, d, side, S, sid)) continue;
+    if (sid != myid) continue;
+    // neighbour state on that side (ghost rule applied for boundaries)
+    int ni = i, nj = j, nk = k;
+    int* c = d == 0 ? &ni : (d == 1 ? &nj : &nk);
+    const int n = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+    *c += side ? 1 : -1;
+    double nv[5];
+    if (*c < 0 || *c >= n) {
+      if (g.bc[2 * d + side] == BC_PERIODIC) {
+        *c = (*c + n) % n;
+      } else {
+        continue;  // a boundary face is never an interface face
+      }
+    }
+    const long long off = offset_of(g, ni, nj, nk);
+    for (int p = 0; p < 5; p++) nv[p] = a.V[p][off];
+    const double vn = nv[d + 1];
+    if (upwind && !(side == 0 ? vn > 0 : vn < 0)) continue;
+    const double nrm = sqrt(nv[1] * nv[1] + nv[2] * nv[2] + nv[3] * nv[3]);
+    weight = upwind ? (side == 0 ? vn / nrm : -vn / nrm) : 1.0;
+    sum_weight += weight;
+    if (counter == 0) {
+      for (int p = 0; p < 5; p++) v[p] = weight * S[p];
+    } else {
+      for (int p = 0; p < 5; p++) v[p] += weight * S[p];
+    }
+    counter++;
+  }
+  if (sum_weight > 0.0) {
+    const double inv = 1.0 / sum_weight;  // Vec5D::operator/= (Vector5D.h:172-181)
+    for (int p = 0; p < 5; p++) v[p] *= inv;
+  }
+  return counter;
+}
+
+// Sequential pass over the changed cells in (k, j, i) order.
+__global__ void k_state_update(StateUpdateArgs a) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const Grid3& g = a.g;
+  const int n = a.nchanged[0];
+  int nun = 0;
+  for (int t = 0; t < n; t++) {
+    const int q = a.changed[t];
+    int i, j, k;
+    cell_coords(g, q, i, j, k);
+    const long long off = offset_of(g, i, j, k);
+    const int myid = a.id[off];
+    double v[5];
+    for (int p = 0; p < 5; p++) v[p] = a.V[p][off];
+    int counter = local_update(a, i, j, k, myid, v, true);
+    if (counter == 0) counter = local_update(a, i, j, k, myid, v, false);
+    if (counter == 0) {
+      nun++;
+      continue;  // unresolved: left as is and counted
+    }
+    // ClipDensityAndPressure(V, ID) at the end of UpdateSolutionAfterTimeStepping
+    a.eos[myid].clip(v);
+    if (a.eos[myid].bad(v)) report(a.err, ERR_STATE, q, 9);
+    for (int p = 0; p < 5; p++) a.V[p][off] = v[p];
+  }
+  a.nchanged[1] = nun;
+}
+
+static int grid1d(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
 }  // namespace m2c
 
-m2cg_status multiphase_create(cudaStream_t, const m2c::Grid3&, const m2c::SchemeK&, const m2cg_scheme&,
-                              const m2cg_material*, int, const m2cg_levelset&, Multiphase** out) {
+using namespace m2c;
+
+// ---------------------------------------------------------------------------
+// host interface
+// ---------------------------------------------------------------------------
+m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk, const m2cg_scheme& scheme,
+                              const m2cg_material* mats, int nmat, const m2cg_levelset& ls, const double* const* xc,
+                              const double* const* dx, Multiphase** out) {
+  (void)mats;
+  (void)nmat;
   *out = nullptr;
-  return M2CG_ERR_UNSUPPORTED;
+  if (scheme.mp_recon != 0) return M2CG_ERR_UNSUPPORTED;            // interface Riemann inputs: constant recon
+  if (scheme.mp_phasechange_type != 0) return M2CG_ERR_UNSUPPORTED; // RIEMANN_SOLUTION update
+  if (ls.material_id != 1) return M2CG_ERR_UNSUPPORTED;
+  if (ls.reinit_first_layer != 0) return M2CG_ERR_UNSUPPORTED;
+  Multiphase* mp = new Multiphase;
+  mp->g = g;
+  mp->sk = sk;
+  mp->scheme = scheme;
+  mp->ls = ls;
+  mp->rp = riemann_params(scheme);
+  mp->ncell = g.plane * g.nz;
+  const long long n = mp->ncell;
+  const long long ninterior = (long long)g.nx * g.ny * g.nz;
+  mp->cap_slots = ninterior < 65536 ? ninterior : (ninterior / 8 > 65536 ? ninterior / 8 : 65536);
+  mp->cap_faces = 3 * mp->cap_slots;
+  bool ok = true;
+  auto A = [&](void** p, size_t bytes) {
+    if (cudaMalloc(p, bytes) != cudaSuccess) ok = false;
+  };
+  A((void**)&mp->d_eos, sizeof(Eos<double>) * MAXMAT);
+  A((void**)&mp->phiN, n * 8);
+  A((void**)&mp->phiA, n * 8);
+  A((void**)&mp->phiB, n * 8);
+  A((void**)&mp->phiT, n * 8);
+  A((void**)&mp->idn, n);
+  A((void**)&mp->slot, n * 4);
+  A((void**)&mp->faces, mp->cap_faces * 3 * 4);
+  A((void**)&mp->counts, 16 * 4);
+  A((void**)&mp->Vsm, mp->cap_slots * 15 * 8);
+  A((void**)&mp->Vsp, mp->cap_slots * 15 * 8);
+  A((void**)&mp->Vmid, mp->cap_slots * 15 * 8);
+  A((void**)&mp->midid, mp->cap_slots * 3 * 4);
+  A((void**)&mp->rsVsm, mp->cap_slots * 15 * 8);
+  A((void**)&mp->rsVsp, mp->cap_slots * 15 * 8);
+  A((void**)&mp->rsValid, mp->cap_slots * 3);
+  A((void**)&mp->scratch, (size_t)IFACE_RIEMANN_THREADS * 2 * 3 * RIEMANN_PATH_CAP * 8);
+  A((void**)&mp->changed, ninterior * 4);
+  mp->nblocks_scan = 148 * 8;
+  A((void**)&mp->blockcnt, mp->nblocks_scan * 4);
+  A((void**)&mp->nchanged, 4 * 4);
+  if (!ok) {
+    multiphase_destroy(mp);
+    return M2CG_ERR_NOMEM;
+  }
+  cudaMemcpyAsync(mp->d_eos, sk.ed, sizeof(Eos<double>) * MAXMAT, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(mp->counts, 0, 16 * 4, s);
+  cudaMemsetAsync(mp->rsValid, 0, mp->cap_slots * 3, s);
+  if (levelset_geom_create(s, g, ls, xc, dx, &mp->lsg) != M2CG_OK) {
+    multiphase_destroy(mp);
+    return M2CG_ERR_NOMEM;
+  }
+  if (ls.reinit_frequency > 0 && reinit_alloc(mp->ncell, &mp->reinit_buf) != M2CG_OK) {
+    multiphase_destroy(mp);
+    return M2CG_ERR_NOMEM;
+  }
+  *out = mp;
+  return M2CG_OK;
 }
-void multiphase_destroy(Multiphase* mp) { delete mp; }
-m2cg_status multiphase_upload_phi(Multiphase*, cudaStream_t, const double*, double*, uint8_t*) { return M2CG_ERR_UNSUPPORTED; }
-m2cg_status multiphase_download_phi(Multiphase*, cudaStream_t, double*) { return M2CG_ERR_UNSUPPORTED; }
-void multiphase_set_step(Multiphase*, int) {}
-m2cg_status multiphase_begin_step(Multiphase*, cudaStream_t, double* const*, const uint8_t*) { return M2CG_ERR_UNSUPPORTED; }
-m2cg_status multiphase_stage(Multiphase*, cudaStream_t, m2c::StageArgs&) { return M2CG_ERR_UNSUPPORTED; }
-m2cg_status multiphase_end_step(Multiphase*, cudaStream_t, double* const*, double* const*, uint8_t*, const double*,
-                                m2c::DevError*, m2cg_counters*) {
-  return M2CG_ERR_UNSUPPORTED;
+
+void multiphase_destroy(Multiphase* mp) {
+  if (!mp) return;
+  cudaFree(mp->d_eos);
+  cudaFree(mp->phiN); cudaFree(mp->phiA); cudaFree(mp->phiB); cudaFree(mp->phiT);
+  cudaFree(mp->idn); cudaFree(mp->slot); cudaFree(mp->faces); cudaFree(mp->counts);
+  cudaFree(mp->Vsm); cudaFree(mp->Vsp); cudaFree(mp->Vmid); cudaFree(mp->midid);
+  cudaFree(mp->rsVsm); cudaFree(mp->rsVsp); cudaFree(mp->rsValid); cudaFree(mp->scratch);
+  cudaFree(mp->changed); cudaFree(mp->blockcnt); cudaFree(mp->nchanged);
+  cudaFree(mp->reinit_buf);
+  levelset_geom_destroy(&mp->lsg);
+  delete mp;
 }
-void multiphase_counters(const Multiphase*, m2cg_counters*) {}
+
+m2cg_status multiphase_upload_phi(Multiphase* mp, cudaStream_t s, const double* phi_host, double* staging,
+                                  uint8_t* id) {
+  (void)id;
+  if (!phi_host) return M2CG_ERR_ARG;
+  const Grid3& g = mp->g;
+  size_t ng = (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+  if (cudaMemcpyAsync(staging, phi_host, ng * 8, cudaMemcpyHostToDevice, s) != cudaSuccess) return M2CG_ERR_CUDA;
+  levelset_unpack(s, g, staging, mp->phiN);
+  return cudaGetLastError() == cudaSuccess ? M2CG_OK : M2CG_ERR_CUDA;
+}
+
+m2cg_status multiphase_download_phi(Multiphase* mp, cudaStream_t s, double* phi_host) {
+  const Grid3& g = mp->g;
+  size_t ng = (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+  double* tmp = nullptr;
+  if (cudaMallocAsync((void**)&tmp, ng * 8, s) != cudaSuccess) return M2CG_ERR_NOMEM;
+  levelset_pack(s, g, mp->lsg, mp->phiN, tmp);
+  cudaMemcpyAsync(phi_host, tmp, ng * 8, cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(tmp, s);
+  return cudaGetLastError() == cudaSuccess ? M2CG_OK : M2CG_ERR_CUDA;
+}
+
+void multiphase_set_step(Multiphase* mp, int time_step) {
+  if (time_step > 0)
+    mp->time_step = time_step;
+  else
+    mp->time_step++;
+}
+
+m2cg_status multiphase_begin_step(Multiphase* mp, cudaStream_t s, double* const* Vn, const uint8_t* id) {
+  (void)Vn;
+  const Grid3& g = mp->g;
+  const long long n = mp->ncell;
+  cudaMemcpyAsync(mp->phiT, mp->phiN, n * 8, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(mp->idn, id, n, cudaMemcpyDeviceToDevice, s);
+  cudaMemsetAsync(mp->counts, 0, 16 * 4, s);
+  k_detect_iface<<<grid1d((long long)g.nx * g.ny * g.nz), 256, 0, s>>>(g, id, mp->slot, mp->faces, mp->counts,
+                                                                        mp->cap_slots, mp->cap_faces);
+  mp->stage = 0;
+  return cudaGetLastError() == cudaSuccess ? M2CG_OK : M2CG_ERR_CUDA;
+}
+
+m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
+  mp->stage = a.stage;
+  // exact Riemann problems at the interface faces
+  IfaceRiemannArgs ra;
+  memset(&ra, 0, sizeof ra);
+  ra.st = a;
+  ra.eos = mp->d_eos;
+  ra.P = mp->rp;
+  ra.faces = mp->faces;
+  ra.counts = mp->counts;
+  ra.cap_faces = mp->cap_faces;
+  ra.Vsm = mp->Vsm;
+  ra.Vsp = mp->Vsp;
+  ra.Vmid = mp->Vmid;
+  ra.midid = mp->midid;
+  if (a.stage == 1 && !a.Ro[0]) {
+    ra.rsVsm = mp->rsVsm;
+    ra.rsVsp = mp->rsVsp;
+    ra.rsValid = mp->rsValid;
+  }
+  ra.scratch = mp->scratch;
+  ra.err = a.err;
+  k_iface_riemann<<<IFACE_RIEMANN_THREADS / 128, 128, 0, s>>>(ra);
+  if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
+  a.iface.slot = mp->slot;
+  a.iface.Vsm = mp->Vsm;
+  a.iface.Vsp = mp->Vsp;
+  a.iface.Vmid = mp->Vmid;
+  a.iface.midid = mp->midid;
+  a.iface.mp_flux = mp->scheme.mp_flux;
+  a.iface.mp_recon = mp->scheme.mp_recon;
+  if (a.Ro[0]) return M2CG_OK;  // residual only: no level-set stage
+  // level-set RK stage with this stage's velocity (loose coupling,
+  // TimeIntegrator.cpp:553-558, 608-614, 658-664)
+  const int r = mp->scheme.rk_order;
+  const double* in = a.stage == 1 ? mp->phiN : (a.stage == 2 ? mp->phiA : mp->phiB);
+  double* outp = (a.stage == r) ? mp->phiN : (a.stage == 1 ? mp->phiA : mp->phiB);
+  return levelset_stage(s, mp->g, mp->sk, mp->lsg, a, in, mp->phiN, outp);
+}
+
+m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* Vold, double* const* Vnew, uint8_t* id,
+                                const double* clock, DevError* err, m2cg_counters* counters) {
+  (void)Vold;
+  (void)clock;
+  const Grid3& g = mp->g;
+  const long long ninterior = (long long)g.nx * g.ny * g.nz;
+  // material ID from the sign change of phi
+  k_update_id<<<grid1d(ninterior), 256, 0, s>>>(g, mp->phiN, mp->phiT, id, mp->ls.material_id);
+  // reinitialisation every `frequency` steps (LevelSetOperator::Reinitialize, 1599-1624)
+  if (mp->ls.reinit_frequency > 0 && mp->time_step % mp->ls.reinit_frequency == 0) {
+    m2cg_status st = levelset_reinitialize(s, g, mp->lsg, mp->ls, mp->phiN, mp->reinit_buf, err);
+    if (st) return st;
+    mp->reinit_calls++;
+  }
+  // ordered list of cells whose ID changed, then the sequential update
+  long long per_block = (ninterior + mp->nblocks_scan - 1) / mp->nblocks_scan;
+  k_count_changed<<<mp->nblocks_scan, 256, 0, s>>>(g, id, mp->idn, mp->blockcnt, per_block);
+  k_scan_blocks<<<1, 1, 0, s>>>(mp->blockcnt, mp->nblocks_scan, mp->nchanged);
+  k_write_changed<<<mp->nblocks_scan, 256, 0, s>>>(g, id, mp->idn, mp->blockcnt, per_block, mp->changed);
+  StateUpdateArgs ua;
+  memset(&ua, 0, sizeof ua);
+  ua.g = g;
+  ua.eos = mp->d_eos;
+  for (int p = 0; p < 5; p++) ua.V[p] = Vnew[p];
+  ua.id = id;
+  ua.idn = mp->idn;
+  ua.slot = mp->slot;
+  ua.rsVsm = mp->rsVsm;
+  ua.rsVsp = mp->rsVsp;
+  ua.rsValid = mp->rsValid;
+  ua.changed = mp->changed;
+  ua.nchanged = mp->nchanged;
+  ua.err = err;
+  k_state_update<<<1, 32, 0, s>>>(ua);
+  if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
+  // step counters (one small read-back per step)
+  int hc[6], hn[2];
+  cudaMemcpyAsync(hc, mp->counts, sizeof hc, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hn, mp->nchanged, sizeof hn, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
+  mp->riemann_calls += hc[5];
+  mp->riemann_iterations += hc[4];
+  mp->riemann_errors += hc[3];
+  mp->unresolved += hn[1];
+  if (hc[2]) return M2CG_ERR_ITER_CAP;  // interface capacity exceeded
+  if (counters) counters->kernel_launches += 8 + 3 * mp->scheme.rk_order;
+  return M2CG_OK;
+}
+
+void multiphase_counters(const Multiphase* mp, m2cg_counters* out) {
+  out->riemann_calls = mp->riemann_calls;
+  out->riemann_iterations = mp->riemann_iterations;
+  out->riemann_errors = mp->riemann_errors;
+  out->reinit_calls = mp->reinit_calls;
+  out->unresolved_cells = mp->unresolved;
+}

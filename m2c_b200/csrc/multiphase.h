@@ -11,8 +11,10 @@ struct Multiphase;
 }
 using m2c::Multiphase;
 
+// xc/dx: host cell centres and widths per axis.
 m2cg_status multiphase_create(cudaStream_t s, const m2c::Grid3& g, const m2c::SchemeK& sk, const m2cg_scheme& scheme,
-                              const m2cg_material* mats, int nmat, const m2cg_levelset& ls, Multiphase** out);
+                              const m2cg_material* mats, int nmat, const m2cg_levelset& ls, const double* const* xc,
+                              const double* const* dx, Multiphase** out);
 void multiphase_destroy(Multiphase* mp);
 m2cg_status multiphase_upload_phi(Multiphase* mp, cudaStream_t s, const double* phi_host, double* staging,
                                   uint8_t* id);

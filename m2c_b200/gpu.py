@@ -29,7 +29,7 @@ class M2CError(RuntimeError):
 class Counters(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in (
         "steps", "cells_updated", "riemann_calls", "riemann_iterations", "riemann_errors",
-        "clipped_cells", "reinit_calls", "kernel_launches")]
+        "clipped_cells", "reinit_calls", "kernel_launches", "unresolved_cells")]
 
 
 def lib():
