@@ -337,8 +337,9 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   // Work items = (x,y) tiles x z-chunks, run by a persistent grid of
   // resident CTAs. Pick the chunk length that minimises rounds x (chunk +
   // pipeline prologue of ~2.5 planes).
+  const int ty = (scheme->precision != M2CG_PREC_MIXED && nls == 1) ? StageTY<double, true>::value : STAGE_TY;
   c->ntx = (c->nx + TX - 1) / TX;
-  c->nty = (c->ny + STAGE_TY - 1) / STAGE_TY;
+  c->nty = (c->ny + ty - 1) / ty;
   {
     int resident = scheme->precision == M2CG_PREC_MIXED ? stage_resident_mixed(scheme->flux, nls == 1)
                                                         : stage_resident_fp64(scheme->flux, nls == 1);

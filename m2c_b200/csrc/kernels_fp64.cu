@@ -6,7 +6,8 @@
 namespace m2c {
 
 size_t stage_smem_fp64(bool multi) {
-  return multi ? sizeof(StageSmemAll<double, STAGE_TY, true>) : sizeof(StageSmemAll<double, STAGE_TY, false>);
+  return multi ? sizeof(StageSmemAll<double, StageTY<double, true>::value, true>)
+               : sizeof(StageSmemAll<double, StageTY<double, false>::value, false>);
 }
 
 cudaError_t launch_stage_fp64(const StageArgs& a, cudaStream_t s, bool multi, int* grid_out) {

@@ -8,7 +8,8 @@
 namespace m2c {
 
 size_t stage_smem_mixed(bool multi) {
-  return multi ? sizeof(StageSmemAll<float, STAGE_TY, true>) : sizeof(StageSmemAll<float, STAGE_TY, false>);
+  return multi ? sizeof(StageSmemAll<float, StageTY<float, true>::value, true>)
+               : sizeof(StageSmemAll<float, StageTY<float, false>::value, false>);
 }
 
 cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s, bool multi, int* grid_out) {

@@ -10,6 +10,10 @@
 namespace m2c {
 
 constexpr int STAGE_TY = 8;
+// Tile height per instantiation: the FP64 two-material kernel (second flux
+// buffers for interface faces) uses 32 x 4 tiles to fit in 227 KB of shared memory.
+template <typename T, bool MULTI> struct StageTY { static constexpr int value = STAGE_TY; };
+template <> struct StageTY<double, true> { static constexpr int value = 4; };
 
 size_t stage_smem_fp64(bool multi);
 size_t stage_smem_mixed(bool multi);
@@ -24,29 +28,31 @@ int stage_resident_mixed(int flux, bool multi);
 
 template <typename T, int FLUX, bool MULTI>
 cudaError_t stage_occupancy(int* per_sm, int* nsm) {
-  auto k = stage_kernel<T, STAGE_TY, FLUX, MULTI>;
-  const size_t smem = sizeof(StageSmemAll<T, STAGE_TY, MULTI>);
+  constexpr int TY = StageTY<T, MULTI>::value;
+  auto k = stage_kernel<T, TY, FLUX, MULTI>;
+  const size_t smem = sizeof(StageSmemAll<T, TY, MULTI>);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0;
   cudaGetDevice(&dev);
   e = cudaDeviceGetAttribute(nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, TX * STAGE_TY, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, TX * TY, smem);
   if (*per_sm < 1) *per_sm = 1;
   return e;
 }
 
 template <typename T, int FLUX, bool MULTI>
 cudaError_t launch_stage_one(const StageArgs& a, cudaStream_t s, int* grid_out) {
-  auto k = stage_kernel<T, STAGE_TY, FLUX, MULTI>;
-  const size_t smem = sizeof(StageSmemAll<T, STAGE_TY, MULTI>);
+  constexpr int TY = StageTY<T, MULTI>::value;
+  auto k = stage_kernel<T, TY, FLUX, MULTI>;
+  const size_t smem = sizeof(StageSmemAll<T, TY, MULTI>);
   int per_sm = 1, nsm = 148;
   cudaError_t e = stage_occupancy<T, FLUX, MULTI>(&per_sm, &nsm);
   if (e != cudaSuccess) return e;
   int grid = a.nitems < per_sm * nsm ? a.nitems : per_sm * nsm;
   if (grid_out) *grid_out = grid;
-  k<<<grid, dim3(TX, STAGE_TY), smem, s>>>(a);
+  k<<<grid, dim3(TX, TY), smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -3,10 +3,12 @@ ExactRiemannSolverBase::ComputeRiemannSolution on seeded two-material
 problems (stiffened-gas pairs, densities 1..1e3, pressures 1e4..1e9,
 velocities +-200).
 
-Where the reference's adaptive solve succeeds, results are expected to agree
-to round-off (FP64, no FMA contraction); the step-size control uses pow(),
-whose last bit may differ from the host C library, so a small fraction of
-problems is allowed to differ at the solver's own tolerance. Problems the
+Where the reference's adaptive solve succeeds, results agree bit for bit
+(FP64, no FMA contraction) except where the step-size control's pow()
+rounds differently from the host C library (neither is correctly rounded):
+then the adaptive step sequence changes and the star states differ at the
+integration tolerance. Bar: >= 97% of problems bit-identical, all within
+1e-9 relative. Problems the
 adaptive solve cannot bracket or converge are flagged (err & 1), the cases
 where the reference retries with its non-adaptive variant.
 """
@@ -31,10 +33,9 @@ def test_riemann_batch_matches_reference(gpu, ref):
     both = ok & (err == 0)
     for a, b in ((gVs, Vs), (gVsm, Vsm), (gVsp, Vsp)):
         rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
-        exact = (rel[both].max(axis=1) <= 1e-12)
-        assert exact.mean() >= 0.99, exact.mean()
-        # the rest agree to the secant tolerance on p* (tol_main = 1e-4)
-        assert rel[both].max() <= 1e-3
+        exact = (rel[both].max(axis=1) == 0.0)
+        assert exact.mean() >= 0.97, exact.mean()
+        assert rel[both].max() <= 1e-9, rel[both].max()
     assert (gid[both] != mid[both]).sum() <= 0.01 * n
     assert it[ok].max() <= s.riem_maxits_main
 
