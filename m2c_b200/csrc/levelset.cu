@@ -310,16 +310,189 @@ void levelset_pack(cudaStream_t s, const Grid3& g, const LsGeom& geo, const doub
   k_ls_pack<<<grid1d((long long)(g.nx + 2) * (g.ny + 2) * (g.nz + 2)), 256, 0, s>>>(g, geo, phi, aos);
 }
 
+// --------------------------------------------------------------------------
+// Reinitialisation (LevelSetReinitializer::ReinitializeFullDomain,
+// LevelSetReinitializer.cpp:74-171) with the FIXED first-layer treatment:
+//   tag the first layer (a face neighbour with phi*phi_nb <= 0, 297-428),
+//   smoothed sign S = phi / sqrt(phi^2 + min(dx,dy,dz)^2) (594-615),
+//   pseudo-time SSP-RK3 of R = -dt S (|grad phi|_Godunov - 1) with the first
+//   layer held fixed (953-1033), stopping when the max residual or the max
+//   relative change drops below the tolerance; on failure the CFL number is
+//   divided by 1.5 and the iteration restarts from the saved phi (154-169).
+// --------------------------------------------------------------------------
+struct ReinitBuf {
+  double* phi1;
+  double* phi2;
+  double* sign;
+  double* phibk;
+  uint8_t* tag;
+  unsigned long long* red;  // [0] max residual bits, [1] max rel. change bits, [2] first-layer count, [3] done flag
+};
+
+static ReinitBuf carve(double* base, long long n) {
+  ReinitBuf b;
+  b.phi1 = base;
+  b.phi2 = base + n;
+  b.sign = base + 2 * n;
+  b.phibk = base + 3 * n;
+  b.red = (unsigned long long*)(base + 4 * n);
+  b.tag = (uint8_t*)(base + 4 * n + 8);
+  return b;
+}
+
 m2cg_status reinit_alloc(long long ncell, double** buf) {
-  (void)ncell;
-  *buf = nullptr;
+  size_t bytes = (size_t)(4 * ncell + 8) * 8 + (size_t)ncell + 64;
+  if (cudaMalloc((void**)buf, bytes) != cudaSuccess) return M2CG_ERR_NOMEM;
   return M2CG_OK;
 }
 
+__global__ void k_reinit_prep(Grid3 g, LsGeom geo, const double* phi, ReinitBuf b) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  unsigned long long tagged = 0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx), j = (int)((q / g.nx) % g.ny), k = (int)(q / ((long long)g.nx * g.ny));
+    const long long off = loff(g, i, j, k);
+    const double p = phi[off];
+    const bool t = p * phi_at(g, geo, phi, i - 1, j, k) <= 0 || p * phi_at(g, geo, phi, i + 1, j, k) <= 0 ||
+                   p * phi_at(g, geo, phi, i, j - 1, k) <= 0 || p * phi_at(g, geo, phi, i, j + 1, k) <= 0 ||
+                   p * phi_at(g, geo, phi, i, j, k - 1) <= 0 || p * phi_at(g, geo, phi, i, j, k + 1) <= 0;
+    b.tag[off] = t ? 1 : 0;
+    tagged += t;
+    const double f = smin(g.dx[i], smin(g.dy[j], g.dz[k]));  // eps = 1
+    b.sign[off] = p / sqrt(p * p + f * f);
+    b.phibk[off] = p;
+  }
+  if (tagged) atomicAdd(&b.red[2], tagged);
+}
+
+// pseudo-time residual at an untagged interior cell (LevelSetReinitializer.cpp:985-1012)
+__device__ __forceinline__ double reinit_local(const Grid3& g, const LsGeom& geo, const double* phi, int i, int j,
+                                               int k, double& local_res) {
+  const double p = phi[loff(g, i, j, k)];
+  const double* X = geo.xg[0];
+  const double* Y = geo.xg[1];
+  const double* Z = geo.xg[2];
+  const double a = (p - phi_at(g, geo, phi, i - 1, j, k)) / (X[i + 1] - X[i]);
+  const double b = (phi_at(g, geo, phi, i + 1, j, k) - p) / (X[i + 2] - X[i + 1]);
+  const double c = (p - phi_at(g, geo, phi, i, j - 1, k)) / (Y[j + 1] - Y[j]);
+  const double d = (phi_at(g, geo, phi, i, j + 1, k) - p) / (Y[j + 2] - Y[j + 1]);
+  const double e = (p - phi_at(g, geo, phi, i, j, k - 1)) / (Z[k + 1] - Z[k]);
+  const double f = (phi_at(g, geo, phi, i, j, k + 1) - p) / (Z[k + 2] - Z[k + 1]);
+  const double ap = smax(a, 0.0), am = smin(a, 0.0);
+  const double bp = smax(b, 0.0), bm = smin(b, 0.0);
+  const double cp = smax(c, 0.0), cm = smin(c, 0.0);
+  const double dp = smax(d, 0.0), dm = smin(d, 0.0);
+  const double ep = smax(e, 0.0), em = smin(e, 0.0);
+  const double fp = smax(f, 0.0), fm = smin(f, 0.0);
+  if (p >= 0)
+    local_res = sqrt(smax(ap * ap, bm * bm) + smax(cp * cp, dm * dm) + smax(ep * ep, fm * fm)) - 1.0;
+  else
+    local_res = sqrt(smax(am * am, bp * bp) + smax(cm * cm, dp * dp) + smax(em * em, fp * fp)) - 1.0;
+  return local_res;
+}
+
+// One RK3 stage of the pseudo-time iteration:
+//   stage 1: out = in + R(in)                     (in = phi, out = phi1)
+//   stage 2: out = 0.25*in + 0.75*phi + 0.25*R(in)  (in = phi1, out = phi2)
+//   stage 3: phi = 1/3*phi + 2/3*in + 2/3*R(in)     (in = phi2, out = phi)
+__global__ void k_reinit_stage(Grid3 g, LsGeom geo, ReinitBuf b, int stage, double cfl, double tol, const double* in,
+                               double* phi, double* out) {
+  if (stage > 1 && b.red[3]) return;  // converged on the residual in stage 1
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  double maxres = 0.0, maxrel = 0.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx), j = (int)((q / g.nx) % g.ny), k = (int)(q / ((long long)g.nx * g.ny));
+    const long long off = loff(g, i, j, k);
+    double R = 0.0;
+    if (!b.tag[off]) {
+      const double dx = smin(g.dx[i], smin(g.dy[j], g.dz[k]));
+      const double dt = cfl * dx;
+      double lr;
+      reinit_local(g, geo, in, i, j, k, lr);
+      if (fabs(lr) <= 1.0)
+        R = -dt * b.sign[off] * lr;
+      else
+        R = -dt * b.sign[off] * lr / fabs(lr);
+      maxres = smax(maxres, fabs(lr));
+    }
+    if (stage == 1) {
+      out[off] = in[off] + R;
+    } else if (stage == 2) {
+      double t = 0.25 * in[off] + 0.75 * phi[off];
+      out[off] = t + 0.25 * R;
+    } else {
+      const double old = phi[off];
+      double t = 1.0 / 3.0 * old + 2.0 / 3.0 * in[off];
+      const double nw = t + 2.0 / 3.0 * R;
+      phi[off] = nw;
+      double le = fabs(nw - old);
+      if (nw != 0) le /= fabs(nw);
+      maxrel = smax(maxrel, le);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    maxres = smax(maxres, __shfl_xor_sync(0xffffffffu, maxres, o));
+    maxrel = smax(maxrel, __shfl_xor_sync(0xffffffffu, maxrel, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (stage == 1 && maxres > 0) atomicMax(&b.red[0], (unsigned long long)__double_as_longlong(maxres));
+    if (stage == 3 && maxrel > 0) atomicMax(&b.red[1], (unsigned long long)__double_as_longlong(maxrel));
+  }
+  (void)tol;
+}
+
+__global__ void k_reinit_check(ReinitBuf b, double tol) {
+  const double r = __longlong_as_double((long long)b.red[0]);
+  b.red[3] = (r < tol) ? 1ull : 0ull;
+}
+
+static double bits_to_double(unsigned long long u) {
+  double d;
+  memcpy(&d, &u, 8);
+  return d;
+}
+
 m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& geo, const m2cg_levelset& ls,
-                                  double* phi, double* buf, DevError* err) {
-  (void)s; (void)g; (void)geo; (void)ls; (void)phi; (void)buf; (void)err;
-  return M2CG_ERR_UNSUPPORTED;
+                                  double* phi, double* buf, DevError* err, double* cfl_state, int* iterations) {
+  (void)err;
+  const long long n = g.plane * g.nz;
+  ReinitBuf b = carve(buf, n);
+  const long long ni = (long long)g.nx * g.ny * g.nz;
+  const int grid = grid1d(ni);
+  cudaMemsetAsync(b.red, 0, 4 * sizeof(unsigned long long), s);
+  k_reinit_prep<<<grid, 256, 0, s>>>(g, geo, phi, b);
+  unsigned long long hred[4];
+  cudaMemcpyAsync(hred, b.red, sizeof hred, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
+  if (hred[2] == 0) return M2CG_OK;  // no interface: nothing to do
+  const double tol = ls.reinit_tol;
+  const int maxIts = ls.reinit_maxits;
+  int total = 0;
+  for (;;) {
+    const double cfl = *cfl_state;
+    int iter;
+    double dphi_max = 0.0;
+    for (iter = 0; iter < maxIts; iter++) {
+      cudaMemsetAsync(b.red, 0, 2 * sizeof(unsigned long long), s);
+      cudaMemsetAsync(b.red + 3, 0, sizeof(unsigned long long), s);
+      k_reinit_stage<<<grid, 256, 0, s>>>(g, geo, b, 1, cfl, tol, phi, phi, b.phi1);
+      k_reinit_check<<<1, 1, 0, s>>>(b, tol);
+      k_reinit_stage<<<grid, 256, 0, s>>>(g, geo, b, 2, cfl, tol, b.phi1, phi, b.phi2);
+      k_reinit_stage<<<grid, 256, 0, s>>>(g, geo, b, 3, cfl, tol, b.phi2, phi, phi);
+      cudaMemcpyAsync(hred, b.red, sizeof hred, cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
+      total++;
+      if (hred[3]) break;  // residual below the tolerance (checked before updating phi)
+      dphi_max = bits_to_double(hred[1]);
+      if (dphi_max < tol) break;
+    }
+    if (iterations) *iterations += total;
+    if (iter < maxIts) return M2CG_OK;
+    if (dphi_max < 0.02) return M2CG_OK;
+    if (cfl < 0.02) return M2CG_ERR_REINIT;
+    *cfl_state = cfl / 1.5;
+    cudaMemcpyAsync(phi, b.phibk, n * 8, cudaMemcpyDeviceToDevice, s);
+  }
 }
 
 }  // namespace m2c

@@ -32,8 +32,10 @@ void levelset_pack(cudaStream_t s, const Grid3& g, const LsGeom& geo, const doub
 m2cg_status levelset_stage(cudaStream_t s, const Grid3& g, const SchemeK& sk, const LsGeom& geo, const StageArgs& a,
                            const double* in, const double* phin, double* out);
 m2cg_status reinit_alloc(long long ncell, double** buf);
+// cfl_state: the pseudo-time CFL number, reduced in place on a failed attempt
+// and kept for later calls (as LevelSetReinitializer::cfl is).
 m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& geo, const m2cg_levelset& ls,
-                                  double* phi, double* buf, DevError* err);
+                                  double* phi, double* buf, DevError* err, double* cfl_state, int* iterations);
 
 }  // namespace m2c
 

@@ -75,6 +75,8 @@ struct Multiphase {
   // host-side counters
   long long riemann_calls = 0, riemann_iterations = 0, riemann_errors = 0, unresolved = 0, reinit_calls = 0;
   double* reinit_buf = nullptr;  // reinitialisation work arrays
+  double reinit_cfl = 0.8;       // pseudo-time CFL, reduced on failed attempts
+  long long reinit_iterations = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -452,6 +454,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   mp->scheme = scheme;
   mp->ls = ls;
   mp->rp = riemann_params(scheme);
+  mp->reinit_cfl = ls.reinit_cfl;
   mp->ncell = g.plane * g.nz;
   const long long n = mp->ncell;
   const long long ninterior = (long long)g.nx * g.ny * g.nz;
@@ -606,9 +609,11 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
   k_update_id<<<grid1d(ninterior), 256, 0, s>>>(g, mp->phiN, mp->phiT, id, mp->ls.material_id);
   // reinitialisation every `frequency` steps (LevelSetOperator::Reinitialize, 1599-1624)
   if (mp->ls.reinit_frequency > 0 && mp->time_step % mp->ls.reinit_frequency == 0) {
-    m2cg_status st = levelset_reinitialize(s, g, mp->lsg, mp->ls, mp->phiN, mp->reinit_buf, err);
+    int its = 0;
+    m2cg_status st = levelset_reinitialize(s, g, mp->lsg, mp->ls, mp->phiN, mp->reinit_buf, err, &mp->reinit_cfl, &its);
     if (st) return st;
     mp->reinit_calls++;
+    mp->reinit_iterations += its;
   }
   // ordered list of cells whose ID changed, then the sequential update
   long long per_block = (ninterior + mp->nblocks_scan - 1) / mp->nblocks_scan;

@@ -32,7 +32,7 @@ def test_bubble_residual_matches_reference(gpu, ref):
 
 @pytest.mark.parametrize("rk", [2, 3])
 def test_bubble_steps_match_reference(gpu, ref, rk):
-    g, s, mats, ls, V, ID, PHI = cases.bubble_case(16, rk=rk, reinit_frequency=-1)
+    g, s, mats, ls, V, ID, PHI = cases.bubble_case(24, rk=rk, reinit_frequency=-1)
     sol, rc = make(gpu, ref, g, s, mats, ls, V, ID, PHI)
     for _ in range(4):
         sol.run(1)
@@ -73,3 +73,43 @@ def test_water_air_tube_matches_reference(gpu, ref):
     assert np.array_equal(inner(IDg), inner(IDr))
     assert rel_err(inner(Vg), inner(Vr)) <= TOL
     assert rel_err(inner(Pg), inner(Pr), axis_last=False) <= TOL
+
+
+def test_bubble_with_reinitialisation_matches_reference(gpu, ref):
+    g, s, mats, ls, V, ID, PHI = cases.bubble_case(24, reinit_frequency=2)
+    sol, rc = make(gpu, ref, g, s, mats, ls, V, ID, PHI)
+    for _ in range(6):
+        sol.run(1)
+        rc.run(1)
+    Vg, IDg, Pg = sol.download()
+    Vr, IDr, Pr = rc.get_state()
+    assert np.array_equal(inner(IDg), inner(IDr))
+    assert rel_err(inner(Vg), inner(Vr)) <= TOL
+    assert rel_err(inner(Pg), inner(Pr), axis_last=False) <= TOL
+    assert sol.counters()["reinit_calls"] == 3
+
+
+def test_mixed_precision_bubble_close_to_fp64(gpu):
+    """Mixed path on the two-material case: IDs identical; density, pressure
+    and velocity (as a vector: v and w are ~0 by symmetry, so their own
+    relative norms measure only symmetry-breaking noise) within 1e-5 relative
+    L1 of the FP64 path after a few steps."""
+    g, s, mats, ls, V, ID, PHI = cases.bubble_case(24, reinit_frequency=2)
+    a = gpu.Solver(g, s, mats, ls)
+    a.upload(V, ID, PHI)
+    s2 = abi.scheme(**{n: getattr(s, n) for n, _ in abi.Scheme._fields_})
+    s2.precision = abi.PREC_MIXED
+    b = gpu.Solver(g, s2, mats, ls)
+    b.upload(V, ID, PHI)
+    a.run(4)
+    b.run(4)
+    Va, IDa, Pa = a.download()
+    Vb, IDb, Pb = b.download()
+    assert np.array_equal(inner(IDa), inner(IDb))
+    la = inner(Va).reshape(-1, 5)
+    lb = inner(Vb).reshape(-1, 5)
+    for c in (0, 4):
+        l1 = np.abs(la[:, c] - lb[:, c]).sum() / np.abs(la[:, c]).sum()
+        assert l1 <= 1e-5, (c, l1)
+    dv = np.linalg.norm(la[:, 1:4] - lb[:, 1:4], axis=1).sum() / np.linalg.norm(la[:, 1:4], axis=1).sum()
+    assert dv <= 1e-5, dv
