@@ -22,6 +22,7 @@ LIM_NONE, LIM_GENMINMOD, LIM_VANALBADA = 0, 1, 2
 RECVAR_PRIMITIVE, RECVAR_CONSERVATIVE, RECVAR_PRIM_CHAR, RECVAR_CONS_CHAR = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 MPFLUX_EXACT, MPFLUX_NUMERICAL, MPFLUX_LLF = 0, 1, 2
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_RIEMANN, ERR_REINIT, ERR_ITER_CAP, ERR_NOMEM, ERR_UNSUPPORTED = range(9)
 LSBC_NONE, LSBC_ZERO_NEUMANN, LSBC_LINEAR_EXTRAPOLATION, LSBC_NON_NEGATIVE = 0, 1, 2, 3
 
 _dp = C.POINTER(C.c_double)

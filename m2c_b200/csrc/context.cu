@@ -45,6 +45,11 @@ static m2cg_status fail(m2cg_status st, const char* fmt, ...) {
 
 extern "C" const char* m2cg_last_error(void) { return g_last_error.c_str(); }
 
+namespace m2c {
+// Sets the text m2cg_last_error() returns, for entry points in other files.
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace m2c
+
 // ---------------------------------------------------------------------------
 // Defaults: IoData constructors of the reference.
 // ---------------------------------------------------------------------------

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -70,11 +71,11 @@ cudaError_t launch_riemann_batch(const RiemannBatchArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+void set_last_error(const char* msg);
+
 }  // namespace m2c
 
 using namespace m2c;
-
-static thread_local char g_riem_err[256];
 
 extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_material* mats, int nmat, int n,
                                           const double* VL, const int* idl, const double* VR, const int* idr,
@@ -102,11 +103,13 @@ extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_
   a.P = riemann_params(*scheme);
   a.path_cap = RIEMANN_PATH_CAP;
   a.scratch_slots = n;
-  size_t bytes_in = (size_t)n * (5 * 8 * 2 + 4 * 2 + 3 * 8 + 8);
-  size_t bytes_out = (size_t)n * (5 * 8 * 3 + 4 * 3);
-  size_t bytes_scratch = (size_t)n * 2 * 3 * RIEMANN_PATH_CAP * sizeof(double);
+  // One allocation holds every array, each starting on a 256-byte boundary.
+  auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t nn = (size_t)n;
+  const size_t total = 5 * rup(nn * 40) + rup(nn * 24) + 5 * rup(nn * 4) + (warm ? rup(nn * 8) : 0) +
+                       rup(sizeof(heos));
+  size_t bytes_scratch = nn * 2 * 3 * RIEMANN_PATH_CAP * sizeof(double);
   char* buf = nullptr;
-  size_t total = bytes_in + bytes_out + sizeof(heos) + 256;
   m2cg_status st = M2CG_OK;
   if (cudaMalloc((void**)&buf, total) != cudaSuccess || cudaMalloc((void**)&a.scratch, bytes_scratch) != cudaSuccess) {
     cudaFree(buf);
@@ -114,33 +117,47 @@ extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_
     return M2CG_ERR_NOMEM;
   }
   char* p = buf;
-  auto take = [&](size_t b) { char* r = p; p += (b + 255) / 256 * 256; return r; };
-  double* dVL = (double*)take(n * 40); double* dVR = (double*)take(n * 40); double* ddir = (double*)take(n * 24);
-  int* didl = (int*)take(n * 4); int* didr = (int*)take(n * 4); double* dwarm = warm ? (double*)take(n * 8) : nullptr;
-  double* dVs = (double*)take(n * 40); double* dVsm = (double*)take(n * 40); double* dVsp = (double*)take(n * 40);
-  int* did = (int*)take(n * 4); int* diters = (int*)take(n * 4); int* derr = (int*)take(n * 4);
+  auto take = [&](size_t b) { char* r = p; p += rup(b); return r; };
+  double* dVL = (double*)take(nn * 40); double* dVR = (double*)take(nn * 40); double* ddir = (double*)take(nn * 24);
+  int* didl = (int*)take(nn * 4); int* didr = (int*)take(nn * 4);
+  double* dwarm = warm ? (double*)take(nn * 8) : nullptr;
+  double* dVs = (double*)take(nn * 40); double* dVsm = (double*)take(nn * 40); double* dVsp = (double*)take(nn * 40);
+  int* did = (int*)take(nn * 4); int* diters = (int*)take(nn * 4); int* derr = (int*)take(nn * 4);
   Eos<double>* deos = (Eos<double>*)take(sizeof(heos));
-  (void)total;
-  cudaMemcpyAsync(dVL, VL, n * 40, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(dVR, VR, n * 40, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(ddir, dir, n * 24, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(didl, idl, n * 4, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(didr, idr, n * 4, cudaMemcpyHostToDevice, s);
-  if (warm) cudaMemcpyAsync(dwarm, warm, n * 8, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(deos, heos, sizeof(heos), cudaMemcpyHostToDevice, s);
-  a.VL = dVL; a.VR = dVR; a.dir = ddir; a.idl = didl; a.idr = didr; a.warm = dwarm;
-  a.Vs = dVs; a.Vsm = dVsm; a.Vsp = dVsp; a.id = did; a.iters = diters; a.err = derr; a.eos = deos;
-  if (launch_riemann_batch(a, s) != cudaSuccess) st = M2CG_ERR_CUDA;
-  cudaMemcpyAsync(Vs, dVs, n * 40, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(Vsm, dVsm, n * 40, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(Vsp, dVsp, n * 40, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(id, did, n * 4, cudaMemcpyDeviceToHost, s);
-  if (iters) cudaMemcpyAsync(iters, diters, n * 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(err, derr, n * 4, cudaMemcpyDeviceToHost, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) st = M2CG_ERR_CUDA;
+  cudaError_t e = cudaSuccess;
+  auto ck = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  if ((size_t)(p - buf) == total) {  // the carve-up stays inside the allocation
+    ck(cudaMemcpyAsync(dVL, VL, nn * 40, cudaMemcpyHostToDevice, s));
+    ck(cudaMemcpyAsync(dVR, VR, nn * 40, cudaMemcpyHostToDevice, s));
+    ck(cudaMemcpyAsync(ddir, dir, nn * 24, cudaMemcpyHostToDevice, s));
+    ck(cudaMemcpyAsync(didl, idl, nn * 4, cudaMemcpyHostToDevice, s));
+    ck(cudaMemcpyAsync(didr, idr, nn * 4, cudaMemcpyHostToDevice, s));
+    if (warm) ck(cudaMemcpyAsync(dwarm, warm, nn * 8, cudaMemcpyHostToDevice, s));
+    ck(cudaMemcpyAsync(deos, heos, sizeof(heos), cudaMemcpyHostToDevice, s));
+    a.VL = dVL; a.VR = dVR; a.dir = ddir; a.idl = didl; a.idr = didr; a.warm = dwarm;
+    a.Vs = dVs; a.Vsm = dVsm; a.Vsp = dVsp; a.id = did; a.iters = diters; a.err = derr; a.eos = deos;
+    if (e == cudaSuccess) ck(launch_riemann_batch(a, s));
+    if (e == cudaSuccess) {
+      ck(cudaMemcpyAsync(Vs, dVs, nn * 40, cudaMemcpyDeviceToHost, s));
+      ck(cudaMemcpyAsync(Vsm, dVsm, nn * 40, cudaMemcpyDeviceToHost, s));
+      ck(cudaMemcpyAsync(Vsp, dVsp, nn * 40, cudaMemcpyDeviceToHost, s));
+      ck(cudaMemcpyAsync(id, did, nn * 4, cudaMemcpyDeviceToHost, s));
+      if (iters) ck(cudaMemcpyAsync(iters, diters, nn * 4, cudaMemcpyDeviceToHost, s));
+      ck(cudaMemcpyAsync(err, derr, nn * 4, cudaMemcpyDeviceToHost, s));
+    }
+    ck(cudaStreamSynchronize(s));
+    if (e != cudaSuccess) {
+      char msg[200];
+      snprintf(msg, sizeof msg, "m2cg_riemann_batch: %s", cudaGetErrorString(e));
+      set_last_error(msg);
+      st = M2CG_ERR_CUDA;
+    }
+  } else {
+    set_last_error("m2cg_riemann_batch: internal buffer layout error");
+    st = M2CG_ERR_ARG;
+  }
   cudaFree(buf);
   cudaFree(a.scratch);
   cudaStreamDestroy(s);
-  (void)g_riem_err;
   return st;
 }
