@@ -221,6 +221,32 @@ m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_material* m
                                const int* idr, const double* dir, const double* warm,
                                double* Vs, int* id, double* Vsm, double* Vsp, int* iters, int* err);
 
+/* The same batched Riemann solve for callers that cannot allocate device
+ * memory: a host application whose memory pool owns the whole GPU, or a
+ * runtime that forbids allocation on the path that calls it. No counterpart
+ * in the reference.
+ *  - All array arguments are DEVICE pointers the caller owns; the call makes
+ *    no allocation (no cudaMalloc or cudaFree, no allocating library call).
+ *  - The solver's integration-path scratch is a file-scope device array of
+ *    M2CG_NOALLOC_MAX_PROBLEMS slots of 24 KiB (24 MiB), held by every device
+ *    that loads the library until the process exits. n beyond
+ *    M2CG_NOALLOC_MAX_PROBLEMS is rejected with M2CG_ERR_ARG and a message.
+ *  - The first call on each device looks up that array's device address
+ *    (with that device current), so make it before any stream capture.
+ *  - The work is queued on `stream` (a cudaStream_t, NULL = legacy default
+ *    stream); the call returns without waiting. All calls share the scratch
+ *    array, so calls that overlap on the GPU (different streams, devices
+ *    excepted) race; order them on one stream.
+ *  - err gains M2CG_RIEMANN_ERR_MATERIAL_ID where idl/idr is outside
+ *    [0, nmat) (outputs of that problem are NaN, id -1). */
+#define M2CG_NOALLOC_MAX_PROBLEMS 1024
+#define M2CG_RIEMANN_ERR_MATERIAL_ID 8
+m2cg_status m2cg_riemann_batch_noalloc(const m2cg_scheme* scheme, const m2cg_material* mats, int nmat,
+                                       int n, const double* VL, const int* idl, const double* VR,
+                                       const int* idr, const double* dir, const double* warm,
+                                       double* Vs, int* id, double* Vsm, double* Vsp, int* iters,
+                                       int* err, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Batched 1D two-material shock tubes of uneven lengths, all advanced in one
  * persistent launch per RK stage, captured in a CUDA graph.
