@@ -221,6 +221,14 @@ m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_material* m
                                const int* idr, const double* dir, const double* warm,
                                double* Vs, int* id, double* Vsm, double* Vsp, int* iters, int* err);
 
+/* The same solve where every problem carries its own material pair:
+ * problem q has material mats[2q] on the left and mats[2q+1] on the right;
+ * id[q] is 0 (left material) or 1 (right). Host pointers. */
+m2cg_status m2cg_riemann_batch_pairs(const m2cg_scheme* scheme, const m2cg_material* mats, int n,
+                                     const double* VL, const double* VR, const double* dir,
+                                     const double* warm, double* Vs, int* id, double* Vsm,
+                                     double* Vsp, int* iters, int* err);
+
 /* The same batched Riemann solve for callers that cannot allocate device
  * memory: a host application whose memory pool owns the whole GPU, or a
  * runtime that forbids allocation on the path that calls it. No counterpart
@@ -270,7 +278,18 @@ m2cg_status m2cg_batch_create(const m2cg_scheme* scheme, int ntubes, const int* 
 m2cg_status m2cg_batch_run(m2cg_batch* b, int nsteps);
 /* Download tube states: V (5 doubles per cell, tubes concatenated), ID per cell. */
 m2cg_status m2cg_batch_download(m2cg_batch* b, double* V, int* ID, double* t_per_tube);
+/* The tuning in use (the autotuner's choice where the caller passed 0). */
 m2cg_status m2cg_batch_get_tuning(const m2cg_batch* b, m2cg_batch_tuning* t);
+/* Counters over all tubes: steps, cell updates, interface Riemann calls,
+ * iterations and errors (as counted at SpaceOperator.cpp:2818), unresolved
+ * cells of the post-step update, kernel launches. */
+m2cg_status m2cg_batch_get_counters(m2cg_batch* b, m2cg_counters* c);
+/* First device error code of each tube (0 = none), ntubes entries. */
+m2cg_status m2cg_batch_tube_errors(m2cg_batch* b, int* codes);
+/* Advance nsteps and return the device time of those steps (CUDA events on
+ * the batch's stream). *ms is written even when a tube reported an error
+ * (the status then says which error; m2cg_batch_tube_errors says where). */
+m2cg_status m2cg_batch_time_steps(m2cg_batch* b, int nsteps, float* ms);
 m2cg_status m2cg_batch_destroy(m2cg_batch* b);
 
 #ifdef __cplusplus

@@ -168,6 +168,77 @@ def riemann_problems(n, seed=3, nmat_pairs=None):
     return mats, VL, idl, VR, idr, dirs
 
 
+def tube_states(n, rng):
+    """Left/right primitive states of n tubes: densities log-uniform in
+    1..1000 kg/m^3, velocities uniform in +-200 m/s (along the tube),
+    pressures log-uniform in 1e4..1e9 Pa."""
+    VL = np.zeros((n, 5))
+    VR = np.zeros((n, 5))
+    for V in (VL, VR):
+        V[:, 0] = 10.0 ** rng.uniform(0.0, 3.0, n)
+        V[:, 1] = rng.uniform(-200.0, 200.0, n)
+        V[:, 4] = 10.0 ** rng.uniform(4.0, 9.0, n)
+    return VL, VR
+
+
+def tubes(ntubes=4096, seed=11, lmin=100, lmax=2000, reject=None):
+    """The batched-tube workload: ntubes independent 1D two-material shock
+    tubes on [0, 1] with seeded lengths uniform in lmin..lmax cells, a
+    stiffened-gas pair per tube (gamma in [1.2, 7], p_inf 0 with probability
+    1/4 else log-uniform in 1e6..1e9 Pa) and the tube_states distribution.
+    `reject(mats, VL, VR) -> bool array` flags tubes to redraw (e.g. those
+    whose initial Riemann problem the solver cannot bracket); redraws come
+    from the same seeded stream. Returns (lens, mats, VL, VR, redrawn)."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(lmin, lmax + 1, ntubes).astype(np.int32)
+    mats = []
+    for _ in range(ntubes):
+        mats += [stiffened_gas_pair(rng), stiffened_gas_pair(rng)]
+    VL, VR = tube_states(ntubes, rng)
+    redrawn = 0
+    for _ in range(20):
+        if reject is None:
+            break
+        bad = np.nonzero(reject(mats, VL, VR))[0]
+        if len(bad) == 0:
+            break
+        redrawn += len(bad)
+        for t in bad:
+            mats[2 * t] = stiffened_gas_pair(rng)
+            mats[2 * t + 1] = stiffened_gas_pair(rng)
+        nl, nr = tube_states(len(bad), rng)
+        VL[bad], VR[bad] = nl, nr
+    return lens, mats, VL, VR, redrawn
+
+
+def tube_scheme(**kw):
+    """Scheme of the batched tubes: HLLC, MUSCL with the van Albada limiter,
+    exact interface Riemann solve (MultiPhase flux NUMERICAL, constant
+    reconstruction at the interface), RK2, CFL 0.5."""
+    d = dict(flux=abi.FLUX_HLLC, limiter=abi.LIM_VANALBADA, rk_order=2, cfl=0.5)
+    d.update(kw)
+    return abi.scheme(**d)
+
+
+def tube_case(n, VL, VR):
+    """One tube as a reference/3D-path case: an n x 1 x 1 grid on [0, 1],
+    INLET ghost holding VL, OUTLET ghost holding VR, symmetry in y and z,
+    phi = 0.5 - x, material 1 where phi < 0. Returns (g, ls, V, ID, PHI)."""
+    g = abi.grid(n, 1, 1, bc=(abi.BC_INLET, abi.BC_OUTLET) + (abi.BC_SYMMETRY,) * 4,
+                 inlet=tuple(VL), outlet=tuple(VR))
+    ls = abi.levelset(material_id=1)
+    x = abi.cell_centres(g)[0]
+    phi = 0.5 - x
+    right = phi < 0
+    V = empty_state(g)
+    V[1, 1, 1:-1] = np.where(right[:, None], np.asarray(VR)[None, :], np.asarray(VL)[None, :])
+    ID = np.zeros(abi.ghosted_shape(g))
+    ID[1, 1, 1:-1] = right.astype(np.float64)
+    PHI = np.zeros(abi.ghosted_shape(g))
+    PHI[1, 1, 1:-1] = phi
+    return g, ls, V, ID, PHI
+
+
 WATER = dict(gamma=6.12, p_c=3.43e8)
 AIR = dict(gamma=1.4, p_c=0.0)
 

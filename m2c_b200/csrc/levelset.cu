@@ -19,6 +19,7 @@
 #include <cstring>
 #include <vector>
 
+#include "fd3.cuh"
 #include "levelset.h"
 
 namespace m2c {
@@ -26,30 +27,6 @@ namespace m2c {
 // --------------------------------------------------------------------------
 // host: geometry and coefficients
 // --------------------------------------------------------------------------
-static void taylor4(double d0, double d1, double d2, double d3, double* c) {
-  // A = [1;d;d^2;d^3] columns, b = (0,1,0,0): Gaussian elimination, partial pivoting
-  double m[4][5] = {{1.0, 1.0, 1.0, 1.0, 0.0},
-                    {d0, d1, d2, d3, 1.0},
-                    {d0 * d0, d1 * d1, d2 * d2, d3 * d3, 0.0},
-                    {d0 * d0 * d0, d1 * d1 * d1, d2 * d2 * d2, d3 * d3 * d3, 0.0}};
-  for (int col = 0; col < 4; col++) {
-    int p = col;
-    for (int r = col + 1; r < 4; r++)
-      if (std::fabs(m[r][col]) > std::fabs(m[p][col])) p = r;
-    if (p != col)
-      for (int q = 0; q <= 4; q++) std::swap(m[col][q], m[p][q]);
-    for (int r = col + 1; r < 4; r++) {
-      double f = m[r][col] / m[col][col];
-      for (int q = col; q <= 4; q++) m[r][q] -= f * m[col][q];
-    }
-  }
-  for (int i = 3; i >= 0; i--) {
-    double s = m[i][4];
-    for (int q = i + 1; q < 4; q++) s -= m[i][q] * c[q];
-    c[i] = s / m[i][i];
-  }
-}
-
 m2cg_status levelset_geom_create(cudaStream_t s, const Grid3& g, const m2cg_levelset& ls, const double* const* xc,
                                  const double* const* dx, LsGeom* out) {
   memset(out, 0, sizeof *out);
@@ -175,10 +152,6 @@ __device__ double phi_at(const Grid3& g, const LsGeom& geo, const double* phi, i
     return val;
   }
   return image;  // ZERO_NEUMANN
-}
-
-__device__ __forceinline__ double fd4(const double* cf, double p0, double p1, double p2, double p3) {
-  return cf[0] * p0 + cf[1] * p1 + cf[2] * p2 + cf[3] * p3;
 }
 
 // -(u . grad phi) with upwind-biased FD3 at cell (i,j,k)

@@ -6,6 +6,7 @@
 // and keeps its rounding.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -62,11 +63,13 @@ RiemannParams riemann_params(const m2cg_scheme& s) {
   return P;
 }
 
+// One thread per path-scratch slot: a.scratch_slots is a multiple of 128, so
+// the grid-stride loop maps every problem of a thread to that thread's slot.
 cudaError_t launch_riemann_batch(const RiemannBatchArgs& a, cudaStream_t s) {
   if (a.n <= 0) return cudaSuccess;
-  int block = 128;
-  long long grid = (a.n + block - 1) / block;
-  if (grid > 148 * 32) grid = 148 * 32;
+  if (a.scratch_slots <= 0 || a.scratch_slots % 128) return cudaErrorInvalidValue;
+  const int block = 128;
+  const long long grid = a.scratch_slots / block;
   k_riemann_batch<<<(int)grid, block, 0, s>>>(a);
   return cudaGetLastError();
 }
@@ -77,43 +80,47 @@ void set_last_error(const char* msg);
 
 using namespace m2c;
 
-extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_material* mats, int nmat, int n,
-                                          const double* VL, const int* idl, const double* VR, const int* idr,
-                                          const double* dir, const double* warm, double* Vs, int* id, double* Vsm,
-                                          double* Vsp, int* iters, int* err) {
-  if (!scheme || !mats || nmat < 1 || nmat > MAXMAT_RIEMANN || n < 0 || !VL || !idl || !VR || !idr || !dir || !Vs ||
-      !id || !Vsm || !Vsp || !err)
-    return M2CG_ERR_ARG;
-  if (n == 0) return M2CG_OK;
-  for (int q = 0; q < n; q++)
-    if (idl[q] < 0 || idl[q] >= nmat || idr[q] < 0 || idr[q] >= nmat) return M2CG_ERR_ARG;
+static Eos<double> eos_of_material(const m2cg_material& m) {
+  MatParams p;
+  p.kind = m.eos; p.gam = m.gamma; p.pc = m.p_c; p.b = m.b; p.q = m.q;
+  p.rhomin = m.rhomin; p.pmin = m.pmin; p.rhomax = m.rhomax; p.pmax = m.pmax;
+  p.failsafe_density = m.failsafe_density;
+  return make_eos<double>(p);
+}
+
+// Host arrays in, host arrays out: one device allocation carved into every
+// array, one for the path scratch, one stream; the material table heos is
+// indexed by idl/idr.
+static m2cg_status riemann_host(const m2cg_scheme& scheme, const std::vector<Eos<double>>& heos, int n,
+                                const double* VL, const int* idl, const double* VR, const int* idr,
+                                const double* dir, const double* warm, double* Vs, int* id, double* Vsm,
+                                double* Vsp, int* iters, int* err) {
   cudaStream_t s;
-  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return M2CG_ERR_CUDA;
-  Eos<double> heos[MAXMAT_RIEMANN];
-  for (int m = 0; m < nmat; m++) {
-    MatParams p;
-    p.kind = mats[m].eos; p.gam = mats[m].gamma; p.pc = mats[m].p_c; p.b = mats[m].b; p.q = mats[m].q;
-    p.rhomin = mats[m].rhomin; p.pmin = mats[m].pmin; p.rhomax = mats[m].rhomax; p.pmax = mats[m].pmax;
-    p.failsafe_density = mats[m].failsafe_density;
-    heos[m] = make_eos<double>(p);
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+    set_last_error("m2cg_riemann_batch: cudaStreamCreate failed (no CUDA device?)");
+    return M2CG_ERR_CUDA;
   }
   RiemannBatchArgs a;
   memset(&a, 0, sizeof a);
   a.n = n;
-  a.P = riemann_params(*scheme);
+  a.P = riemann_params(scheme);
   a.path_cap = RIEMANN_PATH_CAP;
-  a.scratch_slots = n;
+  // one path-scratch slot (24 KiB) per thread, at most 148 x 8 x 128 threads
+  const long long max_slots = 148LL * 8 * 128;
+  a.scratch_slots = std::min<long long>(((long long)n + 127) / 128 * 128, max_slots);
   // One allocation holds every array, each starting on a 256-byte boundary.
   auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t nn = (size_t)n;
+  const size_t eos_bytes = heos.size() * sizeof(Eos<double>);
   const size_t total = 5 * rup(nn * 40) + rup(nn * 24) + 5 * rup(nn * 4) + (warm ? rup(nn * 8) : 0) +
-                       rup(sizeof(heos));
-  size_t bytes_scratch = nn * 2 * 3 * RIEMANN_PATH_CAP * sizeof(double);
+                       rup(eos_bytes);
+  size_t bytes_scratch = (size_t)a.scratch_slots * 2 * 3 * RIEMANN_PATH_CAP * sizeof(double);
   char* buf = nullptr;
   m2cg_status st = M2CG_OK;
   if (cudaMalloc((void**)&buf, total) != cudaSuccess || cudaMalloc((void**)&a.scratch, bytes_scratch) != cudaSuccess) {
     cudaFree(buf);
     cudaStreamDestroy(s);
+    set_last_error("m2cg_riemann_batch: device allocation failed");
     return M2CG_ERR_NOMEM;
   }
   char* p = buf;
@@ -123,7 +130,7 @@ extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_
   double* dwarm = warm ? (double*)take(nn * 8) : nullptr;
   double* dVs = (double*)take(nn * 40); double* dVsm = (double*)take(nn * 40); double* dVsp = (double*)take(nn * 40);
   int* did = (int*)take(nn * 4); int* diters = (int*)take(nn * 4); int* derr = (int*)take(nn * 4);
-  Eos<double>* deos = (Eos<double>*)take(sizeof(heos));
+  Eos<double>* deos = (Eos<double>*)take(eos_bytes);
   cudaError_t e = cudaSuccess;
   auto ck = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
   if ((size_t)(p - buf) == total) {  // the carve-up stays inside the allocation
@@ -133,7 +140,7 @@ extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_
     ck(cudaMemcpyAsync(didl, idl, nn * 4, cudaMemcpyHostToDevice, s));
     ck(cudaMemcpyAsync(didr, idr, nn * 4, cudaMemcpyHostToDevice, s));
     if (warm) ck(cudaMemcpyAsync(dwarm, warm, nn * 8, cudaMemcpyHostToDevice, s));
-    ck(cudaMemcpyAsync(deos, heos, sizeof(heos), cudaMemcpyHostToDevice, s));
+    ck(cudaMemcpyAsync(deos, heos.data(), eos_bytes, cudaMemcpyHostToDevice, s));
     a.VL = dVL; a.VR = dVR; a.dir = ddir; a.idl = didl; a.idr = didr; a.warm = dwarm;
     a.Vs = dVs; a.Vsm = dVsm; a.Vsp = dVsp; a.id = did; a.iters = diters; a.err = derr; a.eos = deos;
     if (e == cudaSuccess) ck(launch_riemann_batch(a, s));
@@ -159,5 +166,41 @@ extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_
   cudaFree(buf);
   cudaFree(a.scratch);
   cudaStreamDestroy(s);
+  return st;
+}
+
+extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_material* mats, int nmat, int n,
+                                          const double* VL, const int* idl, const double* VR, const int* idr,
+                                          const double* dir, const double* warm, double* Vs, int* id, double* Vsm,
+                                          double* Vsp, int* iters, int* err) {
+  if (!scheme || !mats || nmat < 1 || nmat > MAXMAT_RIEMANN || n < 0 || !VL || !idl || !VR || !idr || !dir || !Vs ||
+      !id || !Vsm || !Vsp || !err)
+    return M2CG_ERR_ARG;
+  if (n == 0) return M2CG_OK;
+  for (int q = 0; q < n; q++)
+    if (idl[q] < 0 || idl[q] >= nmat || idr[q] < 0 || idr[q] >= nmat) return M2CG_ERR_ARG;
+  std::vector<Eos<double>> heos(MAXMAT_RIEMANN);
+  for (int m = 0; m < nmat; m++) heos[m] = eos_of_material(mats[m]);
+  return riemann_host(*scheme, heos, n, VL, idl, VR, idr, dir, warm, Vs, id, Vsm, Vsp, iters, err);
+}
+
+extern "C" m2cg_status m2cg_riemann_batch_pairs(const m2cg_scheme* scheme, const m2cg_material* mats, int n,
+                                                const double* VL, const double* VR, const double* dir,
+                                                const double* warm, double* Vs, int* id, double* Vsm, double* Vsp,
+                                                int* iters, int* err) {
+  if (!scheme || !mats || n < 0 || !VL || !VR || !dir || !Vs || !id || !Vsm || !Vsp || !err) return M2CG_ERR_ARG;
+  if (n == 0) return M2CG_OK;
+  std::vector<Eos<double>> heos(2 * (size_t)n);
+  std::vector<int> idl(n), idr(n);
+  for (int q = 0; q < n; q++) {
+    heos[2 * q] = eos_of_material(mats[2 * q]);
+    heos[2 * q + 1] = eos_of_material(mats[2 * q + 1]);
+    idl[q] = 2 * q;
+    idr[q] = 2 * q + 1;
+  }
+  m2cg_status st = riemann_host(*scheme, heos, n, VL, idl.data(), VR, idr.data(), dir, warm, Vs, id, Vsm, Vsp, iters,
+                                err);
+  if (st == M2CG_OK)
+    for (int q = 0; q < n; q++) id[q] = id[q] & 1;
   return st;
 }

@@ -32,6 +32,10 @@ class Counters(C.Structure):
         "clipped_cells", "reinit_calls", "kernel_launches", "unresolved_cells")]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("cells_per_block", C.c_int), ("threads_per_block", C.c_int), ("use_graph", C.c_int)]
+
+
 def lib():
     """Load libm2c_gpu.so (fails loudly when it is missing)."""
     global _lib
@@ -58,6 +62,18 @@ def lib():
     L.m2cg_riemann_batch.argtypes = [C.POINTER(abi.Scheme), C.POINTER(abi.Material), C.c_int, C.c_int, dp, ip, dp,
                                      ip, dp, dp, dp, ip, dp, dp, ip, ip]
     L.m2cg_riemann_batch.restype = C.c_int
+    L.m2cg_riemann_batch_pairs.argtypes = [C.POINTER(abi.Scheme), C.POINTER(abi.Material), C.c_int, dp, dp, dp, dp,
+                                           dp, ip, dp, dp, ip, ip]
+    L.m2cg_riemann_batch_pairs.restype = C.c_int
+    L.m2cg_batch_create.argtypes = [C.POINTER(abi.Scheme), C.c_int, ip, C.POINTER(abi.Material), dp, dp,
+                                    C.POINTER(BatchTuning), C.POINTER(vp)]
+    L.m2cg_batch_run.argtypes = [vp, C.c_int]
+    L.m2cg_batch_download.argtypes = [vp, dp, ip, dp]
+    L.m2cg_batch_get_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
+    L.m2cg_batch_get_counters.argtypes = [vp, C.POINTER(Counters)]
+    L.m2cg_batch_tube_errors.argtypes = [vp, ip]
+    L.m2cg_batch_time_steps.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
+    L.m2cg_batch_destroy.argtypes = [vp]
     L.m2cg_set_device.argtypes = [C.c_int]
     L.m2cg_set_device.restype = C.c_int
     L.m2cg_default_scheme.argtypes = [C.POINTER(abi.Scheme)]
@@ -65,7 +81,9 @@ def lib():
     L.m2cg_default_levelset.argtypes = [C.POINTER(abi.LevelSet)]
     for name in ("m2cg_create", "m2cg_destroy", "m2cg_upload_state", "m2cg_download_state", "m2cg_compute_dt",
                  "m2cg_compute_residual", "m2cg_advance", "m2cg_run", "m2cg_get_counters", "m2cg_time_steps",
-                 "m2cg_get_stream", "m2cg_profile_stages"):
+                 "m2cg_get_stream", "m2cg_profile_stages", "m2cg_batch_create", "m2cg_batch_run",
+                 "m2cg_batch_download", "m2cg_batch_get_tuning", "m2cg_batch_get_counters",
+                 "m2cg_batch_tube_errors", "m2cg_batch_time_steps", "m2cg_batch_destroy"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L
@@ -86,6 +104,33 @@ def riemann_batch(s, mats, VL, idl, VR, idr, dirs, warm=None):
                                    abi.iptr(idr), abi.dptr(dirs), abi.dptr(warm), abi.dptr(Vs), abi.iptr(mid),
                                    abi.dptr(Vsm), abi.dptr(Vsp), abi.iptr(it), abi.iptr(err)))
     return Vs, mid, Vsm, Vsp, it, err
+
+
+def riemann_batch_pairs(s, mats, VL, VR, dirs, warm=None):
+    """Exact Riemann problems where problem q has material mats[2q] on the
+    left and mats[2q+1] on the right. Returns Vs, id (0 left, 1 right), Vsm,
+    Vsp, iterations, err."""
+    n = len(VL)
+    VL, VR, dirs = (np.ascontiguousarray(a, np.float64) for a in (VL, VR, dirs))
+    warm = None if warm is None else np.ascontiguousarray(warm, np.float64)
+    Vs, Vsm, Vsp = np.zeros((n, 5)), np.zeros((n, 5)), np.zeros((n, 5))
+    mid, it, err = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    arr = (abi.Material * len(mats))(*mats)
+    check(lib().m2cg_riemann_batch_pairs(C.byref(s), arr, n, abi.dptr(VL), abi.dptr(VR), abi.dptr(dirs),
+                                         abi.dptr(warm), abi.dptr(Vs), abi.iptr(mid), abi.dptr(Vsm), abi.dptr(Vsp),
+                                         abi.iptr(it), abi.iptr(err)))
+    return Vs, mid, Vsm, Vsp, it, err
+
+
+def tube_rejects(s):
+    """reject() for cases.tubes: tubes whose initial interface Riemann problem
+    the solver reports as failed or path-overflowing are redrawn."""
+    def reject(mats, VL, VR):
+        dirs = np.zeros((len(VL), 3))
+        dirs[:, 0] = 1.0
+        err = riemann_batch_pairs(s, mats, VL, VR, dirs)[5]
+        return err != 0
+    return reject
 
 
 def set_device(device):
@@ -173,6 +218,76 @@ class Solver:
     def close(self):
         if getattr(self, "h", None):
             lib().m2cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Batched 1D two-material shock tubes advanced together on the GPU
+    (m2cg_batch_*): tube t has len[t] cells on [0, 1], materials mats[2t]
+    (left, phi > 0) and mats[2t+1] (right), left/right states VL[t], VR[t],
+    INLET/OUTLET ghosts holding those states. Each tube is what one reference
+    run of the same setup computes (TimeIntegratorRK2/RK3, MultiPhaseOperator)."""
+
+    def __init__(self, s, lens, mats, VL, VR, cells_per_block=0, threads_per_block=0, use_graph=1):
+        L = lib()
+        self.lens = np.ascontiguousarray(lens, np.int32)
+        self.ntubes = len(self.lens)
+        self.ncell = int(self.lens.sum())
+        VL = np.ascontiguousarray(VL, np.float64)
+        VR = np.ascontiguousarray(VR, np.float64)
+        arr = (abi.Material * len(mats))(*mats)
+        tun = BatchTuning(cells_per_block, threads_per_block, use_graph)
+        h = C.c_void_p()
+        check(L.m2cg_batch_create(C.byref(s), self.ntubes, abi.iptr(self.lens), arr, abi.dptr(VL), abi.dptr(VR),
+                                  C.byref(tun), C.byref(h)))
+        self.h = h
+
+    def run(self, nsteps):
+        check(lib().m2cg_batch_run(self.h, nsteps))
+
+    def time_steps(self, nsteps, check_errors=True):
+        """Device time (ms) of nsteps steps. With check_errors=False a tube
+        error does not raise: the time is returned and tube_errors() tells
+        which tubes failed."""
+        ms = C.c_float(-1.0)
+        st = lib().m2cg_batch_time_steps(self.h, nsteps, C.byref(ms))
+        if st and (check_errors or ms.value < 0):
+            check(st)
+        return ms.value
+
+    def download(self):
+        """Returns (list of per-tube V arrays [len, 5], list of ID arrays, t per tube)."""
+        V = np.empty((self.ncell, 5))
+        ID = np.empty(self.ncell, np.int32)
+        t = np.empty(self.ntubes)
+        check(lib().m2cg_batch_download(self.h, abi.dptr(V), abi.iptr(ID), abi.dptr(t)))
+        cuts = np.cumsum(self.lens)[:-1]
+        return np.split(V, cuts), np.split(ID, cuts), t
+
+    def tuning(self):
+        tun = BatchTuning()
+        check(lib().m2cg_batch_get_tuning(self.h, C.byref(tun)))
+        return {n: getattr(tun, n) for n, _ in BatchTuning._fields_}
+
+    def counters(self):
+        c = Counters()
+        check(lib().m2cg_batch_get_counters(self.h, C.byref(c)))
+        return {n: getattr(c, n) for n, _ in Counters._fields_}
+
+    def tube_errors(self):
+        codes = np.zeros(self.ntubes, np.int32)
+        check(lib().m2cg_batch_tube_errors(self.h, abi.iptr(codes)))
+        return codes
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().m2cg_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -187,3 +187,40 @@ def PortCase(g, s, mats, ls=None):
 
 def PortPoint(s, mats):
     return _Point(_load(PORT_SO, "m2cport_"), "m2cport_", s, mats)
+
+
+def _tube_worker(args):
+    """One tube as one reference run (process-pool worker: a reference abort
+    ends only this process). args = (scheme field dict, n, two material field
+    tuples, VL, VR, nsteps); returns (V [n, 5], ID [n], t)."""
+    sd, n, mt, VL, VR, nsteps = args
+    from m2c_b200 import cases
+    s = abi.scheme(**sd)
+    mats = [abi.Material(*m) for m in mt]
+    g, ls, V, ID, PHI = cases.tube_case(n, VL, VR)
+    c = RefCase(g, s, mats, ls)
+    c.set_state(V, ID, PHI)
+    _, t = c.run(nsteps)
+    Vr, IDr, _ = c.get_state()
+    c.close()
+    return Vr[1, 1, 1:-1].copy(), IDr[1, 1, 1:-1].astype(np.int32), t
+
+
+def tubes(s, lens, mats, VL, VR, nsteps, which, processes=8):
+    """Reference runs of the selected tubes (indices `which`) of a batch, in
+    a spawned process pool. Returns a list of (V, ID, t) or None where the
+    reference process failed."""
+    import multiprocessing as mp
+    sd = {f: getattr(s, f) for f, _ in abi.Scheme._fields_}
+    field = lambda m: tuple(getattr(m, f) for f, _ in abi.Material._fields_)
+    jobs = [(sd, int(lens[t]), (field(mats[2 * t]), field(mats[2 * t + 1])), tuple(VL[t]), tuple(VR[t]), nsteps)
+            for t in which]
+    out = []
+    with mp.get_context("spawn").Pool(min(processes, len(jobs))) as pool:
+        res = [pool.apply_async(_tube_worker, (j,)) for j in jobs]
+        for r in res:
+            try:
+                out.append(r.get(timeout=600))
+            except Exception:
+                out.append(None)
+    return out
