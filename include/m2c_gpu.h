@@ -109,6 +109,9 @@ typedef struct {
   int riem_maxits_main, riem_maxits_bracket, riem_maxits_shock, riem_nsteps_rarefaction;
   double riem_tol_main, riem_tol_shock, riem_tol_rarefaction;
   double riem_min_pressure, riem_failure_threshold, riem_pressure_at_failure;
+  /* Warm start of the exact Riemann solve (no reference counterpart): the
+   * bracket tried around a proposed star pressure p is [p(1-d), p(1+d)]. */
+  double riem_warm_delta;
 } m2cg_scheme;
 
 /* One level set (LevelSetSchemeData, IoData.h:653-679; reinit
@@ -183,6 +186,7 @@ typedef struct {
   long long reinit_calls;
   long long kernel_launches;
   long long unresolved_cells;    /* cells that changed material with no usable star state */
+  long long riemann_evaluations; /* star-state evaluations at trial pressures (bracketing + secant) */
 } m2cg_counters;
 m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
 
@@ -223,11 +227,12 @@ m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_material* m
 
 /* The same solve where every problem carries its own material pair:
  * problem q has material mats[2q] on the left and mats[2q+1] on the right;
- * id[q] is 0 (left material) or 1 (right). Host pointers. */
+ * id[q] is 0 (left material) or 1 (right); evals (optional) counts the
+ * star-state evaluations at trial pressures. Host pointers. */
 m2cg_status m2cg_riemann_batch_pairs(const m2cg_scheme* scheme, const m2cg_material* mats, int n,
                                      const double* VL, const double* VR, const double* dir,
                                      const double* warm, double* Vs, int* id, double* Vsm,
-                                     double* Vsp, int* iters, int* err);
+                                     double* Vsp, int* iters, int* evals, int* err);
 
 /* The same batched Riemann solve for callers that cannot allocate device
  * memory: a host application whose memory pool owns the whole GPU, or a
@@ -254,6 +259,46 @@ m2cg_status m2cg_riemann_batch_noalloc(const m2cg_scheme* scheme, const m2cg_mat
                                        const int* idr, const double* dir, const double* warm,
                                        double* Vs, int* id, double* Vsm, double* Vsp, int* iters,
                                        int* err, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Learned warm start for the interface Riemann solve (no counterpart in the
+ * reference). A 16 -> 64 -> 64 -> 64 -> 1 tanh MLP maps dimensionless
+ * features of a problem to log(pstar / pac), pac the acoustic estimate the
+ * solver's bracket search starts from; where the proposal p departs from pac
+ * by more than riem_warm_delta, p(1 -+ riem_warm_delta) replaces the
+ * acoustic starting points of that search. The solver's own iteration and stopping test are
+ * unchanged, so results agree with the cold solve within tol_main.
+ * Training runs on the GPU (FP32 forward + backward kernels, Adam);
+ * inference runs BF16 on tensor cores with FP32 accumulation.
+ * ------------------------------------------------------------------------- */
+#define M2CG_MLP_INPUTS 16
+#define M2CG_MLP_NPARAMS 9473  /* W1[64][16] b1[64] W2[64][64] b2 W3[64][64] b3 w4[64] b4 */
+#define M2CG_MLP_NNORM 34      /* xmean[16] xstd[16] ymean ystd */
+typedef struct m2cg_mlp m2cg_mlp;
+m2cg_status m2cg_mlp_create(unsigned long long seed, m2cg_mlp** out);
+m2cg_status m2cg_mlp_destroy(m2cg_mlp* m);
+m2cg_status m2cg_mlp_get_params(const m2cg_mlp* m, float* params, float* norm);
+m2cg_status m2cg_mlp_set_params(m2cg_mlp* m, const float* params, const float* norm);
+/* Mean-squared-error loss and its gradient with respect to the parameters
+ * for n network inputs Xn [n][16] and targets yn, both already normalised
+ * (host arrays); no update. */
+m2cg_status m2cg_mlp_loss_grad(m2cg_mlp* m, const float* Xn, const float* yn, int n, float* loss,
+                               float* grad);
+/* Train on raw features X [n][16] and targets y = log(pstar / pac): the
+ * normalisation is set from the data, then `steps` Adam steps of `batch`
+ * samples (cosine-decayed learning rate from lr). final_loss: mean loss of
+ * the last 5% of steps, in normalised units. */
+m2cg_status m2cg_mlp_train(m2cg_mlp* m, const float* X, const float* y, int n, int steps, int batch,
+                           float lr, unsigned long long seed, float* final_loss);
+/* Features of problems with per-pair materials (as m2cg_riemann_batch_pairs):
+ * X [n][16], base pressure pac [n], valid [n] (0 where no proposal can be made). */
+m2cg_status m2cg_mlp_features_pairs(const m2cg_material* mats, int n, const double* VL,
+                                    const double* VR, const double* dir, float* X, double* P, int* valid);
+/* Network output (target units) for raw feature rows, BF16 tensor cores. */
+m2cg_status m2cg_mlp_infer(m2cg_mlp* m, const float* X, const int* valid, int n, float* y);
+/* Proposed star pressures for per-pair problems (NaN where none). */
+m2cg_status m2cg_mlp_predict_pairs(m2cg_mlp* m, const m2cg_material* mats, int n, const double* VL,
+                                   const double* VR, const double* dir, double* p);
 
 /* ---------------------------------------------------------------------------
  * Batched 1D two-material shock tubes of uneven lengths, all advanced in one
@@ -290,6 +335,10 @@ m2cg_status m2cg_batch_tube_errors(m2cg_batch* b, int* codes);
  * the batch's stream). *ms is written even when a tube reported an error
  * (the status then says which error; m2cg_batch_tube_errors says where). */
 m2cg_status m2cg_batch_time_steps(m2cg_batch* b, int nsteps, float* ms);
+/* Attach a trained network (NULL detaches): every interface Riemann solve
+ * of the batch then starts from its proposal. The network must outlive the
+ * batch's use of it. */
+m2cg_status m2cg_batch_set_mlp(m2cg_batch* b, const m2cg_mlp* m);
 m2cg_status m2cg_batch_destroy(m2cg_batch* b);
 
 #ifdef __cplusplus

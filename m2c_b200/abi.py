@@ -58,7 +58,7 @@ class Scheme(C.Structure):
         ("riem_nsteps_rarefaction", C.c_int),
         ("riem_tol_main", C.c_double), ("riem_tol_shock", C.c_double), ("riem_tol_rarefaction", C.c_double),
         ("riem_min_pressure", C.c_double), ("riem_failure_threshold", C.c_double),
-        ("riem_pressure_at_failure", C.c_double),
+        ("riem_pressure_at_failure", C.c_double), ("riem_warm_delta", C.c_double),
     ]
 
 
@@ -102,6 +102,7 @@ def scheme(**kw):
     s.riem_min_pressure = -1.0e8
     s.riem_failure_threshold = 0.2
     s.riem_pressure_at_failure = 1.0e-8
+    s.riem_warm_delta = 0.01
     for k, v in kw.items():
         if not hasattr(s, k):
             raise AttributeError(k)
@@ -154,3 +155,34 @@ def iptr(a):
         return None
     assert a.dtype == np.int32 and a.flags.c_contiguous
     return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+# numpy mirror of m2cg_material (C layout: int, padding, nine doubles)
+MATERIAL_DTYPE = np.dtype([("eos", "<i4"), ("gamma", "<f8"), ("p_c", "<f8"), ("b", "<f8"), ("q", "<f8"),
+                           ("rhomin", "<f8"), ("pmin", "<f8"), ("rhomax", "<f8"), ("pmax", "<f8"),
+                           ("failsafe_density", "<f8")], align=True)
+
+
+def material_table(gamma, p_c):
+    """Stiffened-gas materials as a MATERIAL_DTYPE array (fast path for
+    large per-problem material tables), with the IoData defaults."""
+    gamma = np.asarray(gamma, np.float64)
+    t = np.zeros(len(gamma), MATERIAL_DTYPE)
+    t["eos"] = EOS_SG
+    t["gamma"] = gamma
+    t["p_c"] = p_c
+    t["pmin"] = -DBL_MAX
+    t["rhomax"] = DBL_MAX
+    t["pmax"] = DBL_MAX
+    t["failsafe_density"] = 1.0e-10
+    return t
+
+
+def material_array(mats):
+    """Pointer to a C array of m2cg_material from a list of Material or a
+    MATERIAL_DTYPE numpy array (kept alive by the caller)."""
+    if isinstance(mats, np.ndarray):
+        assert mats.dtype == MATERIAL_DTYPE and mats.flags.c_contiguous
+        assert MATERIAL_DTYPE.itemsize == C.sizeof(Material)
+        return mats.ctypes.data_as(C.POINTER(Material))
+    return (Material * len(mats))(*mats)

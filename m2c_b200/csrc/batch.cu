@@ -33,12 +33,15 @@
 
 #include "../../include/m2c_gpu.h"
 #include "fd3.cuh"
+#include "mlp.cuh"
 #include "riemann_batch.h"
 #include "stage.cuh"
 
 namespace m2c {
 
 void set_last_error(const char* msg);
+cudaError_t mlp_warm_device(const m2cg_mlp* m, cudaStream_t s, const float* X, const int* valid, const double* P,
+                            int n, float* y, double* warm);
 
 constexpr int TUBE_IFACE_CAP = 8;        // interface faces tracked per tube
 constexpr int TUBE_RIEMANN_THREADS = 16384; // threads of the Riemann kernel (each owns path scratch)
@@ -68,7 +71,7 @@ struct TubeArgs {
   uint8_t* rsValid;         // [T][CAP]
   int* clip;                // [T][4] clip flag per stage
   int* terr;                // [T] first error code of each tube
-  unsigned long long* cnt;  // [0] Riemann calls, [1] iterations, [2] errors, [3] unresolved, [4] clipped stages
+  unsigned long long* cnt;  // [0] Riemann calls, [1] iterations, [2] errors, [3] unresolved, [5] evaluations
   DevError* err;
   // scheme
   int flux, limiter, rec_linear, slope_zero, mp_flux, rk, vak;
@@ -199,9 +202,36 @@ __global__ void k_tube_riemann(TubeArgs A, TubeStage S) {
     }
     atomicAdd(&A.cnt[0], 1ull);
     atomicAdd(&A.cnt[1], (unsigned long long)rs.iterations);
+    atomicAdd(&A.cnt[5], (unsigned long long)rs.evaluations);
     if (r != RIEM_OK) atomicAdd(&A.cnt[2], 1ull);
     if (r & RIEM_PATH_OVERFLOW) tube_fail(A, t, ERR_ITER_CAP, (int)(o + i), 7);
     if (bad) tube_fail(A, t, ERR_STATE, (int)(o + i), 8);
+  }
+}
+
+// Features of every interface problem of this stage (the states the Riemann
+// kernel will use), for the learned warm start; slots without an interface
+// face are marked invalid.
+__global__ void k_tube_features(TubeArgs A, TubeStage S, float* X, double* P, int* valid) {
+  const long long total = (long long)A.ntubes * TUBE_IFACE_CAP;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total;
+       w += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(w / TUBE_IFACE_CAP), k = (int)(w - (long long)t * TUBE_IFACE_CAP);
+    int ok = 0;
+    if (k < A.nif[t]) {
+      const long long o = A.off[t];
+      const int i = A.iface[w];
+      const uint8_t idL = A.id[o + i - 1], idR = A.id[o + i];
+      const Eos<double>* eos = A.eos + 2 * t;
+      double VL[5], VR[5];
+      tube_state(A, S, eos[idL], o + i - 1, VL);
+      tube_state(A, S, eos[idR], o + i, VR);
+      const double dir[3] = {1.0, 0.0, 0.0};
+      double Pq = 0.0;
+      ok = mlp_features(eos[idL], eos[idR], VL, VR, dir, X + w * MLP_IN, &Pq) ? 1 : 0;
+      P[w] = Pq;
+    }
+    valid[w] = ok;
   }
 }
 
@@ -587,6 +617,13 @@ struct m2cg_batch {
   std::vector<double> hV, hphi;
   std::vector<uint8_t> hid;
   long long launches = 0;
+  // learned warm start (optional)
+  const m2cg_mlp* mlp = nullptr;
+  float* fX = nullptr;
+  double* fP = nullptr;
+  int* fvalid = nullptr;
+  float* fy = nullptr;
+  double* fwarm = nullptr;
 };
 
 static m2cg_status bfail(m2cg_status st, const char* msg) {
@@ -659,6 +696,11 @@ static cudaError_t enqueue_step(m2cg_batch* b, int cur) {
     S.final_stage = s == r;
     S.cur = cur;
     rk_coefs(r, s, S.a_prev, S.a_un, S.bdt_coef);
+    if (b->mlp) {
+      const int nslot = b->ntubes * TUBE_IFACE_CAP;
+      k_tube_features<<<(nslot + 255) / 256, 256, 0, b->stream>>>(A, S, b->fX, b->fP, b->fvalid);
+      mlp_warm_device(b->mlp, b->stream, b->fX, b->fvalid, b->fP, nslot, b->fy, b->fwarm);
+    }
     k_tube_riemann<<<TUBE_RIEMANN_THREADS / 64, 64, 0, b->stream>>>(A, S);
     k_tube_stage<<<b->stage_grid, b->stage_threads, smem, b->stream>>>(A, S);
   }
@@ -962,7 +1004,7 @@ extern "C" m2cg_status m2cg_batch_run(m2cg_batch* b, int nsteps) {
   }
   if (e != cudaSuccess) return bfail(M2CG_ERR_CUDA, cudaGetErrorString(e));
   b->steps += nsteps;
-  b->launches += (long long)nsteps * (2 + 2 * b->scheme.rk_order);
+  b->launches += (long long)nsteps * (2 + (b->mlp ? 5 : 2) * b->scheme.rk_order);
   return batch_check(b);
 }
 
@@ -1012,6 +1054,7 @@ extern "C" m2cg_status m2cg_batch_get_counters(m2cg_batch* b, m2cg_counters* c) 
   c->riemann_errors = (long long)h[2];
   c->unresolved_cells = (long long)h[3];
   c->kernel_launches = b->launches;
+  c->riemann_evaluations = (long long)h[5];
   return M2CG_OK;
 }
 
@@ -1046,15 +1089,37 @@ extern "C" m2cg_status m2cg_batch_time_steps(m2cg_batch* b, int nsteps, float* m
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->steps += nsteps;
-  b->launches += (long long)nsteps * (2 + 2 * b->scheme.rk_order);
+  b->launches += (long long)nsteps * (2 + (b->mlp ? 5 : 2) * b->scheme.rk_order);
   if (st) return st;
   return batch_check(b);
+}
+
+extern "C" m2cg_status m2cg_batch_set_mlp(m2cg_batch* b, const m2cg_mlp* m) {
+  if (!b) return bfail(M2CG_ERR_ARG, "null argument");
+  cudaStreamSynchronize(b->stream);
+  const size_t nslot = (size_t)b->ntubes * TUBE_IFACE_CAP;
+  if (m && !b->fX) {
+    if (cudaMalloc((void**)&b->fX, nslot * MLP_IN * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&b->fP, nslot * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&b->fvalid, nslot * sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&b->fy, nslot * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&b->fwarm, nslot * sizeof(double)) != cudaSuccess)
+      return bfail(M2CG_ERR_NOMEM, "warm-start buffers: allocation failed");
+  }
+  b->mlp = m;
+  b->A.warm = m ? b->fwarm : nullptr;
+  if (b->tuning.use_graph) {
+    cudaError_t e = build_graphs(b);
+    if (e != cudaSuccess) return bfail(M2CG_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return M2CG_OK;
 }
 
 extern "C" m2cg_status m2cg_batch_destroy(m2cg_batch* b) {
   if (!b) return M2CG_OK;
   if (b->stream) cudaStreamSynchronize(b->stream);
   destroy_graphs(b);
+  cudaFree(b->fX); cudaFree(b->fP); cudaFree(b->fvalid); cudaFree(b->fy); cudaFree(b->fwarm);
   for (char* p : b->allocs) cudaFree(p);
   if (b->items) cudaFree(b->items);
   if (b->stream) cudaStreamDestroy(b->stream);

@@ -74,6 +74,7 @@ struct Multiphase {
   int stage = 0;
   // host-side counters
   long long riemann_calls = 0, riemann_iterations = 0, riemann_errors = 0, unresolved = 0, reinit_calls = 0;
+  long long riemann_evaluations = 0;
   double* reinit_buf = nullptr;  // reinitialisation work arrays
   double reinit_cfl = 0.8;       // pseudo-time CFL, reduced on failed attempts
   long long reinit_iterations = 0;
@@ -224,6 +225,7 @@ __global__ void k_iface_riemann(IfaceRiemannArgs a) {
     if (r & RIEM_PATH_OVERFLOW) report(a.err, ERR_ITER_CAP, q, 7);
     if (bad) report(a.err, ERR_STATE, q, 8);
     atomicAdd(&a.counts[4], rs.iterations);
+    atomicAdd(&a.counts[6], rs.evaluations);
     atomicAdd(&a.counts[5], 1);
   }
 }
@@ -637,13 +639,14 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
   k_state_update<<<1, 32, 0, s>>>(ua);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
   // step counters (one small read-back per step)
-  int hc[6], hn[2];
+  int hc[7], hn[2];
   cudaMemcpyAsync(hc, mp->counts, sizeof hc, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hn, mp->nchanged, sizeof hn, cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
   mp->riemann_calls += hc[5];
   mp->riemann_iterations += hc[4];
   mp->riemann_errors += hc[3];
+  mp->riemann_evaluations += hc[6];
   mp->unresolved += hn[1];
   if (hc[2]) return M2CG_ERR_ITER_CAP;  // interface capacity exceeded
   if (counters) counters->kernel_launches += 8 + 3 * mp->scheme.rk_order;
@@ -656,4 +659,5 @@ void multiphase_counters(const Multiphase* mp, m2cg_counters* out) {
   out->riemann_errors = mp->riemann_errors;
   out->reinit_calls = mp->reinit_calls;
   out->unresolved_cells = mp->unresolved;
+  out->riemann_evaluations = mp->riemann_evaluations;
 }

@@ -44,6 +44,7 @@ __global__ void k_riemann_batch(RiemannBatchArgs a) {
     }
     a.id[q] = id;
     if (a.iters) a.iters[q] = rs.iterations;
+    if (a.evals) a.evals[q] = rs.evaluations;
     a.err[q] = r | (bad ? 4 : 0);
   }
 }
@@ -60,6 +61,7 @@ RiemannParams riemann_params(const m2cg_scheme& s) {
   P.min_pressure = s.riem_min_pressure;
   P.failure_threshold = s.riem_failure_threshold;
   P.pressure_at_failure = s.riem_pressure_at_failure;
+  P.warm_delta = s.riem_warm_delta;
   return P;
 }
 
@@ -94,7 +96,7 @@ static Eos<double> eos_of_material(const m2cg_material& m) {
 static m2cg_status riemann_host(const m2cg_scheme& scheme, const std::vector<Eos<double>>& heos, int n,
                                 const double* VL, const int* idl, const double* VR, const int* idr,
                                 const double* dir, const double* warm, double* Vs, int* id, double* Vsm,
-                                double* Vsp, int* iters, int* err) {
+                                double* Vsp, int* iters, int* evals, int* err) {
   cudaStream_t s;
   if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
     set_last_error("m2cg_riemann_batch: cudaStreamCreate failed (no CUDA device?)");
@@ -112,7 +114,7 @@ static m2cg_status riemann_host(const m2cg_scheme& scheme, const std::vector<Eos
   auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t nn = (size_t)n;
   const size_t eos_bytes = heos.size() * sizeof(Eos<double>);
-  const size_t total = 5 * rup(nn * 40) + rup(nn * 24) + 5 * rup(nn * 4) + (warm ? rup(nn * 8) : 0) +
+  const size_t total = 5 * rup(nn * 40) + rup(nn * 24) + 6 * rup(nn * 4) + (warm ? rup(nn * 8) : 0) +
                        rup(eos_bytes);
   size_t bytes_scratch = (size_t)a.scratch_slots * 2 * 3 * RIEMANN_PATH_CAP * sizeof(double);
   char* buf = nullptr;
@@ -130,6 +132,7 @@ static m2cg_status riemann_host(const m2cg_scheme& scheme, const std::vector<Eos
   double* dwarm = warm ? (double*)take(nn * 8) : nullptr;
   double* dVs = (double*)take(nn * 40); double* dVsm = (double*)take(nn * 40); double* dVsp = (double*)take(nn * 40);
   int* did = (int*)take(nn * 4); int* diters = (int*)take(nn * 4); int* derr = (int*)take(nn * 4);
+  int* devals = (int*)take(nn * 4);
   Eos<double>* deos = (Eos<double>*)take(eos_bytes);
   cudaError_t e = cudaSuccess;
   auto ck = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
@@ -142,7 +145,7 @@ static m2cg_status riemann_host(const m2cg_scheme& scheme, const std::vector<Eos
     if (warm) ck(cudaMemcpyAsync(dwarm, warm, nn * 8, cudaMemcpyHostToDevice, s));
     ck(cudaMemcpyAsync(deos, heos.data(), eos_bytes, cudaMemcpyHostToDevice, s));
     a.VL = dVL; a.VR = dVR; a.dir = ddir; a.idl = didl; a.idr = didr; a.warm = dwarm;
-    a.Vs = dVs; a.Vsm = dVsm; a.Vsp = dVsp; a.id = did; a.iters = diters; a.err = derr; a.eos = deos;
+    a.Vs = dVs; a.Vsm = dVsm; a.Vsp = dVsp; a.id = did; a.iters = diters; a.evals = devals; a.err = derr; a.eos = deos;
     if (e == cudaSuccess) ck(launch_riemann_batch(a, s));
     if (e == cudaSuccess) {
       ck(cudaMemcpyAsync(Vs, dVs, nn * 40, cudaMemcpyDeviceToHost, s));
@@ -150,6 +153,7 @@ static m2cg_status riemann_host(const m2cg_scheme& scheme, const std::vector<Eos
       ck(cudaMemcpyAsync(Vsp, dVsp, nn * 40, cudaMemcpyDeviceToHost, s));
       ck(cudaMemcpyAsync(id, did, nn * 4, cudaMemcpyDeviceToHost, s));
       if (iters) ck(cudaMemcpyAsync(iters, diters, nn * 4, cudaMemcpyDeviceToHost, s));
+      if (evals) ck(cudaMemcpyAsync(evals, devals, nn * 4, cudaMemcpyDeviceToHost, s));
       ck(cudaMemcpyAsync(err, derr, nn * 4, cudaMemcpyDeviceToHost, s));
     }
     ck(cudaStreamSynchronize(s));
@@ -181,13 +185,13 @@ extern "C" m2cg_status m2cg_riemann_batch(const m2cg_scheme* scheme, const m2cg_
     if (idl[q] < 0 || idl[q] >= nmat || idr[q] < 0 || idr[q] >= nmat) return M2CG_ERR_ARG;
   std::vector<Eos<double>> heos(MAXMAT_RIEMANN);
   for (int m = 0; m < nmat; m++) heos[m] = eos_of_material(mats[m]);
-  return riemann_host(*scheme, heos, n, VL, idl, VR, idr, dir, warm, Vs, id, Vsm, Vsp, iters, err);
+  return riemann_host(*scheme, heos, n, VL, idl, VR, idr, dir, warm, Vs, id, Vsm, Vsp, iters, nullptr, err);
 }
 
 extern "C" m2cg_status m2cg_riemann_batch_pairs(const m2cg_scheme* scheme, const m2cg_material* mats, int n,
                                                 const double* VL, const double* VR, const double* dir,
                                                 const double* warm, double* Vs, int* id, double* Vsm, double* Vsp,
-                                                int* iters, int* err) {
+                                                int* iters, int* evals, int* err) {
   if (!scheme || !mats || n < 0 || !VL || !VR || !dir || !Vs || !id || !Vsm || !Vsp || !err) return M2CG_ERR_ARG;
   if (n == 0) return M2CG_OK;
   std::vector<Eos<double>> heos(2 * (size_t)n);
@@ -199,7 +203,7 @@ extern "C" m2cg_status m2cg_riemann_batch_pairs(const m2cg_scheme* scheme, const
     idr[q] = 2 * q + 1;
   }
   m2cg_status st = riemann_host(*scheme, heos, n, VL, idl.data(), VR, idr.data(), dir, warm, Vs, id, Vsm, Vsp, iters,
-                                err);
+                                evals, err);
   if (st == M2CG_OK)
     for (int q = 0; q < n; q++) id[q] = id[q] & 1;
   return st;

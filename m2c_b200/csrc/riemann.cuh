@@ -35,6 +35,7 @@ namespace m2c {
 struct RiemannParams {
   int maxIts_main, maxIts_bracket, maxIts_shock, numSteps_rarefaction;
   double tol_main, tol_shock, tol_rarefaction, min_pressure, failure_threshold, pressure_at_failure;
+  double warm_delta;  // half-width of the warm-start bracket, relative to the proposed star pressure
 };
 
 // result flags
@@ -66,6 +67,8 @@ struct RiemannSolver {
   const Eos<double>* eos;  // material table indexed by id
   RPath path1, path3;
   int iterations;          // outer secant iterations of the main loop
+  double warm = NAN;       // proposed star pressure of the current solve (NaN: none)
+  mutable int evaluations; // star-state evaluations at a trial pressure (bracketing + main loop)
 
   // Rarefaction_OneStepRK4 (ExactRiemannSolverBase.cpp:1729-1852)
   M2C_HD bool rk_step(int wave, int id, double rho_0, double u_0, double p_0, double dp, double& rho, double& u,
@@ -144,6 +147,7 @@ struct RiemannSolver {
   M2C_HD bool rho_u_star(int wave, RPath& path, double rho, double u, double p, double ps, int id, double rhos0,
                          double rhos1, double& rhos, double& us, bool* trans_rare, double* Vrare_x0) const {
     const Eos<double>& e = eos[id];
+    if (wave == 1) evaluations++;
     rhos = rho;
     us = u;
     if (p > ps) {  // rarefaction: numerical integration
@@ -403,8 +407,27 @@ struct RiemannSolver {
                               double cr, int idr, double& p0, double& rhol0, double& rhor0, double& ul0, double& ur0,
                               double& p1, double& rhol1, double& rhor1, double& ul1, double& ur1) {
     bool success = true;
-    int found = acoustic_points(rhol, ul, pl, cl, idl, rhor, ur, pr, cr, idr, p0, rhol0, rhor0, ul0, ur0, p1, rhol1,
-                                rhor1, ul1, ur1);
+    int found = 0;
+    // the acoustic (linearised) estimate the reference starts from
+    const double Cl0 = rhol * cl, Cr0 = rhor * cr;
+    const double pac = (Cr0 * pl + Cl0 * pr + Cl0 * Cr0 * (ul - ur)) / (Cl0 + Cr0);
+    if (isfinite(warm) && warm > 0.0 && P.warm_delta > 0.0 && !(fabs(warm - pac) <= P.warm_delta * fabs(pac))) {
+      // warm start: a proposal departing from the acoustic estimate by more
+      // than the bracket width supplies the two points warm (1 -+ d) in place
+      // of the acoustic estimates, when both are feasible; FindInitialInterval
+      // then expands them as it would expand the acoustic pair
+      p0 = warm * (1.0 - P.warm_delta);
+      p1 = warm * (1.0 + P.warm_delta);
+      if (rho_u_star(1, path1, rhol, ul, pl, p0, idl, rhol, (p0 > pl) ? rhol * 1.1 : rhol * 0.9, rhol0, ul0, nullptr,
+                     nullptr) &&
+          rho_u_star(3, path3, rhor, ur, pr, p0, idr, rhor, (p0 > pr) ? rhor * 1.1 : rhor * 0.9, rhor0, ur0, nullptr,
+                     nullptr) &&
+          rho_u_star(1, path1, rhol, ul, pl, p1, idl, rhol, rhol0, rhol1, ul1, nullptr, nullptr) &&
+          rho_u_star(3, path3, rhor, ur, pr, p1, idr, rhor, rhor0, rhor1, ur1, nullptr, nullptr))
+        return true;
+    }
+    found = acoustic_points(rhol, ul, pl, cl, idl, rhor, ur, pr, cr, idr, p0, rhol0, rhor0, ul0, ur0, p1, rhol1,
+                            rhor1, ul1, ur1);
     if (found == 2) return true;
     if (found != 1) {
       double dp = (pl != pr) ? fabs(pl - pr) : 0.5 * pl;
@@ -619,15 +642,19 @@ struct RiemannSolver {
     Vsp[4] = p2;
   }
 
-  // ComputeRiemannSolution (59-342). warm_p (if finite and inside the first
-  // bracket) replaces the first secant iterate: the learned warm start; the
-  // safeguarded loop and its stopping test are unchanged.
+  // ComputeRiemannSolution (59-342).
+  // Warm start (no counterpart in the reference): a finite positive warm_p
+  // supplies the two starting points of the bracket search (see
+  // feasible_points); the bracket expansion, the safeguarded secant loop and
+  // its stopping test are the reference's, so a warm-started solve converges
+  // to the same root within tol_main.
   // Returns RIEM_OK or RIEM_FAILED (| RIEM_PATH_OVERFLOW); *bad_state set if a
   // state the reference aborts on was met.
   M2C_HD int solve(const double* dir, const double* Vm, int idl, const double* Vp, int idr, double* Vs, int& id,
                    double* Vsm, double* Vsp, double warm_p, bool& bad_state) {
     bad_state = false;
     iterations = 0;
+    evaluations = 0;
     double rhol = Vm[0];
     double ul = Vm[1] * dir[0] + Vm[2] * dir[1] + Vm[3] * dir[2];
     double pl = Vm[4];
@@ -658,6 +685,7 @@ struct RiemannSolver {
                Vsp, bad_state);
       return RIEM_OK;
     }
+    warm = warm_p;
     success = initial_interval(rhol, ul, pl, cl, idl, rhor, ur, pr, cr, idr, p0, rhol0, rhor0, ul0, ur0, p1, rhol1,
                                rhor1, ul1, ur1);
     if (!success) {
@@ -678,12 +706,9 @@ struct RiemannSolver {
     double err_p = 1.0, err_u = 1.0;
     p2 = p1;
     f2 = f1;
-    bool use_warm = isfinite(warm_p) && warm_p > p0 && warm_p < p1;
     for (iter = 0; iter < P.maxIts_main; iter++) {
       denom = f1 - f0;
-      if (iter == 0 && use_warm) {
-        p2 = warm_p;
-      } else if (denom == 0) {
+      if (denom == 0) {
         p2 = 0.5 * (p0 + p1);
       } else {
         p2 = p2 - f2 * (p1 - p0) / denom;

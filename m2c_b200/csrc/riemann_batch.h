@@ -28,6 +28,7 @@ struct RiemannBatchArgs {
   double* Vsp;
   int* id;
   int* iters;          // or nullptr
+  int* evals;          // or nullptr: star-state evaluations per problem
   int* err;
   double* scratch;     // integration paths: [slots][2 waves][path_cap][3]
   int path_cap;

@@ -29,7 +29,7 @@ class M2CError(RuntimeError):
 class Counters(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in (
         "steps", "cells_updated", "riemann_calls", "riemann_iterations", "riemann_errors",
-        "clipped_cells", "reinit_calls", "kernel_launches", "unresolved_cells")]
+        "clipped_cells", "reinit_calls", "kernel_launches", "unresolved_cells", "riemann_evaluations")]
 
 
 class BatchTuning(C.Structure):
@@ -63,7 +63,7 @@ def lib():
                                      ip, dp, dp, dp, ip, dp, dp, ip, ip]
     L.m2cg_riemann_batch.restype = C.c_int
     L.m2cg_riemann_batch_pairs.argtypes = [C.POINTER(abi.Scheme), C.POINTER(abi.Material), C.c_int, dp, dp, dp, dp,
-                                           dp, ip, dp, dp, ip, ip]
+                                           dp, ip, dp, dp, ip, ip, ip]
     L.m2cg_riemann_batch_pairs.restype = C.c_int
     L.m2cg_batch_create.argtypes = [C.POINTER(abi.Scheme), C.c_int, ip, C.POINTER(abi.Material), dp, dp,
                                     C.POINTER(BatchTuning), C.POINTER(vp)]
@@ -74,6 +74,17 @@ def lib():
     L.m2cg_batch_tube_errors.argtypes = [vp, ip]
     L.m2cg_batch_time_steps.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
     L.m2cg_batch_destroy.argtypes = [vp]
+    L.m2cg_batch_set_mlp.argtypes = [vp, vp]
+    fp = C.POINTER(C.c_float)
+    L.m2cg_mlp_create.argtypes = [C.c_ulonglong, C.POINTER(vp)]
+    L.m2cg_mlp_destroy.argtypes = [vp]
+    L.m2cg_mlp_get_params.argtypes = [vp, fp, fp]
+    L.m2cg_mlp_set_params.argtypes = [vp, fp, fp]
+    L.m2cg_mlp_loss_grad.argtypes = [vp, fp, fp, C.c_int, fp, fp]
+    L.m2cg_mlp_train.argtypes = [vp, fp, fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, fp]
+    L.m2cg_mlp_features_pairs.argtypes = [C.POINTER(abi.Material), C.c_int, dp, dp, dp, fp, dp, ip]
+    L.m2cg_mlp_infer.argtypes = [vp, fp, ip, C.c_int, fp]
+    L.m2cg_mlp_predict_pairs.argtypes = [vp, C.POINTER(abi.Material), C.c_int, dp, dp, dp, dp]
     L.m2cg_set_device.argtypes = [C.c_int]
     L.m2cg_set_device.restype = C.c_int
     L.m2cg_default_scheme.argtypes = [C.POINTER(abi.Scheme)]
@@ -83,7 +94,10 @@ def lib():
                  "m2cg_compute_residual", "m2cg_advance", "m2cg_run", "m2cg_get_counters", "m2cg_time_steps",
                  "m2cg_get_stream", "m2cg_profile_stages", "m2cg_batch_create", "m2cg_batch_run",
                  "m2cg_batch_download", "m2cg_batch_get_tuning", "m2cg_batch_get_counters",
-                 "m2cg_batch_tube_errors", "m2cg_batch_time_steps", "m2cg_batch_destroy"):
+                 "m2cg_batch_tube_errors", "m2cg_batch_time_steps", "m2cg_batch_destroy", "m2cg_batch_set_mlp",
+                 "m2cg_mlp_create", "m2cg_mlp_destroy", "m2cg_mlp_get_params", "m2cg_mlp_set_params",
+                 "m2cg_mlp_loss_grad", "m2cg_mlp_train", "m2cg_mlp_features_pairs", "m2cg_mlp_infer",
+                 "m2cg_mlp_predict_pairs"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L
@@ -109,17 +123,17 @@ def riemann_batch(s, mats, VL, idl, VR, idr, dirs, warm=None):
 def riemann_batch_pairs(s, mats, VL, VR, dirs, warm=None):
     """Exact Riemann problems where problem q has material mats[2q] on the
     left and mats[2q+1] on the right. Returns Vs, id (0 left, 1 right), Vsm,
-    Vsp, iterations, err."""
+    Vsp, iterations, evaluations, err."""
     n = len(VL)
     VL, VR, dirs = (np.ascontiguousarray(a, np.float64) for a in (VL, VR, dirs))
     warm = None if warm is None else np.ascontiguousarray(warm, np.float64)
     Vs, Vsm, Vsp = np.zeros((n, 5)), np.zeros((n, 5)), np.zeros((n, 5))
-    mid, it, err = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
-    arr = (abi.Material * len(mats))(*mats)
+    mid, it, ev, err = (np.zeros(n, np.int32) for _ in range(4))
+    arr = abi.material_array(mats)
     check(lib().m2cg_riemann_batch_pairs(C.byref(s), arr, n, abi.dptr(VL), abi.dptr(VR), abi.dptr(dirs),
                                          abi.dptr(warm), abi.dptr(Vs), abi.iptr(mid), abi.dptr(Vsm), abi.dptr(Vsp),
-                                         abi.iptr(it), abi.iptr(err)))
-    return Vs, mid, Vsm, Vsp, it, err
+                                         abi.iptr(it), abi.iptr(ev), abi.iptr(err)))
+    return Vs, mid, Vsm, Vsp, it, ev, err
 
 
 def tube_rejects(s):
@@ -128,7 +142,7 @@ def tube_rejects(s):
     def reject(mats, VL, VR):
         dirs = np.zeros((len(VL), 3))
         dirs[:, 0] = 1.0
-        err = riemann_batch_pairs(s, mats, VL, VR, dirs)[5]
+        err = riemann_batch_pairs(s, mats, VL, VR, dirs)[6]
         return err != 0
     return reject
 
@@ -280,6 +294,12 @@ class Batch:
         check(lib().m2cg_batch_get_counters(self.h, C.byref(c)))
         return {n: getattr(c, n) for n, _ in Counters._fields_}
 
+    def set_mlp(self, mlp):
+        """Start every interface Riemann solve from the network's proposal
+        (None detaches)."""
+        check(lib().m2cg_batch_set_mlp(self.h, mlp.h if mlp is not None else None))
+        self._mlp = mlp  # keep it alive while attached
+
     def tube_errors(self):
         codes = np.zeros(self.ntubes, np.int32)
         check(lib().m2cg_batch_tube_errors(self.h, abi.iptr(codes)))
@@ -295,3 +315,88 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def _fptr(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Mlp:
+    """The learned warm start of the interface Riemann solve: a
+    16 -> 64 -> 64 -> 64 -> 1 tanh network proposing log(p*/pac) (pac the
+    acoustic estimate) from
+    dimensionless problem features (m2cg_mlp_*). Trained on the GPU by the
+    library's own FP32 forward/backward kernels; inference is BF16 on tensor
+    cores."""
+    NPARAM = 9473
+    NIN = 16
+    NNORM = 34
+
+    def __init__(self, seed=0):
+        h = C.c_void_p()
+        check(lib().m2cg_mlp_create(seed, C.byref(h)))
+        self.h = h
+
+    def params(self):
+        p = np.empty(self.NPARAM, np.float32)
+        n = np.empty(self.NNORM, np.float32)
+        check(lib().m2cg_mlp_get_params(self.h, _fptr(p), _fptr(n)))
+        return p, n
+
+    def set_params(self, params=None, norm=None):
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        n = None if norm is None else np.ascontiguousarray(norm, np.float32)
+        check(lib().m2cg_mlp_set_params(self.h, _fptr(p), _fptr(n)))
+
+    def loss_grad(self, Xn, yn):
+        Xn = np.ascontiguousarray(Xn, np.float32)
+        yn = np.ascontiguousarray(yn, np.float32)
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(self.NPARAM, np.float32)
+        check(lib().m2cg_mlp_loss_grad(self.h, _fptr(Xn), _fptr(yn), len(yn), _fptr(loss), _fptr(g)))
+        return float(loss[0]), g
+
+    def train(self, X, y, steps=3000, batch=8192, lr=2e-3, seed=0):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = np.zeros(1, np.float32)
+        check(lib().m2cg_mlp_train(self.h, _fptr(X), _fptr(y), len(y), steps, batch, lr, seed, _fptr(loss)))
+        return float(loss[0])
+
+    def infer(self, X, valid=None):
+        X = np.ascontiguousarray(X, np.float32)
+        valid = np.ones(len(X), np.int32) if valid is None else np.ascontiguousarray(valid, np.int32)
+        y = np.zeros(len(X), np.float32)
+        check(lib().m2cg_mlp_infer(self.h, _fptr(X), abi.iptr(valid), len(X), _fptr(y)))
+        return y
+
+    def predict_pairs(self, mats, VL, VR, dirs):
+        VL, VR, dirs = (np.ascontiguousarray(a, np.float64) for a in (VL, VR, dirs))
+        p = np.empty(len(VL))
+        check(lib().m2cg_mlp_predict_pairs(self.h, abi.material_array(mats), len(VL), abi.dptr(VL), abi.dptr(VR),
+                                           abi.dptr(dirs), abi.dptr(p)))
+        return p
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().m2cg_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mlp_features_pairs(mats, VL, VR, dirs):
+    """Network input features of per-pair problems: X [n, 16] (float32),
+    base pressure pac [n], valid [n]."""
+    VL, VR, dirs = (np.ascontiguousarray(a, np.float64) for a in (VL, VR, dirs))
+    n = len(VL)
+    X = np.zeros((n, 16), np.float32)
+    P = np.zeros(n)
+    valid = np.zeros(n, np.int32)
+    check(lib().m2cg_mlp_features_pairs(abi.material_array(mats), n, abi.dptr(VL), abi.dptr(VR), abi.dptr(dirs),
+                                        _fptr(X), abi.dptr(P), abi.iptr(valid)))
+    return X, P, valid

@@ -1,0 +1,79 @@
+"""Training data and training of the learned Riemann warm start.
+
+The network learns the star pressure of two-material interface Riemann
+problems drawn from the batched-tube state distribution (stiffened-gas
+pairs with gamma in [1.2, 7] and p_inf 0 w.p. 1/4 else log-uniform in
+1e6..1e9 Pa; densities log-uniform in 1..1000 kg/m^3, pressures log-uniform
+in 1e4..1e9 Pa, velocities uniform in +-200 m/s). Targets come from the
+library's own exact solver (m2cg_riemann_batch_pairs, the restated
+ExactRiemannSolverBase::ComputeRiemannSolution); training runs on the GPU
+through m2cg_mlp_train.
+"""
+import numpy as np
+
+from . import abi, gpu
+
+
+def sample_problems(n, seed):
+    """n seeded problems: (materials [2n] as a MATERIAL_DTYPE table, VL, VR, dirs)."""
+    rng = np.random.default_rng(seed)
+    gam = rng.uniform(1.2, 7.0, 2 * n)
+    zero = rng.uniform(size=2 * n) < 0.25
+    pinf = np.where(zero, 0.0, 10.0 ** rng.uniform(6.0, 9.0, 2 * n))
+    mats = abi.material_table(gam, pinf)
+    VL = np.zeros((n, 5))
+    VR = np.zeros((n, 5))
+    for V in (VL, VR):
+        V[:, 0] = 10.0 ** rng.uniform(0.0, 3.0, n)
+        V[:, 1] = rng.uniform(-200.0, 200.0, n)
+        V[:, 4] = 10.0 ** rng.uniform(4.0, 9.0, n)
+    dirs = np.zeros((n, 3))
+    dirs[:, 0] = 1.0
+    return mats, VL, VR, dirs
+
+
+def solve(s, mats, VL, VR, dirs, warm=None, chunk=250_000):
+    """Exact solves in chunks; returns dict of arrays (Vs, id, Vsm, Vsp, iters, evals, err)."""
+    out = {k: [] for k in ("Vs", "id", "Vsm", "Vsp", "iters", "evals", "err")}
+    for a in range(0, len(VL), chunk):
+        b = min(len(VL), a + chunk)
+        r = gpu.riemann_batch_pairs(s, mats[2 * a:2 * b], VL[a:b], VR[a:b], dirs[a:b],
+                                    None if warm is None else warm[a:b])
+        for k, v in zip(out, r):
+            out[k].append(v)
+    return {k: np.concatenate(v) for k, v in out.items()}
+
+
+def training_set(n, seed, s=None):
+    """Features X [m, 16] and targets y = log(p*/pac) (pac: the acoustic
+    estimate returned as the features' base pressure) of the solvable
+    problems (solver OK, p* > 0, features valid) among n samples."""
+    s = s or abi.scheme()
+    mats, VL, VR, dirs = sample_problems(n, seed)
+    r = solve(s, mats, VL, VR, dirs)
+    X, P, valid = gpu.mlp_features_pairs(mats, VL, VR, dirs)
+    ps = r["Vsm"][:, 4]
+    keep = (r["err"] == 0) & (ps > 0) & (valid != 0)
+    y = np.log(ps[keep] / P[keep]).astype(np.float32)
+    return X[keep], y, keep.mean()
+
+
+def train(n=2_000_000, steps=6000, batch=8192, lr=2e-3, seed=0, s=None):
+    """Generate n problems, solve them, train a network on the GPU. Returns
+    (Mlp, info)."""
+    X, y, frac = training_set(n, seed, s)
+    net = gpu.Mlp(seed=seed)
+    loss = net.train(X, y, steps=steps, batch=batch, lr=lr, seed=seed)
+    return net, {"samples": int(len(y)), "kept_fraction": float(frac), "final_loss": loss}
+
+
+def save(net, path):
+    p, nrm = net.params()
+    np.savez(path, params=p, norm=nrm)
+
+
+def load(path):
+    d = np.load(path)
+    net = gpu.Mlp()
+    net.set_params(d["params"], d["norm"])
+    return net
