@@ -1,12 +1,13 @@
 """Python handle on the CPU oracles (TEST INFRASTRUCTURE ONLY).
 
-Two oracles share one interface:
   * ``RefCase``/``RefPoint`` over oracle/_ref/libm2c_ref.so: the unmodified
     reference M2C sources compiled in place with single-rank shims
     (oracle/Makefile, target ``ref``), driven like Main.cpp.
-  * ``PortCase``/``PortPoint`` over oracle/_port/libm2c_port.so: this
-    project's own restatement of the same algorithms (oracle/port/), which
-    also supports the periodic boundaries the reference cannot express.
+  * ``DropinCase`` over oracle/_ref/libm2c_dropin.so (target ``dropin``):
+    the same reference driver with its RK integrator replaced by the GPU
+    drop-in m2c_b200/adapter/TimeIntegratorGPU.h. This one runs the product
+    (the GPU library) inside the reference's own loop; tests compare it with
+    RefCase to show the drop-in boundary works.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import
 this module, and only as the checker.
@@ -20,7 +21,7 @@ from m2c_b200 import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libm2c_ref.so")
-PORT_SO = os.path.join(HERE, "_port", "libm2c_port.so")
+DROPIN_SO = os.path.join(HERE, "_ref", "libm2c_dropin.so")
 
 _libs = {}
 
@@ -60,7 +61,7 @@ def _load(path, prefix):
 
 
 def available(which="ref"):
-    return os.path.exists(REF_SO if which == "ref" else PORT_SO)
+    return os.path.exists(REF_SO if which == "ref" else DROPIN_SO)
 
 
 class _Case:
@@ -181,12 +182,8 @@ def RefPoint(s, mats):
     return _Point(_load(REF_SO, "m2cref_"), "m2cref_", s, mats)
 
 
-def PortCase(g, s, mats, ls=None):
-    return _Case(_load(PORT_SO, "m2cport_"), "m2cport_", g, s, mats, ls)
-
-
-def PortPoint(s, mats):
-    return _Point(_load(PORT_SO, "m2cport_"), "m2cport_", s, mats)
+def DropinCase(g, s, mats, ls=None):
+    return _Case(_load(DROPIN_SO, "m2cref_"), "m2cref_", g, s, mats, ls)
 
 
 def _tube_worker(args):

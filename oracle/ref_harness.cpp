@@ -36,6 +36,11 @@
 #include <vector>
 
 #include "../include/m2c_gpu.h"
+#ifdef M2C_DROPIN
+// The drop-in build: the same driver with M2C's RK integrator replaced by
+// the GPU one a maintainer would add (m2c_b200/adapter/TimeIntegratorGPU.h).
+#include "m2c_b200/adapter/TimeIntegratorGPU.h"
+#endif
 
 // Globals the reference expects from its driver (Main.cpp:39-44).
 int verbose = 0;
@@ -234,6 +239,10 @@ void* m2cref_create(const m2cg_grid* g, const m2cg_scheme* s, const m2cg_materia
   }
   c->mpo = new MultiPhaseOperator(c->comm, *c->dms, iod, c->vf, *c->gmi, *c->spo, c->lso);
 
+#ifdef M2C_DROPIN
+  c->integrator = new TimeIntegratorGPU(c->comm, iod, *c->dms, *c->spo, c->lso, *c->mpo, s->precision);
+  return c;
+#endif
   if (iod.ts.expl.type == ExplicitData::FORWARD_EULER)
     c->integrator = new TimeIntegratorFE(c->comm, iod, *c->dms, *c->spo, c->lso, *c->mpo, nullptr, nullptr, nullptr);
   else if (iod.ts.expl.type == ExplicitData::RUNGE_KUTTA_2)
