@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -120,6 +121,10 @@ struct m2cg_ctx {
   // SoA state: V double-buffered (step state), U two stage buffers
   double* V[2][5] = {};
   double* U[2][5] = {};
+  // stage inputs in the compute type: P two stage buffers (clip(C2P(U_s))),
+  // and for the mixed path an FP32 copy of V (Vf, double-buffered with V)
+  void* P[2][5] = {};
+  float* Vf[2][5] = {};
   int cur = 0;
   uint8_t* id = nullptr;
   // mesh
@@ -141,7 +146,6 @@ struct m2cg_ctx {
   bool dtmin_valid = false;
   m2cg_counters counters = {};
   Multiphase* mp = nullptr;  // two-material machinery (nullptr for one material)
-  int zchunk = 32;
   // optional per-stage event timing (benchmark roofline)
   bool profile = false;
   std::vector<cudaEvent_t> ev;  // pairs (before, after) per stage launch
@@ -268,10 +272,17 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   c->plane = c->px * grid->ny;
   c->nalloc = c->plane * grid->nz;
   st = M2CG_OK;
+  const bool mixed = scheme->precision == M2CG_PREC_MIXED;
   for (int b = 0; b < 2; b++)
     for (int p = 0; p < 5; p++) {
       c->V[b][p] = dalloc(c->nalloc, &st);
       c->U[b][p] = dalloc(c->nalloc, &st);
+      if (mixed) {
+        c->P[b][p] = dalloc((c->nalloc + 1) / 2, &st);
+        c->Vf[b][p] = (float*)dalloc((c->nalloc + 1) / 2, &st);
+      } else {
+        c->P[b][p] = dalloc(c->nalloc, &st);
+      }
     }
   if (cudaMalloc((void**)&c->id, c->nalloc) != cudaSuccess) st = fail(M2CG_ERR_NOMEM, "cudaMalloc id failed");
   if (!st) cudaMemsetAsync(c->id, 0, c->nalloc, c->stream);
@@ -340,28 +351,18 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
     m2cg_destroy(c);
     return st;
   }
-  // Work items = (x,y) tiles x z-chunks, run by a persistent grid of
-  // resident CTAs. Pick the chunk length that minimises rounds x (chunk +
-  // pipeline prologue of ~2.5 planes).
+  // The (x,y) tiles x z planes are shared evenly by a persistent grid of
+  // resident CTAs, each share at least 8 planes long (the plane pipeline's
+  // prologue costs about 2.5 planes per segment).
   const int ty = (scheme->precision != M2CG_PREC_MIXED && nls == 1) ? StageTY<double, true>::value : STAGE_TY;
   c->ntx = (c->nx + TX - 1) / TX;
   c->nty = (c->ny + ty - 1) / ty;
   {
-    int resident = scheme->precision == M2CG_PREC_MIXED ? stage_resident_mixed(scheme->flux, nls == 1)
-                                                        : stage_resident_fp64(scheme->flux, nls == 1);
-    const int cand[] = {4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 256};
-    double best = 1e300;
-    int bestc = c->nz;
-    for (int ch : cand) {
-      if (ch > c->nz) ch = c->nz;
-      long long items = (long long)c->ntx * c->nty * ((c->nz + ch - 1) / ch);
-      long long rounds = (items + resident - 1) / resident;
-      double cost = rounds * (ch + 2.5);
-      if (cost < best - 1e-9) { best = cost; bestc = ch; }
-      if (ch == c->nz) break;
-    }
-    c->zchunk = bestc;
-    c->nitems = c->ntx * c->nty * ((c->nz + bestc - 1) / bestc);
+    const int resident = scheme->precision == M2CG_PREC_MIXED ? stage_resident_mixed(scheme->flux, nls == 1)
+                                                              : stage_resident_fp64(scheme->flux, nls == 1);
+    const long long units = (long long)c->ntx * c->nty * c->nz;
+    const long long by_len = (units + 7) / 8;
+    c->nitems = (int)std::max<long long>(1, std::min<long long>(resident, by_len));
   }
   CK(cudaStreamSynchronize(c->stream));
   *out = c;
@@ -375,6 +376,8 @@ extern "C" m2cg_status m2cg_destroy(m2cg_ctx* c) {
     for (int p = 0; p < 5; p++) {
       cudaFree(c->V[b][p]);
       cudaFree(c->U[b][p]);
+      cudaFree(c->P[b][p]);
+      cudaFree(c->Vf[b][p]);
     }
   cudaFree(c->id);
   cudaFree(c->dx); cudaFree(c->dy); cudaFree(c->dz);
@@ -420,6 +423,24 @@ __global__ void k_clip_state(Grid3 g, SchemeK sk, double* v0, double* v1, double
     e.clip(V);
     if (e.bad(V)) report(err, ERR_STATE, (int)q, 0);
     v0[o] = V[0]; v1[o] = V[1]; v2[o] = V[2]; v3[o] = V[3]; v4[o] = V[4];
+  }
+}
+
+struct F5 {
+  float* p[5];
+};
+
+// FP32 copy of the interior state (the mixed path's stage-1 input).
+__global__ void k_to_float(Grid3 g, const double* v0, const double* v1, const double* v2, const double* v3,
+                           const double* v4, F5 f) {
+  long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % g.nx);
+    int j = (int)((q / g.nx) % g.ny);
+    int k = (int)(q / ((long long)g.nx * g.ny));
+    long long o = (long long)k * g.plane + (long long)j * g.px + i;
+    f.p[0][o] = (float)v0[o]; f.p[1][o] = (float)v1[o]; f.p[2][o] = (float)v2[o];
+    f.p[3][o] = (float)v3[o]; f.p[4][o] = (float)v4[o];
   }
 }
 
@@ -581,6 +602,12 @@ extern "C" m2cg_status m2cg_upload_state(m2cg_ctx* c, const double* V, const dou
                                                     D[0], D[1], D[2], D[3], D[4]);
   k_clip_state<<<grid1d(n), 256, 0, c->stream>>>(c->g, c->sk, D[0], D[1], D[2], D[3], D[4], c->id, c->err);
   c->counters.kernel_launches += ID ? 3 : 2;
+  if (c->scheme.precision == M2CG_PREC_MIXED) {
+    F5 f;
+    for (int p = 0; p < 5; p++) f.p[p] = c->Vf[c->cur][p];
+    k_to_float<<<grid1d(n), 256, 0, c->stream>>>(c->g, D[0], D[1], D[2], D[3], D[4], f);
+    c->counters.kernel_launches += 1;
+  }
   CK(cudaGetLastError());
   if (c->mp) {
     st = multiphase_upload_phi(c->mp, c->stream, phi, c->stage_buf, c->id);
@@ -635,7 +662,6 @@ static void rk_coeffs(int r, int s, double& a_prev, double& a_un, double& b) {
 }
 
 static m2cg_status launch_stage(m2cg_ctx* c, StageArgs& a) {
-  a.zchunk = c->zchunk;
   a.ntx = c->ntx;
   a.nty = c->nty;
   a.nitems = c->nitems;
@@ -677,6 +703,7 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
     m2cg_status st = multiphase_begin_step(c->mp, c->stream, Vn, c->id);
     if (st) return st;
   }
+  const bool mixed = c->scheme.precision == M2CG_PREC_MIXED;
   for (int s = 1; s <= r; s++) {
     StageArgs a;
     base_args(c, a);
@@ -688,6 +715,12 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
       a.Us[p] = s == 1 ? nullptr : c->U[(s - 2) & 1][p];
       a.Uo[p] = c->U[(s - 1) & 1][p];
       a.Vo[p] = Vo[p];
+      if (s == 1)
+        a.Pin[p] = mixed ? (const void*)c->Vf[c->cur][p] : (const void*)Vn[p];
+      else
+        a.Pin[p] = c->P[(s - 2) & 1][p];
+      a.Po[p] = s == r ? nullptr : c->P[(s - 1) & 1][p];
+      a.Vfo[p] = (s == r && mixed) ? c->Vf[1 - c->cur][p] : nullptr;
     }
     a.us_clipped = s > 1 ? c->clipflags + (s - 2) : nullptr;
     a.clipped_out = c->clipflags + (s - 1);
@@ -701,8 +734,8 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
   }
   c->cur = 1 - c->cur;
   if (c->mp) {
-    m2cg_status st = multiphase_end_step(c->mp, c->stream, c->V[1 - c->cur], c->V[c->cur], c->id,
-                                         c->clock, c->err, &c->counters);
+    m2cg_status st = multiphase_end_step(c->mp, c->stream, c->V[1 - c->cur], c->V[c->cur],
+                                         mixed ? c->Vf[c->cur] : nullptr, c->id, c->clock, c->err, &c->counters);
     if (st) return st;
     c->dtmin_valid = false;
   } else {
@@ -780,6 +813,7 @@ extern "C" m2cg_status m2cg_compute_residual(m2cg_ctx* c, double* R_host) {
     a.Vn[p] = Vn[p];
     a.Uo[p] = c->U[0][p];
     a.Ro[p] = c->U[1][p];
+    a.Pin[p] = c->scheme.precision == M2CG_PREC_MIXED ? (const void*)c->Vf[c->cur][p] : (const void*)Vn[p];
   }
   if (c->mp) {
     m2cg_status st = multiphase_begin_step(c->mp, c->stream, Vn, c->id);

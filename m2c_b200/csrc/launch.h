@@ -17,8 +17,8 @@ template <> struct StageTY<double, true> { static constexpr int value = 4; };
 
 size_t stage_smem_fp64(bool multi);
 size_t stage_smem_mixed(bool multi);
-// Launch one stage over a.nitems work items on a persistent grid of
-// min(nitems, SMs x resident CTAs per SM) CTAs. *grid_out reports the grid.
+// Launch one stage on a persistent grid of min(nitems, SMs x resident CTAs
+// per SM) CTAs sharing the work evenly. *grid_out reports the grid.
 cudaError_t launch_stage_fp64(const StageArgs& a, cudaStream_t s, bool multi, int* grid_out);
 cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s, bool multi, int* grid_out);
 // Resident CTAs on the whole device of the stage kernel for (flux, multi);

@@ -313,6 +313,7 @@ struct StateUpdateArgs {
   Grid3 g;
   const Eos<double>* eos;
   double* V[5];
+  float* Vf[5];         // FP32 copy of V kept in step (mixed path), or null
   const uint8_t* id;
   const uint8_t* idn;
   const int* slot;
@@ -422,6 +423,8 @@ __global__ void k_state_update(StateUpdateArgs a) {
     a.eos[myid].clip(v);
     if (a.eos[myid].bad(v)) report(a.err, ERR_STATE, q, 9);
     for (int p = 0; p < 5; p++) a.V[p][off] = v[p];
+    if (a.Vf[0])
+      for (int p = 0; p < 5; p++) a.Vf[p][off] = (float)v[p];
   }
   a.nchanged[1] = nun;
 }
@@ -601,7 +604,8 @@ m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
   return levelset_stage(s, mp->g, mp->sk, mp->lsg, a, in, mp->phiN, outp);
 }
 
-m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* Vold, double* const* Vnew, uint8_t* id,
+m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* Vold, double* const* Vnew,
+                                float* const* Vfnew, uint8_t* id,
                                 const double* clock, DevError* err, m2cg_counters* counters) {
   (void)Vold;
   (void)clock;
@@ -627,6 +631,7 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
   ua.g = g;
   ua.eos = mp->d_eos;
   for (int p = 0; p < 5; p++) ua.V[p] = Vnew[p];
+  for (int p = 0; p < 5; p++) ua.Vf[p] = Vfnew ? Vfnew[p] : nullptr;
   ua.id = id;
   ua.idn = mp->idn;
   ua.slot = mp->slot;

@@ -26,6 +26,7 @@ m2cg_status multiphase_begin_step(Multiphase* mp, cudaStream_t s, double* const*
 m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, m2c::StageArgs& a);
 // After the last stage: level-set update, ID update, reinitialisation,
 // state update of cells that changed material.
-m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* Vn, double* const* Vnew, uint8_t* id,
+m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* Vn, double* const* Vnew,
+                                float* const* Vfnew, uint8_t* id,
                                 const double* clock, m2c::DevError* err, m2cg_counters* counters);
 void multiphase_counters(const Multiphase* mp, m2cg_counters* out);

@@ -17,13 +17,18 @@
 // they are rebuilt from interior cells by the boundary rule when loaded.
 //
 // Work decomposition: a CTA owns a 32 x TY column of cells and marches along
-// z through a chunk of planes, keeping a ring of 3 primitive planes (with a
-// 2-cell x/y halo) in shared memory. Iteration m of the plane pipeline:
-//   (1) load plane m+2 (ghost rules applied on the fly),
+// z through a chunk of planes, keeping a ring of 4 primitive planes (with a
+// 2-cell x/y halo) in shared memory. The stage's input is a primitive state
+// in the compute type (V^n for stage 1; for later stages clip(C2P(U_s)),
+// written by the previous stage's update), so planes are copied into the
+// ring with cp.async as they are, and only ghost cells are rewritten by the
+// boundary rule. Iteration m of the plane pipeline:
+//   (1) ghost rules on plane m+2 (landed), cp.async of plane m+3 into the
+//       slot plane m-1 has freed,
 //   (2) slopes + revert mask of every cell of plane m+1 (x -1..32, y -1..TY),
 //   (3) every face flux once: x/y faces of plane m and the z faces m+1/2,
 //   (4) residual + RK update of plane m (z faces m-1/2 and m+1/2 from the
-//       two-plane z-flux ring).
+//       two-plane z-flux ring), writing the next stage's primitive input.
 // Face states follow Reconstructor.cpp: slope-limited primitive values, the
 // first face (in the order l,r,b,t,k,f) failing CheckState reverted to the
 // cell value, every face needing clipping reverted to the cell value, and a
@@ -84,6 +89,9 @@ struct IfaceView {
 struct StageArgs {
   Grid3 g;
   SchemeK s;
+  const void* Pin[5];    // stage input: primitive state in the compute type (see above)
+  void* Po[5];           // non-final stages: clip(C2P(U_new)) in the compute type
+  float* Vfo[5];         // final stage, FP32 compute type: FP32 copy of the new state
   const double* Vn[5];   // V^n (primitive) - step state
   const double* Us[5];   // flux source of stages >= 2 (conserved, raw)
   double* Uo[5];         // stage output (conserved) for non-final stages
@@ -98,8 +106,8 @@ struct StageArgs {
   int* clipped_out;      // set if any cell of this stage's output was clipped
   unsigned long long* dtmin_bits;  // final stage: min dx/(|u|+c) as ordered bits
   DevError* err;
-  int zchunk;            // planes per work item
-  int ntx, nty, nitems;  // tiles in x, y and work items (tiles x z-chunks)
+  int ntx, nty;          // tiles in x and y
+  int nitems;            // CTAs that share the (tile, plane) units evenly
   double* Ro[5];         // if set: write the residual R only (no RK update)
   IfaceView iface;
 };
@@ -118,17 +126,15 @@ struct StageSmem {
   static constexpr int NFX = (TX + 1) * TY;        // x faces of a plane
   static constexpr int NFY = TX * (TY + 1);        // y faces of a plane
   static constexpr int NFZ = TX * TY;              // z faces between two planes
-  T v[3][5][RY][RX];
-  T sig[2][3][5][MY][MX];
+  T v[4][5][RY][RX];          // ring of primitive planes, slot = plane & 3
+  T sig[2][3][5][MY][MX];     // limited slopes (x, y, z) of the mask region, two planes
   T fx[5][NFX];
   T fy[5][NFY];
   T fz[2][5][NFZ];
   uint8_t mask[2][MY][MX];
-  uint8_t real[3][RY][RX];  // 1 = real (interior or periodic image), 0 = ghost / unused
-  uint8_t ids[3][RY][RX];
-  double raw[5][RY * RX];     // next plane as loaded from HBM (V or U, FP64), in flight via cp.async
-  uint8_t rinfo[RY * RX];     // per loaded cell: bit0 real, bits1-2 ghost axis+1, bit3 ghost side
-  uint8_t rid[RY * RX];
+  uint8_t real[4][RY][RX];    // 1 = real (interior or periodic image), 0 = ghost / unused
+  uint8_t ids[4][RY][RX];
+  uint8_t rinfo[RY * RX];     // per loaded cell of the plane in flight: bit0 real, bits1-2 ghost axis+1, bit3 ghost side
   double red[TY * TX / 32];
 };
 
@@ -256,11 +262,23 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_t(T* smem, const T* gmem) {
+  if constexpr (sizeof(T) == 8) cp_async8(smem, gmem);
+  else cp_async4(smem, gmem);
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <typename T> struct StageOcc { static constexpr int value = 1; };
-template <> struct StageOcc<float> { static constexpr int value = 2; };
+#ifndef M2C_STAGE_OCC_F32
+#define M2C_STAGE_OCC_F32 2
+#endif
+template <> struct StageOcc<float> { static constexpr int value = M2C_STAGE_OCC_F32; };
 
 template <typename T, int TY, int FLUX, bool MULTI>
 __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(const __grid_constant__ StageArgs a) {
@@ -283,20 +301,20 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
   const int limiter = a.s.limiter;
   const bool rec_linear = a.s.rec_linear;
   const bool slope_zero = MULTI && a.s.slope_zero_at_interface;
-  const double* const* src = a.stage == 1 ? a.Vn : a.Us;
 
   int i0 = 0, j0 = 0;  // tile origin of the current work item
   uint8_t idreg[LPT];
 
-  auto slot3 = [](int p) { return ((p % 3) + 3) % 3; };
+  auto slot4 = [](int p) { return p & 3; };
   auto plane_is_ghost = [&](int p) { return !zper && (p < 0 || p >= g.nz); };
 
-  // (1a) start fetching plane p: one cp.async per value into the staging
-  // buffer, ghost cells read from their image cell; cell kind kept in rinfo.
+  // (1a) start copying plane p into its ring slot: one cp.async per value,
+  // ghost cells copied from their image cell; cell kind kept in rinfo.
   auto issue_plane = [&](int p) {
     int sz;
     bool farz = false;
     const int kk = resolve_axis(p, g.nz, zper, sz, farz);
+    const int s = slot4(p);
 #pragma unroll
     for (int r = 0; r < LPT; r++) {
       const int q = tid + r * NT;
@@ -309,7 +327,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       const int nghost = (sx >= 0) + (sy >= 0) + (sz >= 0);
       const long long off = (long long)kk * g.plane + (long long)jj * g.px + ii;
 #pragma unroll
-      for (int c = 0; c < 5; c++) cp_async8(&sm.raw[c][q], src[c] + off);
+      for (int c = 0; c < 5; c++) cp_async_t(&sm.v[s][c][ly][lx], static_cast<const T*>(a.Pin[c]) + off);
       uint8_t info = 0;
       if (nghost == 0 && !far) {
         info = 1;
@@ -324,59 +342,77 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     cp_async_commit();
   };
 
-  // (1b) turn the fetched plane into primitive states in the ring: C2P + clip
-  // for stages >= 2 (SpaceOperator::ConservativeToPrimitive +
-  // ClipDensityAndPressure), the boundary rule for ghost cells
-  // (SpaceOperator::ApplyBoundaryConditions), rounding to T.
+  // (1b) the landed plane: boundary rule on ghost cells
+  // (SpaceOperator::ApplyBoundaryConditions), cell kinds and ids.
   auto commit_plane = [&](int p) {
-    const int s = slot3(p);
+    const int s = slot4(p);
 #pragma unroll
     for (int r = 0; r < LPT; r++) {
       const int q = tid + r * NT;
       if (q >= NLOAD) break;
       const int ly = q / S::RX, lx = q - ly * S::RX;
       const uint8_t info = sm.rinfo[q];
-      const uint8_t id = MULTI ? idreg[r] : 0;
-      double V[5];
-      if (a.stage == 1) {
-#pragma unroll
-        for (int c = 0; c < 5; c++) V[c] = sm.raw[c][q];
-      } else {
-        double U[5];
-#pragma unroll
-        for (int c = 0; c < 5; c++) U[c] = sm.raw[c][q];
-        const Eos<double>& e = eos_of<double, MULTI>(a.s, id);
-        e.c2p(U, V);
-        e.clip(V);
-      }
       const int gaxis = (info >> 1) & 3;
       if (gaxis) {
         const int axis = gaxis - 1, side = (info >> 3) & 1;
         const int bc = g.bc[2 * axis + side];
         if (bc == BC_INLET) {
 #pragma unroll
-          for (int c = 0; c < 5; c++) V[c] = g.inlet[c];
+          for (int c = 0; c < 5; c++) sm.v[s][c][ly][lx] = T(g.inlet[c]);
         } else if (bc == BC_OUTLET) {
 #pragma unroll
-          for (int c = 0; c < 5; c++) V[c] = g.outlet[c];
+          for (int c = 0; c < 5; c++) sm.v[s][c][ly][lx] = T(g.outlet[c]);
         } else if (bc == BC_STICKWALL) {
-          V[1] = -V[1]; V[2] = -V[2]; V[3] = -V[3];
+          sm.v[s][1][ly][lx] = -sm.v[s][1][ly][lx];
+          sm.v[s][2][ly][lx] = -sm.v[s][2][ly][lx];
+          sm.v[s][3][ly][lx] = -sm.v[s][3][ly][lx];
         } else {  // SYMMETRY / SLIPWALL: normal velocity flipped
-          if (axis == 0) V[1] = -V[1];
-          else if (axis == 1) V[2] = -V[2];
-          else V[3] = -V[3];
+          sm.v[s][1 + axis][ly][lx] = -sm.v[s][1 + axis][ly][lx];
         }
       }
-#pragma unroll
-      for (int c = 0; c < 5; c++) sm.v[s][c][ly][lx] = T(V[c]);
       sm.real[s][ly][lx] = info & 1;
-      sm.ids[s][ly][lx] = id;
+      sm.ids[s][ly][lx] = MULTI ? idreg[r] : 0;
     }
   };
 
-  // (2) slopes + revert mask of plane p (needs planes p-1, p, p+1 in the ring)
+  // Limited slopes in direction d of the real cell at loaded position
+  // (lx, ly) of plane p (needs planes p-1, p, p+1 for d = 2).
+  auto slopes = [&](int p, int lx, int ly, int d, T* sd) {
+    const int s0 = slot4(p);
+    int sm1 = s0, sp1 = s0, lxm = lx, lxp = lx, lym = ly, lyp = ly;
+    if (d == 0) { lxm = lx - 1; lxp = lx + 1; }
+    else if (d == 1) { lym = ly - 1; lyp = ly + 1; }
+    else { sm1 = slot4(p - 1); sp1 = slot4(p + 1); }
+    if (!rec_linear) {
+#pragma unroll
+      for (int c = 0; c < 5; c++) sd[c] = T(0);
+      return;
+    }
+    const int ia = wrap_index(i0 + lx - 2, g.nx), ja = wrap_index(j0 + ly - 2, g.ny), ka = wrap_index(p, g.nz);
+    const int ix = d == 0 ? ia : (d == 1 ? ja : ka);
+    T A, B;
+    int K = 0;
+    if (limiter == LIM_VANALBADA) {
+      A = T(g.lA[d][ix]); B = T(g.lB[d][ix]); K = g.lK[d][ix];
+    } else {  // generalized minmod uses B/(A+1) only
+      A = T(0); B = T(g.lC[d][ix]);
+    }
+    bool zero = false;
+    if (slope_zero) {
+      const uint8_t id = sm.ids[s0][ly][lx];
+      zero = id != sm.ids[sm1][lym][lxm] || id != sm.ids[sp1][lyp][lxp];
+    }
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+      const T vc = sm.v[s0][c][ly][lx];
+      T sl = limited_slope_c(limiter, A, B, K, alpha, vc - sm.v[sm1][c][lym][lxm], sm.v[sp1][c][lyp][lxp] - vc);
+      sd[c] = zero ? T(0) : sl;
+    }
+  };
+
+  // (2) slopes and revert mask of plane p
   auto mask_plane = [&](int p) {
-    const int sm1 = slot3(p - 1), s0 = slot3(p), sp1 = slot3(p + 1), ms = p & 1;
+    const int s0 = slot4(p), ms = p & 1;
     const int ka = wrap_index(p, g.nz);
     for (int q = tid; q < S::MY * S::MX; q += NT) {
       const int my = q / S::MX, mx = q - my * S::MX;
@@ -385,41 +421,16 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
         sm.mask[ms][my][mx] = 0;
         continue;
       }
-      const int ia = wrap_index(i0 + mx - 1, g.nx), ja = wrap_index(j0 + my - 1, g.ny);
       const uint8_t id = sm.ids[s0][ly][lx];
       const Eos<T>& e = eos_of<T, MULTI>(a.s, id);
-      T Ax, Bx, Ay, By, Az, Bz;
-      int Kx = 0, Ky = 0, Kz = 0;
-      if (limiter == LIM_VANALBADA) {
-        Ax = T(g.lA[0][ia]); Bx = T(g.lB[0][ia]); Kx = g.lK[0][ia];
-        Ay = T(g.lA[1][ja]); By = T(g.lB[1][ja]); Ky = g.lK[1][ja];
-        Az = T(g.lA[2][ka]); Bz = T(g.lB[2][ka]); Kz = g.lK[2][ka];
-      } else {  // generalized minmod uses B/(A+1) only
-        Ax = T(0); Bx = T(g.lC[0][ia]);
-        Ay = T(0); By = T(g.lC[1][ja]);
-        Az = T(0); Bz = T(g.lC[2][ka]);
-      }
-      bool zx = false, zy = false, zz = false;
-      if (slope_zero) {
-        zx = id != sm.ids[s0][ly][lx - 1] || id != sm.ids[s0][ly][lx + 1];
-        zy = id != sm.ids[s0][ly - 1][lx] || id != sm.ids[s0][ly + 1][lx];
-        zz = id != sm.ids[sm1][ly][lx] || id != sm.ids[sp1][ly][lx];
-      }
       T v[5], sx[5], sy[5], sz[5];
 #pragma unroll
+      for (int c = 0; c < 5; c++) v[c] = sm.v[s0][c][ly][lx];
+      slopes(p, lx, ly, 0, sx);
+      slopes(p, lx, ly, 1, sy);
+      slopes(p, lx, ly, 2, sz);
+#pragma unroll
       for (int c = 0; c < 5; c++) {
-        const T vc = sm.v[s0][c][ly][lx];
-        v[c] = vc;
-        if (rec_linear) {
-          sx[c] = limited_slope_c(limiter, Ax, Bx, Kx, alpha, vc - sm.v[s0][c][ly][lx - 1], sm.v[s0][c][ly][lx + 1] - vc);
-          sy[c] = limited_slope_c(limiter, Ay, By, Ky, alpha, vc - sm.v[s0][c][ly - 1][lx], sm.v[s0][c][ly + 1][lx] - vc);
-          sz[c] = limited_slope_c(limiter, Az, Bz, Kz, alpha, vc - sm.v[sm1][c][ly][lx], sm.v[sp1][c][ly][lx] - vc);
-          if (zx) sx[c] = T(0);
-          if (zy) sy[c] = T(0);
-          if (zz) sz[c] = T(0);
-        } else {
-          sx[c] = sy[c] = sz[c] = T(0);
-        }
         sm.sig[ms][0][c][my][mx] = sx[c];
         sm.sig[ms][1][c][my][mx] = sy[c];
         sm.sig[ms][2][c][my][mx] = sz[c];
@@ -427,20 +438,23 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       uint8_t m;
       const int err = cell_faces(e, v, sx, sy, sz, m);
       sm.mask[ms][my][mx] = m;
-      if (err) report(a.err, err, (int)(((long long)ka * g.ny + ja) * g.nx + ia), where + 1);
+      if (err) {
+        const int ia = wrap_index(i0 + mx - 1, g.nx), ja = wrap_index(j0 + my - 1, g.ny);
+        report(a.err, err, (int)(((long long)ka * g.ny + ja) * g.nx + ia), where + 1);
+      }
     }
   };
 
   // Final face state of the real cell at mask-region (mx,my) of plane p:
   // direction d, side 0 = minus face (v - s/2), 1 = plus face (v + s/2).
   auto cell_face = [&](int p, int mx, int my, int d, int side, T* out) {
-    const int s0 = slot3(p), ms = p & 1;
+    const int s0 = slot4(p), ms = p & 1;
     const bool rev = (sm.mask[ms][my][mx] >> (2 * d + side)) & 1u;
 #pragma unroll
     for (int c = 0; c < 5; c++) {
       const T v = sm.v[s0][c][my + 1][mx + 1];
-      const T s = sm.sig[ms][d][c][my][mx];
-      out[c] = rev ? v : (side ? v + T(0.5) * s : v - T(0.5) * s);
+      const T sd = sm.sig[ms][d][c][my][mx];
+      out[c] = rev ? v : (side ? v + T(0.5) * sd : v - T(0.5) * sd);
     }
   };
 
@@ -449,7 +463,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
   // for two materials, the flux seen by the right cell (F2; they differ only
   // at a material interface).
   auto face_flux = [&](int d, int pL, int mxL, int myL, int pR, int mxR, int myR, T* F, T* F2) {
-    const int sL = slot3(pL), sR = slot3(pR);
+    const int sL = slot4(pL), sR = slot4(pR);
     const bool rL = sm.real[sL][myL + 1][mxL + 1], rR = sm.real[sR][myR + 1][mxR + 1];
     if (!rL && !rR) {
 #pragma unroll
@@ -571,13 +585,19 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
   int clipped_local = 0;
   const int tiles = a.ntx * a.nty;
 
-  for (int item = blockIdx.x; item < a.nitems; item += gridDim.x) {
-    const int zc = item / tiles, t2 = item - zc * tiles;
+  // Balanced segments: the (tile, plane) units, ordered tile by tile and
+  // plane by plane within a tile, are split evenly over the CTAs; a CTA runs
+  // the plane pipeline over each tile segment of its share (at most a few).
+  const long long units = (long long)tiles * g.nz;
+  const long long ubeg = units * blockIdx.x / gridDim.x, uend = units * (blockIdx.x + 1) / gridDim.x;
+  for (long long u = ubeg; u < uend;) {
+    const int t2 = (int)(u / g.nz);
+    const int kb = (int)(u - (long long)t2 * g.nz);
+    const int ke = (int)min((long long)g.nz, kb + (uend - u));
+    u += ke - kb;
     const int tyi = t2 / a.ntx, txi = t2 - tyi * a.ntx;
     i0 = txi * TX;
     j0 = tyi * TY;
-    const int kb = zc * a.zchunk;
-    const int ke = min(kb + a.zchunk, g.nz);
     const int gi = i0 + tx, gj = j0 + ty;
     const bool own = gi < g.nx && gj < g.ny;
     double dxi = 0, dyj = 0;
@@ -672,6 +692,10 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       if (a.final_stage) {
 #pragma unroll
         for (int c = 0; c < 5; c++) a.Vo[c][off] = V[c];
+        if (a.Vfo[0]) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) a.Vfo[c][off] = float(V[c]);
+        }
         const double ee = e.energy(V[0], V[4]);
         const double c2 = e.c2(V[0], ee);
         if (c2 < 0.0) report(a.err, ERR_SOUND, (int)off, where + 4);
@@ -682,6 +706,9 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       } else {
 #pragma unroll
         for (int c = 0; c < 5; c++) a.Uo[c][off] = Unew[c];
+        // the next stage's input: clip(C2P(U_new)), as it would recompute it
+#pragma unroll
+        for (int c = 0; c < 5; c++) static_cast<T*>(a.Po[c])[off] = T(V[c]);
       }
     }
   }
