@@ -18,9 +18,16 @@ time over ranks.
 
 --impl reference: the reference's own CPU implementation (the unmodified
 sources built with single-rank shims under oracle/_ref), run on the host
-cores as independent processes, each advancing a bounded 64^3 sample of the
+cores as independent processes, each advancing a bounded 48^3 sample of the
 same physics (symmetry walls instead of periodic: the reference has no
 periodic boundary) by one RK3 step per benchmark step.
+
+Extras (rank 0 at N = 1, skipped by --only-headline), under "extras": the
+384^3 sixteen-bubble cluster (mixed vs FP64, error of mixed against FP64,
+material-ID and level-set sign mismatches), the 4096 batched two-material
+tubes (CUDA-graph replay, autotuned tiles, with and without the learned
+warm start), and the learned warm start's evaluations and iterations saved
+on held-out interface problems (network in m2c_b200/data/warmstart_mlp.npz).
 """
 import argparse
 import json
@@ -49,6 +56,8 @@ def parse():
     p.add_argument("--n", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--only-headline", action="store_true",
+                   help="skip the extra workloads (bubble cluster, batched tubes, learned warm start)")
     return p.parse_args()
 
 
@@ -135,17 +144,146 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """DRAM bytes per cell per stage launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    """DRAM bytes (read + write) per cell per stage launch of the mixed stage
+    kernel, from the committed ncu summary (one stage-2 launch at 160^3), or
+    None."""
+    import re
+    p = os.path.join(ROOT, "profiles", "stage_kernel_mixed_160cube.md")
     if os.path.exists(p):
-        try:
-            return json.load(open(p))
-        except Exception:
-            return None
+        m = re.search(r"traffic_bytes_per_cell_per_launch:\s*([0-9.]+)", open(p).read())
+        if m:
+            return {"bytes_per_cell_per_launch": float(m.group(1))}
     return None
 
 
 # --------------------------------------------------------------------------
+# extra workloads (rank 0, one GPU): the other configurations of the path
+# --------------------------------------------------------------------------
+def extra_bubble(n=384, nbubbles=16, steps=10, warmup=2):
+    """Two-material bubble cluster in water, mixed vs FP64: cell-updates/s,
+    HBM fraction of the algorithmic bytes (RK3: 8 FP64 5-vectors, 8 phi
+    values and 3 ID bytes per cell and step), and the mixed path's error
+    against the FP64 path after the same steps."""
+    import numpy as np
+    from m2c_b200 import abi, cases, gpu
+    res = {}
+    for prec in (abi.PREC_MIXED, abi.PREC_FP64):
+        g, s, mats, ls, V, ID, PHI = cases.bubble_case(n, nbubbles=nbubbles, precision=prec)
+        sol = gpu.Solver(g, s, mats, ls)
+        sol.upload(V, ID, PHI)
+        del V, ID, PHI
+        sol.time_steps(warmup)
+        ms, _ = sol.time_steps(steps)
+        Vd, IDd, Pd = sol.download()
+        res[prec] = (ms, Vd[1:-1, 1:-1, 1:-1].reshape(-1, 5), IDd[1:-1, 1:-1, 1:-1].ravel(),
+                     Pd[1:-1, 1:-1, 1:-1].ravel(), sol.counters())
+        sol.close()
+        del Vd, IDd, Pd
+    cells = n ** 3
+    (mm, Vm, Im, Pm, cm), (mf, Vf, If, Pf, cf) = res[abi.PREC_MIXED], res[abi.PREC_FP64]
+    l1 = lambda a, b: float(np.abs(a - b).sum() / np.abs(b).sum())
+    vel = float(np.linalg.norm(Vm[:, 1:4] - Vf[:, 1:4], axis=1).sum() / np.linalg.norm(Vf[:, 1:4], axis=1).sum())
+    alg = 387.0 * cells * steps
+    peak, kind = measured_peak()
+    out = {"workload": f"bubble cluster {n}^3, {nbubbles} air bubbles in water, HLLC + van Albada, exact interface "
+                       f"Riemann, FD3 level set with reinitialisation every 10 steps, RK3, CFL 0.4",
+           "steps": steps, "after_warmup_steps": warmup,
+           "mixed": {"cell_updates_per_s": cells * steps / (mm / 1e3), "ms_per_step": mm / steps,
+                     "hbm_frac": alg / (mm / 1e3) / 1e9 / peak},
+           "fp64": {"cell_updates_per_s": cells * steps / (mf / 1e3), "ms_per_step": mf / steps,
+                    "hbm_frac": alg / (mf / 1e3) / 1e9 / peak},
+           "mixed_speedup": mf / mm,
+           "mixed_vs_fp64_rel_L1": {"rho": l1(Vm[:, 0], Vf[:, 0]), "velocity": vel, "p": l1(Vm[:, 4], Vf[:, 4])},
+           "material_id_mismatch": int((Im != If).sum()), "phi_sign_mismatch": int(((Pm < 0) != (Pf < 0)).sum()),
+           "riemann_calls_per_step_mixed": cm["riemann_calls"] / (steps + warmup),
+           "peak_kind": kind}
+    return out
+
+
+def extra_tubes(ntubes=4096, steps=200, mlp=None):
+    """Batched 1D two-material tubes (one graph-replayed step sequence, autotuned
+    tiles); tubes whose initial interface problem fails or that fail during a
+    screening run are redrawn (counted)."""
+    import numpy as np
+    from m2c_b200 import cases, gpu
+    s = cases.tube_scheme()
+    lens, mats, VL, VR, redrawn = cases.tubes(ntubes, seed=11, reject=gpu.tube_rejects(s))
+    rng = np.random.default_rng(99)
+    failed_total = 0
+    for _ in range(4):
+        b = gpu.Batch(s, lens, mats, VL, VR)
+        b.time_steps(steps, check_errors=False)
+        bad = np.nonzero(b.tube_errors())[0]
+        b.close()
+        if len(bad) == 0:
+            break
+        failed_total += len(bad)
+        for t in bad:
+            while True:
+                mats[2 * t], mats[2 * t + 1] = cases.stiffened_gas_pair(rng), cases.stiffened_gas_pair(rng)
+                a, c = cases.tube_states(1, rng)
+                VL[t], VR[t] = a[0], c[0]
+                if not gpu.tube_rejects(s)([mats[2 * t], mats[2 * t + 1]], VL[t:t + 1], VR[t:t + 1])[0]:
+                    break
+    out = {"workload": f"{ntubes} two-material shock tubes, 100-2000 cells, HLLC + van Albada, exact interface "
+                       f"Riemann, RK2, CFL 0.5, {steps} steps", "cells": int(lens.sum()),
+           "redrawn_at_t0": int(redrawn), "redrawn_after_failing_run": int(failed_total)}
+    for label, net in (("cold", None), ("warm_start", mlp)):
+        if label == "warm_start" and net is None:
+            continue
+        b = gpu.Batch(s, lens, mats, VL, VR)
+        if net is not None:
+            b.set_mlp(net)
+        ms = b.time_steps(steps, check_errors=False)
+        c = b.counters()
+        out[label] = {"cell_updates_per_s": b.ncell * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                      "tuning": b.tuning(), "failed_tubes": int((b.tube_errors() != 0).sum()),
+                      "riemann_calls": c["riemann_calls"], "riemann_iterations": c["riemann_iterations"],
+                      "riemann_evaluations": c["riemann_evaluations"]}
+        b.close()
+    return out
+
+
+def load_warmstart():
+    """The trained warm-start network committed with the package (trained on
+    the GPU by m2c_b200.warmstart), or None."""
+    from m2c_b200 import warmstart
+    p = os.path.join(ROOT, "m2c_b200", "data", "warmstart_mlp.npz")
+    return warmstart.load(p) if os.path.exists(p) else None
+
+
+def extra_warm_start(net, n=100_000):
+    """Star-state evaluations and secant iterations of the exact interface
+    solve with and without the learned warm start, on held-out problems of
+    the tube distribution; the converged states must agree to the solver's
+    tolerance."""
+    import numpy as np
+    from m2c_b200 import abi, warmstart
+    s = abi.scheme()
+    mats, VL, VR, dirs = warmstart.sample_problems(n, seed=123)
+    cold = warmstart.solve(s, mats, VL, VR, dirs)
+    t0 = time.perf_counter()
+    warm = net.predict_pairs(mats, VL, VR, dirs)
+    t_inf = time.perf_counter() - t0
+    hot = warmstart.solve(s, mats, VL, VR, dirs, warm=warm)
+    both = (cold["err"] == 0) & (hot["err"] == 0)
+    ok = both & (cold["Vsm"][:, 4] > 0) & np.isfinite(warm)
+    rel = np.abs(np.log(warm[ok] / cold["Vsm"][ok, 4]))
+    g = mats["gamma"]
+    pc = mats["p_c"]
+    cl = np.sqrt(g[0::2] * (VL[:, 4] + pc[0::2]) / VL[:, 0])
+    cr = np.sqrt(g[1::2] * (VR[:, 4] + pc[1::2]) / VR[:, 0])
+    du = (np.abs(hot["Vsm"][:, 1] - cold["Vsm"][:, 1]) / np.maximum(cl, cr))[both]
+    return {"problems": n, "solved_both": int(both.sum()),
+            "evaluations_cold": float(cold["evals"][both].mean()), "evaluations_warm": float(hot["evals"][both].mean()),
+            "evaluation_ratio": float(cold["evals"][both].mean() / hot["evals"][both].mean()),
+            "iterations_cold": float(cold["iters"][both].mean()), "iterations_warm": float(hot["iters"][both].mean()),
+            "iteration_ratio": float(cold["iters"][both].mean() / hot["iters"][both].mean()),
+            "prediction_abs_log_error_median": float(np.median(rel)),
+            "star_velocity_diff_over_c_p99": float(np.percentile(du, 99)),
+            "inference_s_host_call": t_inf}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -282,6 +420,19 @@ def main():
                "d2h_bytes_per_step": int(Vo.nbytes), "steps": ne,
                "note": "m2cg_upload_state + m2cg_run(1) + m2cg_download_state per step, ghosted AoS host state"}
 
+    extras = None
+    if rank == 0 and world == 1 and not args.only_headline:
+        extras = {}
+        net = load_warmstart()
+        for name, fn in (("bubble_cluster", lambda: extra_bubble()),
+                         ("batched_tubes", lambda: extra_tubes(mlp=net)),
+                         ("learned_warm_start", lambda: extra_warm_start(net) if net is not None else
+                          {"unavailable": "m2c_b200/data/warmstart_mlp.npz not present"})):
+            try:
+                extras[name] = fn()
+            except Exception as e:  # an extra must not cost the headline line
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -294,11 +445,14 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "m2c::stage_kernel<float,8>", "avg_launch_ms": avg_launch_ms,
-                         "alg_bytes_per_launch": alg_bytes_per_launch},
+                         "alg_bytes_per_launch": alg_bytes_per_launch,
+                         "traffic_source": "ncu dram__bytes_read+write of one stage-2 launch at 160^3, "
+                                           "scaled per cell (profiles/stage_kernel_mixed_160cube.md)"},
             "clocks": clk,
             "fp64": fp64,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "extras": extras,
         }
         print(json.dumps(out))
     if dist:

@@ -77,3 +77,21 @@ def load(path):
     net = gpu.Mlp()
     net.set_params(d["params"], d["norm"])
     return net
+
+
+if __name__ == "__main__":
+    import argparse
+    import os
+    ap = argparse.ArgumentParser(description="train the learned Riemann warm start on the GPU")
+    ap.add_argument("--n", type=int, default=2_000_000, help="sampled problems (solved on the GPU for targets)")
+    ap.add_argument("--steps", type=int, default=20_000)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=3e-3)
+    ap.add_argument("--seed", type=int, default=21)
+    ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                                                   "warmstart_mlp.npz"))
+    a = ap.parse_args()
+    net, info = train(n=a.n, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed)
+    os.makedirs(os.path.dirname(a.out), exist_ok=True)
+    save(net, a.out)
+    print({**info, "out": a.out})
