@@ -10,10 +10,8 @@
 namespace m2c {
 
 constexpr int STAGE_TY = 8;
-// Tile height per instantiation: the FP64 two-material kernel (second flux
-// buffers for interface faces) uses 32 x 4 tiles to fit in 227 KB of shared memory.
+// Tile height per instantiation (32 x 8 for every kernel).
 template <typename T, bool MULTI> struct StageTY { static constexpr int value = STAGE_TY; };
-template <> struct StageTY<double, true> { static constexpr int value = 4; };
 
 size_t stage_smem_fp64(bool multi);
 size_t stage_smem_mixed(bool multi);

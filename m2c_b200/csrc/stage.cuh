@@ -138,20 +138,13 @@ struct StageSmem {
   double red[TY * TX / 32];
 };
 
-// Two-material extra buffers: fluxes of the right-hand cell at interface faces.
-template <typename T, int TY, bool MULTI>
-struct IfaceSmem {
-  T fx2[5][(TX + 1) * TY];
-  T fy2[5][TX * (TY + 1)];
-  T fz2[2][5][TX * TY];
-};
-template <typename T, int TY>
-struct IfaceSmem<T, TY, false> {};
-
+// Shared memory of one CTA. At a material interface face the left and the
+// right cell see different fluxes; only the left cell's is stored, and the
+// right cell's (NUMERICAL interface flux) is recomputed by that cell in the
+// update phase, so the two-material kernel needs no second set of flux tiles.
 template <typename T, int TY, bool MULTI>
 struct StageSmemAll {
   StageSmem<T, TY> b;
-  IfaceSmem<T, TY, MULTI> x;
 };
 
 // Resolve a possibly-outside index along one axis (at most two cells out).
@@ -459,9 +452,9 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
   };
 
   // (3) flux across the face between mask-region cells L (plane pL) and
-  // R = L + e_d (plane pR). Writes the flux seen by the left cell (F) and,
-  // for two materials, the flux seen by the right cell (F2; they differ only
-  // at a material interface).
+  // R = L + e_d (plane pR): the flux seen by the left cell (F). F2 (the right
+  // cell's) equals F except at NUMERICAL interface faces, where the update
+  // phase forms it.
   auto face_flux = [&](int d, int pL, int mxL, int myL, int pR, int mxR, int myR, T* F, T* F2) {
     const int sL = slot4(pL), sR = slot4(pR);
     const bool rL = sm.real[sL][myL + 1][mxL + 1], rR = sm.real[sR][myR + 1][mxR + 1];
@@ -527,7 +520,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
             Sp[c] = T(iv.Vsp[base + c]);
           }
           err = flux_of<T, FLUX>(eos_of<T, MULTI>(a.s, idL), d, WL, Sm, delta, F);
-          if (!err) err = flux_of<T, FLUX>(eos_of<T, MULTI>(a.s, idR), d, Sp, WR, delta, F2);
+          (void)Sp;  // the right cell's flux against Sp is formed in its update
         }
       }
     } else {
@@ -553,30 +546,18 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
         face_flux(0, m, fxi, fyi + 1, m, fxi + 1, fyi + 1, F, F2);
 #pragma unroll
         for (int c = 0; c < 5; c++) sm.fx[c][q] = F[c];
-        if constexpr (MULTI) {
-#pragma unroll
-          for (int c = 0; c < 5; c++) all.x.fx2[c][q] = F2[c];
-        }
       } else if (q < nxy) {                   // y face below (fxi, fyi)
         const int r = q - S::NFX;
         const int fyi = r / TX, fxi = r - fyi * TX;
         face_flux(1, m, fxi + 1, fyi, m, fxi + 1, fyi + 1, F, F2);
 #pragma unroll
         for (int c = 0; c < 5; c++) sm.fy[c][r] = F[c];
-        if constexpr (MULTI) {
-#pragma unroll
-          for (int c = 0; c < 5; c++) all.x.fy2[c][r] = F2[c];
-        }
       } else {                                // z face m+1/2 of column (fxi, fyi)
         const int r = q - nxy;
         const int fyi = r / TX, fxi = r - fyi * TX;
         face_flux(2, m, fxi + 1, fyi + 1, m + 1, fxi + 1, fyi + 1, F, F2);
 #pragma unroll
         for (int c = 0; c < 5; c++) sm.fz[zs][c][r] = F[c];
-        if constexpr (MULTI) {
-#pragma unroll
-          for (int c = 0; c < 5; c++) all.x.fz2[zs][c][r] = F2[c];
-        }
       }
     }
   };
@@ -658,20 +639,42 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       }
       const int fxl = ty * (TX + 1) + tx, fyl = ty * TX + tx, fzc = ty * TX + tx;
       const int zl = m & 1, zr = (m + 1) & 1;
+      // Low faces that are material interfaces under the NUMERICAL interface
+      // flux: this cell's flux is its EOS's numerical flux between the right
+      // star state and its own cell-centred state (SpaceOperator.cpp:2499-2542).
+      T F2[3][5];
+      bool ifc[3] = {false, false, false};
+      if constexpr (MULTI) {
+        if (a.iface.mp_flux == 1) {
+          const int sc = slot4(m), lx = tx + 2, ly = ty + 2;
+          const uint8_t me = sm.ids[sc][ly][lx];
+          ifc[0] = me != sm.ids[sc][ly][lx - 1];
+          ifc[1] = me != sm.ids[sc][ly - 1][lx];
+          ifc[2] = me != sm.ids[slot4(m - 1)][ly][lx];
+          if (ifc[0] || ifc[1] || ifc[2]) {
+            const int slot = a.iface.slot[off];
+            T W[5];
+#pragma unroll
+            for (int c = 0; c < 5; c++) W[c] = sm.v[sc][c][ly][lx];
+            for (int d = 0; d < 3; d++) {
+              if (!ifc[d]) continue;
+              const long long base = ((long long)slot * 3 + d) * 5;
+              T Sp[5];
+#pragma unroll
+              for (int c = 0; c < 5; c++) Sp[c] = T(a.iface.Vsp[base + c]);
+              const int err2 = flux_of<T, FLUX>(eos_of<T, MULTI>(a.s, me), d, Sp, W, delta, F2[d]);
+              if (err2) report(a.err, err2, -1, where + 2);
+            }
+          }
+        }
+      }
 #pragma unroll
       for (int c = 0; c < 5; c++) {
         // low faces: the flux this cell sees as the right-hand cell
         // (SpaceOperator.cpp:2555-2556, 2683-2684, 2810-2811)
-        double fl, gl, hl;
-        if constexpr (MULTI) {
-          fl = double(all.x.fx2[c][fxl]);
-          gl = double(all.x.fy2[c][fyl]);
-          hl = double(all.x.fz2[zl][c][fzc]);
-        } else {
-          fl = double(sm.fx[c][fxl]);
-          gl = double(sm.fy[c][fyl]);
-          hl = double(sm.fz[zl][c][fzc]);
-        }
+        const double fl = double(ifc[0] ? F2[0][c] : sm.fx[c][fxl]);
+        const double gl = double(ifc[1] ? F2[1][c] : sm.fy[c][fyl]);
+        const double hl = double(ifc[2] ? F2[2][c] : sm.fz[zl][c][fzc]);
         double f = 0.0;
         f = f - fl * ax;
         f = f - gl * ay;
