@@ -284,6 +284,22 @@ def extra_warm_start(net, n=100_000):
             "inference_s_host_call": t_inf}
 
 
+def max_over_ranks(x, dist, device):
+    """The slowest rank's time (the replicas' job ends with it)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(cells_per_rank, world, steps, ms_max):
+    """Whole-job cell-updates/s of `world` replicas: all cells updated over
+    the slowest rank's time."""
+    return world * cells_per_rank * steps / (ms_max / 1000.0)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -348,11 +364,9 @@ def main():
     clk = clocks.stop()
     torch.cuda.synchronize()
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, "cuda")
         dist.barrier()
-    value = world * cells * args.steps / (ms / 1000.0)
+    value = replica_value(cells, world, args.steps, ms)
 
     # roofline of the dominant kernel (the fused stage): algorithmic bytes
     # 320 B/cell per RK3 step (8 FP64 5-vectors) over the 3 stage launches
@@ -413,9 +427,7 @@ def main():
             sol.download(out_V=Vo)
         te = time.perf_counter() - t0
         if dist:
-            t = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+            te = max_over_ranks(te, dist, "cuda")
         e2e = {"value": world * cells * ne / te, "unit": UNIT, "h2d_bytes_per_step": int(Vh.nbytes),
                "d2h_bytes_per_step": int(Vo.nbytes), "steps": ne,
                "note": "m2cg_upload_state + m2cg_run(1) + m2cg_download_state per step, ghosted AoS host state"}
