@@ -84,18 +84,21 @@ def fourier_box(n, seed=2024, nmodes=16, kmax=8, amp=0.01, mach_rms=0.3, bc=abi.
 
 
 def random_box(nx, ny, nz, seed=7, bc=(abi.BC_SYMMETRY,) * 6, flux=abi.FLUX_HLLC, limiter=abi.LIM_VANALBADA,
-               rk=3, cfl=0.5, precision=abi.PREC_FP64, water=False):
+               rk=3, cfl=0.5, precision=abi.PREC_FP64, water=False, nasg=False):
     """Small box with smooth seeded fields plus a density/pressure jump: a
     parity workload that exercises every limiter branch and both wave
     directions. water=True uses the stiffened-gas water of the bubble case
-    (gamma 6.12, p_inf 3.43e8 Pa)."""
+    (gamma 6.12, p_inf 3.43e8 Pa); nasg=True the same states with a
+    Noble-Abel stiffened-gas liquid water (gamma 1.19, p_c 7.028e8 Pa,
+    b 6.61e-4 m^3/kg, q -1.177788e6 J/kg)."""
     g = abi.grid(nx, ny, nz, bc=bc, inlet=(1.2, 0.3, 0.0, 0.0, 1.1), outlet=(0.9, 0.0, 0.0, 0.0, 0.8))
     s = abi.scheme(flux=flux, limiter=limiter, rk_order=rk, cfl=cfl, precision=precision)
     rng = np.random.default_rng(seed)
     xc, yc, zc = abi.cell_centres(g)
     Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
-    if water:
-        mats = [abi.material(6.12, 3.43e8)]
+    if water or nasg:
+        mats = [abi.material(6.12, 3.43e8)] if not nasg else \
+            [abi.material(1.19, 7.028e8, eos=abi.EOS_NASG, b=6.61e-4, q=-1.177788e6)]
         rho0, p0, u0 = 1000.0, 1.0e5, 50.0
         if g.bc[0] == abi.BC_INLET:
             g.inlet = (C.c_double * 5)(1100.0, 60.0, 0.0, 0.0, 2.0e8)
@@ -112,7 +115,7 @@ def random_box(nx, ny, nz, seed=7, bc=(abi.BC_SYMMETRY,) * 6, flux=abi.FLUX_HLLC
     V[1:-1, 1:-1, 1:-1, 2] = u0 * (smooth() * 10 - 0.2)
     V[1:-1, 1:-1, 1:-1, 3] = u0 * (smooth() * 10)
     V[1:-1, 1:-1, 1:-1, 4] = p0 * (jump * (1.0 + smooth()) + 0.05)
-    if water:
+    if water or nasg:
         V[1:-1, 1:-1, 1:-1, 4] = np.where(jump > 0.5, 1.0e9, 1.0e5) * (1.0 + smooth())
     return g, s, mats, V
 

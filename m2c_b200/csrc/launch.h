@@ -24,10 +24,10 @@ cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s, bool multi, i
 int stage_resident_fp64(int flux, bool multi);
 int stage_resident_mixed(int flux, bool multi);
 
-template <typename T, int FLUX, bool MULTI>
+template <typename T, int FLUX, bool MULTI, bool CONS = false>
 cudaError_t stage_occupancy(int* per_sm, int* nsm) {
   constexpr int TY = StageTY<T, MULTI>::value;
-  auto k = stage_kernel<T, TY, FLUX, MULTI>;
+  auto k = stage_kernel<T, TY, FLUX, MULTI, CONS>;
   const size_t smem = sizeof(StageSmemAll<T, TY, MULTI>);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -40,13 +40,13 @@ cudaError_t stage_occupancy(int* per_sm, int* nsm) {
   return e;
 }
 
-template <typename T, int FLUX, bool MULTI>
+template <typename T, int FLUX, bool MULTI, bool CONS>
 cudaError_t launch_stage_one(const StageArgs& a, cudaStream_t s, int* grid_out) {
   constexpr int TY = StageTY<T, MULTI>::value;
-  auto k = stage_kernel<T, TY, FLUX, MULTI>;
+  auto k = stage_kernel<T, TY, FLUX, MULTI, CONS>;
   const size_t smem = sizeof(StageSmemAll<T, TY, MULTI>);
   int per_sm = 1, nsm = 148;
-  cudaError_t e = stage_occupancy<T, FLUX, MULTI>(&per_sm, &nsm);
+  cudaError_t e = stage_occupancy<T, FLUX, MULTI, CONS>(&per_sm, &nsm);
   if (e != cudaSuccess) return e;
   int grid = a.nitems < per_sm * nsm ? a.nitems : per_sm * nsm;
   if (grid_out) *grid_out = grid;
@@ -54,15 +54,20 @@ cudaError_t launch_stage_one(const StageArgs& a, cudaStream_t s, int* grid_out) 
   return cudaGetLastError();
 }
 
+template <typename T, int FLUX>
+cudaError_t launch_stage_f(const StageArgs& a, cudaStream_t s, bool multi, int* g) {
+  const bool cons = a.s.rec_cons && a.s.rec_linear;
+  if (multi)
+    return cons ? launch_stage_one<T, FLUX, true, true>(a, s, g) : launch_stage_one<T, FLUX, true, false>(a, s, g);
+  return cons ? launch_stage_one<T, FLUX, false, true>(a, s, g) : launch_stage_one<T, FLUX, false, false>(a, s, g);
+}
+
 template <typename T>
 cudaError_t launch_stage_t(const StageArgs& a, cudaStream_t s, bool multi, int* g) {
   switch (a.s.flux) {
-    case FLUX_ROE:
-      return multi ? launch_stage_one<T, FLUX_ROE, true>(a, s, g) : launch_stage_one<T, FLUX_ROE, false>(a, s, g);
-    case FLUX_LLF:
-      return multi ? launch_stage_one<T, FLUX_LLF, true>(a, s, g) : launch_stage_one<T, FLUX_LLF, false>(a, s, g);
-    default:
-      return multi ? launch_stage_one<T, FLUX_HLLC, true>(a, s, g) : launch_stage_one<T, FLUX_HLLC, false>(a, s, g);
+    case FLUX_ROE: return launch_stage_f<T, FLUX_ROE>(a, s, multi, g);
+    case FLUX_LLF: return launch_stage_f<T, FLUX_LLF>(a, s, multi, g);
+    default: return launch_stage_f<T, FLUX_HLLC>(a, s, multi, g);
   }
 }
 

@@ -67,6 +67,7 @@ struct Grid3 {
 
 struct SchemeK {
   int flux, limiter, rec_linear, slope_zero_at_interface;
+  int rec_cons;            // reconstruct conservative variables (ReconstructionData::CONSERVATIVE)
   double alpha, delta;
   int nmat;
   Eos<double> ed[MAXMAT];  // per-material EOS, FP64 (built on the host)
@@ -273,7 +274,9 @@ template <typename T> struct StageOcc { static constexpr int value = 1; };
 #endif
 template <> struct StageOcc<float> { static constexpr int value = M2C_STAGE_OCC_F32; };
 
-template <typename T, int TY, int FLUX, bool MULTI>
+// CONS: conservative-variable reconstruction (a separate instantiation so
+// the primitive-variable kernels carry none of its code).
+template <typename T, int TY, int FLUX, bool MULTI, bool CONS>
 __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(const __grid_constant__ StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef StageSmem<T, TY> S;
@@ -403,6 +406,45 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     }
   };
 
+  // Limited slopes in direction d of the conservative variables of the real
+  // cell at (lx, ly) of plane p; u is that cell's conservative state, the
+  // neighbours' are formed with their own EOS (Reconstructor.cpp:397-404).
+  auto cons_slopes = [&](int p, int lx, int ly, int d, const T* u, T* sd) {
+    const int s0 = slot4(p);
+    int sm1 = s0, sp1 = s0, lxm = lx, lxp = lx, lym = ly, lyp = ly;
+    if (d == 0) { lxm = lx - 1; lxp = lx + 1; }
+    else if (d == 1) { lym = ly - 1; lyp = ly + 1; }
+    else { sm1 = slot4(p - 1); sp1 = slot4(p + 1); }
+    const int ia = wrap_index(i0 + lx - 2, g.nx), ja = wrap_index(j0 + ly - 2, g.ny), ka = wrap_index(p, g.nz);
+    const int ix = d == 0 ? ia : (d == 1 ? ja : ka);
+    T A, B;
+    int K = 0;
+    if (limiter == LIM_VANALBADA) {
+      A = T(g.lA[d][ix]); B = T(g.lB[d][ix]); K = g.lK[d][ix];
+    } else {
+      A = T(0); B = T(g.lC[d][ix]);
+    }
+    const uint8_t idm = sm.ids[sm1][lym][lxm], idp = sm.ids[sp1][lyp][lxp];
+    bool zero = false;
+    if (slope_zero) {
+      const uint8_t id = sm.ids[s0][ly][lx];
+      zero = id != idm || id != idp;
+    }
+    T vm[5], vp[5], um[5], up[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+      vm[c] = sm.v[sm1][c][lym][lxm];
+      vp[c] = sm.v[sp1][c][lyp][lxp];
+    }
+    eos_of<T, MULTI>(a.s, idm).p2c(vm, um);
+    eos_of<T, MULTI>(a.s, idp).p2c(vp, up);
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+      const T sl = limited_slope_c(limiter, A, B, K, alpha, u[c] - um[c], up[c] - u[c]);
+      sd[c] = zero ? T(0) : sl;
+    }
+  };
+
   // (2) slopes and revert mask of plane p
   auto mask_plane = [&](int p) {
     const int s0 = slot4(p), ms = p & 1;
@@ -419,17 +461,44 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       T v[5], sx[5], sy[5], sz[5];
 #pragma unroll
       for (int c = 0; c < 5; c++) v[c] = sm.v[s0][c][ly][lx];
-      slopes(p, lx, ly, 0, sx);
-      slopes(p, lx, ly, 1, sy);
-      slopes(p, lx, ly, 2, sz);
+      uint8_t m = 0;
+      int err = ERR_NONE;
+      bool cons = false;
+      if (CONS && rec_linear) {
+        // conservative variables: slopes of U, face states C2P(U -+ sigma/2);
+        // any non-physical face sends the cell back to primitive variables
+        // (the RETRY of Reconstructor.cpp:719-775)
+        T u[5];
+        e.p2c(v, u);
+        cons_slopes(p, lx, ly, 0, u, sx);
+        cons_slopes(p, lx, ly, 1, u, sy);
+        cons_slopes(p, lx, ly, 2, u, sz);
+        cons = true;
+        uint8_t clipm = 0;
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+          const T* sg = q < 2 ? sx : (q < 4 ? sy : sz);
+          T uf[5], f[5];
+#pragma unroll
+          for (int c = 0; c < 5; c++) uf[c] = (q & 1) ? u[c] + T(0.5) * sg[c] : u[c] - T(0.5) * sg[c];
+          e.c2p(uf, f);
+          if (e.bad(f)) cons = false;
+          else if (e.needs_clip(f)) clipm |= uint8_t(1u << q);  // SpaceOperator.cpp:3240-3273
+        }
+        if (cons) m = uint8_t(clipm | 0x40);
+      }
+      if (!cons) {
+        slopes(p, lx, ly, 0, sx);
+        slopes(p, lx, ly, 1, sy);
+        slopes(p, lx, ly, 2, sz);
+        err = cell_faces(e, v, sx, sy, sz, m);
+      }
 #pragma unroll
       for (int c = 0; c < 5; c++) {
         sm.sig[ms][0][c][my][mx] = sx[c];
         sm.sig[ms][1][c][my][mx] = sy[c];
         sm.sig[ms][2][c][my][mx] = sz[c];
       }
-      uint8_t m;
-      const int err = cell_faces(e, v, sx, sy, sz, m);
       sm.mask[ms][my][mx] = m;
       if (err) {
         const int ia = wrap_index(i0 + mx - 1, g.nx), ja = wrap_index(j0 + my - 1, g.ny);
@@ -442,7 +511,27 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
   // direction d, side 0 = minus face (v - s/2), 1 = plus face (v + s/2).
   auto cell_face = [&](int p, int mx, int my, int d, int side, T* out) {
     const int s0 = slot4(p), ms = p & 1;
-    const bool rev = (sm.mask[ms][my][mx] >> (2 * d + side)) & 1u;
+    const uint8_t mk = sm.mask[ms][my][mx];
+    const bool rev = (mk >> (2 * d + side)) & 1u;
+    if (CONS && (mk & 0x40)) {  // conservative-variable face state
+      T v[5], u[5], uf[5];
+#pragma unroll
+      for (int c = 0; c < 5; c++) v[c] = sm.v[s0][c][my + 1][mx + 1];
+      if (rev) {
+#pragma unroll
+        for (int c = 0; c < 5; c++) out[c] = v[c];
+        return;
+      }
+      const Eos<T>& e = eos_of<T, MULTI>(a.s, sm.ids[s0][my + 1][mx + 1]);
+      e.p2c(v, u);
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        const T sd = sm.sig[ms][d][c][my][mx];
+        uf[c] = side ? u[c] + T(0.5) * sd : u[c] - T(0.5) * sd;
+      }
+      e.c2p(uf, out);
+      return;
+    }
 #pragma unroll
     for (int c = 0; c < 5; c++) {
       const T v = sm.v[s0][c][my + 1][mx + 1];

@@ -91,6 +91,47 @@ def test_water_stiffened_gas_matches_reference(gpu, ref):
     assert rel_err(inner(Vg), inner(Vr)) <= FP64_TOL
 
 
+@pytest.mark.parametrize("flux", [abi.FLUX_HLLC, abi.FLUX_ROE, abi.FLUX_LLF])
+def test_nasg_water_matches_reference(gpu, ref, flux):
+    """Noble-Abel stiffened gas (VarFcnNASG.h): residual and RK3 steps."""
+    bc = (abi.BC_INLET, abi.BC_OUTLET) + (abi.BC_SYMMETRY,) * 4
+    g, s, mats, V = cases.random_box(30, 9, 8, seed=23 + flux, bc=bc, nasg=True, rk=3, flux=flux)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V)
+    assert rel_err(inner(sol.residual()), inner(rc.residual())) <= FP64_TOL
+    Vg, Vr, _, _ = run_both(gpu, ref, g, s, mats, V, nsteps=5)
+    assert rel_err(inner(Vg), inner(Vr)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("flux", [abi.FLUX_HLLC, abi.FLUX_ROE, abi.FLUX_LLF])
+@pytest.mark.parametrize("limiter", [abi.LIM_GENMINMOD, abi.LIM_VANALBADA])
+def test_conservative_reconstruction_matches_reference(gpu, ref, flux, limiter):
+    """Reconstruction of conservative variables (ReconstructionData::CONSERVATIVE),
+    including the fall-back to primitive variables for cells with a
+    non-physical face (Reconstructor.cpp:719-775): residual and RK3 steps."""
+    bc = (abi.BC_INLET, abi.BC_OUTLET, abi.BC_SLIPWALL, abi.BC_STICKWALL, abi.BC_SYMMETRY, abi.BC_SYMMETRY)
+    g, s, mats, V = cases.random_box(31, 10, 9, seed=41 + flux * 3 + limiter, bc=bc, flux=flux, limiter=limiter)
+    s.rec_var = abi.RECVAR_CONSERVATIVE
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V)
+    assert rel_err(inner(sol.residual()), inner(rc.residual())) <= FP64_TOL
+    Vg, Vr, _, _ = run_both(gpu, ref, g, s, mats, V, nsteps=4)
+    m = face_ghosts_mask(Vg.shape)
+    assert rel_err(Vg[m], Vr[m]) <= FP64_TOL
+
+
+def test_conservative_reconstruction_water_matches_reference(gpu, ref):
+    bc = (abi.BC_INLET, abi.BC_OUTLET) + (abi.BC_SYMMETRY,) * 4
+    g, s, mats, V = cases.random_box(33, 9, 9, seed=29, bc=bc, water=True, rk=3)
+    s.rec_var = abi.RECVAR_CONSERVATIVE
+    Vg, Vr, _, _ = run_both(gpu, ref, g, s, mats, V, nsteps=5)
+    assert rel_err(inner(Vg), inner(Vr)) <= FP64_TOL
+
+
 def test_periodic_box_matches_tiled_reference(gpu, ref):
     """The reference has no periodic boundary: it runs a 3x3x3 tiled copy, whose
     central tile evolves as the periodic box for 2 RK3 steps (reach 6 cells/step)."""
