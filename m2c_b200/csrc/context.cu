@@ -214,8 +214,8 @@ static void upload_vec(T** d, const std::vector<T>& h, cudaStream_t s, m2cg_stat
 static m2cg_status check_scheme(const m2cg_scheme* s, const m2cg_material* mats, int nmat) {
   if (nmat < 1 || nmat > MAXMAT) return fail(M2CG_ERR_ARG, "nmat must be in [1,%d]", MAXMAT);
   if (s->flux < 0 || s->flux > 2) return fail(M2CG_ERR_UNSUPPORTED, "flux %d not supported (ROE/LLF/HLLC)", s->flux);
-  if (s->rec_var != M2CG_RECVAR_PRIMITIVE && s->rec_var != M2CG_RECVAR_CONSERVATIVE)
-    return fail(M2CG_ERR_UNSUPPORTED, "characteristic-variable reconstruction is not implemented on the GPU");
+  if (s->rec_var < M2CG_RECVAR_PRIMITIVE || s->rec_var > M2CG_RECVAR_CONS_CHAR)
+    return fail(M2CG_ERR_ARG, "unknown reconstruction variable type %d", s->rec_var);
   if (s->rk_order < 1 || s->rk_order > 3) return fail(M2CG_ERR_ARG, "rk_order must be 1, 2 or 3");
   for (int m = 0; m < nmat; m++)
     if (mats[m].eos != M2CG_EOS_SG && mats[m].eos != M2CG_EOS_NASG)
@@ -330,7 +330,7 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   sk.limiter = scheme->limiter;
   sk.rec_linear = scheme->rec_type == M2CG_REC_LINEAR;
   sk.slope_zero_at_interface = scheme->slope_near_interface == 0;
-  sk.rec_cons = scheme->rec_var == M2CG_RECVAR_CONSERVATIVE;
+  sk.rec_var = scheme->rec_var;
   sk.alpha = scheme->minmod_coeff;
   sk.delta = scheme->roe_delta;
   sk.nmat = nmat;

@@ -56,7 +56,7 @@ cudaError_t launch_stage_one(const StageArgs& a, cudaStream_t s, int* grid_out) 
 
 template <typename T, int FLUX>
 cudaError_t launch_stage_f(const StageArgs& a, cudaStream_t s, bool multi, int* g) {
-  const bool cons = a.s.rec_cons && a.s.rec_linear;
+  const bool cons = a.s.rec_var != 0 && a.s.rec_linear;
   if (multi)
     return cons ? launch_stage_one<T, FLUX, true, true>(a, s, g) : launch_stage_one<T, FLUX, true, false>(a, s, g);
   return cons ? launch_stage_one<T, FLUX, false, true>(a, s, g) : launch_stage_one<T, FLUX, false, false>(a, s, g);

@@ -208,6 +208,105 @@ M2C_HD T limited_slope(int limiter, T A, T B, int k, T alpha, T dql, T dqr) {
 }
 
 // ---------------------------------------------------------------------------
+// Characteristic variables for reconstruction (FluxFcnBase.h:309-500): the
+// eigenvectors of the flux Jacobian in direction d at the cell state V0.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct CharBasis {
+  T e0, c0, dpdrho0, Gamma0, kin0, un0, alpha0, beta0;
+  T n[3];
+  bool ok;  // c0^2 >= 0 (the reference aborts otherwise)
+};
+
+template <typename T>
+M2C_HD void char_basis(const Eos<T>& eos, int d, const T* V0, CharBasis<T>& b) {
+  b.e0 = eos.energy(V0[0], V0[4]);
+  T c2 = eos.c2(V0[0], b.e0);
+  b.ok = !(c2 < T(0));
+  b.c0 = b.ok ? sqrt(c2) : T(0);
+  b.dpdrho0 = eos.dpdrho(V0[0], b.e0);
+  b.Gamma0 = eos.big_gamma(V0[0], b.e0);
+  b.kin0 = T(0.5) * (V0[1] * V0[1] + V0[2] * V0[2] + V0[3] * V0[3]);
+  b.un0 = V0[d + 1];
+  b.n[0] = d == 0 ? T(1) : T(0);
+  b.n[1] = d == 1 ? T(1) : T(0);
+  b.n[2] = d == 2 ? T(1) : T(0);
+  b.alpha0 = V0[0] * b.Gamma0 / (V0[4] * b.Gamma0 + V0[0] * b.dpdrho0);
+  b.beta0 = (b.e0 - b.kin0 + V0[4] / V0[0]) * b.alpha0;
+}
+
+// dW = R0^{-1} x (the conservative-space left eigenvectors)
+template <typename T>
+M2C_HD void char_rinv(const CharBasis<T>& b, const T* V0, const T* x, T* dW) {
+  T R[5][5];
+  R[0][0] = T(0.5) * (T(1) - b.beta0 + b.un0 / b.c0);
+  for (int i = 0; i < 3; i++) R[0][1 + i] = T(-0.5) * (b.alpha0 * V0[1 + i] + b.n[i] / b.c0);
+  R[0][4] = b.alpha0 / T(2);
+  for (int i = 0; i < 3; i++) R[1 + i][0] = -V0[1 + i] + (b.beta0 + b.un0) * b.n[i];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      R[1 + i][1 + j] = (i == j ? T(1) : T(0)) + b.alpha0 * b.n[i] * V0[1 + j] - b.n[i] * b.n[j];
+  for (int i = 0; i < 3; i++) R[1 + i][4] = -b.alpha0 * b.n[i];
+  R[4][0] = T(0.5) * (T(1) - b.beta0 - b.un0 / b.c0);
+  for (int i = 0; i < 3; i++) R[4][1 + i] = T(-0.5) * (b.alpha0 * V0[1 + i] - b.n[i] / b.c0);
+  R[4][4] = b.alpha0 / T(2);
+  for (int i = 0; i < 5; i++) {
+    T acc = T(0);
+    for (int j = 0; j < 5; j++) acc += R[i][j] * x[j];
+    dW[i] = acc;
+  }
+}
+
+// R0 dW (the conservative-space right eigenvectors)
+template <typename T>
+M2C_HD void char_r(const CharBasis<T>& b, const T* V0, const T* dW, T* y) {
+  const T H0 = b.e0 + b.kin0 + V0[4] / V0[0];
+  T R[5][5];
+  R[0][0] = T(1);
+  for (int i = 0; i < 3; i++) R[0][1 + i] = b.n[i];
+  R[0][4] = T(1);
+  for (int i = 0; i < 3; i++) R[1 + i][0] = V0[1 + i] - b.c0 * b.n[i];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) R[1 + i][1 + j] = (i == j ? T(1) : T(0)) + V0[1 + i] * b.n[j] - b.n[i] * b.n[j];
+  for (int i = 0; i < 3; i++) R[1 + i][4] = V0[1 + i] + b.c0 * b.n[i];
+  R[4][0] = H0 - b.un0 * b.c0;
+  const T param = b.e0 + b.kin0 - b.dpdrho0 / b.Gamma0 - b.un0;
+  for (int i = 0; i < 3; i++) R[4][1 + i] = V0[1 + i] + param * b.n[i];
+  R[4][4] = H0 + b.un0 * b.c0;
+  for (int i = 0; i < 5; i++) {
+    T acc = T(0);
+    for (int j = 0; j < 5; j++) acc += R[i][j] * dW[j];
+    y[i] = acc;
+  }
+}
+
+// PrimitiveToPrimitiveCharacteristic: dW = R0^{-1} Q0 dV
+template <typename T>
+M2C_HD void prim_to_char(const CharBasis<T>& b, const T* V0, const T* dV, T* dW) {
+  const T Q51 = b.e0 + b.kin0 - b.dpdrho0 / b.Gamma0;
+  T t[5];
+  t[0] = dV[0];
+  t[1] = V0[1] * dV[0] + V0[0] * dV[1];
+  t[2] = V0[2] * dV[0] + V0[0] * dV[2];
+  t[3] = V0[3] * dV[0] + V0[0] * dV[3];
+  t[4] = Q51 * dV[0] + V0[0] * V0[1] * dV[1] + V0[0] * V0[2] * dV[2] + V0[0] * V0[3] * dV[3] + T(1) / b.Gamma0 * dV[4];
+  char_rinv(b, V0, t, dW);
+}
+
+// PrimitiveCharacteristicToPrimitive: dV = Qbar^{-1} R0 dW
+template <typename T>
+M2C_HD void char_to_prim(const CharBasis<T>& b, const T* V0, const T* dW, T* dV) {
+  T t[5];
+  char_r(b, V0, dW, t);
+  dV[0] = t[0];
+  dV[1] = -V0[1] / V0[0] * t[0] + t[1] / V0[0];
+  dV[2] = -V0[2] / V0[0] * t[0] + t[2] / V0[0];
+  dV[3] = -V0[3] / V0[0] * t[0] + t[3] / V0[0];
+  dV[4] = ((-b.e0 + b.kin0) * b.Gamma0 + b.dpdrho0) * t[0] -
+          b.Gamma0 * (V0[1] * t[1] + V0[2] * t[2] + V0[3] * t[3] - t[4]);
+}
+
+// ---------------------------------------------------------------------------
 // Physical flux in direction d (0 x / F, 1 y / G, 2 z / H).
 // ---------------------------------------------------------------------------
 template <typename T>

@@ -67,7 +67,8 @@ struct Grid3 {
 
 struct SchemeK {
   int flux, limiter, rec_linear, slope_zero_at_interface;
-  int rec_cons;            // reconstruct conservative variables (ReconstructionData::CONSERVATIVE)
+  int rec_var;             // ReconstructionData::VariableType: 0 primitive, 1 conservative,
+                           // 2 primitive characteristic, 3 conservative characteristic
   double alpha, delta;
   int nmat;
   Eos<double> ed[MAXMAT];  // per-material EOS, FP64 (built on the host)
@@ -274,8 +275,8 @@ template <typename T> struct StageOcc { static constexpr int value = 1; };
 #endif
 template <> struct StageOcc<float> { static constexpr int value = M2C_STAGE_OCC_F32; };
 
-// CONS: conservative-variable reconstruction (a separate instantiation so
-// the primitive-variable kernels carry none of its code).
+// CONS: reconstruction in conservative or characteristic variables (a
+// separate instantiation so the primitive-variable kernels carry none of it).
 template <typename T, int TY, int FLUX, bool MULTI, bool CONS>
 __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(const __grid_constant__ StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -406,10 +407,15 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     }
   };
 
-  // Limited slopes in direction d of the conservative variables of the real
-  // cell at (lx, ly) of plane p; u is that cell's conservative state, the
-  // neighbours' are formed with their own EOS (Reconstructor.cpp:397-404).
-  auto cons_slopes = [&](int p, int lx, int ly, int d, const T* u, T* sd) {
+  // Limited slopes in direction d of the real cell at (lx, ly) of plane p in
+  // the scheme's non-primitive variables (Reconstructor.cpp:397-404, 469-651):
+  // differences of the conservative variables (rv 1, 3; neighbours converted
+  // with their own EOS) or of the primitive ones (rv 2), projected on the
+  // characteristic basis at the cell state (rv 2, 3) and limited there, then
+  // mapped back. u is the cell's conservative state. Returns false where the
+  // basis does not exist (c^2 < 0; the reference aborts).
+  auto nonprim_slopes = [&](int p, int lx, int ly, int d, int rv, const Eos<T>& e, const T* v, const T* u,
+                            T* sd) -> bool {
     const int s0 = slot4(p);
     int sm1 = s0, sp1 = s0, lxm = lx, lxp = lx, lym = ly, lyp = ly;
     if (d == 0) { lxm = lx - 1; lxp = lx + 1; }
@@ -430,19 +436,54 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       const uint8_t id = sm.ids[s0][ly][lx];
       zero = id != idm || id != idp;
     }
-    T vm[5], vp[5], um[5], up[5];
+    T qm[5], qp[5], dl[5], dr[5];
 #pragma unroll
     for (int c = 0; c < 5; c++) {
-      vm[c] = sm.v[sm1][c][lym][lxm];
-      vp[c] = sm.v[sp1][c][lyp][lxp];
+      qm[c] = sm.v[sm1][c][lym][lxm];
+      qp[c] = sm.v[sp1][c][lyp][lxp];
     }
-    eos_of<T, MULTI>(a.s, idm).p2c(vm, um);
-    eos_of<T, MULTI>(a.s, idp).p2c(vp, up);
+    const bool uspace = rv != 2;
+    if (uspace) {
+      T t[5];
+      eos_of<T, MULTI>(a.s, idm).p2c(qm, t);
+#pragma unroll
+      for (int c = 0; c < 5; c++) qm[c] = t[c];
+      eos_of<T, MULTI>(a.s, idp).p2c(qp, t);
+#pragma unroll
+      for (int c = 0; c < 5; c++) qp[c] = t[c];
+    }
+    const T* q0 = uspace ? u : v;
 #pragma unroll
     for (int c = 0; c < 5; c++) {
-      const T sl = limited_slope_c(limiter, A, B, K, alpha, u[c] - um[c], up[c] - u[c]);
-      sd[c] = zero ? T(0) : sl;
+      dl[c] = q0[c] - qm[c];
+      dr[c] = qp[c] - q0[c];
     }
+    bool ok = true;
+    if (rv == 1) {
+#pragma unroll
+      for (int c = 0; c < 5; c++) sd[c] = limited_slope_c(limiter, A, B, K, alpha, dl[c], dr[c]);
+    } else {
+      CharBasis<T> cb;
+      char_basis(e, d, v, cb);
+      ok = cb.ok;
+      T wl[5], wr[5], sw[5];
+      if (rv == 2) {
+        prim_to_char(cb, v, dl, wl);
+        prim_to_char(cb, v, dr, wr);
+      } else {
+        char_rinv(cb, v, dl, wl);
+        char_rinv(cb, v, dr, wr);
+      }
+#pragma unroll
+      for (int c = 0; c < 5; c++) sw[c] = limited_slope_c(limiter, A, B, K, alpha, wl[c], wr[c]);
+      if (rv == 2) char_to_prim(cb, v, sw, sd);
+      else char_r(cb, v, sw, sd);
+    }
+    if (zero) {
+#pragma unroll
+      for (int c = 0; c < 5; c++) sd[c] = T(0);
+    }
+    return ok;
   };
 
   // (2) slopes and revert mask of plane p
@@ -465,33 +506,42 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       int err = ERR_NONE;
       bool cons = false;
       if (CONS && rec_linear) {
-        // conservative variables: slopes of U, face states C2P(U -+ sigma/2);
-        // any non-physical face sends the cell back to primitive variables
-        // (the RETRY of Reconstructor.cpp:719-775)
+        // non-primitive variables; any non-physical face sends the cell back
+        // to primitive variables (the RETRY of Reconstructor.cpp:719-775)
+        const int rv = a.s.rec_var;
+        const bool uspace = rv != 2;
         T u[5];
         e.p2c(v, u);
-        cons_slopes(p, lx, ly, 0, u, sx);
-        cons_slopes(p, lx, ly, 1, u, sy);
-        cons_slopes(p, lx, ly, 2, u, sz);
+        bool okb = nonprim_slopes(p, lx, ly, 0, rv, e, v, u, sx);
+        okb = nonprim_slopes(p, lx, ly, 1, rv, e, v, u, sy) && okb;
+        okb = nonprim_slopes(p, lx, ly, 2, rv, e, v, u, sz) && okb;
+        if (!okb) err = ERR_SOUND;
         cons = true;
         uint8_t clipm = 0;
 #pragma unroll
         for (int q = 0; q < 6; q++) {
           const T* sg = q < 2 ? sx : (q < 4 ? sy : sz);
-          T uf[5], f[5];
+          T f[5];
+          if (uspace) {
+            T uf[5];
 #pragma unroll
-          for (int c = 0; c < 5; c++) uf[c] = (q & 1) ? u[c] + T(0.5) * sg[c] : u[c] - T(0.5) * sg[c];
-          e.c2p(uf, f);
+            for (int c = 0; c < 5; c++) uf[c] = (q & 1) ? u[c] + T(0.5) * sg[c] : u[c] - T(0.5) * sg[c];
+            e.c2p(uf, f);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 5; c++) f[c] = (q & 1) ? v[c] + T(0.5) * sg[c] : v[c] - T(0.5) * sg[c];
+          }
           if (e.bad(f)) cons = false;
           else if (e.needs_clip(f)) clipm |= uint8_t(1u << q);  // SpaceOperator.cpp:3240-3273
         }
-        if (cons) m = uint8_t(clipm | 0x40);
+        if (cons) m = uint8_t(clipm | (uspace ? 0x40 : 0));
       }
       if (!cons) {
         slopes(p, lx, ly, 0, sx);
         slopes(p, lx, ly, 1, sy);
         slopes(p, lx, ly, 2, sz);
-        err = cell_faces(e, v, sx, sy, sz, m);
+        const int err2 = cell_faces(e, v, sx, sy, sz, m);
+        if (err2) err = err2;
       }
 #pragma unroll
       for (int c = 0; c < 5; c++) {

@@ -105,15 +105,18 @@ def test_nasg_water_matches_reference(gpu, ref, flux):
     assert rel_err(inner(Vg), inner(Vr)) <= FP64_TOL
 
 
+@pytest.mark.parametrize("rec_var", [abi.RECVAR_CONSERVATIVE, abi.RECVAR_PRIM_CHAR, abi.RECVAR_CONS_CHAR])
 @pytest.mark.parametrize("flux", [abi.FLUX_HLLC, abi.FLUX_ROE, abi.FLUX_LLF])
 @pytest.mark.parametrize("limiter", [abi.LIM_GENMINMOD, abi.LIM_VANALBADA])
-def test_conservative_reconstruction_matches_reference(gpu, ref, flux, limiter):
-    """Reconstruction of conservative variables (ReconstructionData::CONSERVATIVE),
-    including the fall-back to primitive variables for cells with a
-    non-physical face (Reconstructor.cpp:719-775): residual and RK3 steps."""
+def test_nonprimitive_reconstruction_matches_reference(gpu, ref, flux, limiter, rec_var):
+    """Reconstruction in conservative, primitive-characteristic and
+    conservative-characteristic variables (ReconstructionData::VariableType,
+    FluxFcnBase.h:309-500), including the fall-back to primitive variables
+    for cells with a non-physical face (Reconstructor.cpp:719-775): residual
+    and RK3 steps."""
     bc = (abi.BC_INLET, abi.BC_OUTLET, abi.BC_SLIPWALL, abi.BC_STICKWALL, abi.BC_SYMMETRY, abi.BC_SYMMETRY)
     g, s, mats, V = cases.random_box(31, 10, 9, seed=41 + flux * 3 + limiter, bc=bc, flux=flux, limiter=limiter)
-    s.rec_var = abi.RECVAR_CONSERVATIVE
+    s.rec_var = rec_var
     sol = gpu.Solver(g, s, mats)
     sol.upload(V)
     rc = ref.RefCase(g, s, mats)
@@ -124,10 +127,11 @@ def test_conservative_reconstruction_matches_reference(gpu, ref, flux, limiter):
     assert rel_err(Vg[m], Vr[m]) <= FP64_TOL
 
 
-def test_conservative_reconstruction_water_matches_reference(gpu, ref):
+@pytest.mark.parametrize("rec_var", [abi.RECVAR_CONSERVATIVE, abi.RECVAR_PRIM_CHAR, abi.RECVAR_CONS_CHAR])
+def test_nonprimitive_reconstruction_water_matches_reference(gpu, ref, rec_var):
     bc = (abi.BC_INLET, abi.BC_OUTLET) + (abi.BC_SYMMETRY,) * 4
     g, s, mats, V = cases.random_box(33, 9, 9, seed=29, bc=bc, water=True, rk=3)
-    s.rec_var = abi.RECVAR_CONSERVATIVE
+    s.rec_var = rec_var
     Vg, Vr, _, _ = run_both(gpu, ref, g, s, mats, V, nsteps=5)
     assert rel_err(inner(Vg), inner(Vr)) <= FP64_TOL
 
