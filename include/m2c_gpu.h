@@ -112,6 +112,9 @@ typedef struct {
   /* Warm start of the exact Riemann solve (no reference counterpart): the
    * bracket tried around a proposed star pressure p is [p(1-d), p(1+d)]. */
   double riem_warm_delta;
+  /* MultiPhaseData::riemann_normal: direction of the interface Riemann
+   * problem, 0 LEVEL_SET (gradient of phi), 1 MESH (face normal), 2 AVERAGE */
+  int mp_riemann_normal;
 } m2cg_scheme;
 
 /* One level set (LevelSetSchemeData, IoData.h:653-679; reinit

@@ -22,6 +22,7 @@ LIM_NONE, LIM_GENMINMOD, LIM_VANALBADA = 0, 1, 2
 RECVAR_PRIMITIVE, RECVAR_CONSERVATIVE, RECVAR_PRIM_CHAR, RECVAR_CONS_CHAR = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 MPFLUX_EXACT, MPFLUX_NUMERICAL, MPFLUX_LLF = 0, 1, 2
+RIEMANN_NORMAL_LEVEL_SET, RIEMANN_NORMAL_MESH, RIEMANN_NORMAL_AVERAGE = 0, 1, 2
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_RIEMANN, ERR_REINIT, ERR_ITER_CAP, ERR_NOMEM, ERR_UNSUPPORTED = range(9)
 LSBC_NONE, LSBC_ZERO_NEUMANN, LSBC_LINEAR_EXTRAPOLATION, LSBC_NON_NEGATIVE = 0, 1, 2, 3
 
@@ -59,6 +60,7 @@ class Scheme(C.Structure):
         ("riem_tol_main", C.c_double), ("riem_tol_shock", C.c_double), ("riem_tol_rarefaction", C.c_double),
         ("riem_min_pressure", C.c_double), ("riem_failure_threshold", C.c_double),
         ("riem_pressure_at_failure", C.c_double), ("riem_warm_delta", C.c_double),
+        ("mp_riemann_normal", C.c_int),
     ]
 
 
@@ -103,6 +105,7 @@ def scheme(**kw):
     s.riem_failure_threshold = 0.2
     s.riem_pressure_at_failure = 1.0e-8
     s.riem_warm_delta = 0.01
+    s.mp_riemann_normal = RIEMANN_NORMAL_MESH
     for k, v in kw.items():
         if not hasattr(s, k):
             raise AttributeError(k)

@@ -95,6 +95,7 @@ class TimeIntegratorGPU : public TimeIntegratorBase {
     s.mp_phasechange_type = (int)iod.multiphase.phasechange_type;
     s.mp_phasechange_dir = (int)iod.multiphase.phasechange_dir;
     s.mp_apply_failsafe_density = (int)iod.multiphase.apply_failsafe_density;
+    s.mp_riemann_normal = (int)iod.multiphase.riemann_normal;
     const ExactRiemannSolverData& r = iod.exact_riemann;
     s.riem_maxits_main = r.maxIts_main;
     s.riem_maxits_bracket = r.maxIts_bracket;

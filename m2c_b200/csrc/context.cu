@@ -82,6 +82,7 @@ extern "C" void m2cg_default_scheme(m2cg_scheme* s) {
   s->riem_failure_threshold = 0.2;
   s->riem_pressure_at_failure = 1.0e-8;
   s->riem_warm_delta = 0.01;
+  s->mp_riemann_normal = 1;  // MultiPhaseData::MESH (IoData.cpp:1408)
 }
 
 extern "C" void m2cg_default_material(m2cg_material* m) {

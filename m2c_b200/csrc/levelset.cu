@@ -21,6 +21,7 @@
 
 #include "fd3.cuh"
 #include "levelset.h"
+#include "ls_device.cuh"
 
 namespace m2c {
 
@@ -107,53 +108,6 @@ void levelset_geom_destroy(LsGeom* geo) {
 // --------------------------------------------------------------------------
 // device: phi with the boundary rule
 // --------------------------------------------------------------------------
-__device__ __forceinline__ long long loff(const Grid3& g, int i, int j, int k) {
-  return (long long)k * g.plane + (long long)j * g.px + i;
-}
-
-// phi at (i,j,k) where at most one index is one cell outside (face ghost),
-// or any index outside on a periodic axis.
-__device__ double phi_at(const Grid3& g, const LsGeom& geo, const double* phi, int i, int j, int k) {
-  int c[3] = {i, j, k};
-  const int n[3] = {g.nx, g.ny, g.nz};
-  int gaxis = -1, gside = 0;
-  for (int a = 0; a < 3; a++) {
-    if (c[a] >= 0 && c[a] < n[a]) continue;
-    if (g.bc[2 * a] == BC_PERIODIC) {
-      c[a] = c[a] < 0 ? c[a] + n[a] : c[a] - n[a];
-      continue;
-    }
-    gaxis = a;
-    gside = c[a] < 0 ? 0 : 1;
-  }
-  if (gaxis < 0) return phi[loff(g, c[0], c[1], c[2])];
-  // face ghost: LevelSetOperator::ApplyBoundaryConditions
-  const int a = gaxis, nA = n[a];
-  const int bc = geo.bc[2 * a + gside];
-  int im[3] = {c[0], c[1], c[2]};
-  im[a] = gside == 0 ? 0 : nA - 1;
-  const double image = phi[loff(g, im[0], im[1], im[2])];
-  if (bc == M2CG_LSBC_LINEAR_EXTRAPOLATION || bc == M2CG_LSBC_NON_NEGATIVE) {
-    double val = image;
-    const double* X = geo.xg[a];
-    if (nA >= 2) {  // LevelSetOperator.cpp:957 (i+2<NX at i=-1) and 967 (i-2>=0 at i=NX)
-      int i1 = gside == 0 ? 0 : nA - 1, i2 = gside == 0 ? 1 : nA - 2;
-      int p1[3] = {im[0], im[1], im[2]}, p2[3] = {im[0], im[1], im[2]};
-      p1[a] = i1;
-      p2[a] = i2;
-      const double r = X[(gside == 0 ? -1 : nA) + 1], r1 = X[i1 + 1], r2 = X[i2 + 1];
-      const double f1 = phi[loff(g, p1[0], p1[1], p1[2])], f2 = phi[loff(g, p2[0], p2[1], p2[2])];
-      val = f1 + (f2 - f1) / (r2 - r1) * (r - r1);
-    }
-    if (bc == M2CG_LSBC_NON_NEGATIVE) {
-      const double d2wall = 0.5 * fabs(X[im[a] + 1] - X[(gside == 0 ? -1 : nA) + 1]);
-      val = smax(-d2wall, val);
-    }
-    return val;
-  }
-  return image;  // ZERO_NEUMANN
-}
-
 // -(u . grad phi) with upwind-biased FD3 at cell (i,j,k)
 __device__ double ls_residual(const Grid3& g, const LsGeom& geo, const double* phi, int i, int j, int k, double u,
                               double v, double w) {

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "levelset.h"
+#include "ls_device.cuh"
 #include "multiphase.h"
 #include "riemann_batch.h"
 
@@ -171,11 +172,15 @@ struct IfaceRiemannArgs {
   uint8_t* rsValid;
   double* scratch;
   DevError* err;
+  int normal_mode;        // MultiPhaseData::riemann_normal
+  const double* phi;      // phi^n (the reference's loose coupling uses the step's phi)
+  LsGeom geo;
 };
 
 // One exact Riemann problem per interface face (SpaceOperator.cpp:2499-2523):
-// MESH normal, cell-centred states (constant reconstruction at the interface),
-// star states clipped with each side's EOS, stage-1 results kept.
+// direction by the riemann_normal rule, cell-centred states (constant
+// reconstruction at the interface), star states clipped with each side's EOS,
+// stage-1 results kept.
 __global__ void k_iface_riemann(IfaceRiemannArgs a) {
   const Grid3& g = a.st.g;
   long long nf = a.counts[1];
@@ -200,7 +205,8 @@ __global__ void k_iface_riemann(IfaceRiemannArgs a) {
     double VL[5], VR[5];
     stage_state(a.st, a.eos, offL, idL, VL);
     stage_state(a.st, a.eos, offR, idR, VR);
-    double dir[3] = {d == 0 ? 1.0 : 0.0, d == 1 ? 1.0 : 0.0, d == 2 ? 1.0 : 0.0};
+    double dir[3];
+    riemann_direction(a.normal_mode, g, a.geo, a.phi, i, j, k, d, idR, idL, dir);
     double Vs[5], Vsm[5], Vsp[5];
     int mid = 0;
     bool bad = false;
@@ -586,6 +592,9 @@ m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
   }
   ra.scratch = mp->scratch;
   ra.err = a.err;
+  ra.normal_mode = mp->scheme.mp_riemann_normal;
+  ra.phi = mp->phiN;
+  ra.geo = mp->lsg;
   k_iface_riemann<<<IFACE_RIEMANN_THREADS / 128, 128, 0, s>>>(ra);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
   a.iface.slot = mp->slot;

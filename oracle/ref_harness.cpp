@@ -107,6 +107,7 @@ void fill_scheme(IoData& iod, const m2cg_scheme& s) {
   iod.multiphase.phasechange_type = (MultiPhaseData::PhaseChangeType)s.mp_phasechange_type;
   iod.multiphase.phasechange_dir = (MultiPhaseData::PhaseChangeDirection)s.mp_phasechange_dir;
   iod.multiphase.apply_failsafe_density = (MultiPhaseData::OnOff)s.mp_apply_failsafe_density;
+  iod.multiphase.riemann_normal = (MultiPhaseData::RiemannNormal)s.mp_riemann_normal;
   ExactRiemannSolverData& r = iod.exact_riemann;
   r.maxIts_main = s.riem_maxits_main;
   r.maxIts_bracket = s.riem_maxits_bracket;
