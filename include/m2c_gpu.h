@@ -218,7 +218,12 @@ const char* m2cg_last_error(void);
  * ExactRiemannSolverBase.cpp:59-342), FP64, one problem per thread.
  * Inputs per problem: VL[5], VR[5] primitive states, idl/idr material ids,
  * dir[3] unit normal. Outputs: Vs[5] state at xi=0, id, Vsm[5], Vsp[5]
- * star states, iterations (outer secant iterations), err (0 OK).
+ * star states, iterations (outer secant iterations, both solver variants),
+ * err: 0 OK; bit 1 not solved (where the adaptive solve cannot bracket or
+ * converge, the non-adaptive variant of ExactRiemannSolverBase.cpp:2199-2945
+ * solves again, as the reference does, and bit 1 means it failed too; the
+ * outputs then hold the reference's best-effort answer); bit 2 the
+ * integration-path scratch ran out; bit 4 a state the reference aborts on.
  * Host pointers; the call copies in and out.
  * warm (optional, may be NULL): an initial star-pressure guess per problem;
  * NaN entries mean "no guess".

@@ -11,6 +11,12 @@
 //                                            cached integration path; Hugoniot root)
 //   Rarefaction_OneStepRK4        1729-1852 (Cash-Karp/Fehlberg step in pressure)
 //   HugoniotEquation              ExactRiemannSolverBase.h:58-75
+// and the retry the reference makes when the adaptive solve cannot bracket
+// the root or does not converge, ExactRiemannSolverNonAdaptive:
+//   ComputeRiemannSolution        2199-2470 (same main loop, no retry)
+//   ComputeRhoUStar               2476-2845 (rarefaction by classical RK4 steps
+//                                            in pressure; same Hugoniot root)
+//   Rarefaction_OneStepRK4        2850-2945
 // The step sequence, branch structure and floating-point expressions follow
 // the reference so that, compiled without FMA contraction, results agree
 // with it to round-off. The step-size control's pow(x, 0.25) and pow(x, 0.2)
@@ -41,8 +47,9 @@ struct RiemannParams {
 // result flags
 enum {
   RIEM_OK = 0,
-  RIEM_FAILED = 1,           // the reference would retry with ExactRiemannSolverNonAdaptive
+  RIEM_FAILED = 1,           // not solved (the non-adaptive retry included)
   RIEM_PATH_OVERFLOW = 2,    // integration-path scratch exhausted
+  RIEM_RETRY = 0x100,        // internal: the adaptive solve hands over to the non-adaptive one
 };
 
 // Integration path: points (p, rho, u) with decreasing pressure.
@@ -69,6 +76,122 @@ struct RiemannSolver {
   int iterations;          // outer secant iterations of the main loop
   double warm = NAN;       // proposed star pressure of the current solve (NaN: none)
   mutable int evaluations; // star-state evaluations at a trial pressure (bracketing + main loop)
+  bool nonadaptive = false; // ExactRiemannSolverNonAdaptive's ComputeRhoUStar in place of the adaptive one
+  bool retried = false;     // the last solve went through the non-adaptive retry
+
+  // ExactRiemannSolverNonAdaptive::Rarefaction_OneStepRK4 (2850-2945): one
+  // classical RK4 step of d(rho)/dp = 1/c^2, du/dp = -+1/(rho c).
+  M2C_HD bool rk4_step(int wave, int id, double rho_0, double u_0, double p_0, double dp, double& rho, double& u,
+                       double& p, double& xi) const {
+    const Eos<double>& e = eos[id];
+    dp = -dp;
+    double e_0 = e.energy(rho_0, p_0);
+    double c_0_square = e.c2(rho_0, e_0);
+    if (rho_0 <= 0 || c_0_square < 0) return false;
+    double c_0 = sqrt(c_0_square);
+    double rho_1 = rho_0 + 0.5 * dp / c_0_square;
+    double p_1 = p_0 + 0.5 * dp;
+    double e_1 = e.energy(rho_1, p_1);
+    double c_1_square = e.c2(rho_1, e_1);
+    if (rho_1 <= 0 || c_1_square < 0) return false;
+    double c_1 = sqrt(c_1_square);
+    double rho_2 = rho_0 + 0.5 * dp / c_1_square;
+    double p_2 = p_1;
+    double e_2 = e.energy(rho_2, p_2);
+    double c_2_square = e.c2(rho_2, e_2);
+    if (rho_2 <= 0 || c_2_square < 0) return false;
+    double c_2 = sqrt(c_2_square);
+    double rho_3 = rho_0 + dp / c_2_square;
+    double p_3 = p_0 + dp;
+    double e_3 = e.energy(rho_3, p_3);
+    double c_3_square = e.c2(rho_3, e_3);
+    if (rho_3 <= 0 || c_3_square < 0) return false;
+    double c_3 = sqrt(c_3_square);
+    double drho = 1.0 / 6.0 * dp * (1. / c_0_square + 2.0 * (1. / c_1_square + 1. / c_2_square) + 1. / c_3_square);
+    double du = 1.0 / 6.0 * dp *
+                (1. / c_0 / rho_0 + 2.0 * (1. / c_1 / rho_1 + 1. / c_2 / rho_2) + 1. / c_3 / rho_3);
+    if (isnan(du)) return false;
+    rho = rho_0 + drho;
+    p = p_0 + dp;
+    u = (wave == 1) ? u_0 - du : u_0 + du;
+    double ee = e.energy(rho, p);
+    double c = e.c2(rho, ee);
+    if (rho <= 0 || c < 0) return false;
+    c = sqrt(c);
+    xi = (wave == 1) ? u - c : u + c;
+    return true;
+  }
+
+  // Rarefaction branch of ExactRiemannSolverNonAdaptive::ComputeRhoUStar
+  // (2487-2633): steps in pressure of at most (p - ps)/numSteps, grown by at
+  // most 4x per step, from the deepest cached path point above ps.
+  M2C_HD bool rarefaction_nonadaptive(int wave, RPath& path, double rho, double u, double p, double ps, int id,
+                                      double& rhos, double& us, bool* trans_rare, double* Vrare_x0) const {
+    const Eos<double>& e = eos[id];
+    double rhos_0 = rho, us_0 = u, ps_0 = p, xi_0;
+    double rhos_1 = rho, us_1 = u, ps_1 = p, xi_1 = 0.0;
+    double dp_target = (p - ps) / P.numSteps_rarefaction;
+    double ee = e.energy(rho, p);
+    double dpdrho = e.dpdrho(rho, ee);
+    double drho_op1 = (p - ps) / dpdrho / P.numSteps_rarefaction;
+    double drho_op2 = rho / (2.5 * P.numSteps_rarefaction);
+    double drho_target = smin(drho_op1, drho_op2);
+    double dp = smin(dp_target, drho_target * dpdrho);
+    double pressure_endpoint_tol = P.tol_rarefaction * smax(1.0, fabs(p));
+    double c = e.c2(rho, ee);
+    if (rho <= 0 || c < 0) return false;
+    c = sqrt(c);
+    int index0 = 0;
+    if (path.n > 1) {
+      for (int j = path.n - 1; j >= 0; j--) {
+        if (path.P(j) > ps) {
+          index0 = j;
+          break;
+        }
+      }
+      ps_0 = path.P(index0);
+      rhos_0 = path.R(index0);
+      us_0 = path.U(index0);
+      dp = smin((p - ps) / P.numSteps_rarefaction, ps_0 - ps);
+    }
+    double xi = (wave == 1) ? u - c : u + c;
+    xi_0 = xi;
+    const int moreSteps = 5;
+    for (int i = 0; i < P.numSteps_rarefaction * moreSteps; i++) {
+      if (fabs(ps_1 - ps) <= pressure_endpoint_tol) {
+        rhos = rhos_1;
+        us = us_1;
+        return !e.bad(rhos, ps);
+      }
+      bool ok = rk4_step(wave, id, rhos_0, us_0, ps_0, dp, rhos_1, us_1, ps_1, xi_1);
+      if (!ok) {
+        dp = dp / 2.0;
+        if (dp == 0.0) break;
+        continue;
+      }
+      if (ps_1 - ps < -pressure_endpoint_tol) {
+        dp = ps_0 - ps;
+        continue;
+      }
+      if (ps_1 < path.P(path.n - 1)) path.push(ps_1, rhos_1, us_1);
+      if (trans_rare && Vrare_x0 && xi_0 * xi_1 <= 0) {  // transonic rarefaction
+        *trans_rare = true;
+        double w0 = fabs(xi_1), w1 = fabs(xi_0);
+        double ww = w0 + w1;
+        w0 /= ww;
+        w1 /= ww;
+        Vrare_x0[0] = w0 * rhos_0 + w1 * rhos_1;
+        Vrare_x0[1] = w0 * us_0 + w1 * us_1;
+        Vrare_x0[2] = w0 * ps_0 + w1 * ps_1;
+      }
+      dp = smin(smin(dp_target, ps_1 - ps), 4.0 * dp);
+      rhos_0 = rhos_1;
+      us_0 = us_1;
+      ps_0 = ps_1;
+      xi_0 = xi_1;
+    }
+    return false;  // did not reach ps (both of the reference's outcomes fail)
+  }
 
   // Rarefaction_OneStepRK4 (ExactRiemannSolverBase.cpp:1729-1852)
   M2C_HD bool rk_step(int wave, int id, double rho_0, double u_0, double p_0, double dp, double& rho, double& u,
@@ -150,6 +273,8 @@ struct RiemannSolver {
     if (wave == 1) evaluations++;
     rhos = rho;
     us = u;
+    if (p > ps && nonadaptive) return rarefaction_nonadaptive(wave, path, rho, u, p, ps, id, rhos, us, trans_rare,
+                                                              Vrare_x0);
     if (p > ps) {  // rarefaction: numerical integration
       double rhos_0 = rho, us_0 = u, ps_0 = p, xi_0;
       double rhos_1 = rho, us_1 = u, ps_1 = p, xi_1 = 0.0;
@@ -655,6 +780,30 @@ struct RiemannSolver {
     bad_state = false;
     iterations = 0;
     evaluations = 0;
+    nonadaptive = false;
+    retried = false;
+    warm = warm_p;
+    int r = 0, overflow = 0;
+    // one loop, so that the solver body is inlined once
+    for (int pass = 0; pass < 2; pass++) {
+      r = attempt(dir, Vm, idl, Vp, idr, Vs, id, Vsm, Vsp, bad_state);
+      overflow |= r & RIEM_PATH_OVERFLOW;
+      if (!(r & RIEM_RETRY)) break;
+      // ExactRiemannSolverBase.cpp:173-188 and 327-330: a fresh
+      // ExactRiemannSolverNonAdaptive (empty integration paths, acoustic
+      // starting points) solves the problem again and its result is returned
+      nonadaptive = true;
+      retried = true;
+      warm = NAN;
+    }
+    nonadaptive = false;
+    return r | overflow;
+  }
+
+  // One solve by the adaptive (nonadaptive = false) or the non-adaptive
+  // solver: ComputeRiemannSolution (59-342) / (2199-2470).
+  M2C_HD int attempt(const double* dir, const double* Vm, int idl, const double* Vp, int idr, double* Vs, int& id,
+                     double* Vsm, double* Vsp, bool& bad_state) {
     double rhol = Vm[0];
     double ul = Vm[1] * dir[0] + Vm[2] * dir[1] + Vm[3] * dir[2];
     double pl = Vm[4];
@@ -685,19 +834,27 @@ struct RiemannSolver {
                Vsp, bad_state);
       return RIEM_OK;
     }
-    warm = warm_p;
     success = initial_interval(rhol, ul, pl, cl, idl, rhor, ur, pr, cr, idr, p0, rhol0, rhor0, ul0, ur0, p1, rhol1,
                                rhor1, ul1, ur1);
     if (!success) {
-      // the reference fills a best-effort answer, then retries with the
-      // non-adaptive solver and returns its result (173-188)
+      // a best-effort answer at p1 (173-188, 2302-2335); the adaptive solver
+      // then hands over to the non-adaptive one, which returns it as failed
       success = rho_u_star(1, path1, rhol, ul, pl, p1, idl, rhol0, rhol0 * 1.1, rhol2, ul2, &trans_rare, Vrare_x0);
       success = success && rho_u_star(3, path3, rhor, ur, pr, p1, idr, rhor0, rhol0 * 1.1, rhor2, ur2, &trans_rare,
                                       Vrare_x0);
-      if (success)
+      if (success) {
         finalize(dir, Vm, Vp, rhol, ul, pl, idl, rhor, ur, pr, idr, rhol2, rhor2, 0.5 * (ul2 + ur2), p1, trans_rare,
                  Vrare_x0, Vs, id, Vsm, Vsp, bad_state);
-      return RIEM_FAILED | ((path1.overflow || path3.overflow) ? RIEM_PATH_OVERFLOW : 0);
+      } else {  // the initial states as the solution
+        for (int i = 0; i < 5; i++) {
+          Vsm[i] = Vm[i];
+          Vsp[i] = Vp[i];
+        }
+        const double u_avg = 0.5 * (ul + ur);
+        id = u_avg >= 0 ? idl : idr;
+        for (int i = 0; i < 5; i++) Vs[i] = u_avg >= 0 ? Vm[i] : Vp[i];
+      }
+      return (nonadaptive ? RIEM_FAILED : RIEM_RETRY) | ((path1.overflow || path3.overflow) ? RIEM_PATH_OVERFLOW : 0);
     }
     f0 = ul0 - ur0;
     f1 = ul1 - ur1;
@@ -745,12 +902,12 @@ struct RiemannSolver {
         break;
       trans_rare = false;
     }
-    iterations = iter + 1;
+    iterations += iter + 1;
     double u2 = 0.5 * (ul2 + ur2);
     finalize(dir, Vm, Vp, rhol, ul, pl, idl, rhor, ur, pr, idr, rhol2, rhor2, u2, p2, trans_rare, Vrare_x0, Vs, id,
              Vsm, Vsp, bad_state);
     int flags = (path1.overflow || path3.overflow) ? RIEM_PATH_OVERFLOW : 0;
-    if (iter == P.maxIts_main) return RIEM_FAILED | flags;
+    if (iter == P.maxIts_main) return (nonadaptive ? RIEM_FAILED : RIEM_RETRY) | flags;
     return RIEM_OK | flags;
   }
 };

@@ -1,0 +1,62 @@
+// Test harness: the library's exact Riemann solver (m2c_b200/csrc/riemann.cuh)
+// compiled for the host with g++ (no FMA contraction, the host C library's
+// pow and sqrt), so that it can be compared with the reference's own solver
+// bit for bit. Not part of the library.
+#include <cmath>
+#include <vector>
+
+#include "../../include/m2c_gpu.h"
+#include "../../m2c_b200/csrc/riemann.cuh"
+
+using namespace m2c;
+
+extern "C" int host_riemann(const m2cg_scheme* s, const m2cg_material* mats, int nmat, int n, const double* dir,
+                            const double* VL, const int* idl, const double* VR, const int* idr, double* Vs, int* id,
+                            double* Vsm, double* Vsp, int* err, int* retried) {
+  std::vector<Eos<double>> eos(nmat);
+  for (int m = 0; m < nmat; m++) {
+    MatParams p;
+    p.kind = mats[m].eos;
+    p.gam = mats[m].gamma;
+    p.pc = mats[m].p_c;
+    p.b = mats[m].b;
+    p.q = mats[m].q;
+    p.rhomin = mats[m].rhomin;
+    p.pmin = mats[m].pmin;
+    p.rhomax = mats[m].rhomax;
+    p.pmax = mats[m].pmax;
+    p.failsafe_density = mats[m].failsafe_density;
+    eos[m] = make_eos<double>(p);
+  }
+  RiemannParams P;
+  P.maxIts_main = s->riem_maxits_main;
+  P.maxIts_bracket = s->riem_maxits_bracket;
+  P.maxIts_shock = s->riem_maxits_shock;
+  P.numSteps_rarefaction = s->riem_nsteps_rarefaction;
+  P.tol_main = s->riem_tol_main;
+  P.tol_shock = s->riem_tol_shock;
+  P.tol_rarefaction = s->riem_tol_rarefaction;
+  P.min_pressure = s->riem_min_pressure;
+  P.failure_threshold = s->riem_failure_threshold;
+  P.pressure_at_failure = s->riem_pressure_at_failure;
+  P.warm_delta = s->riem_warm_delta;
+  const int cap = 512;  // the device solver's path capacity (riemann_batch.h)
+  std::vector<double> scratch(2 * 3 * cap);
+  RiemannSolver rs;
+  rs.P = P;
+  rs.eos = eos.data();
+  rs.path1.pt = scratch.data();
+  rs.path1.cap = cap;
+  rs.path3.pt = scratch.data() + 3 * cap;
+  rs.path3.cap = cap;
+  for (int q = 0; q < n; q++) {
+    bool bad = false;
+    int mid = 0;
+    int r = rs.solve(dir + 3 * q, VL + 5 * q, idl[q], VR + 5 * q, idr[q], Vs + 5 * q, mid, Vsm + 5 * q, Vsp + 5 * q,
+                     NAN, bad);
+    id[q] = mid;
+    err[q] = r | (bad ? 4 : 0);
+    retried[q] = rs.retried ? 1 : 0;
+  }
+  return 0;
+}
