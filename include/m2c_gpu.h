@@ -188,10 +188,31 @@ typedef struct {
   long long clipped_cells;       /* ClipDensityAndPressure counts */
   long long reinit_calls;
   long long kernel_launches;
-  long long unresolved_cells;    /* cells that changed material with no usable star state */
+  long long unresolved_cells;    /* cells that changed material and that neither the star states nor
+                                    the extrapolation could update (handed to FixUnresolvedNodes) */
   long long riemann_evaluations; /* star-state evaluations at trial pressures (bracketing + secant) */
+  long long failsafe_cells;      /* cells given the material's failsafe density (no valid neighbour
+                                    within 10 layers, MultiPhaseOperator.cpp:1352-1369) */
 } m2cg_counters;
 m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
+
+/* MultiPhaseOperator::UpdateStateVariablesAfterInterfaceMotion
+ * (MultiPhaseOperator.cpp:823-1400) on the context's resident state: every
+ * interior cell whose ID (the context's, as uploaded or advanced) differs from
+ * IDn (host, ghosted layout of m2cg_upload_state) gets its state from the
+ * stage-1 star states of its interface faces (phasechange_type
+ * RIEMANN_SOLUTION) or from its neighbours (EXTRAPOLATION), then
+ * FixUnresolvedNodes, then ClipDensityAndPressure. use_stored_riemann_solutions
+ * = 1 uses the star states stored by the last m2cg_advance (IDn must then be
+ * the IDs at the start of that step; M2CG_ERR_ARG if no step ran since the
+ * last upload); 0 passes none, as an empty RiemannSolutions does. m2cg_advance
+ * calls the same update at the end of every step. *unresolved (may be NULL)
+ * receives the cells handed to FixUnresolvedNodes. With
+ * apply_failsafe_density Off, a background cell with no valid neighbour
+ * within 10 layers would need the level-set correction of
+ * TimeIntegrator.cpp:742-761, which is not built: M2CG_ERR_UNSUPPORTED. */
+m2cg_status m2cg_update_states_after_interface_motion(m2cg_ctx* ctx, const double* IDn,
+                                                      int use_stored_riemann_solutions, int* unresolved);
 
 /* Run nsteps CFL-limited steps with the state resident in device memory and
  * report their device time (CUDA events on the context's stream) and the

@@ -23,6 +23,8 @@ RECVAR_PRIMITIVE, RECVAR_CONSERVATIVE, RECVAR_PRIM_CHAR, RECVAR_CONS_CHAR = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 MPFLUX_EXACT, MPFLUX_NUMERICAL, MPFLUX_LLF = 0, 1, 2
 RIEMANN_NORMAL_LEVEL_SET, RIEMANN_NORMAL_MESH, RIEMANN_NORMAL_AVERAGE = 0, 1, 2
+PHASECHANGE_RIEMANN_SOLUTION, PHASECHANGE_EXTRAPOLATION = 0, 1
+PHASECHANGE_ALL, PHASECHANGE_UPWIND = 0, 1
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_RIEMANN, ERR_REINIT, ERR_ITER_CAP, ERR_NOMEM, ERR_UNSUPPORTED = range(9)
 LSBC_NONE, LSBC_ZERO_NEUMANN, LSBC_LINEAR_EXTRAPOLATION, LSBC_NON_NEGATIVE = 0, 1, 2, 3
 

@@ -145,6 +145,7 @@ struct m2cg_ctx {
   double* stage_buf = nullptr;
   size_t stage_bytes = 0;
   bool dtmin_valid = false;
+  bool rs_valid = false;  // the multiphase star states stored by the last step match the resident state
   m2cg_counters counters = {};
   Multiphase* mp = nullptr;  // two-material machinery (nullptr for one material)
   // optional per-stage event timing (benchmark roofline)
@@ -611,10 +612,34 @@ extern "C" m2cg_status m2cg_upload_state(m2cg_ctx* c, const double* V, const dou
     c->counters.kernel_launches += 1;
   }
   CK(cudaGetLastError());
+  c->rs_valid = false;
   if (c->mp) {
     st = multiphase_upload_phi(c->mp, c->stream, phi, c->stage_buf, c->id);
     if (st) return st;
   }
+  st = compute_dtmin(c);
+  if (st) return st;
+  return check_device_error(c);
+}
+
+extern "C" m2cg_status m2cg_update_states_after_interface_motion(m2cg_ctx* c, const double* IDn, int use_rs,
+                                                                 int* unresolved) {
+  if (!c || !IDn) return fail(M2CG_ERR_ARG, "null argument");
+  if (!c->mp) return fail(M2CG_ERR_ARG, "no level set: no cell changes material");
+  if (use_rs && !c->rs_valid) return fail(M2CG_ERR_ARG, "no star states stored since the last upload");
+  size_t ng = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  m2cg_status st = ensure_stage_buf(c, ng * sizeof(double));
+  if (st) return st;
+  long long n = (long long)c->nx * c->ny * c->nz;
+  CK(cudaMemcpyAsync(c->stage_buf, IDn, ng * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  k_unpack_id<<<grid1d(n), 256, 0, c->stream>>>(c->stage_buf, c->nx, c->ny, c->nz, c->px, c->plane,
+                                                 multiphase_idn(c->mp));
+  CK(cudaGetLastError());
+  const bool mixed = c->scheme.precision == M2CG_PREC_MIXED;
+  st = multiphase_update_states(c->mp, c->stream, c->V[c->cur], mixed ? c->Vf[c->cur] : nullptr, c->id, c->err,
+                                use_rs != 0, unresolved);
+  if (st) return st;
+  c->counters.kernel_launches += 5;
   st = compute_dtmin(c);
   if (st) return st;
   return check_device_error(c);
@@ -740,6 +765,7 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
                                          mixed ? c->Vf[c->cur] : nullptr, c->id, c->clock, c->err, &c->counters);
     if (st) return st;
     c->dtmin_valid = false;
+    c->rs_valid = true;
   } else {
     c->dtmin_valid = want_dtmin;
   }
@@ -818,6 +844,7 @@ extern "C" m2cg_status m2cg_compute_residual(m2cg_ctx* c, double* R_host) {
     a.Pin[p] = c->scheme.precision == M2CG_PREC_MIXED ? (const void*)c->Vf[c->cur][p] : (const void*)Vn[p];
   }
   if (c->mp) {
+    c->rs_valid = false;  // the interface slots are reassigned
     m2cg_status st = multiphase_begin_step(c->mp, c->stream, Vn, c->id);
     if (st) return st;
     st = multiphase_stage(c->mp, c->stream, a);

@@ -75,7 +75,9 @@ struct Multiphase {
   int stage = 0;
   // host-side counters
   long long riemann_calls = 0, riemann_iterations = 0, riemann_errors = 0, unresolved = 0, reinit_calls = 0;
-  long long riemann_evaluations = 0;
+  long long riemann_evaluations = 0, failsafe_cells = 0;
+  uint8_t* mask = nullptr;       // [interior cells] unresolved-list membership, zero between updates
+  double failsafe[MAXMAT] = {};  // MaterialModelData::failsafe_density
   double* reinit_buf = nullptr;  // reinitialisation work arrays
   double reinit_cfl = 0.8;       // pseudo-time CFL, reduced on failed attempts
   long long reinit_iterations = 0;
@@ -326,10 +328,16 @@ struct StateUpdateArgs {
   const double* rsVsm;
   const double* rsVsp;
   const uint8_t* rsValid;
-  const int* changed;
-  int* nchanged;        // [0] count, [1] unresolved (out)
-  int* unresolved;      // list (reuses the tail of `changed`)
+  int* changed;         // ordered changed cells; the unresolved ones are compacted into its head
+  int* nchanged;        // [0] changed, [1] unresolved after the first pass, [2] still unresolved, [3] failsafe
   DevError* err;
+  int use_rs;           // stage-1 Riemann solutions of this step are available
+  int type;             // MultiPhaseData::phasechange_type: 0 RIEMANN_SOLUTION, 1 EXTRAPOLATION
+  int upwind;           // MultiPhaseData::phasechange_dir == UPWIND
+  int failsafe;         // MultiPhaseData::apply_failsafe_density == On
+  LsGeom geo;           // cell-centre coordinates (one ghost per side)
+  uint8_t* mask;        // [interior cells] member of the unresolved list (all zero between calls)
+  double failsafe_rho[MAXMAT];  // MaterialModelData::failsafe_density
 };
 
 // Star state stored on one face of cell (i,j,k): side 0 = its low face
@@ -405,7 +413,85 @@ __device__ int local_update(const StateUpdateArgs& a, int i, int j, int k, int m
   return counter;
 }
 
-// Sequential pass over the changed cells in (k, j, i) order.
+__device__ __forceinline__ void centre(const LsGeom& geo, int i, int j, int k, double* x) {
+  x[0] = geo.xg[0][i + 1];
+  x[1] = geo.xg[1][j + 1];
+  x[2] = geo.xg[2][k + 1];
+}
+
+__device__ __forceinline__ bool outside(const Grid3& g, int i, int j, int k) {
+  return i < 0 || i >= g.nx || j < 0 || j >= g.ny || k < 0 || k >= g.nz;
+}
+
+__device__ __forceinline__ double norm3(const double* a) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+
+// max(0, (x0 - x1)/|x0 - x1| . v1/|v1|), the upwind weight of a neighbour at
+// x1 with velocity v1 for the cell at x0 (Vec3D::operator/= multiplies by the
+// reciprocal). *dist receives |x0 - x1|.
+__device__ __forceinline__ double upwind_weight(const double* x0, const double* x1, const double* nv, double* dist) {
+  double v1[3] = {nv[1], nv[2], nv[3]};
+  const double v1norm = norm3(v1);
+  if (v1norm != 0) {
+    const double inv = 1.0 / v1norm;
+    v1[0] *= inv; v1[1] *= inv; v1[2] *= inv;
+  }
+  double d[3] = {x0[0] - x1[0], x0[1] - x1[1], x0[2] - x1[2]};
+  const double dn = norm3(d);
+  *dist = dn;
+  const double inv = 1.0 / dn;
+  d[0] *= inv; d[1] *= inv; d[2] *= inv;
+  const double w = d[0] * v1[0] + d[1] * v1[1] + d[2] * v1[2];
+  return w > 0.0 ? w : 0.0;
+}
+
+// UpdateStateVariablesByExtrapolation, one cell (MultiPhaseOperator.cpp:1032-1128):
+// weighted average of the 26 neighbours that keep the cell's new ID and did
+// not change ID themselves; false if no weight.
+__device__ bool extrapolate(const StateUpdateArgs& a, int i, int j, int k, int myid, double* v) {
+  const Grid3& g = a.g;
+  double x0[3];
+  centre(a.geo, i, j, k, x0);
+  double sum_weight = 0.0, vsum[5] = {0, 0, 0, 0, 0};
+  for (int nk = k - 1; nk <= k + 1; nk++)
+    for (int nj = j - 1; nj <= j + 1; nj++)
+      for (int ni = i - 1; ni <= i + 1; ni++) {
+        if (outside(g, ni, nj, nk)) continue;
+        const long long off = offset_of(g, ni, nj, nk);
+        if (a.id[off] != myid) continue;
+        if (a.id[off] != a.idn[off]) continue;
+        double x1[3], nv[5];
+        centre(a.geo, ni, nj, nk, x1);
+        for (int p = 0; p < 5; p++) nv[p] = a.V[p][off];
+        double weight;
+        if (!a.upwind) {
+          double d[3] = {x0[0] - x1[0], x0[1] - x1[1], x0[2] - x1[2]};
+          weight = 1.0 / norm3(d);
+        } else {
+          double dist;
+          weight = upwind_weight(x0, x1, nv, &dist);
+        }
+        if (weight > 0) {
+          sum_weight += weight;
+          for (int p = 0; p < 5; p++) vsum[p] += weight * nv[p];
+        }
+      }
+  if (sum_weight == 0) return false;
+  for (int p = 0; p < 5; p++) v[p] = vsum[p] / sum_weight;  // Vec5D::operator/ divides
+  return true;
+}
+
+__device__ __forceinline__ void store(const StateUpdateArgs& a, long long off, const double* v) {
+  for (int p = 0; p < 5; p++) a.V[p][off] = v[p];
+  if (a.Vf[0])
+    for (int p = 0; p < 5; p++) a.Vf[p][off] = (float)v[p];
+}
+
+// Sequential pass over the changed cells in (k, j, i) order
+// (UpdateStateVariablesByRiemannSolutions, MultiPhaseOperator.cpp:857-911, or
+// ...ByExtrapolation, 1032-1151), then FixUnresolvedNodes (1156-1400) over
+// the cells neither could update, in the same order. Every updated cell is
+// clipped and checked (ClipDensityAndPressure after the update,
+// TimeIntegrator.cpp:767).
 __global__ void k_state_update(StateUpdateArgs a) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   const Grid3& g = a.g;
@@ -419,21 +505,120 @@ __global__ void k_state_update(StateUpdateArgs a) {
     const int myid = a.id[off];
     double v[5];
     for (int p = 0; p < 5; p++) v[p] = a.V[p][off];
-    int counter = local_update(a, i, j, k, myid, v, true);
-    if (counter == 0) counter = local_update(a, i, j, k, myid, v, false);
-    if (counter == 0) {
-      nun++;
-      continue;  // unresolved: left as is and counted
+    bool done;
+    if (a.type == 1) {
+      done = extrapolate(a, i, j, k, myid, v);
+    } else {
+      int counter = a.use_rs ? local_update(a, i, j, k, myid, v, true) : 0;
+      if (counter == 0 && a.use_rs) counter = local_update(a, i, j, k, myid, v, false);
+      done = counter != 0;
     }
-    // ClipDensityAndPressure(V, ID) at the end of UpdateSolutionAfterTimeStepping
+    if (!done) {
+      a.changed[nun++] = q;  // unresolved: compacted in order into the head of the list
+      a.mask[q] = 1;
+      continue;
+    }
     a.eos[myid].clip(v);
     if (a.eos[myid].bad(v)) report(a.err, ERR_STATE, q, 9);
-    for (int p = 0; p < 5; p++) a.V[p][off] = v[p];
-    if (a.Vf[0])
-      for (int p = 0; p < 5; p++) a.Vf[p][off] = (float)v[p];
+    store(a, off, v);
   }
   a.nchanged[1] = nun;
+  // FixUnresolvedNodes. `reset` is set once per call, not per cell, as in the
+  // reference (1183): from the second cell with an upwind neighbour on, the
+  // upwind sum adds to the cell's current state instead of replacing it.
+  bool reset = false;
+  int still = 0, nfailsafe = 0;
+  for (int t = 0; t < nun; t++) {
+    const int q = a.changed[t];
+    int i, j, k;
+    cell_coords(g, q, i, j, k);
+    const long long off = offset_of(g, i, j, k);
+    const int myid = a.id[off];
+    double x0[3];
+    centre(a.geo, i, j, k, x0);
+    double v[5], vtmp[5] = {0, 0, 0, 0, 0};
+    for (int p = 0; p < 5; p++) v[p] = a.V[p][off];
+    double sum_weight = 0.0, sum_weight2 = 0.0;
+    for (int nk = k - 1; nk <= k + 1; nk++)
+      for (int nj = j - 1; nj <= j + 1; nj++)
+        for (int ni = i - 1; ni <= i + 1; ni++) {
+          if (outside(g, ni, nj, nk)) continue;
+          const long long noff = offset_of(g, ni, nj, nk);
+          if (a.id[noff] != myid) continue;
+          if (ni == i && nj == j && nk == k) continue;
+          if (a.mask[((long long)nk * g.ny + nj) * g.nx + ni]) continue;
+          double x1[3], nv[5], dist;
+          centre(a.geo, ni, nj, nk, x1);
+          for (int p = 0; p < 5; p++) nv[p] = a.V[p][noff];
+          const double weight = upwind_weight(x0, x1, nv, &dist);
+          if (weight > 0) {
+            sum_weight += weight;
+            if (reset) {
+              for (int p = 0; p < 5; p++) v[p] += weight * nv[p];
+            } else {
+              for (int p = 0; p < 5; p++) v[p] = weight * nv[p];
+              reset = true;
+            }
+          }
+          const double w2 = 1.0 / dist;
+          for (int p = 0; p < 5; p++) vtmp[p] += w2 * nv[p];
+          sum_weight2 += w2;
+        }
+    bool done = false;
+    if (a.upwind && sum_weight > 0) {
+      const double inv = 1.0 / sum_weight;  // Vec5D::operator/=
+      for (int p = 0; p < 5; p++) v[p] *= inv;
+      done = true;
+    } else if (sum_weight2 > 0) {
+      for (int p = 0; p < 5; p++) v[p] = vtmp[p] / sum_weight2;
+      done = true;
+    } else {
+      // last resort: keep velocity and pressure, take the density from the
+      // nearest layer (up to 10) that has valid cells, inverse-distance weighted
+      double density = 0.0;
+      for (int layer = 1; layer <= 10 && !done; layer++) {
+        for (int nk = k - layer; nk <= k + layer; nk++)
+          for (int nj = j - layer; nj <= j + layer; nj++)
+            for (int ni = i - layer; ni <= i + layer; ni++) {
+              if (outside(g, ni, nj, nk)) continue;
+              const long long noff = offset_of(g, ni, nj, nk);
+              if (a.id[noff] != myid) continue;
+              if (ni == i && nj == j && nk == k) continue;
+              if (a.mask[((long long)nk * g.ny + nj) * g.nx + ni]) continue;
+              double x1[3];
+              centre(a.geo, ni, nj, nk, x1);
+              double d[3] = {x1[0] - x0[0], x1[1] - x0[1], x1[2] - x0[2]};
+              const double dist = norm3(d);
+              sum_weight += 1.0 / dist;
+              density += (1.0 / dist) * a.V[0][noff];
+            }
+        if (sum_weight > 0) {
+          v[0] = density / sum_weight;
+          done = true;
+        }
+      }
+      if (!done) {
+        if (myid != 0 || a.failsafe) {
+          v[0] = a.failsafe_rho[myid];
+          nfailsafe++;
+          done = true;
+        } else {
+          still++;  // left for the level-set correction, which is not built: reported by the host
+        }
+      }
+    }
+    if (done) {
+      a.eos[myid].clip(v);
+      if (a.eos[myid].bad(v)) report(a.err, ERR_STATE, q, 9);
+      store(a, off, v);
+    }
+  }
+  for (int t = 0; t < nun; t++) a.mask[a.changed[t]] = 0;
+  a.nchanged[2] = still;
+  a.nchanged[3] = nfailsafe;
 }
+
+void set_last_error(const char* msg);
 
 static int grid1d(long long n) {
   long long b = (n + 255) / 256;
@@ -452,11 +637,9 @@ using namespace m2c;
 m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk, const m2cg_scheme& scheme,
                               const m2cg_material* mats, int nmat, const m2cg_levelset& ls, const double* const* xc,
                               const double* const* dx, Multiphase** out) {
-  (void)mats;
-  (void)nmat;
   *out = nullptr;
-  if (scheme.mp_recon != 0) return M2CG_ERR_UNSUPPORTED;            // interface Riemann inputs: constant recon
-  if (scheme.mp_phasechange_type != 0) return M2CG_ERR_UNSUPPORTED; // RIEMANN_SOLUTION update
+  if (scheme.mp_recon != 0) return M2CG_ERR_UNSUPPORTED;  // interface Riemann inputs: constant recon
+  if (scheme.mp_phasechange_type != 0 && scheme.mp_phasechange_type != 1) return M2CG_ERR_UNSUPPORTED;
   if (ls.material_id != 1) return M2CG_ERR_UNSUPPORTED;
   if (ls.reinit_first_layer != 0) return M2CG_ERR_UNSUPPORTED;
   Multiphase* mp = new Multiphase;
@@ -467,6 +650,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   mp->rp = riemann_params(scheme);
   mp->reinit_cfl = ls.reinit_cfl;
   mp->ncell = g.plane * g.nz;
+  for (int m = 0; m < nmat && m < MAXMAT; m++) mp->failsafe[m] = mats[m].failsafe_density;
   const long long n = mp->ncell;
   const long long ninterior = (long long)g.nx * g.ny * g.nz;
   mp->cap_slots = ninterior < 65536 ? ninterior : (ninterior / 8 > 65536 ? ninterior / 8 : 65536);
@@ -496,6 +680,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   mp->nblocks_scan = 148 * 8;
   A((void**)&mp->blockcnt, mp->nblocks_scan * 4);
   A((void**)&mp->nchanged, 4 * 4);
+  A((void**)&mp->mask, ninterior);
   if (!ok) {
     multiphase_destroy(mp);
     return M2CG_ERR_NOMEM;
@@ -503,6 +688,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   cudaMemcpyAsync(mp->d_eos, sk.ed, sizeof(Eos<double>) * MAXMAT, cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(mp->counts, 0, 16 * 4, s);
   cudaMemsetAsync(mp->rsValid, 0, mp->cap_slots * 3, s);
+  cudaMemsetAsync(mp->mask, 0, ninterior, s);
   if (levelset_geom_create(s, g, ls, xc, dx, &mp->lsg) != M2CG_OK) {
     multiphase_destroy(mp);
     return M2CG_ERR_NOMEM;
@@ -522,7 +708,7 @@ void multiphase_destroy(Multiphase* mp) {
   cudaFree(mp->idn); cudaFree(mp->slot); cudaFree(mp->faces); cudaFree(mp->counts);
   cudaFree(mp->Vsm); cudaFree(mp->Vsp); cudaFree(mp->Vmid); cudaFree(mp->midid);
   cudaFree(mp->rsVsm); cudaFree(mp->rsVsp); cudaFree(mp->rsValid); cudaFree(mp->scratch);
-  cudaFree(mp->changed); cudaFree(mp->blockcnt); cudaFree(mp->nchanged);
+  cudaFree(mp->changed); cudaFree(mp->blockcnt); cudaFree(mp->nchanged); cudaFree(mp->mask);
   cudaFree(mp->reinit_buf);
   levelset_geom_destroy(&mp->lsg);
   delete mp;
@@ -630,6 +816,18 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
     mp->reinit_calls++;
     mp->reinit_iterations += its;
   }
+  m2cg_status st = multiphase_update_states(mp, s, Vnew, Vfnew, id, err, true, nullptr);
+  if (st) return st;
+  if (counters) counters->kernel_launches += 8 + 3 * mp->scheme.rk_order;
+  return M2CG_OK;
+}
+
+uint8_t* multiphase_idn(Multiphase* mp) { return mp->idn; }
+
+m2cg_status multiphase_update_states(Multiphase* mp, cudaStream_t s, double* const* V, float* const* Vf, uint8_t* id,
+                                     DevError* err, bool use_rs, int* unresolved) {
+  const Grid3& g = mp->g;
+  const long long ninterior = (long long)g.nx * g.ny * g.nz;
   // ordered list of cells whose ID changed, then the sequential update
   long long per_block = (ninterior + mp->nblocks_scan - 1) / mp->nblocks_scan;
   k_count_changed<<<mp->nblocks_scan, 256, 0, s>>>(g, id, mp->idn, mp->blockcnt, per_block);
@@ -639,8 +837,8 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
   memset(&ua, 0, sizeof ua);
   ua.g = g;
   ua.eos = mp->d_eos;
-  for (int p = 0; p < 5; p++) ua.V[p] = Vnew[p];
-  for (int p = 0; p < 5; p++) ua.Vf[p] = Vfnew ? Vfnew[p] : nullptr;
+  for (int p = 0; p < 5; p++) ua.V[p] = V[p];
+  for (int p = 0; p < 5; p++) ua.Vf[p] = Vf ? Vf[p] : nullptr;
   ua.id = id;
   ua.idn = mp->idn;
   ua.slot = mp->slot;
@@ -650,20 +848,35 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
   ua.changed = mp->changed;
   ua.nchanged = mp->nchanged;
   ua.err = err;
+  ua.use_rs = use_rs ? 1 : 0;
+  ua.type = mp->scheme.mp_phasechange_type;
+  ua.upwind = mp->scheme.mp_phasechange_dir == 1;
+  ua.failsafe = mp->scheme.mp_apply_failsafe_density != 0;
+  ua.geo = mp->lsg;
+  ua.mask = mp->mask;
+  for (int m = 0; m < MAXMAT; m++) ua.failsafe_rho[m] = mp->failsafe[m];
   k_state_update<<<1, 32, 0, s>>>(ua);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
   // step counters (one small read-back per step)
-  int hc[7], hn[2];
+  int hc[7], hn[4];
   cudaMemcpyAsync(hc, mp->counts, sizeof hc, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hn, mp->nchanged, sizeof hn, cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
-  mp->riemann_calls += hc[5];
-  mp->riemann_iterations += hc[4];
-  mp->riemann_errors += hc[3];
-  mp->riemann_evaluations += hc[6];
+  if (use_rs) {
+    mp->riemann_calls += hc[5];
+    mp->riemann_iterations += hc[4];
+    mp->riemann_errors += hc[3];
+    mp->riemann_evaluations += hc[6];
+    if (hc[2]) return M2CG_ERR_ITER_CAP;  // interface capacity exceeded
+  }
   mp->unresolved += hn[1];
-  if (hc[2]) return M2CG_ERR_ITER_CAP;  // interface capacity exceeded
-  if (counters) counters->kernel_launches += 8 + 3 * mp->scheme.rk_order;
+  mp->failsafe_cells += hn[3];
+  if (unresolved) *unresolved = hn[1];
+  if (hn[2]) {
+    set_last_error("unresolved background cells with apply_failsafe_density Off need the level-set "
+                   "correction of unresolved cells, which is not supported");
+    return M2CG_ERR_UNSUPPORTED;
+  }
   return M2CG_OK;
 }
 
@@ -674,4 +887,5 @@ void multiphase_counters(const Multiphase* mp, m2cg_counters* out) {
   out->reinit_calls = mp->reinit_calls;
   out->unresolved_cells = mp->unresolved;
   out->riemann_evaluations = mp->riemann_evaluations;
+  out->failsafe_cells = mp->failsafe_cells;
 }

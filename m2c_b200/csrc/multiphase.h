@@ -30,3 +30,9 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
                                 float* const* Vfnew, uint8_t* id,
                                 const double* clock, m2c::DevError* err, m2cg_counters* counters);
 void multiphase_counters(const Multiphase* mp, m2cg_counters* out);
+// The state update of cells whose ID differs from the step-start IDs
+// (multiphase_idn): Riemann-solution or extrapolation pass, FixUnresolvedNodes,
+// clip. use_rs: the stage-1 star states of the last step are valid for these IDs.
+m2cg_status multiphase_update_states(Multiphase* mp, cudaStream_t s, double* const* V, float* const* Vf, uint8_t* id,
+                                     m2c::DevError* err, bool use_rs, int* unresolved);
+uint8_t* multiphase_idn(Multiphase* mp);

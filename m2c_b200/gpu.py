@@ -29,7 +29,8 @@ class M2CError(RuntimeError):
 class Counters(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in (
         "steps", "cells_updated", "riemann_calls", "riemann_iterations", "riemann_errors",
-        "clipped_cells", "reinit_calls", "kernel_launches", "unresolved_cells", "riemann_evaluations")]
+        "clipped_cells", "reinit_calls", "kernel_launches", "unresolved_cells", "riemann_evaluations",
+        "failsafe_cells")]
 
 
 class BatchTuning(C.Structure):
@@ -223,6 +224,17 @@ class Solver:
         c = Counters()
         check(lib().m2cg_get_counters(self.h, C.byref(c)))
         return {n: getattr(c, n) for n, _ in Counters._fields_}
+
+    def update_states_after_motion(self, IDn, use_stored_riemann_solutions=False):
+        """UpdateStateVariablesAfterInterfaceMotion on the resident state
+        against the step-start IDs IDn (ghosted layout); returns the number of
+        cells handed to FixUnresolvedNodes."""
+        IDn = np.ascontiguousarray(IDn, dtype=np.float64)
+        n = C.c_int()
+        check(lib().m2cg_update_states_after_interface_motion(self.h, abi.dptr(IDn),
+                                                              int(bool(use_stored_riemann_solutions)),
+                                                              C.byref(n)))
+        return n.value
 
     def stream(self):
         p = C.c_void_p()

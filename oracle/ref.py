@@ -39,6 +39,8 @@ def _load(path, prefix):
                             C.POINTER(abi.LevelSet), C.c_int]
     f("set_state").argtypes = [vp, dp, dp, dp]
     f("get_state").argtypes = [vp, dp, dp, dp]
+    f("update_states_after_motion").restype = C.c_int
+    f("update_states_after_motion").argtypes = [vp, dp]
     f("compute_dt").restype = C.c_double
     f("compute_dt").argtypes = [vp]
     f("compute_residual").argtypes = [vp, dp]
@@ -92,6 +94,13 @@ class _Case:
 
     def compute_dt(self):
         return self._f("compute_dt")(self.h)
+
+    def update_states_after_motion(self, IDn):
+        """UpdateStateVariablesAfterInterfaceMotion against the step-start IDs
+        IDn (ghosted layout), no stored Riemann solutions; returns the number
+        of cells still unresolved."""
+        IDn = np.ascontiguousarray(IDn, dtype=np.float64)
+        return self._f("update_states_after_motion")(self.h, abi.dptr(IDn))
 
     def residual(self):
         R = np.zeros(abi.ghosted_shape(self.g, 5))

@@ -290,6 +290,24 @@ void m2cref_get_state(void* h, double* V, double* ID, double* phi) {
       copy_out(*c->Phi[l], phi + l * (size_t)(c->NX + 2) * (c->NY + 2) * (c->NZ + 2), 1, c->NX, c->NY, c->NZ);
 }
 
+// MultiPhaseOperator::UpdateStateVariablesAfterInterfaceMotion with the given
+// step-start IDs and no stored Riemann solutions (an empty RiemannSolutions),
+// followed by the clip and boundary conditions of
+// TimeIntegratorBase::UpdateSolutionAfterTimeStepping (TimeIntegrator.cpp:767-768).
+// Returns the number of cells still unresolved.
+int m2cref_update_states_after_motion(void* h, const double* IDn) {
+  RefCase* c = (RefCase*)h;
+  SpaceVariable3D idn(c->comm, &(c->dms->ghosted1_1dof));
+  copy_in(idn, IDn, 1, c->NX, c->NY, c->NZ);
+  RiemannSolutions rs;
+  std::vector<Int3> unresolved;
+  int n = c->mpo->UpdateStateVariablesAfterInterfaceMotion(idn, *c->ID, *c->V, rs, nullptr, unresolved);
+  c->spo->ClipDensityAndPressure(*c->V, *c->ID);
+  c->spo->ApplyBoundaryConditions(*c->V);
+  idn.Destroy();
+  return n;
+}
+
 double m2cref_compute_dt(void* h) {
   RefCase* c = (RefCase*)h;
   double dt = 0.0, cfl = 0.0;

@@ -83,6 +83,91 @@ def test_riemann_normal_matches_reference(gpu, ref, normal, rk):
         assert rel_err(inner(other.download()[0]), inner(Vg)) > 1e3 * TOL
 
 
+def phase_change_case(ptype, pdir, blob_only=False, seed=1):
+    """Crafted inputs for the update of cells that changed material, on a
+    16x14x12 water/air box with seeded states: blob A (radius 2.5 cells) is
+    air now and was water at the step start; cube B grew by one layer of
+    cells (0 -> 1); slab C shrank (1 -> 0). With no stored star states every
+    changed cell of the RIEMANN_SOLUTION update goes to FixUnresolvedNodes,
+    whose upwind, inverse-distance and layer-density fallbacks all run; with
+    blob A alone no valid neighbour is within 10 layers and the failsafe
+    density (2.5) is applied."""
+    nx, ny, nz = 16, 14, 12
+    g = abi.grid(nx, ny, nz, x=(0, 0.016), y=(0, 0.014), z=(0, 0.012), bc=(abi.BC_SYMMETRY,) * 6)
+    s = abi.scheme(flux=abi.FLUX_HLLC, limiter=abi.LIM_VANALBADA, rk_order=2, cfl=0.5)
+    s.mp_phasechange_type = ptype
+    s.mp_phasechange_dir = pdir
+    mats = [abi.material(**cases.WATER), abi.material(**cases.AIR)]
+    mats[1].failsafe_density = 2.5
+    ls = abi.levelset(material_id=1, reinit_frequency=-1)
+    rng = np.random.default_rng(seed)
+    V = cases.empty_state(g)
+    inside = V[1:-1, 1:-1, 1:-1]
+    inside[..., 0] = rng.uniform(1.0, 3.0, inside.shape[:3])
+    inside[..., 1:4] = rng.uniform(-50, 50, inside.shape[:3] + (3,))
+    inside[..., 4] = rng.uniform(1e5, 3e5, inside.shape[:3])
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    cur = np.zeros((nz, ny, nx))
+    old = np.zeros((nz, ny, nx))
+    cur[(i - 4) ** 2 + (j - 4) ** 2 + (k - 4) ** 2 <= 6.25] = 1
+    if not blob_only:
+        cur[(i >= 9) & (i <= 14) & (j >= 6) & (j <= 12) & (k >= 5) & (k <= 10)] = 1
+        old[(i >= 10) & (i <= 13) & (j >= 7) & (j <= 11) & (k >= 6) & (k <= 9)] = 1
+        slab = (j >= 9) & (j <= 12) & (k >= 7) & (k <= 10)
+        old[slab & (i >= 1) & (i <= 5)] = 1
+        cur[slab & (i >= 4) & (i <= 5)] = 1
+    ID = np.zeros(abi.ghosted_shape(g))
+    IDn = np.zeros(abi.ghosted_shape(g))
+    ID[1:-1, 1:-1, 1:-1] = cur
+    IDn[1:-1, 1:-1, 1:-1] = old
+    PHI = np.where(ID > 0, -1e-3, 1e-3)
+    return g, s, mats, ls, V, ID, IDn, PHI
+
+
+@pytest.mark.parametrize("ptype,pdir,blob_only", [
+    (abi.PHASECHANGE_RIEMANN_SOLUTION, abi.PHASECHANGE_UPWIND, False),
+    (abi.PHASECHANGE_EXTRAPOLATION, abi.PHASECHANGE_UPWIND, False),
+    (abi.PHASECHANGE_EXTRAPOLATION, abi.PHASECHANGE_ALL, False),
+    (abi.PHASECHANGE_RIEMANN_SOLUTION, abi.PHASECHANGE_UPWIND, True),
+    (abi.PHASECHANGE_EXTRAPOLATION, abi.PHASECHANGE_ALL, True)])
+def test_update_after_interface_motion_matches_reference(gpu, ref, ptype, pdir, blob_only):
+    """MultiPhaseOperator::UpdateStateVariablesAfterInterfaceMotion (Riemann
+    solutions or extrapolation, then FixUnresolvedNodes) on crafted ID
+    changes: identical states to the reference."""
+    g, s, mats, ls, V, ID, IDn, PHI = phase_change_case(ptype, pdir, blob_only)
+    sol, rc = make(gpu, ref, g, s, mats, ls, V, ID, PHI)
+    assert rc.update_states_after_motion(IDn) == 0
+    nun = sol.update_states_after_motion(IDn)
+    Vg = inner(sol.download()[0])
+    Vr = inner(rc.get_state()[0])
+    assert rel_err(Vg, Vr) <= 1e-13
+    changed = inner(ID) != inner(IDn)
+    if blob_only:
+        assert nun == changed.sum()
+        assert sol.counters()["failsafe_cells"] == changed.sum()
+        assert (Vg[..., 0][changed] == 2.5).all()
+    elif ptype == abi.PHASECHANGE_RIEMANN_SOLUTION:
+        assert nun == changed.sum()  # no star states: everything goes to FixUnresolvedNodes
+    assert sol.counters()["failsafe_cells"] == (changed.sum() if blob_only else 0)
+
+
+def test_extrapolation_update_bubble_matches_reference(gpu, ref):
+    """phasechange_type EXTRAPOLATION with upwinding through whole steps of
+    the obliquely moving bubble."""
+    g, s, mats, ls, V, ID, PHI = moving_bubble(abi.RIEMANN_NORMAL_MESH, 2)
+    s.mp_phasechange_type = abi.PHASECHANGE_EXTRAPOLATION
+    sol, rc = make(gpu, ref, g, s, mats, ls, V, ID, PHI)
+    for _ in range(6):
+        sol.run(1)
+        rc.run(1)
+    Vg, IDg, Pg = sol.download()
+    Vr, IDr, Pr = rc.get_state()
+    assert np.array_equal(inner(IDg), inner(IDr))
+    assert (inner(IDg) != inner(ID)).sum() > 0
+    assert rel_err(inner(Vg), inner(Vr)) <= TOL
+    assert rel_err(inner(Pg), inner(Pr), axis_last=False) <= TOL
+
+
 def test_water_air_tube_matches_reference(gpu, ref):
     """1D water/air shock tube through the 3D path: the interface moves across
     cells, so IDs change and the Riemann-solution state update runs."""
