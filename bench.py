@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--only-headline", action="store_true",
                    help="skip the extra workloads (bubble cluster, batched tubes, learned warm start)")
+    p.add_argument("--bubble", type=int, default=0, metavar="N",
+                   help="run only the bubble-cluster workload at N^3 (for profiling) and print its JSON")
     return p.parse_args()
 
 
@@ -66,6 +68,9 @@ def parse():
 # --------------------------------------------------------------------------
 def _cpu_worker(args):
     n, steps, seed = args
+    # the reference prints mesh statistics on stdout: keep the JSON line alone there
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
     sys.path.insert(0, ROOT)
     from m2c_b200 import abi, cases
     from oracle import ref
@@ -307,6 +312,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     n = args.n
     cells = n ** 3
+
+    if args.bubble:
+        print(json.dumps(extra_bubble(n=args.bubble, steps=args.steps, warmup=args.warmup)))
+        return
 
     if args.impl == "reference":
         if rank != 0:
