@@ -118,10 +118,14 @@ typedef struct {
 } m2cg_scheme;
 
 /* One level set (LevelSetSchemeData, IoData.h:653-679; reinit
- * LevelSetReinitializationData, IoData.h:628-651). Finite-difference
- * UPWIND_CENTRAL_3 solver, full domain. */
+ * LevelSetReinitializationData, IoData.h:628-651), full domain, with the
+ * finite-difference UPWIND_CENTRAL_3 solver (the reference's default) or the
+ * finite-volume solver (MUSCL of phi and of the velocity, ROE / LLF / UPWIND
+ * flux, phi div(u) source). Enum values are the reference's. */
 enum { M2CG_LSBC_NONE = 0, M2CG_LSBC_ZERO_NEUMANN = 1, M2CG_LSBC_LINEAR_EXTRAPOLATION = 2,
        M2CG_LSBC_NON_NEGATIVE = 3 };
+enum { M2CG_LS_FINITE_VOLUME = 0, M2CG_LS_FINITE_DIFFERENCE = 1 };
+enum { M2CG_LSFLUX_ROE = 0, M2CG_LSFLUX_LLF = 1, M2CG_LSFLUX_UPWIND = 2 };
 typedef struct {
   int material_id;        /* material in the phi<0 region */
   int bc[6];
@@ -130,6 +134,12 @@ typedef struct {
   double reinit_cfl;
   double reinit_tol;
   int reinit_first_layer; /* 0 FIXED (only FIXED is implemented) */
+  int solver;             /* M2CG_LS_FINITE_DIFFERENCE (default) or M2CG_LS_FINITE_VOLUME */
+  int flux;               /* finite volume: M2CG_LSFLUX_*, default ROE */
+  double delta;           /* finite volume: entropy-fix coefficient of the ROE flux (0.2) */
+  int rec_type;           /* finite volume ReconstructionData: 0 CONSTANT, 1 LINEAR (default) */
+  int limiter;            /* finite volume: 0 NONE (default), 1 GENERALIZED_MINMOD, 2 VANALBADA */
+  double minmod_coeff;    /* finite volume: generalized minmod coefficient (1.2) */
 } m2cg_levelset;
 
 /* Fill a scheme/material/level-set struct with the reference's defaults

@@ -70,7 +70,8 @@ class LevelSet(C.Structure):
     _fields_ = [
         ("material_id", C.c_int), ("bc", C.c_int * 6), ("reinit_frequency", C.c_int),
         ("reinit_maxits", C.c_int), ("reinit_cfl", C.c_double), ("reinit_tol", C.c_double),
-        ("reinit_first_layer", C.c_int),
+        ("reinit_first_layer", C.c_int), ("solver", C.c_int), ("flux", C.c_int), ("delta", C.c_double),
+        ("rec_type", C.c_int), ("limiter", C.c_int), ("minmod_coeff", C.c_double),
     ]
 
 
@@ -115,10 +116,15 @@ def scheme(**kw):
     return s
 
 
+LS_FINITE_VOLUME, LS_FINITE_DIFFERENCE = 0, 1
+LSFLUX_ROE, LSFLUX_LLF, LSFLUX_UPWIND = 0, 1, 2
+
+
 def levelset(material_id=1, bc=(LSBC_ZERO_NEUMANN,) * 6, reinit_frequency=-1, reinit_maxits=30,
-             reinit_cfl=0.8, reinit_tol=2.0e-4, reinit_first_layer=0):
+             reinit_cfl=0.8, reinit_tol=2.0e-4, reinit_first_layer=0, solver=LS_FINITE_DIFFERENCE,
+             flux=LSFLUX_ROE, delta=0.2, rec_type=1, limiter=0, minmod_coeff=1.2):
     return LevelSet(material_id, (C.c_int * 6)(*bc), reinit_frequency, reinit_maxits, reinit_cfl,
-                    reinit_tol, reinit_first_layer)
+                    reinit_tol, reinit_first_layer, solver, flux, delta, rec_type, limiter, minmod_coeff)
 
 
 def grid(nx, ny, nz, x=(0.0, 1.0), y=(0.0, 1.0), z=(0.0, 1.0), bc=(BC_SYMMETRY,) * 6,

@@ -121,6 +121,12 @@ class TimeIntegratorGPU : public TimeIntegratorBase {
       ls.reinit_cfl = d.reinit.cfl;
       ls.reinit_tol = d.reinit.convergence_tolerance;
       ls.reinit_first_layer = (int)d.reinit.firstLayerTreatment;
+      ls.solver = (int)d.solver;
+      ls.flux = (int)d.flux;
+      ls.delta = d.delta;
+      ls.rec_type = (int)d.rec.type;
+      ls.limiter = (int)d.rec.limiter;
+      ls.minmod_coeff = d.rec.generalized_minmod_coeff;
     }
     m2cg_status st = m2cg_create(&g, &s, mats.data(), (int)mats.size(), nls ? &ls : nullptr, nls, &ctx);
     if (st != M2CG_OK) fail(st);

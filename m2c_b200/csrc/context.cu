@@ -105,6 +105,12 @@ extern "C" void m2cg_default_levelset(m2cg_levelset* l) {
   l->reinit_cfl = 0.8;
   l->reinit_tol = 2.0e-4;
   l->reinit_first_layer = 0;
+  l->solver = M2CG_LS_FINITE_DIFFERENCE;
+  l->flux = M2CG_LSFLUX_ROE;
+  l->delta = 0.2;
+  l->rec_type = 1;                     // ReconstructionData (IoData.cpp:1049-1058)
+  l->limiter = 0;
+  l->minmod_coeff = 1.2;
 }
 
 // ---------------------------------------------------------------------------

@@ -15,6 +15,7 @@
 // in coefficient form. That behaviour is reproduced (cr1y).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -78,8 +79,38 @@ m2cg_status levelset_geom_create(cudaStream_t s, const Grid3& g, const m2cg_leve
     cr1y[4 * j + 1] = -1.0 / d;
     cr1y[4 * j + 2] = 1.0 / d;
   }
+  // finite-volume solver: widths with ghosts and the level set's limiter
+  // coefficients (Reconstructor::Setup, Reconstructor.cpp:53-121)
+  std::vector<double> wg[3], fA[3], fB[3], fK[3];
+  for (int a = 0; a < 3; a++) {
+    const int n = nn[a];
+    const bool per = g.bc[2 * a] == BC_PERIODIC;
+    wg[a].assign(n + 2, 0.0);
+    for (int i = 0; i < n; i++) wg[a][i + 1] = dx[a][i];
+    wg[a][0] = dx[a][0];
+    wg[a][n + 1] = dx[a][n - 1];
+    fA[a].assign(n, 0.0);
+    fB[a].assign(n, 0.0);
+    fK[a].assign(n, 0.0);
+    for (int i = 0; i < n; i++) {
+      const double dm = i > 0 ? dx[a][i - 1] : (per ? dx[a][n - 1] : dx[a][0]);
+      const double dp = i < n - 1 ? dx[a][i + 1] : (per ? dx[a][0] : dx[a][n - 1]);
+      fA[a][i] = (dm + dx[a][i]) / (dx[a][i] + dp);
+      fB[a][i] = 2.0 * dx[a][i] / (dx[a][i] + dp);
+      if (ls.solver == M2CG_LS_FINITE_VOLUME && ls.limiter == M2CG_LIM_VANALBADA) {
+        int k;
+        for (k = 2; k < 1000; k++) {
+          const double rhs = 2.0 / (1.0 + pow((k - 1.0) / k, k - 1) / k) * std::min(fA[a][i], 1.0);
+          if (fB[a][i] <= rhs) break;
+        }
+        if (k >= 999) return M2CG_ERR_ARG;
+        fK[a][i] = k;
+      }
+    }
+  }
   size_t total = 0;
-  for (int a = 0; a < 3; a++) total += xg[a].size() + cl[a].size() + cr[a].size();
+  for (int a = 0; a < 3; a++)
+    total += xg[a].size() + cl[a].size() + cr[a].size() + wg[a].size() + fA[a].size() + fB[a].size() + fK[a].size();
   total += cr1y.size();
   if (cudaMalloc((void**)&out->base, total * 8) != cudaSuccess) return M2CG_ERR_NOMEM;
   double* p = out->base;
@@ -95,6 +126,18 @@ m2cg_status levelset_geom_create(cudaStream_t s, const Grid3& g, const m2cg_leve
     out->cr[a] = put(cr[a]);
   }
   out->cr1y = put(cr1y);
+  for (int a = 0; a < 3; a++) {
+    out->wg[a] = put(wg[a]);
+    out->fA[a] = put(fA[a]);
+    out->fB[a] = put(fB[a]);
+    out->fK[a] = put(fK[a]);
+  }
+  out->solver = ls.solver;
+  out->flux = ls.flux;
+  out->rec_linear = ls.rec_type == 1;
+  out->limiter = ls.limiter;
+  out->delta = ls.delta;
+  out->alpha = ls.minmod_coeff;
   for (int q = 0; q < 6; q++) out->bc[q] = ls.bc[q];
   cudaStreamSynchronize(s);
   return M2CG_OK;
@@ -178,6 +221,171 @@ __global__ void k_ls_stage(LsStageArgs a) {
   }
 }
 
+// --------------------------------------------------------------------------
+// Finite-volume residual (LevelSetOperator::ComputeResidualFVM, 1237-1297):
+// MUSCL face values of phi (Reconstructor::Reconstruct, 1 dof) and of the
+// normal velocity (Reconstructor::ReconstructIn1D, Reconstructor.cpp:908-1122),
+// the level set's flux at every face (ComputeLocalAdvectionFlux, 1516-1550)
+// divided by the width of the face's right cell, and phi (u_x + v_y + w_z)
+// with the limited velocity slopes (AddSourceTerm, 1552-1570). A cell's sum
+// is taken in the order the reference's face loop (1342-1419) reaches it:
+// + its low x, y, z faces, then - its high x, y, z faces.
+// --------------------------------------------------------------------------
+
+// Velocity component c (1..3) of the stage at cell (i,j,k), interior or one
+// cell outside (a face ghost: SpaceOperator::ApplyBoundaryConditions).
+__device__ double ls_vel(const LsStageArgs& a, int i, int j, int k, int c) {
+  const Grid3& g = a.g;
+  int x[3] = {i, j, k};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  int gaxis = -1, gside = 0;
+  for (int d = 0; d < 3; d++) {
+    if (x[d] >= 0 && x[d] < n[d]) continue;
+    if (g.bc[2 * d] == BC_PERIODIC) {
+      x[d] = x[d] < 0 ? x[d] + n[d] : x[d] - n[d];
+      continue;
+    }
+    gaxis = d;
+    gside = x[d] < 0 ? 0 : 1;
+    x[d] = x[d] < 0 ? 0 : n[d] - 1;
+  }
+  if (gaxis >= 0) {
+    const int bc = g.bc[2 * gaxis + gside];
+    if (bc == BC_INLET) return g.inlet[c];
+    if (bc == BC_OUTLET) return g.outlet[c];
+  }
+  const long long off = loff(g, x[0], x[1], x[2]);
+  double u;
+  if (a.stage == 1) {
+    u = a.Vn[c][off];
+  } else {
+    const double inv = 1.0 / a.Us[0][off];
+    u = a.Us[c][off] * inv;
+  }
+  if (gaxis >= 0) {
+    const int bc = g.bc[2 * gaxis + gside];
+    if (bc == BC_STICKWALL || c == gaxis + 1) u = -u;
+  }
+  return u;
+}
+
+// Limited slope of a scalar along axis d at axis index c
+// (Reconstructor.cpp:964-997 and 580-611 for one dof).
+__device__ __forceinline__ double ls_slope(const LsGeom& geo, int d, int c, double qm, double q0, double qp) {
+  if (!geo.rec_linear) return 0.0;
+  const double dq0 = q0 - qm, dq1 = qp - q0;
+  if (geo.limiter == LIM_GENMINMOD) return lim_genminmod(geo.fA[d][c], geo.fB[d][c], geo.alpha, dq0, dq1);
+  if (geo.limiter == LIM_VANALBADA) {
+    const int kay = (int)round(geo.fK[d][c]);
+    return lim_vanalbada(geo.fA[d][c], geo.fB[d][c], kay, dq0, dq1);
+  }
+  return 0.5 * (dq0 + dq1);
+}
+
+__device__ __forceinline__ void step(int d, int* x, int s) { x[d] += s; }
+
+// Face value of phi (vel = false) or of the axis-d velocity (vel = true) of
+// cell x on its low (hi = 0) or high (hi = 1) side along d. x may be one
+// cell outside along d: the ghost-layer rules of the two reconstructions
+// (Reconstructor.cpp:815-875 for phi, 1040-1108 for the velocity, where the
+// wall branches write the ghost's other side, so the side a face uses keeps
+// its initial zero).
+__device__ double ls_face_value(const LsStageArgs& a, int d, const int* x, int hi, bool vel) {
+  const Grid3& g = a.g;
+  const LsGeom& geo = a.geo;
+  const int n = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+  int c[3] = {x[0], x[1], x[2]};
+  if (c[d] < 0 || c[d] >= n) {
+    if (g.bc[2 * d] == BC_PERIODIC) {
+      c[d] = c[d] < 0 ? c[d] + n : c[d] - n;
+    } else {
+      const int bc = g.bc[2 * d + (c[d] < 0 ? 0 : 1)];
+      const bool dirichlet = bc == BC_INLET || bc == BC_OUTLET;
+      if (vel) return dirichlet ? ls_vel(a, c[0], c[1], c[2], d + 1) : 0.0;
+      if (dirichlet || !geo.rec_linear) return phi_at(g, geo, a.in, c[0], c[1], c[2]);
+      // wall: the image's face value on the ghost's own side (vr[ghost] =
+      // vl[image] below, vl[ghost] = vr[image] above)
+      hi = c[d] < 0 ? 0 : 1;
+      c[d] = c[d] < 0 ? 0 : n - 1;
+    }
+  }
+  int m[3] = {c[0], c[1], c[2]}, p[3] = {c[0], c[1], c[2]};
+  step(d, m, -1);
+  step(d, p, 1);
+  double q0, qm, qp;
+  if (vel) {
+    q0 = ls_vel(a, c[0], c[1], c[2], d + 1);
+    qm = ls_vel(a, m[0], m[1], m[2], d + 1);
+    qp = ls_vel(a, p[0], p[1], p[2], d + 1);
+  } else {
+    q0 = a.in[loff(g, c[0], c[1], c[2])];
+    qm = phi_at(g, geo, a.in, m[0], m[1], m[2]);
+    qp = phi_at(g, geo, a.in, p[0], p[1], p[2]);
+  }
+  const double sigma = ls_slope(geo, d, c[d], qm, q0, qp);
+  return hi ? q0 + 0.5 * sigma : q0 - 0.5 * sigma;
+}
+
+// LevelSetOperator::ComputeLocalAdvectionFlux (1516-1550)
+__device__ __forceinline__ double ls_local_flux(const LsGeom& geo, double phim, double phip, double um, double up) {
+  if (geo.flux == M2CG_LSFLUX_UPWIND) {
+    const double vmid = 0.5 * (um + up);
+    if (vmid > 0) return phim * um;
+    if (vmid < 0) return phip * up;
+    return 0.5 * (phim * um + phip * up);
+  }
+  if (geo.flux == M2CG_LSFLUX_LLF) return 0.5 * (phim * um + phip * up) - 0.5 * smax(fabs(um), fabs(up)) * (phip - phim);
+  double lam = fabs(0.5 * (um + up));
+  const double tol = smax(fabs(um), fabs(up)) * geo.delta;
+  if (lam < tol) lam = (lam * lam + tol * tol) / (2 * tol);
+  return 0.5 * (phim * um + phip * up) - 0.5 * lam * (phip - phim);
+}
+
+// Flux through the low face (along d) of cell r, divided by r's width.
+__device__ double ls_face_flux(const LsStageArgs& a, int d, const int* r) {
+  int l[3] = {r[0], r[1], r[2]};
+  step(d, l, -1);
+  const double phim = ls_face_value(a, d, l, 1, false), phip = ls_face_value(a, d, r, 0, false);
+  const double um = ls_face_value(a, d, l, 1, true), up = ls_face_value(a, d, r, 0, true);
+  return ls_local_flux(a.geo, phim, phip, um, up) / a.geo.wg[d][r[d] + 1];
+}
+
+__global__ void k_ls_fvm_stage(LsStageArgs a) {
+  const Grid3& g = a.g;
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  const double dt = a.clock[1];
+  const double bdt = a.bdt_coef * dt;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx), j = (int)((q / g.nx) % g.ny), k = (int)(q / ((long long)g.nx * g.ny));
+    const long long off = loff(g, i, j, k);
+    const int x[3] = {i, j, k};
+    double R = 0.0;
+    for (int d = 0; d < 3; d++) R += ls_face_flux(a, d, x);
+    for (int d = 0; d < 3; d++) {
+      int r[3] = {i, j, k};
+      step(d, r, 1);
+      R -= ls_face_flux(a, d, r);
+    }
+    // source term with the limited velocity slopes (slope = sigma / width)
+    double div[3];
+    for (int d = 0; d < 3; d++) {
+      int m[3] = {i, j, k}, p[3] = {i, j, k};
+      step(d, m, -1);
+      step(d, p, 1);
+      const double sigma = ls_slope(a.geo, d, x[d], ls_vel(a, m[0], m[1], m[2], d + 1),
+                                    ls_vel(a, i, j, k, d + 1), ls_vel(a, p[0], p[1], p[2], d + 1));
+      div[d] = sigma / a.geo.wg[d][x[d] + 1];
+    }
+    R += a.in[off] * (div[0] + div[1] + div[2]);
+    double base;
+    if (a.stage == 1)
+      base = a.phin[off];
+    else
+      base = a.a_prev * a.in[off] + a.a_un * a.phin[off];
+    a.out[off] = base + bdt * R;
+  }
+}
+
 static int grid1d(long long n) {
   long long b = (n + 255) / 256;
   if (b > 148 * 16) b = 148 * 16;
@@ -204,7 +412,10 @@ m2cg_status levelset_stage(cudaStream_t s, const Grid3& g, const SchemeK& sk, co
   la.in = in;
   la.phin = phin;
   la.out = out;
-  k_ls_stage<<<grid1d((long long)g.nx * g.ny * g.nz), 256, 0, s>>>(la);
+  if (geo.solver == M2CG_LS_FINITE_VOLUME)
+    k_ls_fvm_stage<<<grid1d((long long)g.nx * g.ny * g.nz), 256, 0, s>>>(la);
+  else
+    k_ls_stage<<<grid1d((long long)g.nx * g.ny * g.nz), 256, 0, s>>>(la);
   return cudaGetLastError() == cudaSuccess ? M2CG_OK : M2CG_ERR_CUDA;
 }
 

@@ -1,6 +1,7 @@
 // Level-set transport on the GPU: finite-difference UPWIND_CENTRAL_3 residual
 // (LevelSetOperator::ComputeResidualFDM_FullDomain, LevelSetOperator.cpp:1066-1140,
-// GradientCalculatorFD3.cpp:54-470), boundary rules
+// GradientCalculatorFD3.cpp:54-470) or finite-volume residual
+// (LevelSetOperator::ComputeResidualFVM, 1237-1297, 1342-1419, 1516-1570), boundary rules
 // (LevelSetOperator::ApplyBoundaryConditions, 934-1034) and reinitialisation
 // (LevelSetReinitializer::ReinitializeFullDomain).
 #pragma once
@@ -17,6 +18,16 @@ struct LsGeom {
   const double* cl[3];   // left-biased FD3 coefficients [n][4] (third order where i > 0)
   const double* cr[3];   // right-biased FD3 coefficients [n][4] (third order where i < n-1)
   const double* cr1y;    // right-biased first-order y coefficients [ny][4] (see levelset.cu)
+  // finite-volume solver: widths incl. one ghost per side (index c+1; a
+  // ghost has the width of its boundary cell, SpaceOperator::ResetGhostLayer)
+  // and the level set's own limiter coefficients per axis index
+  // (Reconstructor::Setup with the level set's ReconstructionData)
+  const double* wg[3];
+  const double* fA[3];
+  const double* fB[3];
+  const double* fK[3];   // van Albada exponent (an integer held in a double; 0 otherwise)
+  int solver, flux, rec_linear, limiter;
+  double delta, alpha;
   int bc[6];             // LevelSetSchemeData::BcType per side
   double* base;          // single allocation holding the arrays above
 };

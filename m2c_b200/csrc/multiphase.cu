@@ -37,6 +37,11 @@ namespace m2c {
 // Threads running Riemann problems at once (each owns an integration-path
 // scratch region of 2 x RIEMANN_PATH_CAP x 3 doubles).
 constexpr int IFACE_RIEMANN_THREADS = 148 * 4 * 128;
+// Resident CTAs of 128 threads per SM the interface Riemann kernel is
+// compiled for (register budget 65536 / (128 * M2C_IFACE_MINB) per thread).
+#ifndef M2C_IFACE_MINB
+#define M2C_IFACE_MINB 2
+#endif
 
 struct Multiphase {
   Grid3 g;
@@ -71,6 +76,7 @@ struct Multiphase {
   int* blockcnt = nullptr;     // per-block counts for the ordered compaction
   int* nchanged = nullptr;     // [0] changed, [1] unresolved
   int nblocks_scan = 0;
+  int iface_blocks = 0;          // resident CTAs of k_iface_riemann (at most IFACE_RIEMANN_THREADS / 128)
   int time_step = 0;
   int stage = 0;
   // host-side counters
@@ -182,13 +188,17 @@ struct IfaceRiemannArgs {
 // One exact Riemann problem per interface face (SpaceOperator.cpp:2499-2523):
 // direction by the riemann_normal rule, cell-centred states (constant
 // reconstruction at the interface), star states clipped with each side's EOS,
-// stage-1 results kept.
-__global__ void k_iface_riemann(IfaceRiemannArgs a) {
+// stage-1 results kept. The grid holds only resident CTAs and every thread
+// takes the next unsolved face from a counter when it finishes one, so a
+// thread that met a hard problem is not also handed more, and lanes of a warp
+// do not idle while another lane iterates (problems take from one to hundreds
+// of star-state evaluations).
+__global__ void __launch_bounds__(128, M2C_IFACE_MINB) k_iface_riemann(IfaceRiemannArgs a) {
   const Grid3& g = a.st.g;
   long long nf = a.counts[1];
   if (nf > a.cap_faces) nf = a.cap_faces;
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  int* next = &a.counts[8 + a.st.stage];  // zeroed at the start of the step
   RiemannSolver rs;
   rs.P = a.P;
   rs.eos = a.eos;
@@ -196,7 +206,7 @@ __global__ void k_iface_riemann(IfaceRiemannArgs a) {
   rs.path1.cap = RIEMANN_PATH_CAP;
   rs.path3.pt = rs.path1.pt + 3 * RIEMANN_PATH_CAP;
   rs.path3.cap = RIEMANN_PATH_CAP;
-  for (long long f = tid; f < nf; f += nthreads) {
+  for (long long f = atomicAdd(next, 1); f < nf; f = atomicAdd(next, 1)) {
     const int q = a.faces[3 * f], s = a.faces[3 * f + 1], d = a.faces[3 * f + 2];
     int i, j, k;
     cell_coords(g, q, i, j, k);
@@ -642,6 +652,10 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   if (scheme.mp_phasechange_type != 0 && scheme.mp_phasechange_type != 1) return M2CG_ERR_UNSUPPORTED;
   if (ls.material_id != 1) return M2CG_ERR_UNSUPPORTED;
   if (ls.reinit_first_layer != 0) return M2CG_ERR_UNSUPPORTED;
+  if (ls.solver != M2CG_LS_FINITE_VOLUME && ls.solver != M2CG_LS_FINITE_DIFFERENCE) return M2CG_ERR_ARG;
+  if (ls.solver == M2CG_LS_FINITE_VOLUME &&
+      (ls.flux < 0 || ls.flux > 2 || ls.rec_type < 0 || ls.rec_type > 1 || ls.limiter < 0 || ls.limiter > 2))
+    return M2CG_ERR_ARG;
   Multiphase* mp = new Multiphase;
   mp->g = g;
   mp->sk = sk;
@@ -678,6 +692,15 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   A((void**)&mp->scratch, (size_t)IFACE_RIEMANN_THREADS * 2 * 3 * RIEMANN_PATH_CAP * 8);
   A((void**)&mp->changed, ninterior * 4);
   mp->nblocks_scan = 148 * 8;
+  {
+    int per_sm = 0, dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_iface_riemann, 128, 0) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    const int blocks = per_sm * nsm;
+    mp->iface_blocks = blocks < IFACE_RIEMANN_THREADS / 128 ? blocks : IFACE_RIEMANN_THREADS / 128;
+  }
   A((void**)&mp->blockcnt, mp->nblocks_scan * 4);
   A((void**)&mp->nchanged, 4 * 4);
   A((void**)&mp->mask, ninterior);
@@ -781,7 +804,7 @@ m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
   ra.normal_mode = mp->scheme.mp_riemann_normal;
   ra.phi = mp->phiN;
   ra.geo = mp->lsg;
-  k_iface_riemann<<<IFACE_RIEMANN_THREADS / 128, 128, 0, s>>>(ra);
+  k_iface_riemann<<<mp->iface_blocks, 128, 0, s>>>(ra);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
   a.iface.slot = mp->slot;
   a.iface.Vsm = mp->Vsm;

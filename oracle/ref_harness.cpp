@@ -193,6 +193,12 @@ void* m2cref_create(const m2cg_grid* g, const m2cg_scheme* s, const m2cg_materia
     d->reinit.cfl = ls[l].reinit_cfl;
     d->reinit.convergence_tolerance = ls[l].reinit_tol;
     d->reinit.firstLayerTreatment = (LevelSetReinitializationData::FirstLayerTreatment)ls[l].reinit_first_layer;
+    d->solver = (LevelSetSchemeData::Solver)ls[l].solver;
+    d->flux = (LevelSetSchemeData::Flux)ls[l].flux;
+    d->delta = ls[l].delta;
+    d->rec.type = (ReconstructionData::Reconstruction)ls[l].rec_type;
+    d->rec.limiter = (ReconstructionData::Limiter)ls[l].limiter;
+    d->rec.generalized_minmod_coeff = ls[l].minmod_coeff;
     iod.schemes.ls.dataMap[l] = d;
   }
   iod.finalize();
