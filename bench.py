@@ -425,7 +425,7 @@ def main():
         ne = max(3, min(args.steps, 10))
         sol.upload(Vh)
         sol.run(1)
-        sol.download(out_V=Vo)
+        sol.download(out_V=Vo, with_id=False)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -433,7 +433,7 @@ def main():
         for _ in range(ne):
             sol.upload(Vh)
             sol.run(1)
-            sol.download(out_V=Vo)
+            sol.download(out_V=Vo, with_id=False)
         te = time.perf_counter() - t0
         if dist:
             te = max_over_ranks(te, dist, "cuda")

@@ -155,12 +155,16 @@ void levelset_geom_destroy(LsGeom* geo) {
 __device__ double ls_residual(const Grid3& g, const LsGeom& geo, const double* phi, int i, int j, int k, double u,
                               double v, double w) {
   const int n[3] = {g.nx, g.ny, g.nz};
-  const double pc = phi[loff(g, i, j, k)];
+  const long long off = loff(g, i, j, k);
+  const long long stride[3] = {1, g.px, g.plane};
+  const double pc = phi[off];
   double lo[3], hi[3];
   for (int a = 0; a < 3; a++) {
     const int c = a == 0 ? i : (a == 1 ? j : k);
     const bool per = g.bc[2 * a] == BC_PERIODIC;
+    // neighbours inside the domain are read directly, the rest by the ghost rule
     auto P = [&](int dc) {
+      if (c + dc >= 0 && c + dc < n[a]) return phi[off + dc * stride[a]];
       return phi_at(g, geo, phi, i + (a == 0 ? dc : 0), j + (a == 1 ? dc : 0), k + (a == 2 ? dc : 0));
     };
     const double* X = geo.xg[a];  // X[c+1] = coordinate of index c
@@ -196,13 +200,15 @@ struct LsStageArgs {
   double* out;
 };
 
-__global__ void k_ls_stage(LsStageArgs a) {
+// Thread (x, y) of CTA (bx, by, bz) owns cells (32 bx + x, 8 by + y, k),
+// k = bz, bz + gridDim.z, ...
+__global__ void __launch_bounds__(256) k_ls_stage(LsStageArgs a) {
   const Grid3& g = a.g;
-  const long long n = (long long)g.nx * g.ny * g.nz;
   const double dt = a.clock[1];
   const double bdt = a.bdt_coef * dt;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q % g.nx), j = (int)((q / g.nx) % g.ny), k = (int)(q / ((long long)g.nx * g.ny));
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  for (int k = blockIdx.z; k < g.nz; k += gridDim.z) {
     const long long off = loff(g, i, j, k);
     double u, v, w;
     if (a.stage == 1) {
@@ -415,7 +421,7 @@ m2cg_status levelset_stage(cudaStream_t s, const Grid3& g, const SchemeK& sk, co
   if (geo.solver == M2CG_LS_FINITE_VOLUME)
     k_ls_fvm_stage<<<grid1d((long long)g.nx * g.ny * g.nz), 256, 0, s>>>(la);
   else
-    k_ls_stage<<<grid1d((long long)g.nx * g.ny * g.nz), 256, 0, s>>>(la);
+    k_ls_stage<<<dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 65535 ? g.nz : 65535), dim3(32, 8), 0, s>>>(la);
   return cudaGetLastError() == cudaSuccess ? M2CG_OK : M2CG_ERR_CUDA;
 }
 
@@ -506,16 +512,24 @@ __global__ void k_reinit_prep(Grid3 g, LsGeom geo, const double* phi, ReinitBuf 
 // pseudo-time residual at an untagged interior cell (LevelSetReinitializer.cpp:985-1012)
 __device__ __forceinline__ double reinit_local(const Grid3& g, const LsGeom& geo, const double* phi, int i, int j,
                                                int k, double& local_res) {
-  const double p = phi[loff(g, i, j, k)];
+  const long long off = loff(g, i, j, k);
+  const double p = phi[off];
   const double* X = geo.xg[0];
   const double* Y = geo.xg[1];
   const double* Z = geo.xg[2];
-  const double a = (p - phi_at(g, geo, phi, i - 1, j, k)) / (X[i + 1] - X[i]);
-  const double b = (phi_at(g, geo, phi, i + 1, j, k) - p) / (X[i + 2] - X[i + 1]);
-  const double c = (p - phi_at(g, geo, phi, i, j - 1, k)) / (Y[j + 1] - Y[j]);
-  const double d = (phi_at(g, geo, phi, i, j + 1, k) - p) / (Y[j + 2] - Y[j + 1]);
-  const double e = (p - phi_at(g, geo, phi, i, j, k - 1)) / (Z[k + 1] - Z[k]);
-  const double f = (phi_at(g, geo, phi, i, j, k + 1) - p) / (Z[k + 2] - Z[k + 1]);
+  // neighbours inside the domain are read directly, the rest by the ghost rule
+  const double pxm = i > 0 ? phi[off - 1] : phi_at(g, geo, phi, i - 1, j, k);
+  const double pxp = i < g.nx - 1 ? phi[off + 1] : phi_at(g, geo, phi, i + 1, j, k);
+  const double pym = j > 0 ? phi[off - g.px] : phi_at(g, geo, phi, i, j - 1, k);
+  const double pyp = j < g.ny - 1 ? phi[off + g.px] : phi_at(g, geo, phi, i, j + 1, k);
+  const double pzm = k > 0 ? phi[off - g.plane] : phi_at(g, geo, phi, i, j, k - 1);
+  const double pzp = k < g.nz - 1 ? phi[off + g.plane] : phi_at(g, geo, phi, i, j, k + 1);
+  const double a = (p - pxm) / (X[i + 1] - X[i]);
+  const double b = (pxp - p) / (X[i + 2] - X[i + 1]);
+  const double c = (p - pym) / (Y[j + 1] - Y[j]);
+  const double d = (pyp - p) / (Y[j + 2] - Y[j + 1]);
+  const double e = (p - pzm) / (Z[k + 1] - Z[k]);
+  const double f = (pzp - p) / (Z[k + 2] - Z[k + 1]);
   const double ap = smax(a, 0.0), am = smin(a, 0.0);
   const double bp = smax(b, 0.0), bm = smin(b, 0.0);
   const double cp = smax(c, 0.0), cm = smin(c, 0.0);
@@ -533,13 +547,14 @@ __device__ __forceinline__ double reinit_local(const Grid3& g, const LsGeom& geo
 //   stage 1: out = in + R(in)                     (in = phi, out = phi1)
 //   stage 2: out = 0.25*in + 0.75*phi + 0.25*R(in)  (in = phi1, out = phi2)
 //   stage 3: phi = 1/3*phi + 2/3*in + 2/3*R(in)     (in = phi2, out = phi)
-__global__ void k_reinit_stage(Grid3 g, LsGeom geo, ReinitBuf b, int stage, double cfl, double tol, const double* in,
-                               double* phi, double* out) {
+// Thread (x, y) of CTA (bx, by, bz) owns cell (32 bx + x, 8 by + y, bz): no
+// index division, rows of 32 consecutive cells per warp.
+__global__ void __launch_bounds__(256) k_reinit_stage(Grid3 g, LsGeom geo, ReinitBuf b, int stage, double cfl,
+                                                      double tol, const double* in, double* phi, double* out) {
   if (stage > 1 && b.red[3]) return;  // converged on the residual in stage 1
-  const long long n = (long long)g.nx * g.ny * g.nz;
   double maxres = 0.0, maxrel = 0.0;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q % g.nx), j = (int)((q / g.nx) % g.ny), k = (int)(q / ((long long)g.nx * g.ny));
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
     const long long off = loff(g, i, j, k);
     double R = 0.0;
     if (!b.tag[off]) {
@@ -597,6 +612,7 @@ m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& 
   ReinitBuf b = carve(buf, n);
   const long long ni = (long long)g.nx * g.ny * g.nz;
   const int grid = grid1d(ni);
+  const dim3 grid3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 65535 ? g.nz : 65535), block3(32, 8);
   cudaMemsetAsync(b.red, 0, 4 * sizeof(unsigned long long), s);
   k_reinit_prep<<<grid, 256, 0, s>>>(g, geo, phi, b);
   unsigned long long hred[4];
@@ -613,10 +629,10 @@ m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& 
     for (iter = 0; iter < maxIts; iter++) {
       cudaMemsetAsync(b.red, 0, 2 * sizeof(unsigned long long), s);
       cudaMemsetAsync(b.red + 3, 0, sizeof(unsigned long long), s);
-      k_reinit_stage<<<grid, 256, 0, s>>>(g, geo, b, 1, cfl, tol, phi, phi, b.phi1);
+      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 1, cfl, tol, phi, phi, b.phi1);
       k_reinit_check<<<1, 1, 0, s>>>(b, tol);
-      k_reinit_stage<<<grid, 256, 0, s>>>(g, geo, b, 2, cfl, tol, b.phi1, phi, b.phi2);
-      k_reinit_stage<<<grid, 256, 0, s>>>(g, geo, b, 3, cfl, tol, b.phi2, phi, phi);
+      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 2, cfl, tol, b.phi1, phi, b.phi2);
+      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 3, cfl, tol, b.phi2, phi, phi);
       cudaMemcpyAsync(hred, b.red, sizeof hred, cudaMemcpyDeviceToHost, s);
       if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
       total++;

@@ -39,8 +39,12 @@ namespace m2c {
 constexpr int IFACE_RIEMANN_THREADS = 148 * 4 * 128;
 // Resident CTAs of 128 threads per SM the interface Riemann kernel is
 // compiled for (register budget 65536 / (128 * M2C_IFACE_MINB) per thread).
+// Measured on the 384^3 bubble cluster (mixed, 10 steps): 2 CTAs (255
+// registers) 130.7 ms per step, 3 (168) 125.9 ms, 4 (128, with spills to L1)
+// 122.2 ms: the solve is latency-bound, so more resident warps win over the
+// spill traffic.
 #ifndef M2C_IFACE_MINB
-#define M2C_IFACE_MINB 2
+#define M2C_IFACE_MINB 4
 #endif
 
 struct Multiphase {

@@ -178,9 +178,11 @@ class Solver:
         phi = None if phi is None else np.ascontiguousarray(phi, np.float64)
         check(lib().m2cg_upload_state(self.h, abi.dptr(V), abi.dptr(ID), abi.dptr(phi)))
 
-    def download(self, out_V=None, out_ID=None, out_phi=None):
+    def download(self, out_V=None, out_ID=None, out_phi=None, with_id=True):
+        """Host copies of V (and of the material IDs unless with_id is False,
+        and of phi when there is a level set), ghosted layout."""
         V = out_V if out_V is not None else np.empty(abi.ghosted_shape(self.g, 5))
-        ID = out_ID if out_ID is not None else np.empty(abi.ghosted_shape(self.g))
+        ID = out_ID if out_ID is not None else (np.empty(abi.ghosted_shape(self.g)) if with_id else None)
         phi = out_phi if out_phi is not None else (np.empty(abi.ghosted_shape(self.g)) if self.nls else None)
         check(lib().m2cg_download_state(self.h, abi.dptr(V), abi.dptr(ID), abi.dptr(phi)))
         return V, ID, phi
