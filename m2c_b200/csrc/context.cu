@@ -363,7 +363,9 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   // The (x,y) tiles x z planes are shared evenly by a persistent grid of
   // resident CTAs, each share at least 8 planes long (the plane pipeline's
   // prologue costs about 2.5 planes per segment).
-  const int ty = (scheme->precision != M2CG_PREC_MIXED && nls == 1) ? StageTY<double, true>::value : STAGE_TY;
+  const int ty = scheme->precision == M2CG_PREC_MIXED
+                     ? StageTY<float, false>::value
+                     : (nls == 1 ? StageTY<double, true>::value : StageTY<double, false>::value);
   c->ntx = (c->nx + TX - 1) / TX;
   c->nty = (c->ny + ty - 1) / ty;
   {

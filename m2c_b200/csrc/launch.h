@@ -10,8 +10,13 @@
 namespace m2c {
 
 constexpr int STAGE_TY = 8;
-// Tile height per instantiation (32 x 8 for every kernel).
+#ifndef M2C_STAGE_TY_F32
+#define M2C_STAGE_TY_F32 16
+#endif
+// Tile height per instantiation: 32 x 8 for the FP64 kernels, 32 x 16 for
+// the FP32 (mixed) kernels.
 template <typename T, bool MULTI> struct StageTY { static constexpr int value = STAGE_TY; };
+template <bool MULTI> struct StageTY<float, MULTI> { static constexpr int value = M2C_STAGE_TY_F32; };
 
 size_t stage_smem_fp64(bool multi);
 size_t stage_smem_mixed(bool multi);
