@@ -465,7 +465,7 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "m2c::stage_kernel<float,8>", "avg_launch_ms": avg_launch_ms,
+                         "kernel": "m2c::stage_kernel<float,16>", "avg_launch_ms": avg_launch_ms,
                          "alg_bytes_per_launch": alg_bytes_per_launch,
                          "traffic_source": "ncu dram__bytes_read+write of one stage-2 launch at 160^3, "
                                            "scaled per cell (profiles/stage_kernel_mixed_160cube.md)"},
