@@ -85,6 +85,35 @@ def _cpu_worker(args):
     return times
 
 
+def _cpu_bubble_worker(args):
+    n, nbubbles, steps, seed = args
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    sys.path.insert(0, ROOT)
+    from m2c_b200 import cases
+    from oracle import ref
+    g, s, mats, ls, V, ID, PHI = cases.bubble_case(n, nbubbles=nbubbles, seed=seed)
+    c = ref.RefCase(g, s, mats, ls)
+    c.set_state(V, ID, PHI)
+    t0 = time.perf_counter()
+    c.run(steps)
+    return time.perf_counter() - t0
+
+
+def cpu_reference_bubble(n=48, nbubbles=16, steps=12, cores=None):
+    """The reference on the bubble-cluster physics at n^3 (the 384^3 case does
+    not fit its memory model on the host): `cores` independent processes,
+    `steps` steps each (reinitialisation every 10 steps); cell-updates/s of
+    all processes together."""
+    import multiprocessing as mp
+    cores = cores or min(os.cpu_count() or 1, 64)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        times = pool.map(_cpu_bubble_worker, [(n, nbubbles, steps, 5 + r) for r in range(cores)])
+    return {"value": cores * n ** 3 * steps / max(times), "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{cores} processes x one {n}^3 cluster of {nbubbles} bubbles (same physics), {steps} RK3 "
+                      f"steps each (reinitialisation every 10 steps)"}
+
+
 def cpu_reference(steps, warmup, cores=None):
     """Run the reference on `cores` processes; returns per-step wall times
     (max over processes) and the cell count per step (all processes)."""
@@ -190,7 +219,8 @@ def extra_bubble(n=384, nbubbles=16, steps=10, warmup=2):
     vel = float(np.linalg.norm(Vm[:, 1:4] - Vf[:, 1:4], axis=1).sum() / np.linalg.norm(Vf[:, 1:4], axis=1).sum())
     alg = 387.0 * cells * steps
     peak, kind = measured_peak()
-    out = {"workload": f"bubble cluster {n}^3, {nbubbles} air bubbles in water, HLLC + van Albada, exact interface "
+    kind = "single bubble" if nbubbles == 1 else "bubble cluster"
+    out = {"workload": f"{kind} {n}^3, {nbubbles} air bubble(s) in water, HLLC + van Albada, exact interface "
                        f"Riemann, FD3 level set with reinitialisation every 10 steps, RK3, CFL 0.4",
            "steps": steps, "after_warmup_steps": warmup,
            "mixed": {"cell_updates_per_s": cells * steps / (mm / 1e3), "ms_per_step": mm / steps,
@@ -446,6 +476,9 @@ def main():
         extras = {}
         net = load_warmstart()
         for name, fn in (("bubble_cluster", lambda: extra_bubble()),
+                         ("bubble_cluster_cpu_reference", lambda: cpu_reference_bubble()
+                          if not args.no_cpu_baseline else {"skipped": "--no-cpu-baseline"}),
+                         ("single_bubble_192", lambda: extra_bubble(n=192, nbubbles=1, steps=500, warmup=3)),
                          ("batched_tubes", lambda: extra_tubes(mlp=net)),
                          ("learned_warm_start", lambda: extra_warm_start(net) if net is not None else
                           {"unavailable": "m2c_b200/data/warmstart_mlp.npz not present"})):
