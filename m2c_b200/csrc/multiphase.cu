@@ -65,7 +65,10 @@ struct Multiphase {
   // interface faces
   int* slot = nullptr;     // per cell: slot of its low faces (valid where flagged)
   int* faces = nullptr;    // [cap_faces][3]: cell offset, slot, direction
-  int* counts = nullptr;   // [0] slots, [1] faces, [2] overflow, [3] riemann errors, [4] iterations (low), [5] calls
+  int* counts = nullptr;   // [0] slots, [1] faces, [2] overflow, [3] riemann errors, [4] iterations (low), [5] calls,
+                           // [6] evaluations, [8 + stage] work counters, [12..15] wave-pattern bucket sizes
+  int* order = nullptr;    // [cap_faces] faces grouped by wave pattern (the solve order of a stage)
+  uint8_t* pattern = nullptr;  // [cap_faces] wave pattern of each face at this stage
   long long cap_slots = 0, cap_faces = 0;
   double* Vsm = nullptr;   // [slot][3][5] current stage
   double* Vsp = nullptr;
@@ -184,10 +187,66 @@ struct IfaceRiemannArgs {
   uint8_t* rsValid;
   double* scratch;
   DevError* err;
+  const int* order;       // faces grouped by wave pattern
+  uint8_t* pattern;       // classification scratch
+  int* group_out;         // the same array as order, written by k_iface_group
   int normal_mode;        // MultiPhaseData::riemann_normal
   const double* phi;      // phi^n (the reference's loose coupling uses the step's phi)
   LsGeom geo;
 };
+
+// Wave pattern of each interface problem from the acoustic star-pressure
+// estimate (the solver's own first trial point): bit 1 left shock, bit 0
+// right shock. Solving the problems grouped by pattern keeps the lanes of a
+// warp in the same branches of the star-state evaluation (Hugoniot root or
+// rarefaction integration on each side); the results do not depend on the
+// order. Counts per pattern go to counts[12..15].
+__global__ void k_iface_classify(IfaceRiemannArgs a) {
+  const Grid3& g = a.st.g;
+  long long nf = a.counts[1];
+  if (nf > a.cap_faces) nf = a.cap_faces;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+    const int q = a.faces[3 * f], d = a.faces[3 * f + 2];
+    int i, j, k;
+    cell_coords(g, q, i, j, k);
+    int ni, nj, nk;
+    low_neighbour(g, i, j, k, d, ni, nj, nk);
+    const long long offR = offset_of(g, i, j, k), offL = offset_of(g, ni, nj, nk);
+    const uint8_t idR = a.st.id[offR], idL = a.st.id[offL];
+    double VL[5], VR[5];
+    stage_state(a.st, a.eos, offL, idL, VL);
+    stage_state(a.st, a.eos, offR, idR, VR);
+    const double c2l = a.eos[idL].c2(VL[0], a.eos[idL].energy(VL[0], VL[4]));
+    const double c2r = a.eos[idR].c2(VR[0], a.eos[idR].energy(VR[0], VR[4]));
+    int pat = 0;
+    if (c2l > 0 && c2r > 0 && VL[0] > 0 && VR[0] > 0) {
+      const double Cl = VL[0] * sqrt(c2l), Cr = VR[0] * sqrt(c2r);
+      const double p0 = (Cr * VL[4] + Cl * VR[4] + Cl * Cr * (VL[1 + d] - VR[1 + d])) / (Cl + Cr);
+      pat = (p0 > VL[4] ? 2 : 0) | (p0 > VR[4] ? 1 : 0);
+    }
+    a.pattern[f] = (uint8_t)pat;
+    atomicAdd(&a.counts[12 + pat], 1);
+  }
+}
+
+__global__ void k_iface_group(IfaceRiemannArgs a) {
+  long long nf = a.counts[1];
+  if (nf > a.cap_faces) nf = a.cap_faces;
+  __shared__ int base[4];
+  if (threadIdx.x == 0) {
+    int o = 0;
+    for (int c = 0; c < 4; c++) {
+      base[c] = o;
+      o += a.counts[12 + c];
+    }
+  }
+  __syncthreads();
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+    const int pat = a.pattern[f];
+    const int pos = atomicAdd(&a.counts[16 + pat], 1);
+    a.group_out[base[pat] + pos] = (int)f;
+  }
+}
 
 // One exact Riemann problem per interface face (SpaceOperator.cpp:2499-2523):
 // direction by the riemann_normal rule, cell-centred states (constant
@@ -210,7 +269,8 @@ __global__ void __launch_bounds__(128, M2C_IFACE_MINB) k_iface_riemann(IfaceRiem
   rs.path1.cap = RIEMANN_PATH_CAP;
   rs.path3.pt = rs.path1.pt + 3 * RIEMANN_PATH_CAP;
   rs.path3.cap = RIEMANN_PATH_CAP;
-  for (long long f = atomicAdd(next, 1); f < nf; f = atomicAdd(next, 1)) {
+  for (long long w = atomicAdd(next, 1); w < nf; w = atomicAdd(next, 1)) {
+    const long long f = a.order[w];
     const int q = a.faces[3 * f], s = a.faces[3 * f + 1], d = a.faces[3 * f + 2];
     int i, j, k;
     cell_coords(g, q, i, j, k);
@@ -685,7 +745,9 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   A((void**)&mp->idn, n);
   A((void**)&mp->slot, n * 4);
   A((void**)&mp->faces, mp->cap_faces * 3 * 4);
-  A((void**)&mp->counts, 16 * 4);
+  A((void**)&mp->order, mp->cap_faces * 4);
+  A((void**)&mp->pattern, mp->cap_faces);
+  A((void**)&mp->counts, 32 * 4);
   A((void**)&mp->Vsm, mp->cap_slots * 15 * 8);
   A((void**)&mp->Vsp, mp->cap_slots * 15 * 8);
   A((void**)&mp->Vmid, mp->cap_slots * 15 * 8);
@@ -733,6 +795,7 @@ void multiphase_destroy(Multiphase* mp) {
   cudaFree(mp->d_eos);
   cudaFree(mp->phiN); cudaFree(mp->phiA); cudaFree(mp->phiB); cudaFree(mp->phiT);
   cudaFree(mp->idn); cudaFree(mp->slot); cudaFree(mp->faces); cudaFree(mp->counts);
+  cudaFree(mp->order); cudaFree(mp->pattern);
   cudaFree(mp->Vsm); cudaFree(mp->Vsp); cudaFree(mp->Vmid); cudaFree(mp->midid);
   cudaFree(mp->rsVsm); cudaFree(mp->rsVsp); cudaFree(mp->rsValid); cudaFree(mp->scratch);
   cudaFree(mp->changed); cudaFree(mp->blockcnt); cudaFree(mp->nchanged); cudaFree(mp->mask);
@@ -808,6 +871,12 @@ m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
   ra.normal_mode = mp->scheme.mp_riemann_normal;
   ra.phi = mp->phiN;
   ra.geo = mp->lsg;
+  ra.order = mp->order;
+  ra.pattern = mp->pattern;
+  ra.group_out = mp->order;
+  cudaMemsetAsync(mp->counts + 12, 0, 8 * sizeof(int), s);
+  k_iface_classify<<<148 * 8, 256, 0, s>>>(ra);
+  k_iface_group<<<148 * 8, 256, 0, s>>>(ra);
   k_iface_riemann<<<mp->iface_blocks, 128, 0, s>>>(ra);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
   a.iface.slot = mp->slot;
