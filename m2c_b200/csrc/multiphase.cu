@@ -66,7 +66,7 @@ struct Multiphase {
   int* slot = nullptr;     // per cell: slot of its low faces (valid where flagged)
   int* faces = nullptr;    // [cap_faces][3]: cell offset, slot, direction
   int* counts = nullptr;   // [0] slots, [1] faces, [2] overflow, [3] riemann errors, [4] iterations (low), [5] calls,
-                           // [6] evaluations, [8 + stage] work counters, [12..15] wave-pattern bucket sizes
+                           // [6] evaluations, [8 + stage] work counters, [16...] wave-pattern group sizes
   int* order = nullptr;    // [cap_faces] faces grouped by wave pattern (the solve order of a stage)
   uint8_t* pattern = nullptr;  // [cap_faces] wave pattern of each face at this stage
   long long cap_slots = 0, cap_faces = 0;
@@ -195,9 +195,15 @@ struct IfaceRiemannArgs {
   LsGeom geo;
 };
 
+// Groups: 4 wave patterns x IFACE_STRENGTHS rarefaction strengths; sizes in
+// counts[IFACE_GROUP0 ...], fill positions in the IFACE_GROUPS entries after.
+constexpr int IFACE_STRENGTHS = 8;
+constexpr int IFACE_GROUPS = 4 * IFACE_STRENGTHS;
+constexpr int IFACE_GROUP0 = 16;
+
 // Wave pattern of each interface problem from the acoustic star-pressure
 // estimate (the solver's own first trial point): bit 1 left shock, bit 0
-// right shock. Solving the problems grouped by pattern keeps the lanes of a
+// right shock, refined by the pressure ratio of the stronger rarefaction. Solving the problems grouped by pattern keeps the lanes of a
 // warp in the same branches of the star-state evaluation (Hugoniot root or
 // rarefaction integration on each side); the results do not depend on the
 // order. Counts per pattern go to counts[12..15].
@@ -222,28 +228,34 @@ __global__ void k_iface_classify(IfaceRiemannArgs a) {
     if (c2l > 0 && c2r > 0 && VL[0] > 0 && VR[0] > 0) {
       const double Cl = VL[0] * sqrt(c2l), Cr = VR[0] * sqrt(c2r);
       const double p0 = (Cr * VL[4] + Cl * VR[4] + Cl * Cr * (VL[1 + d] - VR[1 + d])) / (Cl + Cr);
-      pat = (p0 > VL[4] ? 2 : 0) | (p0 > VR[4] ? 1 : 0);
+      // strength of the stronger rarefaction (its pressure ratio, in octaves)
+      double r = 1.0;
+      if (p0 < VL[4] && p0 > 0) r = fmax(r, VL[4] / p0);
+      if (p0 < VR[4] && p0 > 0) r = fmax(r, VR[4] / p0);
+      int oct = (int)log2(r);
+      oct = oct < 0 ? 0 : (oct > IFACE_STRENGTHS - 1 ? IFACE_STRENGTHS - 1 : oct);
+      pat = ((p0 > VL[4] ? 2 : 0) | (p0 > VR[4] ? 1 : 0)) * IFACE_STRENGTHS + oct;
     }
     a.pattern[f] = (uint8_t)pat;
-    atomicAdd(&a.counts[12 + pat], 1);
+    atomicAdd(&a.counts[IFACE_GROUP0 + pat], 1);
   }
 }
 
 __global__ void k_iface_group(IfaceRiemannArgs a) {
   long long nf = a.counts[1];
   if (nf > a.cap_faces) nf = a.cap_faces;
-  __shared__ int base[4];
+  __shared__ int base[IFACE_GROUPS];
   if (threadIdx.x == 0) {
     int o = 0;
-    for (int c = 0; c < 4; c++) {
+    for (int c = 0; c < IFACE_GROUPS; c++) {
       base[c] = o;
-      o += a.counts[12 + c];
+      o += a.counts[IFACE_GROUP0 + c];
     }
   }
   __syncthreads();
   for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
     const int pat = a.pattern[f];
-    const int pos = atomicAdd(&a.counts[16 + pat], 1);
+    const int pos = atomicAdd(&a.counts[IFACE_GROUP0 + IFACE_GROUPS + pat], 1);
     a.group_out[base[pat] + pos] = (int)f;
   }
 }
@@ -747,7 +759,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   A((void**)&mp->faces, mp->cap_faces * 3 * 4);
   A((void**)&mp->order, mp->cap_faces * 4);
   A((void**)&mp->pattern, mp->cap_faces);
-  A((void**)&mp->counts, 32 * 4);
+  A((void**)&mp->counts, (IFACE_GROUP0 + 2 * IFACE_GROUPS) * 4);
   A((void**)&mp->Vsm, mp->cap_slots * 15 * 8);
   A((void**)&mp->Vsp, mp->cap_slots * 15 * 8);
   A((void**)&mp->Vmid, mp->cap_slots * 15 * 8);
@@ -874,7 +886,7 @@ m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
   ra.order = mp->order;
   ra.pattern = mp->pattern;
   ra.group_out = mp->order;
-  cudaMemsetAsync(mp->counts + 12, 0, 8 * sizeof(int), s);
+  cudaMemsetAsync(mp->counts + IFACE_GROUP0, 0, 2 * IFACE_GROUPS * sizeof(int), s);
   k_iface_classify<<<148 * 8, 256, 0, s>>>(ra);
   k_iface_group<<<148 * 8, 256, 0, s>>>(ra);
   k_iface_riemann<<<mp->iface_blocks, 128, 0, s>>>(ra);
