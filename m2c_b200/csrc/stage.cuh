@@ -747,6 +747,15 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       commit_plane(m + 2);
       __syncthreads();
       if (m + 3 <= ke + 1) issue_plane(m + 3);  // in flight during the work below
+      if (m >= kb && own) {  // the update's FP64 inputs of plane m into L1 while the faces are computed
+        const long long offp = (long long)m * g.plane + (long long)gj * g.px + gi;
+#pragma unroll
+        for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.Vn[c] + offp));
+        if (a.stage != 1) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.Us[c] + offp));
+        }
+      }
       if (m + 1 >= kb - 1 && !plane_is_ghost(m + 1)) mask_plane(m + 1);
       __syncthreads();
       if (m >= kb - 1) faces(m, m >= kb);
