@@ -18,8 +18,13 @@
 
 #if defined(__CUDACC__)
 #define M2C_HD __host__ __device__ __forceinline__
+// Large helpers called from many sites (the Riemann solver's star-state
+// evaluation): one out-of-line copy keeps the kernel's code within the
+// instruction cache.
+#define M2C_HD_OUTLINE __host__ __device__ __noinline__
 #else
 #define M2C_HD inline
+#define M2C_HD_OUTLINE inline
 #endif
 
 namespace m2c {

@@ -267,7 +267,7 @@ struct RiemannSolver {
   };
 
   // ComputeRhoUStar (ExactRiemannSolverBase.cpp:1169-1580). Returns success.
-  M2C_HD bool rho_u_star(int wave, RPath& path, double rho, double u, double p, double ps, int id, double rhos0,
+  M2C_HD_OUTLINE bool rho_u_star(int wave, RPath& path, double rho, double u, double p, double ps, int id, double rhos0,
                          double rhos1, double& rhos, double& us, bool* trans_rare, double* Vrare_x0) const {
     const Eos<double>& e = eos[id];
     if (wave == 1) evaluations++;
