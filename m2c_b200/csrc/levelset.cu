@@ -583,11 +583,23 @@ __global__ void __launch_bounds__(256) k_reinit_stage(Grid3 g, LsGeom geo, Reini
       maxrel = smax(maxrel, le);
     }
   }
+  // maxima over the CTA (warp shuffles, then its 8 warps), one atomic per CTA:
+  // per-warp atomics on one address serialised at L2 and bounded the kernel
   for (int o = 16; o > 0; o >>= 1) {
     maxres = smax(maxres, __shfl_xor_sync(0xffffffffu, maxres, o));
     maxrel = smax(maxrel, __shfl_xor_sync(0xffffffffu, maxrel, o));
   }
-  if ((threadIdx.x & 31) == 0) {
+  __shared__ double wres[8], wrel[8];
+  if (threadIdx.x == 0) {
+    wres[threadIdx.y] = maxres;
+    wrel[threadIdx.y] = maxrel;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int w = 1; w < 8; w++) {
+      maxres = smax(maxres, wres[w]);
+      maxrel = smax(maxrel, wrel[w]);
+    }
     if (stage == 1 && maxres > 0) atomicMax(&b.red[0], (unsigned long long)__double_as_longlong(maxres));
     if (stage == 3 && maxrel > 0) atomicMax(&b.red[1], (unsigned long long)__double_as_longlong(maxrel));
   }
@@ -612,7 +624,8 @@ m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& 
   ReinitBuf b = carve(buf, n);
   const long long ni = (long long)g.nx * g.ny * g.nz;
   const int grid = grid1d(ni);
-  const dim3 grid3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 65535 ? g.nz : 65535), block3(32, 8);
+  // each CTA walks a column of planes (k = bz, bz + 64, ...)
+  const dim3 grid3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 64 ? g.nz : 64), block3(32, 8);
   cudaMemsetAsync(b.red, 0, 4 * sizeof(unsigned long long), s);
   k_reinit_prep<<<grid, 256, 0, s>>>(g, geo, phi, b);
   unsigned long long hred[4];
