@@ -512,14 +512,15 @@ __global__ void k_pack_state(Grid3 g, const double* s0, const double* s1, const 
 
 // CFL sweep (SpaceOperator::FindExtremeValuesOfFlowVariables, 2128-2198):
 // min over cells of min(dx/(|u|+c), dy/(|v|+c), dz/(|w|+c)).
-__global__ void k_cfl(Grid3 g, SchemeK sk, const double* v0, const double* v1, const double* v2, const double* v3,
-                      const double* v4, const uint8_t* id, unsigned long long* dtmin, DevError* err) {
-  long long n = (long long)g.nx * g.ny * g.nz;
+// 2D CTAs of 32 x 8 cells over (i, j) walking a column of planes; the
+// minimum is reduced per CTA (one atomic each).
+__global__ void __launch_bounds__(256) k_cfl(Grid3 g, SchemeK sk, const double* v0, const double* v1,
+                                             const double* v2, const double* v3, const double* v4,
+                                             const uint8_t* id, unsigned long long* dtmin, DevError* err) {
   double best = 1.0e300;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    int i = (int)(q % g.nx);
-    int j = (int)((q / g.nx) % g.ny);
-    int k = (int)(q / ((long long)g.nx * g.ny));
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
+    const long long q = ((long long)k * g.ny + j) * g.nx + i;
     long long o = (long long)k * g.plane + (long long)j * g.px + i;
     const Eos<double>& e = sk.ed[id && id[o] < sk.nmat ? id[o] : 0];
     double rho = v0[o], p = v4[o];
@@ -530,7 +531,13 @@ __global__ void k_cfl(Grid3 g, SchemeK sk, const double* v0, const double* v1, c
     best = smin(best, r);
   }
   for (int o = 16; o > 0; o >>= 1) best = smin(best, __shfl_xor_sync(0xffffffffu, best, o));
-  if ((threadIdx.x & 31) == 0 && best < 1.0e300) atomicMin(dtmin, (unsigned long long)__double_as_longlong(best));
+  __shared__ double wbest[8];
+  if (threadIdx.x == 0) wbest[threadIdx.y] = best;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int w = 1; w < 8; w++) best = smin(best, wbest[w]);
+    if (best < 1.0e300) atomicMin(dtmin, (unsigned long long)__double_as_longlong(best));
+  }
 }
 
 __global__ void k_reset_dtmin(unsigned long long* dtmin) { *dtmin = 0x7ff0000000000000ull; }
@@ -589,7 +596,8 @@ static m2cg_status ensure_stage_buf(m2cg_ctx* c, size_t bytes) {
 static m2cg_status compute_dtmin(m2cg_ctx* c) {
   k_reset_dtmin<<<1, 1, 0, c->stream>>>(c->dtmin);
   double** V = c->V[c->cur];
-  k_cfl<<<grid1d((long long)c->nx * c->ny * c->nz), 256, 0, c->stream>>>(c->g, c->sk, V[0], V[1], V[2], V[3], V[4],
+  k_cfl<<<dim3((c->nx + 31) / 32, (c->ny + 7) / 8, c->nz < 64 ? c->nz : 64), dim3(32, 8), 0, c->stream>>>(
+      c->g, c->sk, V[0], V[1], V[2], V[3], V[4],
                                                                          c->id, c->dtmin, c->err);
   c->counters.kernel_launches += 2;
   CK(cudaGetLastError());

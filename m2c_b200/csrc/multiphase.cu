@@ -123,12 +123,15 @@ __device__ __forceinline__ bool low_neighbour(const Grid3& g, int i, int j, int 
 }
 
 // Collect interface faces: every low face whose two cells carry different IDs.
+// 2D CTAs of 32 x 8 cells over (i, j), walking a column of planes; slots
+// and face entries are taken in arrival order (any order serves: every
+// later pass addresses them through slot[] and faces[]).
 __global__ void k_detect_iface(Grid3 g, const uint8_t* id, int* slot, int* faces, int* counts, long long cap_slots,
                                long long cap_faces) {
-  long long n = (long long)g.nx * g.ny * g.nz;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    cell_coords(g, q, i, j, k);
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  for (int k = blockIdx.z; k < g.nz; k += gridDim.z) {
+    const long long q = ((long long)k * g.ny + j) * g.nx + i;
     const long long off = offset_of(g, i, j, k);
     const uint8_t me = id[off];
     int mask = 0;
@@ -327,11 +330,11 @@ __global__ void __launch_bounds__(128, M2C_IFACE_MINB) k_iface_riemann(IfaceRiem
 // Material ID from the sign change of phi (MultiPhaseOperator.cpp:150-202):
 // with one level set and two materials a swept cell becomes the level set's
 // material where phi < 0 and material 0 otherwise.
+// 2D CTAs of 32 x 8 cells over (i, j), walking a column of planes.
 __global__ void k_update_id(Grid3 g, const double* phi, const double* phi0, uint8_t* id, int ls_mat) {
-  long long n = (long long)g.nx * g.ny * g.nz;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    cell_coords(g, q, i, j, k);
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  for (int k = blockIdx.z; k < g.nz; k += gridDim.z) {
     const long long off = offset_of(g, i, j, k);
     const double p = phi[off], p0 = phi0[off];
     if (p * p0 > 0.0) continue;
@@ -852,7 +855,8 @@ m2cg_status multiphase_begin_step(Multiphase* mp, cudaStream_t s, double* const*
   cudaMemcpyAsync(mp->phiT, mp->phiN, n * 8, cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(mp->idn, id, n, cudaMemcpyDeviceToDevice, s);
   cudaMemsetAsync(mp->counts, 0, 16 * 4, s);
-  k_detect_iface<<<grid1d((long long)g.nx * g.ny * g.nz), 256, 0, s>>>(g, id, mp->slot, mp->faces, mp->counts,
+  k_detect_iface<<<dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 64 ? g.nz : 64), dim3(32, 8), 0, s>>>(
+      g, id, mp->slot, mp->faces, mp->counts,
                                                                         mp->cap_slots, mp->cap_faces);
   mp->stage = 0;
   return cudaGetLastError() == cudaSuccess ? M2CG_OK : M2CG_ERR_CUDA;
@@ -915,7 +919,8 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
   const Grid3& g = mp->g;
   const long long ninterior = (long long)g.nx * g.ny * g.nz;
   // material ID from the sign change of phi
-  k_update_id<<<grid1d(ninterior), 256, 0, s>>>(g, mp->phiN, mp->phiT, id, mp->ls.material_id);
+  k_update_id<<<dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 64 ? g.nz : 64), dim3(32, 8), 0, s>>>(
+      g, mp->phiN, mp->phiT, id, mp->ls.material_id);
   // reinitialisation every `frequency` steps (LevelSetOperator::Reinitialize, 1599-1624)
   if (mp->ls.reinit_frequency > 0 && mp->time_step % mp->ls.reinit_frequency == 0) {
     int its = 0;
