@@ -158,7 +158,8 @@ __device__ double ls_residual(const Grid3& g, const LsGeom& geo, const double* p
   const long long off = loff(g, i, j, k);
   const long long stride[3] = {1, g.px, g.plane};
   const double pc = phi[off];
-  double lo[3], hi[3];
+  const double vel[3] = {u, v, w};
+  double term[3];
   for (int a = 0; a < 3; a++) {
     const int c = a == 0 ? i : (a == 1 ? j : k);
     const bool per = g.bc[2 * a] == BC_PERIODIC;
@@ -168,22 +169,26 @@ __device__ double ls_residual(const Grid3& g, const LsGeom& geo, const double* p
       return phi_at(g, geo, phi, i + (a == 0 ? dc : 0), j + (a == 1 ? dc : 0), k + (a == 2 ? dc : 0));
     };
     const double* X = geo.xg[a];  // X[c+1] = coordinate of index c
-    // left-biased (a, c, e)
-    if (c - 2 >= -1 || per) {
-      lo[a] = fd4(geo.cl[a] + 4 * c, P(-2), P(-1), pc, P(1));
+    // only the upwind-biased derivative is used: left-biased where the
+    // velocity is >= 0 (a, c, e), right-biased otherwise (b, d, f)
+    double der;
+    if (vel[a] >= 0) {
+      if (c - 2 >= -1 || per)
+        der = fd4(geo.cl[a] + 4 * c, P(-2), P(-1), pc, P(1));
+      else
+        der = (pc - P(-1)) / (X[c + 1] - X[c]);
     } else {
-      lo[a] = (pc - P(-1)) / (X[c + 1] - X[c]);
+      if (c + 2 <= n[a] || per) {
+        const double* cf = geo.cr[a] + 4 * c;
+        if (a == 1 && !per && !(i < g.ny - 1)) cf = geo.cr1y + 4 * c;
+        der = fd4(cf, P(-1), pc, P(1), P(2));
+      } else {
+        der = (P(1) - pc) / (X[c + 2] - X[c + 1]);
+      }
     }
-    // right-biased (b, d, f)
-    if (c + 2 <= n[a] || per) {
-      const double* cf = geo.cr[a] + 4 * c;
-      if (a == 1 && !per && !(i < g.ny - 1)) cf = geo.cr1y + 4 * c;
-      hi[a] = fd4(cf, P(-1), pc, P(1), P(2));
-    } else {
-      hi[a] = (P(1) - pc) / (X[c + 2] - X[c + 1]);
-    }
+    term[a] = der * vel[a];
   }
-  double r = (u >= 0 ? lo[0] * u : hi[0] * u) + (v >= 0 ? lo[1] * v : hi[1] * v) + (w >= 0 ? lo[2] * w : hi[2] * w);
+  double r = term[0] + term[1] + term[2];
   return r * -1.0;
 }
 
