@@ -235,8 +235,8 @@ __global__ void k_iface_classify(IfaceRiemannArgs a) {
       double r = 1.0;
       if (p0 < VL[4] && p0 > 0) r = fmax(r, VL[4] / p0);
       if (p0 < VR[4] && p0 > 0) r = fmax(r, VR[4] / p0);
-      int oct = (int)log2(r);
-      oct = oct < 0 ? 0 : (oct > IFACE_STRENGTHS - 1 ? IFACE_STRENGTHS - 1 : oct);
+      const double lr = log2(r);  // r may be +inf: compare before converting
+      const int oct = lr >= IFACE_STRENGTHS - 1 ? IFACE_STRENGTHS - 1 : (lr > 0 ? (int)lr : 0);
       pat = ((p0 > VL[4] ? 2 : 0) | (p0 > VR[4] ? 1 : 0)) * IFACE_STRENGTHS + oct;
     }
     a.pattern[f] = (uint8_t)pat;
