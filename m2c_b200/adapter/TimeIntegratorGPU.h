@@ -9,7 +9,8 @@
 // ghosted local vectors (SpaceVariable3D::GetDataPointer), advances them by
 // one explicit RK step on the GPU (m2cg_advance) and writes them back, ghost
 // layers included. The scope is the GPU path's: one structured subdomain
-// (a single-rank run), one level set, primitive-variable MUSCL.
+// (a single-rank run), at most one level set (finite-difference or
+// finite-volume), MUSCL in any of the reference's variable types.
 //
 // Built against the reference's headers (IoData.h, TimeIntegrator.h,
 // MeshGenerator.h) and linked with libm2c_gpu.so.
