@@ -283,8 +283,14 @@ m2cg_status m2cg_riemann_batch_pairs(const m2cg_scheme* scheme, const m2cg_mater
  *    M2CG_NOALLOC_MAX_PROBLEMS slots of 24 KiB (24 MiB), held by every device
  *    that loads the library until the process exits. n beyond
  *    M2CG_NOALLOC_MAX_PROBLEMS is rejected with M2CG_ERR_ARG and a message.
- *  - The first call on each device looks up that array's device address
- *    (with that device current), so make it before any stream capture.
+ *  - Each call outside a stream capture looks up that array's device address
+ *    with the current device (so a device reset cannot leave a stale one);
+ *    a call made while `stream` is captured reuses the address of the last
+ *    uncaptured call on that device, so make one call (n = 0 is enough)
+ *    before any capture. Under lazy module loading (the CUDA default) that
+ *    first call is also when the driver places the 24 MiB array on the
+ *    device: a caller whose memory pool will take the whole device makes it
+ *    before the pool reserves its memory.
  *  - The work is queued on `stream` (a cudaStream_t, NULL = legacy default
  *    stream); the call returns without waiting. All calls share the scratch
  *    array, so calls that overlap on the GPU (different streams, devices

@@ -88,12 +88,17 @@ __global__ void k_riemann_batch_noalloc(const __grid_constant__ NoAllocArgs p) {
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_setup_mutex;
-double* g_paths_on_device[MAX_DEVICES];  // device address of g_noalloc_paths, per device
+double* g_paths_on_device[MAX_DEVICES];  // last looked-up device address of g_noalloc_paths, per device
 
 // The host-side name g_noalloc_paths is only a stand-in for the symbol; the
-// address a kernel may use is looked up once per device, with that device
-// current.
-m2cg_status paths_address(double** out) {
+// address a kernel may use is looked up with the device current. Outside a
+// stream capture it is looked up again on every call (a table lookup in the
+// runtime), so a device reset, after which the module is loaded again and
+// the array may sit elsewhere, cannot leave a stale address behind. While
+// `stream` is being captured the address of the last call outside a capture
+// is used: a capture must follow at least one call on that device since the
+// last reset.
+m2cg_status paths_address(cudaStream_t stream, double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) {
@@ -104,8 +109,13 @@ m2cg_status paths_address(double** out) {
     set_last_error("m2cg_riemann_batch_noalloc: device ordinal beyond the supported range");
     return M2CG_ERR_UNSUPPORTED;
   }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) {
+    cudaGetLastError();  // an implicit-capture query error is not this call's failure
+    cap = cudaStreamCaptureStatusActive;
+  }
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_paths_on_device[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, g_noalloc_paths);
     if (e != cudaSuccess) {
@@ -116,6 +126,10 @@ m2cg_status paths_address(double** out) {
       return M2CG_ERR_CUDA;
     }
     g_paths_on_device[dev] = (double*)ptr;
+  } else if (!g_paths_on_device[dev]) {
+    set_last_error("m2cg_riemann_batch_noalloc: first call on this device made during a stream capture; "
+                   "make one call (n = 0 is enough) before capturing");
+    return M2CG_ERR_ARG;
   }
   *out = g_paths_on_device[dev];
   return M2CG_OK;
@@ -141,7 +155,7 @@ extern "C" m2cg_status m2cg_riemann_batch_noalloc(const m2cg_scheme* scheme, con
     return M2CG_ERR_ARG;
   }
   double* paths = nullptr;
-  m2cg_status st = paths_address(&paths);
+  m2cg_status st = paths_address((cudaStream_t)stream, &paths);
   if (st != M2CG_OK) return st;
   if (n == 0) return M2CG_OK;
   NoAllocArgs p;

@@ -20,12 +20,15 @@
 // The step sequence, branch structure and floating-point expressions follow
 // the reference so that, compiled without FMA contraction, results agree
 // with it to round-off. The step-size control's pow(x, 0.25) and pow(x, 0.2)
-// round the last bit differently from the host C library (neither is
-// correctly rounded): a step one ulp longer changes the integrated
-// rarefaction in its last bits (about 30% of seeded problems), and where it
-// changes which steps are accepted (about 1%) the secant iteration takes
-// another path and the star states agree to its tolerance (up to ~2e-7
-// relative measured, within tol_main).
+// are the correctly rounded ones (crpow.cuh) on the host and the device
+// alike, so a GPU solve is bit-identical to the host build of this file; the
+// reference's C-library pow rounds the other way on about 6e-4 of these
+// calls, and only the problems that meet such a call can differ from the
+// reference (a step one ulp longer changes the integrated rarefaction in its
+// last bits; measured on seeded problems: about 1.2% of them, largest
+// relative difference ~6e-12). A host build can select the C library's pow
+// instead (M2C_RIEMANN_POW_QUARTER / M2C_RIEMANN_POW_FIFTH) to reproduce the
+// reference bit for bit.
 //
 // The two integration-path caches of the reference (std::vector members
 // integrationPath1/3, ExactRiemannSolverBase.h:28-29) live in a per-problem
@@ -34,7 +37,15 @@
 #pragma once
 #include <float.h>
 
+#include "crpow.cuh"
 #include "physics.cuh"
+
+#ifndef M2C_RIEMANN_POW_QUARTER
+#define M2C_RIEMANN_POW_QUARTER(x) cr_pow_quarter(x)
+#endif
+#ifndef M2C_RIEMANN_POW_FIFTH
+#define M2C_RIEMANN_POW_FIFTH(x) cr_pow_fifth(x)
+#endif
 
 namespace m2c {
 
@@ -332,13 +343,13 @@ struct RiemannSolver {
         double dpTemp = dp;
         const double safety = 0.9;
         if (rhoErrScaled >= errBar && dp > dp_min_adaption) {
-          dpTemp = safety * dp * pow(fabs(errBar / rhoErrScaled), 0.25);
+          dpTemp = safety * dp * M2C_RIEMANN_POW_QUARTER(fabs(errBar / rhoErrScaled));
           dpTemp = smax(smax(dpTemp, 0.2 * dp), dp_min_adaption);
           dp = smin(dpTemp, ps_0 - ps);
           continue;
         }
         if (uErrScaled >= errBar && dp > dp_min_adaption) {
-          dpTemp = safety * dp * pow(fabs(errBar / uErrScaled), 0.25);
+          dpTemp = safety * dp * M2C_RIEMANN_POW_QUARTER(fabs(errBar / uErrScaled));
           dpTemp = smax(smax(dpTemp, 0.2 * dp), dp_min_adaption);
           dp = smin(dpTemp, ps_0 - ps);
           continue;
@@ -354,8 +365,8 @@ struct RiemannSolver {
           Vrare_x0[1] = w0 * us_0 + w1 * us_1;
           Vrare_x0[2] = w0 * ps_0 + w1 * ps_1;
         }
-        double dpTemp_rho = safety * dp * pow(fabs(errBar / rhoErrScaled), 0.2);
-        double dpTemp_u = safety * dp * pow(fabs(errBar / uErrScaled), 0.2);
+        double dpTemp_rho = safety * dp * M2C_RIEMANN_POW_FIFTH(fabs(errBar / rhoErrScaled));
+        double dpTemp_u = safety * dp * M2C_RIEMANN_POW_FIFTH(fabs(errBar / uErrScaled));
         dpTemp = smin(dpTemp_rho, dpTemp_u);
         dpTemp = smin(dpTemp, 10 * dp);
         dpTemp = smax(dpTemp, dp_min_adaption);

@@ -3,6 +3,11 @@
   * ``RefCase``/``RefPoint`` over oracle/_ref/libm2c_ref.so: the unmodified
     reference M2C sources compiled in place with single-rank shims
     (oracle/Makefile, target ``ref``), driven like Main.cpp.
+  * ``RefCaseCR``/``RefPointCR`` over oracle/_ref/libm2c_ref_crpow.so
+    (target ``refcr``): the same reference build with pow(x, 0.25) and
+    pow(x, 0.2) correctly rounded (oracle/ref_shim/crpow_interpose.cpp), as
+    the GPU's Riemann solver computes them; every other operation is the
+    unmodified reference's.
   * ``DropinCase`` over oracle/_ref/libm2c_dropin.so (target ``dropin``):
     the same reference driver with its RK integrator replaced by the GPU
     drop-in m2c_b200/adapter/TimeIntegratorGPU.h. This one runs the product
@@ -22,6 +27,7 @@ from m2c_b200 import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libm2c_ref.so")
 DROPIN_SO = os.path.join(HERE, "_ref", "libm2c_dropin.so")
+CR_SO = os.path.join(HERE, "_ref", "libm2c_ref_crpow.so")
 
 _libs = {}
 
@@ -63,7 +69,7 @@ def _load(path, prefix):
 
 
 def available(which="ref"):
-    return os.path.exists(REF_SO if which == "ref" else DROPIN_SO)
+    return os.path.exists({"ref": REF_SO, "crpow": CR_SO, "dropin": DROPIN_SO}[which])
 
 
 class _Case:
@@ -191,6 +197,14 @@ def RefPoint(s, mats):
     return _Point(_load(REF_SO, "m2cref_"), "m2cref_", s, mats)
 
 
+def RefCaseCR(g, s, mats, ls=None):
+    return _Case(_load(CR_SO, "m2cref_"), "m2cref_", g, s, mats, ls)
+
+
+def RefPointCR(s, mats):
+    return _Point(_load(CR_SO, "m2cref_"), "m2cref_", s, mats)
+
+
 def DropinCase(g, s, mats, ls=None):
     return _Case(_load(DROPIN_SO, "m2cref_"), "m2cref_", g, s, mats, ls)
 
@@ -198,13 +212,13 @@ def DropinCase(g, s, mats, ls=None):
 def _tube_worker(args):
     """One tube as one reference run (process-pool worker: a reference abort
     ends only this process). args = (scheme field dict, n, two material field
-    tuples, VL, VR, nsteps); returns (V [n, 5], ID [n], t)."""
-    sd, n, mt, VL, VR, nsteps = args
+    tuples, VL, VR, nsteps, crpow); returns (V [n, 5], ID [n], t)."""
+    sd, n, mt, VL, VR, nsteps, crpow = args
     from m2c_b200 import cases
     s = abi.scheme(**sd)
     mats = [abi.Material(*m) for m in mt]
     g, ls, V, ID, PHI = cases.tube_case(n, VL, VR)
-    c = RefCase(g, s, mats, ls)
+    c = (RefCaseCR if crpow else RefCase)(g, s, mats, ls)
     c.set_state(V, ID, PHI)
     _, t = c.run(nsteps)
     Vr, IDr, _ = c.get_state()
@@ -212,15 +226,16 @@ def _tube_worker(args):
     return Vr[1, 1, 1:-1].copy(), IDr[1, 1, 1:-1].astype(np.int32), t
 
 
-def tubes(s, lens, mats, VL, VR, nsteps, which, processes=8):
+def tubes(s, lens, mats, VL, VR, nsteps, which, processes=8, crpow=False):
     """Reference runs of the selected tubes (indices `which`) of a batch, in
-    a spawned process pool. Returns a list of (V, ID, t) or None where the
+    a spawned process pool (crpow: the build with correctly rounded
+    step-control pow). Returns a list of (V, ID, t) or None where the
     reference process failed."""
     import multiprocessing as mp
     sd = {f: getattr(s, f) for f, _ in abi.Scheme._fields_}
     field = lambda m: tuple(getattr(m, f) for f, _ in abi.Material._fields_)
-    jobs = [(sd, int(lens[t]), (field(mats[2 * t]), field(mats[2 * t + 1])), tuple(VL[t]), tuple(VR[t]), nsteps)
-            for t in which]
+    jobs = [(sd, int(lens[t]), (field(mats[2 * t]), field(mats[2 * t + 1])), tuple(VL[t]), tuple(VR[t]), nsteps,
+             crpow) for t in which]
     out = []
     with mp.get_context("spawn").Pool(min(processes, len(jobs))) as pool:
         res = [pool.apply_async(_tube_worker, (j,)) for j in jobs]

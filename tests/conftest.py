@@ -1,4 +1,6 @@
+import ctypes
 import os
+import subprocess
 import sys
 
 import pytest
@@ -36,3 +38,13 @@ def ref():
     if not r.available("ref"):
         pytest.skip("reference oracle not built (make -C oracle ref)")
     return r
+
+
+@pytest.fixture(scope="session")
+def host_riemann_lib(tmp_path_factory):
+    """The library's exact Riemann solver compiled for the host
+    (tests/host/riemann_host.cpp)."""
+    out = str(tmp_path_factory.mktemp("riemann_host") / "libriemann_host.so")
+    src = os.path.join(ROOT, "tests", "host", "riemann_host.cpp")
+    subprocess.run(["g++", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", out, src], check=True)
+    return ctypes.CDLL(out)

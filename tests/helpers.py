@@ -1,5 +1,9 @@
 """Comparison helpers for parity tests."""
+import ctypes as C
+
 import numpy as np
+
+from m2c_b200 import abi
 
 
 def rel_err(a, b, axis_last=True):
@@ -30,3 +34,22 @@ def face_ghosts_mask(shape):
     out = ((k == 0) | (k == nz - 1)).astype(int) + ((j == 0) | (j == ny - 1)).astype(int) + \
           ((i == 0) | (i == nx - 1)).astype(int)
     return out <= 1
+
+
+def host_riemann(lib, s, mats, VL, idl, VR, idr, dirs, libm=True):
+    """Solve with the host build of the library's exact Riemann solver
+    (tests/host/riemann_host.cpp): libm=True takes pow from the C library as
+    the reference does, libm=False the correctly rounded roots the GPU uses.
+    Returns (Vs, id, Vsm, Vsp, err, retried, misrounded): misrounded[q]
+    counts problem q's step-control pow calls where the C library's result is
+    not the correctly rounded one."""
+    n = len(VL)
+    table = (abi.Material * len(mats))(*mats)
+    Vs, Vsm, Vsp = np.zeros((n, 5)), np.zeros((n, 5)), np.zeros((n, 5))
+    mid, err, retried = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    mis = np.zeros(n, np.int32)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    args = [np.ascontiguousarray(a) for a in (dirs, VL, np.asarray(idl, np.int32), VR, np.asarray(idr, np.int32))]
+    lib.host_riemann(C.byref(s), table, len(mats), n, *[p(a) for a in args], p(Vs), p(mid), p(Vsm), p(Vsp),
+                     p(err), p(retried), int(bool(libm)), p(mis))
+    return Vs, mid, Vsm, Vsp, err, retried, mis

@@ -1,10 +1,36 @@
 // Test harness: the library's exact Riemann solver (m2c_b200/csrc/riemann.cuh)
-// compiled for the host with g++ (no FMA contraction, the host C library's
-// pow and sqrt), so that it can be compared with the reference's own solver
-// bit for bit. Not part of the library.
+// compiled for the host with g++ (no FMA contraction). Two builds of the
+// rarefaction step control's pow(x, 0.25) / pow(x, 0.2), chosen per call of
+// host_riemann:
+//   libm = 1: the host C library's pow, as the reference calls it, so the
+//             solver can be compared with the reference's own bit for bit;
+//   libm = 0: the correctly rounded roots of crpow.cuh, which the GPU uses,
+//             so the GPU can be compared with this build bit for bit.
+// Either way every call also evaluates the other one and counts, per
+// problem, the calls where the two differ (the C library's pow is not
+// correctly rounded there). Not part of the library.
 #include <cmath>
 #include <vector>
 
+#include "../../m2c_b200/csrc/crpow.cuh"
+
+static int g_libm = 1;
+static int g_misrounded = 0;
+
+static double host_pow_quarter(double x) {
+  const double a = std::pow(x, 0.25), b = m2c::cr_pow_quarter(x);
+  if (a != b) g_misrounded++;
+  return g_libm ? a : b;
+}
+
+static double host_pow_fifth(double x) {
+  const double a = std::pow(x, 0.2), b = m2c::cr_pow_fifth(x);
+  if (a != b) g_misrounded++;
+  return g_libm ? a : b;
+}
+
+#define M2C_RIEMANN_POW_QUARTER(x) host_pow_quarter(x)
+#define M2C_RIEMANN_POW_FIFTH(x) host_pow_fifth(x)
 #include "../../include/m2c_gpu.h"
 #include "../../m2c_b200/csrc/riemann.cuh"
 
@@ -12,7 +38,8 @@ using namespace m2c;
 
 extern "C" int host_riemann(const m2cg_scheme* s, const m2cg_material* mats, int nmat, int n, const double* dir,
                             const double* VL, const int* idl, const double* VR, const int* idr, double* Vs, int* id,
-                            double* Vsm, double* Vsp, int* err, int* retried) {
+                            double* Vsm, double* Vsp, int* err, int* retried, int libm, int* misrounded) {
+  g_libm = libm;
   std::vector<Eos<double>> eos(nmat);
   for (int m = 0; m < nmat; m++) {
     MatParams p;
@@ -52,11 +79,13 @@ extern "C" int host_riemann(const m2cg_scheme* s, const m2cg_material* mats, int
   for (int q = 0; q < n; q++) {
     bool bad = false;
     int mid = 0;
+    g_misrounded = 0;
     int r = rs.solve(dir + 3 * q, VL + 5 * q, idl[q], VR + 5 * q, idr[q], Vs + 5 * q, mid, Vsm + 5 * q, Vsp + 5 * q,
                      NAN, bad);
     id[q] = mid;
     err[q] = r | (bad ? 4 : 0);
     retried[q] = rs.retried ? 1 : 0;
+    if (misrounded) misrounded[q] = g_misrounded;
   }
   return 0;
 }

@@ -1,50 +1,29 @@
 """The library's exact Riemann solver (csrc/riemann.cuh) compiled for the
 host against the reference's ExactRiemannSolverBase::ComputeRiemannSolution,
-both on the CPU with the same C library: every output of every problem must
-be bit-identical, including the problems the adaptive solve cannot bracket or
-converge, which both hand to the non-adaptive solver
-(ExactRiemannSolverBase.cpp:173-188, 327-330, 2199-2945). On the GPU the only
-remaining difference is the last bit of pow() and sqrt() in the rarefaction
-step control (bounded in test_gpu_riemann)."""
-import ctypes as C
-import os
-import subprocess
+both on the CPU.
 
+With the C library's pow in the rarefaction step control (as the reference
+calls it) every output of every problem is bit-identical, including the
+problems the adaptive solve cannot bracket or converge, which both hand to
+the non-adaptive solver (ExactRiemannSolverBase.cpp:173-188, 327-330,
+2199-2945). With the correctly rounded pow the GPU uses (crpow.cuh), a
+problem can differ from the reference only if one of its step-control pow
+calls is one the C library does not round correctly; the GPU tests compare
+the GPU with this second build bit for bit."""
 import numpy as np
 import pytest
 
 from m2c_b200 import abi, cases
-
-HERE = os.path.dirname(os.path.abspath(__file__))
-
-
-@pytest.fixture(scope="module")
-def host_lib(tmp_path_factory):
-    out = str(tmp_path_factory.mktemp("riemann_host") / "libriemann_host.so")
-    src = os.path.join(HERE, "host", "riemann_host.cpp")
-    subprocess.run(["g++", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", out, src], check=True)
-    return C.CDLL(out)
-
-
-def host_riemann(lib, s, mats, VL, idl, VR, idr, dirs):
-    n = len(VL)
-    table = (abi.Material * len(mats))(*mats)
-    Vs, Vsm, Vsp = np.zeros((n, 5)), np.zeros((n, 5)), np.zeros((n, 5))
-    mid, err, retried = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
-    p = lambda a: a.ctypes.data_as(C.c_void_p)
-    args = [np.ascontiguousarray(a) for a in (dirs, VL, np.asarray(idl, np.int32), VR, np.asarray(idr, np.int32))]
-    lib.host_riemann(C.byref(s), table, len(mats), n, *[p(a) for a in args], p(Vs), p(mid), p(Vsm), p(Vsp),
-                     p(err), p(retried))
-    return Vs, mid, Vsm, Vsp, err, retried
+from tests.helpers import host_riemann
 
 
 @pytest.mark.parametrize("seed", [3, 5])
-def test_host_solver_bit_identical_to_reference(ref, host_lib, seed):
+def test_host_solver_bit_identical_to_reference(ref, host_riemann_lib, seed):
     n = 2000
     mats, VL, idl, VR, idr, dirs = cases.riemann_problems(n, seed=seed)
     s = abi.scheme()
     Vs, mid, Vsm, Vsp, err = ref.RefPoint(s, mats).riemann(dirs, VL, idl, VR, idr)
-    hVs, hmid, hVsm, hVsp, herr, retried = host_riemann(host_lib, s, mats, VL, idl, VR, idr, dirs)
+    hVs, hmid, hVsm, hVsp, herr, retried, mis = host_riemann(host_riemann_lib, s, mats, VL, idl, VR, idr, dirs)
     for a, b in ((hVs, Vs), (hVsm, Vsm), (hVsp, Vsp)):
         assert np.array_equal(a, b, equal_nan=True)
     assert np.array_equal(hmid, mid)
@@ -52,3 +31,78 @@ def test_host_solver_bit_identical_to_reference(ref, host_lib, seed):
     # the non-adaptive retry runs on these problems and rescues some of them
     assert retried.sum() > 0
     assert ((retried != 0) & (err == 0)).sum() > 0
+    # the C library misrounds a small share of the step-control pow calls
+    assert 0 < (mis > 0).mean() < 0.25
+
+
+@pytest.mark.parametrize("seed", [3, 5])
+def test_correctly_rounded_pow_differs_only_where_libm_misrounds(ref, host_riemann_lib, seed):
+    """Problems whose pow calls the C library rounds correctly are
+    bit-identical to the reference; the others stay within 1e-11."""
+    n = 2000
+    mats, VL, idl, VR, idr, dirs = cases.riemann_problems(n, seed=seed)
+    s = abi.scheme()
+    Vs, mid, Vsm, Vsp, err = ref.RefPoint(s, mats).riemann(dirs, VL, idl, VR, idr)
+    hVs, hmid, hVsm, hVsp, herr, retried, mis = host_riemann(host_riemann_lib, s, mats, VL, idl, VR, idr, dirs,
+                                                             libm=False)
+    same = np.ones(n, bool)
+    worst = np.zeros(n)
+    for a, b in ((hVs, Vs), (hVsm, Vsm), (hVsp, Vsp)):
+        same &= np.array([np.array_equal(a[q], b[q], equal_nan=True) for q in range(n)])
+        worst = np.maximum(worst, np.nan_to_num(np.abs(a - b) / np.maximum(np.abs(b), 1e-300), nan=0.0).max(axis=1))
+    assert same[mis == 0].all()
+    assert np.array_equal((herr & 1) != 0, err != 0)
+    assert worst[err == 0].max() <= 1e-11, worst.max()
+
+
+def test_correctly_rounded_roots_against_quad_precision(tmp_path):
+    """cr_pow_quarter / cr_pow_fifth against libquadmath's powq rounded to
+    double, on every binade of positive doubles and on the step control's
+    range."""
+    import ctypes as C
+    import os
+    import subprocess
+    src = tmp_path / "crq.cpp"
+    src.write_text(r'''
+#include <quadmath.h>
+#include <cstdint>
+#include <cstring>
+#include "crpow.cuh"
+extern "C" long check(long n, unsigned long long seed, double* worst_x) {
+  long bad = 0;
+  uint64_t s = seed;
+  for (long i = 0; i < n; i++) {
+    s ^= s << 13; s ^= s >> 7; s ^= s << 17;
+    double x;
+    if (i & 1) { uint64_t b = s & 0x7fefffffffffffffull; memcpy(&x, &b, 8); if (x == 0) continue; }
+    else { double u = (double)(s >> 11) * 0x1p-53; x = exp(log(1e-12) + u * (log(1e16) - log(1e-12))); }
+    const double q4 = (double)powq((__float128)x, (__float128)0.25);
+    const double q5 = (double)powq((__float128)x, (__float128)0.2);
+    if (m2c::cr_pow_quarter(x) != q4 || m2c::cr_pow_fifth(x) != q5) { bad++; *worst_x = x; }
+  }
+  return bad;
+}
+''')
+    so = str(tmp_path / "libcrq.so")
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "m2c_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-I" + csrc, "-o", so, str(src),
+                    "-lquadmath"], check=True)
+    lib = C.CDLL(so)
+    lib.check.restype = C.c_long
+    wx = C.c_double(0.0)
+    assert lib.check(400_000, 88172645463325252, C.byref(wx)) == 0, wx.value
+    import math
+    from ctypes import CDLL
+    # special values behave like pow for these exponents
+    sp = tmp_path / "sp.cpp"
+    sp.write_text('#include "crpow.cuh"\nextern "C" double q(double x){return m2c::cr_pow_quarter(x);}\n'
+                  'extern "C" double f(double x){return m2c::cr_pow_fifth(x);}\n')
+    so2 = str(tmp_path / "libsp.so")
+    subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-I" + csrc, "-o", so2, str(sp)], check=True)
+    L = CDLL(so2)
+    L.q.restype = L.f.restype = C.c_double
+    L.q.argtypes = L.f.argtypes = [C.c_double]
+    assert L.q(0.0) == 0.0 and L.f(0.0) == 0.0
+    assert L.q(math.inf) == math.inf and L.f(math.inf) == math.inf
+    assert math.isnan(L.q(math.nan)) and math.isnan(L.f(-1.0))
+    assert L.q(16.0) == 2.0 and L.f(32.0) == 2.0
