@@ -1,33 +1,44 @@
 """Benchmark: cell-updates/s per RK step of the explicit finite-volume step.
 
-Workload (one GPU holds it): the 3D single-material periodic box, 256^3
-cells, ideal gas gamma 1.4, rho = 1 and p = 1/1.4 perturbed by 16 seeded
-Fourier modes (|k| in 1..8, 1%), solenoidal velocity with RMS Mach 0.3,
-generalized Roe flux with generalized minmod MUSCL (alpha 1), RK3, CFL 0.4.
-The headline runs the mixed path (FP32 reconstruction/flux, FP64 state);
-the FP64 path is timed on the same state and the L1 difference between the
-two is reported.
+Headline workload (one GPU holds it): the 384^3 two-material bubble cluster.
+A 2 cm cube of water (stiffened gas, gamma 6.12, p_inf 3.43e8 Pa, 1000
+kg/m^3, 1e5 Pa) holds 16 seeded air bubbles (gamma 1.4, 1.2 kg/m^3, radii
+0.5-1.5 mm); a planar shock carrying the post-shock water state at 1e9 Pa
+runs in from x = 0 (INLET post-shock, OUTLET ambient water, symmetry on the
+other faces). HLLC + van Albada MUSCL, exact two-material Riemann problems at
+the interface faces, FD3 level set with reinitialisation every 10 steps,
+RK3, CFL 0.4. The timed window starts when the shock front reaches the
+nearest bubble (the front coming from x = 5 mm meets only still water on its
+way there, so that moment's state is the initial one with the front two
+cells upstream of the nearest bubble surface): the timed steps solve the
+interface Riemann problems of the bubbles the shock is hitting. The headline
+runs the mixed path (FP32 reconstruction/flux; FP64 state, water pressure
+recovery and Riemann solves); the FP64 path runs the same steps from the
+same state and the mixed path's error against it is reported.
 
-A "step" is one full RK3 step (3 fused stage launches + the device clock).
-Inputs are larger than L2 (5 x 128 MiB per state array), so no explicit
-flush is needed between steps.
+A "step" is one full RK3 step (3 interface Riemann pre-passes, 3 fused
+stage launches, 3 level-set stages, ID and state update, amortised
+reinitialisation, device clock). Inputs are larger than L2 (5 x 453 MB per
+state array), so no explicit flush is needed between steps.
 
-Multi-GPU: the north-star path does not shard; --gpus N runs N independent
-replicas (one per GPU, "scaling": "weak"), value = all cells updated / max
-time over ranks.
+Multi-GPU: the path does not shard; --gpus N runs N independent replicas
+(one per GPU, "scaling": "weak"), value = all cells updated / max time over
+ranks.
 
 --impl reference: the reference's own CPU implementation (the unmodified
 sources built with single-rank shims under oracle/_ref), run on the host
-cores as independent processes, each advancing a bounded 48^3 sample of the
-same physics (symmetry walls instead of periodic: the reference has no
-periodic boundary) by one RK3 step per benchmark step.
+cores as independent processes, each advancing one 48^3 tile of the same
+384^3 state (same cell size and physics; the domain's boundary rule on
+faces on the domain boundary, symmetry walls on the others) by one RK3 step
+per benchmark step; the tiles are a seeded sample of the 512 tiles.
 
 Extras (rank 0 at N = 1, skipped by --only-headline), under "extras": the
-384^3 sixteen-bubble cluster (mixed vs FP64, error of mixed against FP64,
-material-ID and level-set sign mismatches), the 4096 batched two-material
-tubes (CUDA-graph replay, autotuned tiles, with and without the learned
-warm start), and the learned warm start's evaluations and iterations saved
-on held-out interface problems (network in m2c_b200/data/warmstart_mlp.npz).
+256^3 single-material periodic box (mixed vs FP64, with its own roofline,
+CPU figure and end-to-end figure), the 192^3 single bubble over 500 steps,
+the 4096 batched two-material tubes (CUDA-graph replay, autotuned tiles,
+with and without the learned warm start), and the learned warm start's
+evaluations and iterations saved on held-out interface problems (network in
+m2c_b200/data/warmstart_mlp.npz).
 """
 import argparse
 import json
@@ -36,45 +47,131 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "cell-updates/s per RK step (RK3, 256^3 periodic box, mixed FP32/FP64)"
+METRIC = "cell-updates/s per RK step (RK3, 384^3 two-material bubble cluster, mixed FP32/FP64)"
 UNIT = "cell-updates/s"
-CPU_SAMPLE_N = 48
+CLUSTER_N = 384
+CLUSTER_BUBBLES = 16
+TILE = 48
+BOX_SAMPLE_N = 48
+
+# DRAM bytes (read + write) per cell of one launch of the two-material FP32
+# stage kernel, from an ncu capture of the same kernel on the 192^3 cluster
+# (stage-1 launch, 138 B per cell; the capture and its command are under
+# profiles/).
+STAGE_MULTI_TRAFFIC_B_PER_CELL = 138.0
+# The same for the single-material FP32 stage kernel (stage-2 launch, 160^3
+# periodic box).
+STAGE_SINGLE_TRAFFIC_B_PER_CELL = 164.9
+# Algorithmic bytes of one stage launch: the FP64 conserved state of an RK3
+# step (8 five-vectors, 320 B per cell) over its three stages, plus, with two
+# materials, the material-ID byte the stage reads.
+ALG_STAGE_SINGLE = 320.0 / 3.0
+ALG_STAGE_MULTI = 320.0 / 3.0 + 1.0
+# Algorithmic bytes of a two-material RK3 step per cell: 320 B state, 64 B
+# level set (8 phi values), 3 ID bytes.
+ALG_STEP_MULTI = 387.0
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--n", type=int, default=256)
+    p.add_argument("--n", type=int, default=CLUSTER_N, help="cluster grid size (cells per axis)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64 leg of the headline")
     p.add_argument("--only-headline", action="store_true",
-                   help="skip the extra workloads (bubble cluster, batched tubes, learned warm start)")
+                   help="skip the extra workloads (periodic box, single bubble, batched tubes, warm start)")
     p.add_argument("--bubble", type=int, default=0, metavar="N",
-                   help="run only the bubble-cluster workload at N^3 (for profiling) and print its JSON")
+                   help="run only the cluster workload at N^3, mixed then FP64, and print its JSON (profiling)")
+    p.add_argument("--box", type=int, default=0, metavar="N",
+                   help="run only the periodic-box workload at N^3 and print its JSON (profiling)")
     return p.parse_args()
 
 
+def config(n, world):
+    return {"workload": f"bubble cluster {n}^3: 16 air bubbles (0.5-1.5 mm) in water, 2 cm cube, 1 GPa planar "
+                        f"shock timed from its first contact with a bubble; HLLC + van Albada, exact interface "
+                        f"Riemann, FD3 level set, reinitialisation every 10 steps, RK3, CFL 0.4",
+            "cells": n ** 3, "flush": "inputs larger than L2 (no explicit flush)",
+            "parallelism": f"replicas x{world}"}
+
+
+def cluster_case(n, precision, tile=None):
+    from m2c_b200 import cases
+    return cases.bubble_case(n, nbubbles=CLUSTER_BUBBLES, precision=precision, shock_front="contact", tile=tile)
+
+
 # --------------------------------------------------------------------------
-# CPU reference leg (also the cpu_baseline): independent processes
+# CPU reference legs (the reference arm and the cpu_baseline): independent
+# processes, spawned before any GPU work
 # --------------------------------------------------------------------------
-def _cpu_worker(args):
-    n, steps, seed = args
+def _quiet():
     # the reference prints mesh statistics on stdout: keep the JSON line alone there
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
     sys.path.insert(0, ROOT)
+
+
+def cluster_tiles(n, count, seed=7):
+    """A seeded sample of `count` of the (n/48)^3 tiles of the cluster grid
+    (origins in cells)."""
+    import numpy as np
+    m = n // TILE
+    order = np.random.default_rng(seed).permutation(m ** 3)[:count]
+    return [(int(t % m) * TILE, int((t // m) % m) * TILE, int(t // (m * m)) * TILE) for t in order]
+
+
+def _cpu_cluster_worker(args):
+    n, origin, steps = args
+    _quiet()
+    from m2c_b200 import abi
+    from oracle import ref
+    g, s, mats, ls, V, ID, PHI = cluster_case(n, abi.PREC_FP64, tile=((TILE,) * 3, origin))
+    c = ref.RefCase(g, s, mats, ls)
+    c.set_state(V, ID, PHI)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        c.run(1)
+        times.append(time.perf_counter() - t0)
+    interface = bool(((ID[1:-1, 1:-1, 1:-1] > 0).any()))
+    p = V[1:-1, 1:-1, 1:-1, 4]
+    shocked = bool((p > 1.0e8).any() and (p < 1.0e8).any())
+    return times, interface, shocked
+
+
+def cpu_reference_cluster(n, steps, warmup, cores=None):
+    """The reference on `cores` tiles of the cluster state, one process per
+    tile; per benchmark step the slowest process's step time. Returns
+    (per-step seconds, cells per step, cores, sample text)."""
+    import multiprocessing as mp
+    cores = cores or min(os.cpu_count() or 1, 64)
+    tiles = cluster_tiles(n, cores)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_cpu_cluster_worker, [(n, t, warmup + steps) for t in tiles])
+    per_step = [max(r[0][warmup + w] for r in res) for w in range(steps)]
+    nif = sum(1 for r in res if r[1])
+    nsh = sum(1 for r in res if r[2])
+    sample = (f"{cores} processes x one {TILE}^3 tile of the {n}^3 cluster state (seeded sample of "
+              f"{(n // TILE) ** 3} tiles; {nif} hold bubble cells, {nsh} the shock front), {steps} RK3 steps "
+              f"each after {warmup}, FP64, reinitialisation every 10 steps")
+    return per_step, cores * TILE ** 3, cores, sample
+
+
+def _cpu_box_worker(args):
+    n, steps, seed = args
+    _quiet()
     from m2c_b200 import abi, cases
     from oracle import ref
-    g, s, mats, V = cases.fourier_box(CPU_SAMPLE_N if n is None else n, seed=seed, bc=abi.BC_SYMMETRY)
+    g, s, mats, V = cases.fourier_box(n, seed=seed, bc=abi.BC_SYMMETRY)
     c = ref.RefCase(g, s, mats)
     c.set_state(V)
     times = []
@@ -85,46 +182,16 @@ def _cpu_worker(args):
     return times
 
 
-def _cpu_bubble_worker(args):
-    n, nbubbles, steps, seed = args
-    devnull = os.open(os.devnull, os.O_WRONLY)
-    os.dup2(devnull, 1)
-    sys.path.insert(0, ROOT)
-    from m2c_b200 import cases
-    from oracle import ref
-    g, s, mats, ls, V, ID, PHI = cases.bubble_case(n, nbubbles=nbubbles, seed=seed)
-    c = ref.RefCase(g, s, mats, ls)
-    c.set_state(V, ID, PHI)
-    t0 = time.perf_counter()
-    c.run(steps)
-    return time.perf_counter() - t0
-
-
-def cpu_reference_bubble(n=48, nbubbles=16, steps=12, cores=None):
-    """The reference on the bubble-cluster physics at n^3 (the 384^3 case does
-    not fit its memory model on the host): `cores` independent processes,
-    `steps` steps each (reinitialisation every 10 steps); cell-updates/s of
-    all processes together."""
+def cpu_reference_box(steps, warmup, cores=None):
     import multiprocessing as mp
     cores = cores or min(os.cpu_count() or 1, 64)
     with mp.get_context("spawn").Pool(cores) as pool:
-        times = pool.map(_cpu_bubble_worker, [(n, nbubbles, steps, 5 + r) for r in range(cores)])
-    return {"value": cores * n ** 3 * steps / max(times), "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"{cores} processes x one {n}^3 cluster of {nbubbles} bubbles (same physics), {steps} RK3 "
-                      f"steps each (reinitialisation every 10 steps)"}
-
-
-def cpu_reference(steps, warmup, cores=None):
-    """Run the reference on `cores` processes; returns per-step wall times
-    (max over processes) and the cell count per step (all processes)."""
-    import multiprocessing as mp
-    cores = cores or min(os.cpu_count() or 1, 64)
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        res = pool.map(_cpu_worker, [(CPU_SAMPLE_N, warmup + steps, 100 + r) for r in range(cores)])
+        res = pool.map(_cpu_box_worker, [(BOX_SAMPLE_N, warmup + steps, 100 + r) for r in range(cores)])
     per_step = [max(r[w + warmup] for r in res) for w in range(steps)]
-    cells = cores * CPU_SAMPLE_N ** 3
-    return per_step, cells, cores
+    return {"value": cores * BOX_SAMPLE_N ** 3 * steps / sum(per_step), "unit": UNIT, "cores": cores,
+            "kind": "reference",
+            "sample": f"{cores} processes x one {BOX_SAMPLE_N}^3 box (symmetry walls), {steps} RK3 steps each "
+                      f"after {warmup}"}
 
 
 # --------------------------------------------------------------------------
@@ -177,27 +244,185 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes (read + write) per cell per stage launch of the mixed stage
-    kernel, from the committed ncu summary (one stage-2 launch at 160^3), or
-    None."""
-    import re
-    p = os.path.join(ROOT, "profiles", "stage_kernel_mixed_160cube.md")
-    if os.path.exists(p):
-        m = re.search(r"traffic_bytes_per_cell_per_launch:\s*([0-9.]+)", open(p).read())
-        if m:
-            return {"bytes_per_cell_per_launch": float(m.group(1))}
-    return None
+def _l1(a, b):
+    import numpy as np
+    return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+
+
+# --------------------------------------------------------------------------
+# the headline: the bubble cluster, mixed, in its contact window
+# --------------------------------------------------------------------------
+def cluster_run(n, steps, warmup, with_fp64=True, clocks=None, dist=None):
+    """Mixed path on the cluster: `warmup` steps, then `steps` timed steps,
+    then 2 steps with the stage launches timed one by one. With with_fp64,
+    the FP64 path runs the same steps from the same state (timed alike) and
+    the two are compared. Returns a dict (and keeps the mixed solver open
+    under "_solver" with the case arrays under "_case" for the e2e leg)."""
+    import numpy as np
+    from m2c_b200 import abi, gpu
+    cells = n ** 3
+    case = cluster_case(n, abi.PREC_MIXED)
+    g, s, mats, ls, V, ID, PHI = case
+    sol = gpu.Solver(g, s, mats, ls)
+    sol.upload(V, ID, PHI)
+    sol.time_steps(warmup)
+    c0 = sol.counters()
+    if dist:
+        dist.barrier()
+    if clocks:
+        clocks.start()
+    ms, launches = sol.time_steps(steps)
+    clk = clocks.stop() if clocks else None
+    c1 = sol.counters()
+    stage_ms, nstage, _ = sol.profile_stages(2)
+    peak, _ = measured_peak()
+    d = {k: (c1[k] - c0[k]) / steps for k in c1}
+    out = {"ms": ms, "launches": launches, "clocks": clk,
+           "per_step": {"riemann_calls": d["riemann_calls"], "riemann_nontrivial": d["riemann_nontrivial"],
+                        "riemann_iterations": d["riemann_iterations"],
+                        "riemann_evaluations": d["riemann_evaluations"],
+                        "cells_changed_material_unresolved": d["unresolved_cells"],
+                        "reinitialisations": d["reinit_calls"], "kernel_launches": launches / steps},
+           "stage_avg_ms": stage_ms / nstage, "stage_launches_profiled": nstage,
+           "hbm_frac_step": ALG_STEP_MULTI * cells * steps / (ms / 1e3) / 1e9 / peak}
+    if with_fp64:
+        s64 = abi.scheme(**{f: getattr(s, f) for f, _ in abi.Scheme._fields_})
+        s64.precision = abi.PREC_FP64
+        b = gpu.Solver(g, s64, mats, ls)
+        b.upload(V, ID, PHI)
+        b.time_steps(warmup)
+        ms64, _ = b.time_steps(steps)
+        st64, n64, _ = b.profile_stages(2)  # the same step count as the mixed leg
+        Vm, Im, Pm = sol.download()
+        Vf, If, Pf = b.download()
+        b.close()
+        inner = np.s_[1:-1, 1:-1, 1:-1]
+        vm, vf = Vm[inner].reshape(-1, 5), Vf[inner].reshape(-1, 5)
+        vel = float(np.linalg.norm(vm[:, 1:4] - vf[:, 1:4], axis=1).sum() /
+                    np.linalg.norm(vf[:, 1:4], axis=1).sum())
+        linf = lambda a, c: float(np.abs(a - c).max() / np.abs(c).max())
+        out["fp64"] = {"value": cells * steps / (ms64 / 1e3), "ms_per_step": ms64 / steps,
+                       "hbm_frac_step": ALG_STEP_MULTI * cells * steps / (ms64 / 1e3) / 1e9 / peak,
+                       "stage_avg_ms": st64 / n64,
+                       "stage_hbm_frac": ALG_STAGE_MULTI * cells / (st64 / n64 / 1e3) / 1e9 / peak,
+                       "mixed_speedup": ms64 / ms,
+                       "mixed_vs_fp64_rel_L1": {"rho": _l1(vm[:, 0], vf[:, 0]), "velocity": vel,
+                                                "p": _l1(vm[:, 4], vf[:, 4]),
+                                                "phi": _l1(Pm[inner].ravel(), Pf[inner].ravel())},
+                       "mixed_vs_fp64_rel_Linf": {"rho": linf(vm[:, 0], vf[:, 0]), "p": linf(vm[:, 4], vf[:, 4])},
+                       "material_id_mismatch": int((Im[inner] != If[inner]).sum()),
+                       "phi_sign_mismatch": int(((Pm[inner] < 0) != (Pf[inner] < 0)).sum()),
+                       "after_steps": warmup + steps + 2}
+        del Vm, Im, Pm, Vf, If, Pf
+    out["_solver"] = sol
+    out["_case"] = case
+    return out
+
+
+def cluster_e2e(sol, case, steps, dist=None):
+    """The same metric through the public C-ABI: the host state in the
+    reference's ghosted AoS layout (V, material ID and phi) in pinned memory,
+    m2cg_upload_state + m2cg_run(1) + m2cg_download_state per step."""
+    import torch
+    g, s, mats, ls, V, ID, PHI = case
+    pin = lambda a: torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy()
+    Vh, Ih, Ph = pin(V), pin(ID), pin(PHI)
+    Vh[...] = V
+    Ih[...] = ID
+    Ph[...] = PHI
+    Vo, Io, Po = pin(V), pin(ID), pin(PHI)
+    sol.upload(Vh, Ih, Ph)
+    sol.run(1)
+    sol.download(out_V=Vo, out_ID=Io, out_phi=Po)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sol.upload(Vh, Ih, Ph)
+        sol.run(1)
+        sol.download(out_V=Vo, out_ID=Io, out_phi=Po)
+    te = time.perf_counter() - t0
+    return te, int(Vh.nbytes + Ih.nbytes + Ph.nbytes)
 
 
 # --------------------------------------------------------------------------
 # extra workloads (rank 0, one GPU): the other configurations of the path
 # --------------------------------------------------------------------------
-def extra_bubble(n=384, nbubbles=16, steps=10, warmup=2):
-    """Two-material bubble cluster in water, mixed vs FP64: cell-updates/s,
-    HBM fraction of the algorithmic bytes (RK3: 8 FP64 5-vectors, 8 phi
-    values and 3 ID bytes per cell and step), and the mixed path's error
-    against the FP64 path after the same steps."""
+def extra_box(n=256, steps=20, warmup=3, cpu=True):
+    """The 256^3 single-material periodic box (ideal gas, Roe + generalized
+    minmod, RK3, CFL 0.4), mixed vs FP64, with its stage kernel's roofline,
+    a reference-CPU figure and an end-to-end figure."""
+    import numpy as np
+    import torch
+    from m2c_b200 import abi, cases, gpu
+    cells = n ** 3
+    g, s, mats, V = cases.fourier_box(n, precision=abi.PREC_MIXED, seed=2024)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    sol.time_steps(warmup)
+    ms, _ = sol.time_steps(steps)
+    stage_ms, nstage, _ = sol.profile_stages(3)
+    avg = stage_ms / nstage
+    peak, peak_kind = measured_peak()
+    achieved = ALG_STAGE_SINGLE * cells / (avg / 1e3) / 1e9
+    s64 = abi.scheme(**{f: getattr(s, f) for f, _ in abi.Scheme._fields_})
+    s64.precision = abi.PREC_FP64
+    b = gpu.Solver(g, s64, mats)
+    b.upload(V)
+    b.time_steps(warmup)
+    ms64, _ = b.time_steps(steps)
+    st64, n64, _ = b.profile_stages(3)
+    b.close()
+    a = gpu.Solver(g, s, mats)
+    a.upload(V)
+    c = gpu.Solver(g, s64, mats)
+    c.upload(V)
+    a.run(steps)
+    c.run(steps)
+    Va, _, _ = a.download()
+    Vb, _, _ = c.download()
+    a.close()
+    c.close()
+    ia, ib = Va[1:-1, 1:-1, 1:-1].reshape(-1, 5), Vb[1:-1, 1:-1, 1:-1].reshape(-1, 5)
+    l1 = (np.abs(ia - ib).sum(0) / np.abs(ib).sum(0)).tolist()
+    Vh = torch.empty(V.shape, dtype=torch.float64, pin_memory=True).numpy()
+    Vh[...] = V
+    Vo = torch.empty(V.shape, dtype=torch.float64, pin_memory=True).numpy()
+    sol.upload(Vh)
+    sol.run(1)
+    sol.download(out_V=Vo, with_id=False)
+    ne = 5
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        sol.upload(Vh)
+        sol.run(1)
+        sol.download(out_V=Vo, with_id=False)
+    te = time.perf_counter() - t0
+    sol.close()
+    out = {"workload": f"periodic box {n}^3, ideal gas, Roe + generalized minmod, RK3, CFL 0.4",
+           "mixed": {"cell_updates_per_s": cells * steps / (ms / 1e3), "ms_per_step": ms / steps},
+           "fp64": {"cell_updates_per_s": cells * steps / (ms64 / 1e3), "ms_per_step": ms64 / steps,
+                    "stage_avg_ms": st64 / n64,
+                    "stage_hbm_frac": ALG_STAGE_SINGLE * cells / (st64 / n64 / 1e3) / 1e9 / peak},
+           "mixed_speedup": ms64 / ms,
+           "mixed_vs_fp64_rel_L1": dict(zip(["rho", "u", "v", "w", "p"], l1)),
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_kind": peak_kind,
+                        "traffic": STAGE_SINGLE_TRAFFIC_B_PER_CELL * cells,
+                        "kernel": "m2c::stage_kernel<float,16,ROE,single>", "avg_launch_ms": avg,
+                        "alg_bytes_per_launch": ALG_STAGE_SINGLE * cells},
+           "e2e": {"value": cells * ne / te, "unit": UNIT, "h2d_bytes_per_step": int(Vh.nbytes),
+                   "d2h_bytes_per_step": int(Vo.nbytes), "steps": ne}}
+    if cpu:
+        out["cpu_reference"] = cpu_reference_box(6, 1)
+    return out
+
+
+def extra_bubble(n=192, nbubbles=1, steps=500, warmup=3):
+    """Single bubble (192^3, 500 steps), mixed vs FP64: cell-updates/s, HBM
+    fraction of the algorithmic bytes, and the mixed path's error against the
+    FP64 path after the same steps."""
     import numpy as np
     from m2c_b200 import abi, cases, gpu
     res = {}
@@ -207,62 +432,44 @@ def extra_bubble(n=384, nbubbles=16, steps=10, warmup=2):
         sol.upload(V, ID, PHI)
         del V, ID, PHI
         sol.time_steps(warmup)
+        c0 = sol.counters()
         ms, _ = sol.time_steps(steps)
+        c1 = sol.counters()
         Vd, IDd, Pd = sol.download()
         res[prec] = (ms, Vd[1:-1, 1:-1, 1:-1].reshape(-1, 5), IDd[1:-1, 1:-1, 1:-1].ravel(),
-                     Pd[1:-1, 1:-1, 1:-1].ravel(), sol.counters())
+                     Pd[1:-1, 1:-1, 1:-1].ravel(), {k: c1[k] - c0[k] for k in c1})
         sol.close()
         del Vd, IDd, Pd
     cells = n ** 3
     (mm, Vm, Im, Pm, cm), (mf, Vf, If, Pf, cf) = res[abi.PREC_MIXED], res[abi.PREC_FP64]
-    l1 = lambda a, b: float(np.abs(a - b).sum() / np.abs(b).sum())
     vel = float(np.linalg.norm(Vm[:, 1:4] - Vf[:, 1:4], axis=1).sum() / np.linalg.norm(Vf[:, 1:4], axis=1).sum())
-    alg = 387.0 * cells * steps
-    peak, kind = measured_peak()
-    kind = "single bubble" if nbubbles == 1 else "bubble cluster"
-    out = {"workload": f"{kind} {n}^3, {nbubbles} air bubble(s) in water, HLLC + van Albada, exact interface "
-                       f"Riemann, FD3 level set with reinitialisation every 10 steps, RK3, CFL 0.4",
-           "steps": steps, "after_warmup_steps": warmup,
-           "mixed": {"cell_updates_per_s": cells * steps / (mm / 1e3), "ms_per_step": mm / steps,
-                     "hbm_frac": alg / (mm / 1e3) / 1e9 / peak},
-           "fp64": {"cell_updates_per_s": cells * steps / (mf / 1e3), "ms_per_step": mf / steps,
-                    "hbm_frac": alg / (mf / 1e3) / 1e9 / peak},
-           "mixed_speedup": mf / mm,
-           "mixed_vs_fp64_rel_L1": {"rho": l1(Vm[:, 0], Vf[:, 0]), "velocity": vel, "p": l1(Vm[:, 4], Vf[:, 4])},
-           "material_id_mismatch": int((Im != If).sum()), "phi_sign_mismatch": int(((Pm < 0) != (Pf < 0)).sum()),
-           "riemann_calls_per_step_mixed": cm["riemann_calls"] / (steps + warmup),
-           "peak_kind": kind}
-    return out
+    alg = ALG_STEP_MULTI * cells * steps
+    peak, _ = measured_peak()
+    return {"workload": f"single bubble {n}^3, radius 2 mm at the centre, HLLC + van Albada, exact interface "
+                        f"Riemann, FD3 level set with reinitialisation every 10 steps, RK3, CFL 0.4",
+            "steps": steps, "after_warmup_steps": warmup,
+            "mixed": {"cell_updates_per_s": cells * steps / (mm / 1e3), "ms_per_step": mm / steps,
+                      "hbm_frac": alg / (mm / 1e3) / 1e9 / peak},
+            "fp64": {"cell_updates_per_s": cells * steps / (mf / 1e3), "ms_per_step": mf / steps,
+                     "hbm_frac": alg / (mf / 1e3) / 1e9 / peak},
+            "mixed_speedup": mf / mm,
+            "mixed_vs_fp64_rel_L1": {"rho": _l1(Vm[:, 0], Vf[:, 0]), "velocity": vel, "p": _l1(Vm[:, 4], Vf[:, 4])},
+            "material_id_mismatch": int((Im != If).sum()), "phi_sign_mismatch": int(((Pm < 0) != (Pf < 0)).sum()),
+            "riemann_calls_per_step_mixed": cm["riemann_calls"] / steps,
+            "riemann_nontrivial_per_step_mixed": cm["riemann_nontrivial"] / steps}
 
 
 def extra_tubes(ntubes=4096, steps=200, mlp=None):
-    """Batched 1D two-material tubes (one graph-replayed step sequence, autotuned
-    tiles); tubes whose initial interface problem fails or that fail during a
-    screening run are redrawn (counted)."""
-    import numpy as np
+    """Batched 1D two-material tubes (one graph-replayed step sequence,
+    autotuned tiles); tubes whose initial interface problem fails are
+    redrawn (counted)."""
     from m2c_b200 import cases, gpu
     s = cases.tube_scheme()
     lens, mats, VL, VR, redrawn = cases.tubes(ntubes, seed=11, reject=gpu.tube_rejects(s))
-    rng = np.random.default_rng(99)
-    failed_total = 0
-    for _ in range(4):
-        b = gpu.Batch(s, lens, mats, VL, VR)
-        b.time_steps(steps, check_errors=False)
-        bad = np.nonzero(b.tube_errors())[0]
-        b.close()
-        if len(bad) == 0:
-            break
-        failed_total += len(bad)
-        for t in bad:
-            while True:
-                mats[2 * t], mats[2 * t + 1] = cases.stiffened_gas_pair(rng), cases.stiffened_gas_pair(rng)
-                a, c = cases.tube_states(1, rng)
-                VL[t], VR[t] = a[0], c[0]
-                if not gpu.tube_rejects(s)([mats[2 * t], mats[2 * t + 1]], VL[t:t + 1], VR[t:t + 1])[0]:
-                    break
     out = {"workload": f"{ntubes} two-material shock tubes, 100-2000 cells, HLLC + van Albada, exact interface "
                        f"Riemann, RK2, CFL 0.5, {steps} steps", "cells": int(lens.sum()),
-           "redrawn_at_t0": int(redrawn), "redrawn_after_failing_run": int(failed_total)}
+           "redrawn_at_t0": int(redrawn)}
+    peak, _ = measured_peak()
     for label, net in (("cold", None), ("warm_start", mlp)):
         if label == "warm_start" and net is None:
             continue
@@ -271,7 +478,9 @@ def extra_tubes(ntubes=4096, steps=200, mlp=None):
             b.set_mlp(net)
         ms = b.time_steps(steps, check_errors=False)
         c = b.counters()
+        # RK2: 5 FP64 five-vectors (200 B) + 5 phi values (40 B) per cell and step
         out[label] = {"cell_updates_per_s": b.ncell * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                      "hbm_frac": 240.0 * b.ncell * steps / (ms / 1e3) / 1e9 / peak,
                       "tuning": b.tuning(), "failed_tubes": int((b.tube_errors() != 0).sum()),
                       "riemann_calls": c["riemann_calls"], "riemann_iterations": c["riemann_iterations"],
                       "riemann_evaluations": c["riemann_evaluations"]}
@@ -335,150 +544,104 @@ def replica_value(cells_per_rank, world, steps, ms_max):
     return world * cells_per_rank * steps / (ms_max / 1000.0)
 
 
+def reference_arm(args, world):
+    per_step, ccells, cores, sample = cpu_reference_cluster(args.n, args.steps, args.warmup)
+    tot = sum(per_step)
+    v = ccells * len(per_step) / tot
+    print(json.dumps({
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * tot / len(per_step), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubble cluster)",
+        "config": config(args.n, world), "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    n = args.n
-    cells = n ** 3
-
-    if args.bubble:
-        print(json.dumps(extra_bubble(n=args.bubble, steps=args.steps, warmup=args.warmup)))
-        return
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        per_step, ccells, cores = cpu_reference(args.steps, args.warmup)
-        tot = sum(per_step)
-        v = ccells * len(per_step) / tot
-        sample = f"{cores} processes x one {CPU_SAMPLE_N}^3 box (symmetry walls), 1 RK3 step each per benchmark step"
-        print(json.dumps({
-            "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000 * tot / len(per_step), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Fourier modes)",
-            "config": {"workload": f"periodic box {n}^3 RK3 Roe/minmod, sampled on CPU as {CPU_SAMPLE_N}^3 boxes",
-                       "flush": "inputs larger than L2"},
-            "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }))
+        if rank == 0:
+            reference_arm(args, world)
+        return
+
+    if args.box:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(extra_box(n=args.box, steps=args.steps, warmup=args.warmup, cpu=False)))
         return
 
     # CPU baseline first (spawned processes, before any GPU work), rank 0, N=1 only
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.bubble:
         try:
-            per_step, ccells, cores = cpu_reference(12, 1)
+            per_step, ccells, cores, sample = cpu_reference_cluster(args.n, 12, 1)
             cpu = {"value": ccells * len(per_step) / sum(per_step), "unit": UNIT, "cores": cores,
-                   "kind": "reference",
-                   "sample": f"{cores} processes x one {CPU_SAMPLE_N}^3 box, 12 RK3 steps each (after 1 warm-up)"}
+                   "kind": "reference", "sample": sample}
         except Exception as e:  # the oracle build is missing on this host
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
-    import numpy as np
     import torch
     dist = None
     if world > 1:
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     else:
         torch.cuda.set_device(0)
-    from m2c_b200 import abi, cases, gpu
+    from m2c_b200 import gpu
     gpu.set_device(local if world > 1 else 0)
-
-    g, s, mats, V = cases.fourier_box(n, precision=abi.PREC_MIXED, seed=2024 + rank)
-    sol = gpu.Solver(g, s, mats)
-    sol.upload(V)
-    sol.time_steps(args.warmup)
+    n = args.bubble or args.n
+    cells = n ** 3
 
     clocks = Clocks(local if world > 1 else 0)
-    if dist:
-        dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
-    ms, launches = sol.time_steps(args.steps)
-    clk = clocks.stop()
-    torch.cuda.synchronize()
+    r = cluster_run(n, args.steps, args.warmup, with_fp64=(rank == 0 and not args.no_fp64), clocks=clocks,
+                    dist=dist)
+    ms = r["ms"]
     if dist:
         ms = max_over_ranks(ms, dist, "cuda")
         dist.barrier()
     value = replica_value(cells, world, args.steps, ms)
-
-    # roofline of the dominant kernel (the fused stage): algorithmic bytes
-    # 320 B/cell per RK3 step (8 FP64 5-vectors) over the 3 stage launches
-    prof_steps = 3
-    stage_ms, nlaunch, _ = sol.profile_stages(prof_steps)
-    avg_launch_ms = stage_ms / nlaunch
-    alg_bytes_per_launch = 320.0 * cells / 3.0
-    achieved = alg_bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9
     peak, peak_kind = measured_peak()
-    tr = profiled_traffic()
-    traffic = tr["bytes_per_cell_per_launch"] * cells if tr else None
+    achieved = ALG_STAGE_MULTI * cells / (r["stage_avg_ms"] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": STAGE_MULTI_TRAFFIC_B_PER_CELL * cells, "peak_kind": peak_kind,
+                "kernel": "m2c::stage_kernel<float,16,HLLC,two materials>", "avg_launch_ms": r["stage_avg_ms"],
+                "alg_bytes_per_launch": ALG_STAGE_MULTI * cells,
+                "step_hbm_frac": r["hbm_frac_step"],
+                "traffic_source": "ncu dram__bytes_read+write per cell of the two-material stage kernel "
+                                  "(192^3 cluster), scaled to the launch's cells"}
+    if args.bubble:
+        out = {k: v for k, v in r.items() if not k.startswith("_")}
+        out.update({"value": value, "roofline": roofline, "ms_per_step": ms / args.steps})
+        r["_solver"].close()
+        print(json.dumps(out))
+        return
 
-    # FP64 path on the same state, and the L1 difference to it
-    fp64 = None
-    if rank == 0:
-        s64 = abi.scheme(**{f: getattr(s, f) for f, _ in abi.Scheme._fields_})
-        s64.precision = abi.PREC_FP64
-        sol64 = gpu.Solver(g, s64, mats)
-        sol64.upload(V)
-        sol64.time_steps(args.warmup)
-        ms64, _ = sol64.time_steps(args.steps)
-        # L1 after the same number of steps from the same initial state
-        a = gpu.Solver(g, s, mats)
-        a.upload(V)
-        b = gpu.Solver(g, s64, mats)
-        b.upload(V)
-        a.run(args.steps)
-        b.run(args.steps)
-        Va, _, _ = a.download()
-        Vb, _, _ = b.download()
-        ia, ib = Va[1:-1, 1:-1, 1:-1].reshape(-1, 5), Vb[1:-1, 1:-1, 1:-1].reshape(-1, 5)
-        l1 = (np.abs(ia - ib).sum(0) / np.abs(ib).sum(0)).tolist()
-        linf = (np.abs(ia - ib).max(0) / np.abs(ib).max(0)).tolist()
-        fp64 = {"value": cells * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
-                "mixed_speedup": ms64 / ms, "mixed_vs_fp64_rel_L1": dict(zip(["rho", "u", "v", "w", "p"], l1)),
-                "mixed_vs_fp64_rel_Linf": dict(zip(["rho", "u", "v", "w", "p"], linf)),
-                "after_steps": args.steps}
-        del a, b, sol64
-
-    # end to end through the public API: host state in pinned memory,
-    # upload + one step + download per step
     e2e = None
     if not args.no_e2e:
-        Vh = torch.empty(V.shape, dtype=torch.float64, pin_memory=True).numpy()
-        Vh[...] = V
-        Vo = torch.empty(V.shape, dtype=torch.float64, pin_memory=True).numpy()
-        ne = max(3, min(args.steps, 10))
-        sol.upload(Vh)
-        sol.run(1)
-        sol.download(out_V=Vo, with_id=False)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(ne):
-            sol.upload(Vh)
-            sol.run(1)
-            sol.download(out_V=Vo, with_id=False)
-        te = time.perf_counter() - t0
+        ne = 3
+        te, nbytes = cluster_e2e(r["_solver"], r["_case"], ne, dist)
         if dist:
             te = max_over_ranks(te, dist, "cuda")
-        e2e = {"value": world * cells * ne / te, "unit": UNIT, "h2d_bytes_per_step": int(Vh.nbytes),
-               "d2h_bytes_per_step": int(Vo.nbytes), "steps": ne,
-               "note": "m2cg_upload_state + m2cg_run(1) + m2cg_download_state per step, ghosted AoS host state"}
+        e2e = {"value": world * cells * ne / te, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": ne,
+               "note": "m2cg_upload_state(V, ID, phi) + m2cg_run(1) + m2cg_download_state(V, ID, phi) per step, "
+                       "ghosted AoS host state in pinned memory"}
+    r["_solver"].close()
+    del r["_solver"], r["_case"]
 
     extras = None
     if rank == 0 and world == 1 and not args.only_headline:
         extras = {}
         net = load_warmstart()
-        for name, fn in (("bubble_cluster", lambda: extra_bubble()),
-                         ("bubble_cluster_cpu_reference", lambda: cpu_reference_bubble()
-                          if not args.no_cpu_baseline else {"skipped": "--no-cpu-baseline"}),
-                         ("single_bubble_192", lambda: extra_bubble(n=192, nbubbles=1, steps=500, warmup=3)),
+        for name, fn in (("periodic_box_256", lambda: extra_box(cpu=not args.no_cpu_baseline)),
+                         ("single_bubble_192", lambda: extra_bubble()),
                          ("batched_tubes", lambda: extra_tubes(mlp=net)),
                          ("learned_warm_start", lambda: extra_warm_start(net) if net is not None else
                           {"unavailable": "m2c_b200/data/warmstart_mlp.npz not present"})):
@@ -491,19 +654,13 @@ def main():
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 flux / f64 state", "data": "synthetic (seeded Fourier modes)",
-            "config": {"workload": f"periodic box {n}^3, ideal gas, Roe + generalized minmod, RK3, CFL 0.4, mixed",
-                       "cells": cells, "flush": "inputs larger than L2 (no explicit flush)",
-                       "parallelism": f"replicas x{world}"},
-            "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "m2c::stage_kernel<float,16>", "avg_launch_ms": avg_launch_ms,
-                         "alg_bytes_per_launch": alg_bytes_per_launch,
-                         "traffic_source": "ncu dram__bytes_read+write of one stage-2 launch at 160^3, "
-                                           "scaled per cell (profiles/stage_kernel_mixed_160cube.md)"},
-            "clocks": clk,
-            "fp64": fp64,
+            "vs_baseline": None, "dtype": "f32 flux / f64 state", "data": "synthetic (seeded bubble cluster)",
+            "config": config(n, world),
+            "gpu_launches": int(r["launches"]),
+            "roofline": roofline,
+            "clocks": r["clocks"],
+            "interface_work_per_step": r["per_step"],
+            "fp64": r.get("fp64"),
             "cpu_baseline": cpu,
             "e2e": e2e,
             "extras": extras,

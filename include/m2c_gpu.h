@@ -203,6 +203,8 @@ typedef struct {
   long long riemann_evaluations; /* star-state evaluations at trial pressures (bracketing + secant) */
   long long failsafe_cells;      /* cells given the material's failsafe density (no valid neighbour
                                     within 10 layers, MultiPhaseOperator.cpp:1352-1369) */
+  long long riemann_nontrivial;  /* interface Riemann problems not answered by the trivial branch
+                                    (equal normal velocity and pressure, ExactRiemannSolverBase.cpp:129-134) */
 } m2cg_counters;
 m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
 

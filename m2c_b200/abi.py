@@ -145,10 +145,35 @@ def ghosted_shape(g, dof=None):
     return s + (dof,) if dof else s
 
 
+def set_mesh(g, axis, widths):
+    """Give axis 0/1/2 of g a non-uniform mesh: cell widths `widths` (length
+    n) laid end to end from the axis' lower bound; the centres and widths
+    are kept alive on g and passed through m2cg_grid's xc/dx (yc/dy, zc/dz)."""
+    w = np.ascontiguousarray(widths, dtype=np.float64)
+    lo = (g.x0, g.y0, g.z0)[axis]
+    faces = lo + np.concatenate(([0.0], np.cumsum(w)))
+    c = np.ascontiguousarray(0.5 * (faces[:-1] + faces[1:]))
+    keep = getattr(g, "_mesh", {})
+    keep[axis] = (c, w)
+    g._mesh = keep
+    pc, pw = c.ctypes.data_as(C.POINTER(C.c_double)), w.ctypes.data_as(C.POINTER(C.c_double))
+    if axis == 0:
+        g.xc, g.dx, g.xmax = pc, pw, float(faces[-1])
+    elif axis == 1:
+        g.yc, g.dy, g.ymax = pc, pw, float(faces[-1])
+    else:
+        g.zc, g.dz, g.zmax = pc, pw, float(faces[-1])
+
+
 def cell_centres(g):
-    """Cell centres as MeshGenerator::ComputeMesh1DUniform (MeshGenerator.cpp:146-158)."""
+    """Cell centres as MeshGenerator::ComputeMesh1DUniform (MeshGenerator.cpp:146-158),
+    or the ones given with set_mesh."""
     out = []
-    for n, a, b in ((g.nx, g.x0, g.xmax), (g.ny, g.y0, g.ymax), (g.nz, g.z0, g.zmax)):
+    mesh = getattr(g, "_mesh", {})
+    for axis, (n, a, b) in enumerate(((g.nx, g.x0, g.xmax), (g.ny, g.y0, g.ymax), (g.nz, g.z0, g.zmax))):
+        if axis in mesh:
+            out.append(mesh[axis][0].copy())
+            continue
         h = (b - a) / n
         out.append(np.array([a + 0.5 * h + i * h for i in range(n)]))
     return out

@@ -83,15 +83,40 @@ def fourier_box(n, seed=2024, nmodes=16, kmax=8, amp=0.01, mach_rms=0.3, bc=abi.
     return g, s, mats, V
 
 
+def stretched_widths(n, span, kind, seed=0):
+    """Cell widths of a non-uniform mesh of n cells over `span`: "grow"
+    (geometric, ratio 1.05), "shrink" (ratio 1/1.04) or "jitter" (seeded
+    +-25% around uniform)."""
+    if kind == "grow":
+        w = 1.05 ** np.arange(n)
+    elif kind == "shrink":
+        w = (1.0 / 1.04) ** np.arange(n)
+    else:
+        w = 1.0 + np.random.default_rng(seed).uniform(-0.25, 0.25, n)
+    return w * (span / w.sum())
+
+
+def stretch(g, kinds=("grow", "shrink", "jitter"), seed=0):
+    """Non-uniform widths on every axis of g with more than one cell."""
+    for axis, (n, a, b) in enumerate(((g.nx, g.x0, g.xmax), (g.ny, g.y0, g.ymax), (g.nz, g.z0, g.zmax))):
+        if n > 1:
+            abi.set_mesh(g, axis, stretched_widths(n, b - a, kinds[axis], seed + axis))
+    return g
+
+
 def random_box(nx, ny, nz, seed=7, bc=(abi.BC_SYMMETRY,) * 6, flux=abi.FLUX_HLLC, limiter=abi.LIM_VANALBADA,
-               rk=3, cfl=0.5, precision=abi.PREC_FP64, water=False, nasg=False):
+               rk=3, cfl=0.5, precision=abi.PREC_FP64, water=False, nasg=False, mesh=None):
     """Small box with smooth seeded fields plus a density/pressure jump: a
     parity workload that exercises every limiter branch and both wave
     directions. water=True uses the stiffened-gas water of the bubble case
     (gamma 6.12, p_inf 3.43e8 Pa); nasg=True the same states with a
     Noble-Abel stiffened-gas liquid water (gamma 1.19, p_c 7.028e8 Pa,
-    b 6.61e-4 m^3/kg, q -1.177788e6 J/kg)."""
+    b 6.61e-4 m^3/kg, q -1.177788e6 J/kg). mesh: None (uniform) or a
+    function applied to the grid before the fields are laid out (e.g.
+    stretch)."""
     g = abi.grid(nx, ny, nz, bc=bc, inlet=(1.2, 0.3, 0.0, 0.0, 1.1), outlet=(0.9, 0.0, 0.0, 0.0, 0.8))
+    if mesh is not None:
+        mesh(g)
     s = abi.scheme(flux=flux, limiter=limiter, rk_order=rk, cfl=cfl, precision=precision)
     rng = np.random.default_rng(seed)
     xc, yc, zc = abi.cell_centres(g)
@@ -259,7 +284,7 @@ def post_shock_sg(rho0, p0, p1, gamma, p_c):
 
 
 def bubble_case(n, nbubbles=1, seed=5, rk=3, cfl=0.4, precision=abi.PREC_FP64, reinit_frequency=10,
-                radius=2.0e-3, radii=(0.5e-3, 1.5e-3), shape=None):
+                radius=2.0e-3, radii=(0.5e-3, 1.5e-3), shape=None, shock_front=0.005, tile=None, mesh=None):
     """Shock-induced collapse of air bubble(s) in water in a 2 cm cube:
     water is stiffened gas (gamma 6.12, p_inf 3.43e8 Pa, rho 1000, p 1e5),
     air is gamma 1.4 (rho 1.2, p 1e5); a planar shock from the post-shock
@@ -270,14 +295,44 @@ def bubble_case(n, nbubbles=1, seed=5, rk=3, cfl=0.4, precision=abi.PREC_FP64, r
     radius 2 mm at the centre; otherwise seeded non-overlapping bubbles with
     radii uniform in `radii`, at least two cells apart, fully inside.
     The level set is the signed distance to the nearest bubble surface
-    (material 1, air, where phi < 0)."""
+    (material 1, air, where phi < 0).
+
+    shock_front: x of the shock front in metres, or "contact": the moment
+    the front, coming from x = 5 mm through still water, reaches the
+    nearest bubble. Ahead of the front the water is uniform and at rest, so
+    that moment's state is this initial state with the front two cells
+    upstream of the nearest bubble surface.
+
+    tile: None, or (shape, origin) of a sub-box of the grid in cells, e.g.
+    ((48, 48, 48), (i0, j0, k0)): the same state restricted to those cells
+    (same cell size), with the domain's boundary conditions on faces that
+    lie on the domain boundary and symmetry walls on the others. Used to
+    run bounded samples of a large case on the CPU reference.
+
+    mesh: None (uniform) or a function applied to the grid before the
+    fields are laid out (e.g. stretch)."""
     L = 0.02
     nx, ny, nz = shape if shape else (n, n, n)
     rho1, u1 = post_shock_sg(1000.0, 1.0e5, 1.0e9, **WATER)
     post = (rho1, u1, 0.0, 0.0, 1.0e9)
-    g = abi.grid(nx, ny, nz, x=(0.0, L), y=(0.0, L), z=(0.0, L),
-                 bc=(abi.BC_INLET, abi.BC_OUTLET) + (abi.BC_SYMMETRY,) * 4,
-                 inlet=post, outlet=(1000.0, 0.0, 0.0, 0.0, 1.0e5))
+    bc = [abi.BC_INLET, abi.BC_OUTLET] + [abi.BC_SYMMETRY] * 4
+    lo, hi = (0.0, 0.0, 0.0), (L, L, L)
+    cells = (nx, ny, nz)
+    if tile is not None:
+        ext, org = tile
+        h3 = (L / nx, L / ny, L / nz)
+        lo = tuple(org[a] * h3[a] for a in range(3))
+        hi = tuple((org[a] + ext[a]) * h3[a] for a in range(3))
+        for a, full in enumerate((nx, ny, nz)):
+            if org[a] > 0:
+                bc[2 * a] = abi.BC_SYMMETRY
+            if org[a] + ext[a] < full:
+                bc[2 * a + 1] = abi.BC_SYMMETRY
+        cells = tuple(ext)
+    g = abi.grid(*cells, x=(lo[0], hi[0]), y=(lo[1], hi[1]), z=(lo[2], hi[2]), bc=tuple(bc), inlet=post,
+                 outlet=(1000.0, 0.0, 0.0, 0.0, 1.0e5))
+    if mesh is not None:
+        mesh(g)
     s = abi.scheme(flux=abi.FLUX_HLLC, limiter=abi.LIM_VANALBADA, rk_order=rk, cfl=cfl, precision=precision)
     mats = [abi.material(**WATER), abi.material(**AIR)]
     ls = abi.levelset(material_id=1, reinit_frequency=reinit_frequency)
@@ -307,7 +362,9 @@ def bubble_case(n, nbubbles=1, seed=5, rk=3, cfl=0.4, precision=abi.PREC_FP64, r
     ID = np.zeros(abi.ghosted_shape(g))
     PHI = np.zeros(abi.ghosted_shape(g))
     inner = np.s_[1:-1, 1:-1, 1:-1]
-    shocked = X < 0.005
+    if shock_front == "contact":
+        shock_front = min(c[0] - r for c, r in zip(centres, rads)) - 2 * h
+    shocked = X < shock_front
     V[inner + (0,)] = np.where(shocked, rho1, 1000.0)
     V[inner + (1,)] = np.where(shocked, u1, 0.0)
     V[inner + (4,)] = np.where(shocked, 1.0e9, 1.0e5)

@@ -66,7 +66,8 @@ struct Multiphase {
   int* slot = nullptr;     // per cell: slot of its low faces (valid where flagged)
   int* faces = nullptr;    // [cap_faces][3]: cell offset, slot, direction
   int* counts = nullptr;   // [0] slots, [1] faces, [2] overflow, [3] riemann errors, [4] iterations (low), [5] calls,
-                           // [6] evaluations, [8 + stage] work counters, [16...] wave-pattern group sizes
+                           // [6] evaluations, [7] non-trivial calls, [8 + stage] work counters,
+                           // [16...] wave-pattern group sizes
   int* order = nullptr;    // [cap_faces] faces grouped by wave pattern (the solve order of a stage)
   uint8_t* pattern = nullptr;  // [cap_faces] wave pattern of each face at this stage
   long long cap_slots = 0, cap_faces = 0;
@@ -88,7 +89,7 @@ struct Multiphase {
   int stage = 0;
   // host-side counters
   long long riemann_calls = 0, riemann_iterations = 0, riemann_errors = 0, unresolved = 0, reinit_calls = 0;
-  long long riemann_evaluations = 0, failsafe_cells = 0;
+  long long riemann_evaluations = 0, failsafe_cells = 0, riemann_nontrivial = 0;
   uint8_t* mask = nullptr;       // [interior cells] unresolved-list membership, zero between updates
   double failsafe[MAXMAT] = {};  // MaterialModelData::failsafe_density
   double* reinit_buf = nullptr;  // reinitialisation work arrays
@@ -324,6 +325,7 @@ __global__ void __launch_bounds__(128, M2C_IFACE_MINB) k_iface_riemann(IfaceRiem
     atomicAdd(&a.counts[4], rs.iterations);
     atomicAdd(&a.counts[6], rs.evaluations);
     atomicAdd(&a.counts[5], 1);
+    if (rs.evaluations > 0) atomicAdd(&a.counts[7], 1);  // not answered by the trivial branch
   }
 }
 
@@ -971,7 +973,7 @@ m2cg_status multiphase_update_states(Multiphase* mp, cudaStream_t s, double* con
   k_state_update<<<1, 32, 0, s>>>(ua);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
   // step counters (one small read-back per step)
-  int hc[7], hn[4];
+  int hc[8], hn[4];
   cudaMemcpyAsync(hc, mp->counts, sizeof hc, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hn, mp->nchanged, sizeof hn, cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
@@ -980,6 +982,7 @@ m2cg_status multiphase_update_states(Multiphase* mp, cudaStream_t s, double* con
     mp->riemann_iterations += hc[4];
     mp->riemann_errors += hc[3];
     mp->riemann_evaluations += hc[6];
+    mp->riemann_nontrivial += hc[7];
     if (hc[2]) return M2CG_ERR_ITER_CAP;  // interface capacity exceeded
   }
   mp->unresolved += hn[1];
@@ -1001,4 +1004,5 @@ void multiphase_counters(const Multiphase* mp, m2cg_counters* out) {
   out->unresolved_cells = mp->unresolved;
   out->riemann_evaluations = mp->riemann_evaluations;
   out->failsafe_cells = mp->failsafe_cells;
+  out->riemann_nontrivial = mp->riemann_nontrivial;
 }

@@ -30,7 +30,7 @@ class Counters(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in (
         "steps", "cells_updated", "riemann_calls", "riemann_iterations", "riemann_errors",
         "clipped_cells", "reinit_calls", "kernel_launches", "unresolved_cells", "riemann_evaluations",
-        "failsafe_cells")]
+        "failsafe_cells", "riemann_nontrivial")]
 
 
 class BatchTuning(C.Structure):

@@ -279,3 +279,60 @@ def test_mixed_precision_bubble_close_to_fp64(gpu):
         assert l1 <= 1e-5, (c, l1)
     dv = np.linalg.norm(la[:, 1:4] - lb[:, 1:4], axis=1).sum() / np.linalg.norm(la[:, 1:4], axis=1).sum()
     assert dv <= 1e-5, dv
+
+
+@pytest.mark.parametrize("mp_flux,mp_recon", [(abi.MPFLUX_EXACT, 0), (abi.MPFLUX_LLF, 0),
+                                              (abi.MPFLUX_NUMERICAL, 1), (abi.MPFLUX_EXACT, 1)])
+def test_interface_flux_options_match_reference(gpu, ref, mp_flux, mp_recon):
+    """MultiPhaseData::flux EXACT (Godunov flux of the Riemann state at
+    xi = 0), LOCAL_LAX_FRIEDRICHS (LLF across the interface, no Riemann
+    problem in the flux) and NUMERICAL, with CONSTANT or LINEAR
+    reconstruction of the interface states (SpaceOperator.cpp:2486-2542),
+    through whole steps of the obliquely moving bubble."""
+    g, s, mats, ls, V, ID, PHI = moving_bubble(abi.RIEMANN_NORMAL_MESH, 3)
+    s.mp_flux = mp_flux
+    s.mp_recon = mp_recon
+    sol, rc = make(gpu, ref, g, s, mats, ls, V, ID, PHI)
+    for _ in range(4):
+        sol.run(1)
+        rc.run(1)
+    Vg, IDg, Pg = sol.download()
+    Vr, IDr, Pr = rc.get_state()
+    assert np.array_equal(inner(IDg), inner(IDr))
+    assert rel_err(inner(Vg), inner(Vr)) <= TOL
+    assert rel_err(inner(Pg), inner(Pr), axis_last=False) <= TOL
+
+
+@pytest.mark.parametrize("lsbc", [abi.LSBC_LINEAR_EXTRAPOLATION, abi.LSBC_NON_NEGATIVE])
+def test_level_set_boundary_rules_match_reference(gpu, ref, lsbc):
+    """LevelSetSchemeData bc LINEAR_EXTRAPOLATION and NON_NEGATIVE
+    (LevelSetOperator.cpp:934-1034) on every face: the obliquely moving
+    bubble's level set is advected through the faces, so the FD3 stencils
+    next to them read the ghost layers."""
+    g, s, mats, ls, V, ID, PHI = moving_bubble(abi.RIEMANN_NORMAL_MESH, 2)
+    ls.bc = (type(ls.bc))(*([lsbc] * 6))
+    sol, rc = make(gpu, ref, g, s, mats, ls, V, ID, PHI)
+    for _ in range(4):
+        sol.run(1)
+        rc.run(1)
+    Vg, IDg, Pg = sol.download()
+    Vr, IDr, Pr = rc.get_state()
+    assert np.array_equal(inner(IDg), inner(IDr))
+    assert rel_err(inner(Vg), inner(Vr)) <= TOL
+    assert rel_err(inner(Pg), inner(Pr), axis_last=False) <= TOL
+
+
+def test_bubble_on_stretched_mesh_matches_reference(gpu, ref):
+    """Two materials on a non-uniform mesh: limiter coefficients, FD3
+    level-set coefficients (GradientCalculatorFD3.cpp:300-470) and the
+    reinitialisation all see per-cell widths."""
+    g, s, mats, ls, V, ID, PHI = cases.bubble_case(20, reinit_frequency=2, mesh=cases.stretch)
+    sol, rc = make(gpu, ref, g, s, mats, ls, V, ID, PHI)
+    for _ in range(4):
+        sol.run(1)
+        rc.run(1)
+    Vg, IDg, Pg = sol.download()
+    Vr, IDr, Pr = rc.get_state()
+    assert np.array_equal(inner(IDg), inner(IDr))
+    assert rel_err(inner(Vg), inner(Vr)) <= TOL
+    assert rel_err(inner(Pg), inner(Pr), axis_last=False) <= TOL
