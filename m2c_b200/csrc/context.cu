@@ -5,6 +5,8 @@
 // and the RK step driver.
 //
 // Compiled with -fmad=false (the small kernels here feed the FP64 path).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -132,6 +134,15 @@ struct m2cg_ctx {
   // and for the mixed path an FP32 copy of V (Vf, double-buffered with V)
   void* P[2][5] = {};
   float* Vf[2][5] = {};
+  // Each five-component buffer is one allocation (component c at c * cstride
+  // elements), so that one 4D tensor map covers all five arrays: the stage
+  // kernel stages a plane of all components with one tensor copy.
+  long long cstride = 0;
+  void* blk[4][2] = {};      // allocations of V, U, P, Vf (per buffer b)
+  // tensor maps of the stage inputs: [0..1] the step state in the compute
+  // type (Vf[b] mixed, V[b] FP64), [2..3] P[b]
+  CUtensorMap tmap[4];
+  bool tma_ok = false;       // maps built (else the kernel copies values one by one)
   int cur = 0;
   uint8_t* id = nullptr;
   // mesh
@@ -158,6 +169,48 @@ struct m2cg_ctx {
   bool profile = false;
   std::vector<cudaEvent_t> ev;  // pairs (before, after) per stage launch
 };
+
+// Tensor maps (cuTensorMapEncodeTiled, reached through the runtime's
+// driver entry point, so the library links only the CUDA runtime) of the
+// stage kernel's plane input: 4D (x, y, z, component) over one
+// five-component buffer, box = one plane of a tile with its halo,
+// STAGE_TMA_BX x (TY + 4) x 1 x 5 elements. Out-of-range x/y cells read as
+// zero; the kernel rebuilds them by the boundary rule.
+static m2cg_status encode_stage_map(m2cg_ctx* c, CUtensorMap* m, const void* base, bool f32, int ty) {
+  static PFN_cuTensorMapEncodeTiled encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return fail(M2CG_ERR_CUDA, "cuTensorMapEncodeTiled not available from the driver");
+    encode = (PFN_cuTensorMapEncodeTiled)fn;
+  }
+  const size_t es = f32 ? 4 : 8;
+  cuuint64_t dims[4] = {(cuuint64_t)c->nx, (cuuint64_t)c->ny, (cuuint64_t)c->nz, 5};
+  cuuint64_t strides[3] = {(cuuint64_t)(c->px * es), (cuuint64_t)(c->plane * es), (cuuint64_t)(c->cstride * es)};
+  cuuint32_t box[4] = {(cuuint32_t)STAGE_TMA_BX, (cuuint32_t)(ty + 4), 1, 5};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = encode(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+                      const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(M2CG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return M2CG_OK;
+}
+
+// A map that cannot be encoded leaves tma_ok false: the stage kernel then
+// copies plane values one by one.
+static m2cg_status make_stage_tensor_maps(m2cg_ctx* c) {
+  const bool mixed = c->scheme.precision == M2CG_PREC_MIXED;
+  const int ty = mixed ? StageTY<float, false>::value : StageTY<double, false>::value;
+  for (int b = 0; b < 2; b++) {
+    m2cg_status st = encode_stage_map(c, &c->tmap[b], mixed ? c->blk[3][b] : c->blk[0][b], mixed, ty);
+    if (!st) st = encode_stage_map(c, &c->tmap[2 + b], c->blk[2][b], mixed, ty);
+    if (st) return st;  // the stage kernel then copies plane values one by one
+  }
+  c->tma_ok = true;
+  return M2CG_OK;
+}
 
 static double* dalloc(size_t n, m2cg_status* st) {
   void* p = nullptr;
@@ -281,17 +334,29 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   c->nalloc = c->plane * grid->nz;
   st = M2CG_OK;
   const bool mixed = scheme->precision == M2CG_PREC_MIXED;
-  for (int b = 0; b < 2; b++)
+  c->cstride = (c->nalloc + 63) / 64 * 64;
+  const long long cs = c->cstride;
+  for (int b = 0; b < 2; b++) {
+    double* v = dalloc(5 * cs, &st);
+    double* u = dalloc(5 * cs, &st);
+    void* pb = mixed ? (void*)dalloc(5 * cs / 2, &st) : (void*)dalloc(5 * cs, &st);
+    float* vf = mixed ? (float*)dalloc(5 * cs / 2, &st) : nullptr;
+    c->blk[0][b] = v;
+    c->blk[1][b] = u;
+    c->blk[2][b] = pb;
+    c->blk[3][b] = vf;
     for (int p = 0; p < 5; p++) {
-      c->V[b][p] = dalloc(c->nalloc, &st);
-      c->U[b][p] = dalloc(c->nalloc, &st);
+      c->V[b][p] = v ? v + p * cs : nullptr;
+      c->U[b][p] = u ? u + p * cs : nullptr;
       if (mixed) {
-        c->P[b][p] = dalloc((c->nalloc + 1) / 2, &st);
-        c->Vf[b][p] = (float*)dalloc((c->nalloc + 1) / 2, &st);
+        c->P[b][p] = pb ? (void*)((float*)pb + p * cs) : nullptr;
+        c->Vf[b][p] = vf ? vf + p * cs : nullptr;
       } else {
-        c->P[b][p] = dalloc(c->nalloc, &st);
+        c->P[b][p] = pb ? (void*)((double*)pb + p * cs) : nullptr;
       }
     }
+  }
+  if (!st) make_stage_tensor_maps(c);
   if (cudaMalloc((void**)&c->id, c->nalloc) != cudaSuccess) st = fail(M2CG_ERR_NOMEM, "cudaMalloc id failed");
   if (!st) cudaMemsetAsync(c->id, 0, c->nalloc, c->stream);
   axis_mesh(grid->nx, grid->x0, grid->xmax, grid->xc, grid->dx, c->hxc, c->hdx);
@@ -383,13 +448,8 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
 extern "C" m2cg_status m2cg_destroy(m2cg_ctx* c) {
   if (!c) return M2CG_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (int b = 0; b < 2; b++)
-    for (int p = 0; p < 5; p++) {
-      cudaFree(c->V[b][p]);
-      cudaFree(c->U[b][p]);
-      cudaFree(c->P[b][p]);
-      cudaFree(c->Vf[b][p]);
-    }
+  for (int q = 0; q < 4; q++)
+    for (int b = 0; b < 2; b++) cudaFree(c->blk[q][b]);
   cudaFree(c->id);
   cudaFree(c->dx); cudaFree(c->dy); cudaFree(c->dz);
   for (int a = 0; a < 3; a++) { cudaFree(c->lA[a]); cudaFree(c->lB[a]); cudaFree(c->lK[a]); cudaFree(c->lC[a]); }
@@ -729,6 +789,7 @@ static m2cg_status launch_stage(m2cg_ctx* c, StageArgs& a) {
 
 static void base_args(m2cg_ctx* c, StageArgs& a) {
   memset(&a, 0, sizeof a);
+  a.use_tma = c->tma_ok && c->g.bc[0] != BC_PERIODIC && c->g.bc[2] != BC_PERIODIC;
   a.g = c->g;
   a.s = c->sk;
   a.id = c->id;
@@ -765,6 +826,7 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
       a.Po[p] = s == r ? nullptr : c->P[(s - 1) & 1][p];
       a.Vfo[p] = (s == r && mixed) ? c->Vf[1 - c->cur][p] : nullptr;
     }
+    a.tin = c->tmap[s == 1 ? c->cur : 2 + ((s - 2) & 1)];
     a.us_clipped = s > 1 ? c->clipflags + (s - 2) : nullptr;
     a.clipped_out = c->clipflags + (s - 1);
     a.dtmin_bits = (a.final_stage && want_dtmin && !c->mp) ? c->dtmin : nullptr;
@@ -859,6 +921,7 @@ extern "C" m2cg_status m2cg_compute_residual(m2cg_ctx* c, double* R_host) {
     a.Ro[p] = c->U[1][p];
     a.Pin[p] = c->scheme.precision == M2CG_PREC_MIXED ? (const void*)c->Vf[c->cur][p] : (const void*)Vn[p];
   }
+  a.tin = c->tmap[c->cur];
   if (c->mp) {
     c->rs_valid = false;  // the interface slots are reassigned
     m2cg_status st = multiphase_begin_step(c->mp, c->stream, Vn, c->id);

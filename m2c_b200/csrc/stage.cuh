@@ -21,9 +21,17 @@
 // 2-cell x/y halo) in shared memory. The stage's input is a primitive state
 // in the compute type (V^n for stage 1; for later stages clip(C2P(U_s)),
 // written by the previous stage's update), so planes are copied into the
-// ring with cp.async as they are, and only ghost cells are rewritten by the
-// boundary rule. Iteration m of the plane pipeline:
-//   (1) ghost rules on plane m+2 (landed), cp.async of plane m+3 into the
+// ring as they lie in HBM and only ghost cells are rewritten by the boundary
+// rule. A plane of all five components lands with ONE tensor copy
+// (cp.async.bulk.tensor over a 4D map x, y, z, component of the
+// five-component buffer; box 40 x (TY+4) x 1 x 5 starting at x = i0-4, a
+// 16-byte boundary; completion counted on an mbarrier per ring slot),
+// issued by one thread; cells outside the domain in x/y arrive as zeros and
+// take their value from their image cell by the boundary rule. Where x or y
+// is periodic the halo wraps around the domain, which a tiled copy cannot
+// express; those launches copy each value with cp.async from its wrapped
+// position instead. Iteration m of the plane pipeline:
+//   (1) ghost rules on plane m+2 (landed), copy of plane m+3 into the
 //       slot plane m-1 has freed,
 //   (2) slopes + revert mask of every cell of plane m+1 (x -1..32, y -1..TY),
 //   (3) every face flux once: x/y faces of plane m and the z faces m+1/2,
@@ -34,12 +42,21 @@
 // cell value, every face needing clipping reverted to the cell value, and a
 // remaining CheckState failure reported as an error (never a trap).
 #pragma once
+#include <cuda.h>  // CUtensorMap
+
 #include "physics.cuh"
 
 namespace m2c {
 
 constexpr int MAXMAT = 4;
 constexpr int TX = 32;
+// Width of the plane box in x: cells i0-4 .. i0+35 (the tile's loaded
+// columns i0-2 .. i0+33 plus two unused columns each side, so that the box
+// starts on a 16-byte boundary for 4- and 8-byte elements).
+constexpr int STAGE_TMA_BX = 40;
+// Upper bound of mbarrier polls for one plane copy (a copy from valid
+// addresses always lands; the bound turns a fault into an error status).
+constexpr int STAGE_TMA_POLLS = 1 << 22;
 
 enum { BC_NONE = 0, BC_INLET = 1, BC_OUTLET = 2, BC_SLIPWALL = 3, BC_STICKWALL = 4, BC_SYMMETRY = 5,
        BC_PERIODIC = 100 };
@@ -112,6 +129,8 @@ struct StageArgs {
   int nitems;            // CTAs that share the (tile, plane) units evenly
   double* Ro[5];         // if set: write the residual R only (no RK update)
   IfaceView iface;
+  int use_tma;           // planes by tensor copy (x and y not periodic, maps built)
+  CUtensorMap tin;       // 4D map of the stage input (Pin as one five-component buffer)
 };
 
 __device__ __forceinline__ void report(DevError* e, int code, int cell, int where) {
@@ -124,11 +143,12 @@ __device__ __forceinline__ void report(DevError* e, int code, int cell, int wher
 template <typename T, int TY>
 struct StageSmem {
   static constexpr int RX = TX + 4, RY = TY + 4;   // loaded region: x -2..TX+1, y -2..TY+1
+  static constexpr int BX = STAGE_TMA_BX;          // stored columns: x -4..TX+3 (loaded column lx at lx + 2)
   static constexpr int MX = TX + 2, MY = TY + 2;   // mask region: x -1..TX, y -1..TY
   static constexpr int NFX = (TX + 1) * TY;        // x faces of a plane
   static constexpr int NFY = TX * (TY + 1);        // y faces of a plane
   static constexpr int NFZ = TX * TY;              // z faces between two planes
-  T v[4][5][RY][RX];          // ring of primitive planes, slot = plane & 3
+  alignas(128) T v[4][5][RY][BX];  // ring of primitive planes, slot = plane & 3 (tensor-copy boxes)
   T sig[2][3][5][MY][MX];     // limited slopes (x, y, z) of the mask region, two planes
   T fx[5][NFX];
   T fy[5][NFY];
@@ -136,8 +156,8 @@ struct StageSmem {
   uint8_t mask[2][MY][MX];
   uint8_t real[4][RY][RX];    // 1 = real (interior or periodic image), 0 = ghost / unused
   uint8_t ids[4][RY][RX];
-  uint8_t rinfo[RY * RX];     // per loaded cell of the plane in flight: bit0 real, bits1-2 ghost axis+1, bit3 ghost side
   double red[TY * TX / 32];
+  unsigned long long bar[4];  // one mbarrier per ring slot (tensor copies)
 };
 
 // Shared memory of one CTA. At a material interface face the left and the
@@ -148,6 +168,9 @@ template <typename T, int TY, bool MULTI>
 struct StageSmemAll {
   StageSmem<T, TY> b;
 };
+
+// Value c of loaded cell (lx, ly) in ring slot sl.
+#define M2C_VV(sl, c, ly, lx) sm.v[sl][c][ly][(lx) + 2]
 
 // Resolve a possibly-outside index along one axis (at most two cells out).
 // Returns the interior index to read; sets ghost side (-1 none, 0 low, 1 high)
@@ -284,7 +307,7 @@ template <> struct StageOcc<float> { static constexpr int value = M2C_STAGE_OCC_
 // separate instantiation so the primitive-variable kernels carry none of it).
 template <typename T, int TY, int FLUX, bool MULTI, bool CONS>
 __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(const __grid_constant__ StageArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   typedef StageSmem<T, TY> S;
   typedef StageSmemAll<T, TY, MULTI> SA;
   SA& all = *reinterpret_cast<SA*>(smem_raw);
@@ -306,75 +329,166 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
 
   int i0 = 0, j0 = 0;  // tile origin of the current work item
   uint8_t idreg[LPT];
+  // Plane copies: tensor copies unless x or y is periodic (CTA-uniform).
+  const bool use_tma = a.use_tma != 0;
+  constexpr unsigned TMA_BYTES = 5u * S::RY * S::BX * sizeof(T);
+  unsigned tma_phase = 0;  // bit s: parity of the next completion of slot s's mbarrier
+  if (use_tma) {
+    if (tid == 0) {
+      for (int q = 0; q < 4; q++) {
+        const unsigned bar = (unsigned)__cvta_generic_to_shared(&sm.bar[q]);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&a.tin)) : "memory");
+    }
+    __syncthreads();
+  }
 
   auto slot4 = [](int p) { return p & 3; };
   auto plane_is_ghost = [&](int p) { return !zper && (p < 0 || p >= g.nz); };
 
-  // (1a) start copying plane p into its ring slot: one cp.async per value,
-  // ghost cells copied from their image cell; cell kind kept in rinfo.
-  auto issue_plane = [&](int p) {
-    int sz;
-    bool farz = false;
-    const int kk = resolve_axis(p, g.nz, zper, sz, farz);
-    const int s = slot4(p);
+  // Per tile, for each loaded cell of this thread: its in-plane offset (the
+  // image cell for ghosts, the wrapped cell for periodic halos) and its kind
+  // in x and y: bits 0-1 x ghost side + 1 (0 none, 1 low, 2 high), bits 2-3
+  // the same for y, bit 4 far (outside by more than one cell, not periodic).
+  int xyoff[LPT];
+  uint8_t xyinfo[LPT];
+  auto tile_setup = [&]() {
 #pragma unroll
     for (int r = 0; r < LPT; r++) {
       const int q = tid + r * NT;
       if (q >= NLOAD) break;
       const int ly = q / S::RX, lx = q - ly * S::RX;
       int sx, sy;
-      bool far = farz;
+      bool far = false;
       const int ii = resolve_axis(i0 + lx - 2, g.nx, xper, sx, far);
       const int jj = resolve_axis(j0 + ly - 2, g.ny, yper, sy, far);
-      const int nghost = (sx >= 0) + (sy >= 0) + (sz >= 0);
-      const long long off = (long long)kk * g.plane + (long long)jj * g.px + ii;
-#pragma unroll
-      for (int c = 0; c < 5; c++) cp_async_t(&sm.v[s][c][ly][lx], static_cast<const T*>(a.Pin[c]) + off);
-      uint8_t info = 0;
-      if (nghost == 0 && !far) {
-        info = 1;
-      } else if (nghost == 1 && !far) {
-        const int axis = sx >= 0 ? 0 : (sy >= 0 ? 1 : 2);
-        const int side = sx >= 0 ? sx : (sy >= 0 ? sy : sz);
-        info = uint8_t(((axis + 1) << 1) | (side << 3));
-      }
-      sm.rinfo[q] = info;
-      if (MULTI) idreg[r] = a.id[off];
+      xyoff[r] = jj * (int)g.px + ii;
+      xyinfo[r] = uint8_t((sx + 1) | ((sy + 1) << 2) | (far ? 16 : 0));
     }
-    cp_async_commit();
   };
 
-  // (1b) the landed plane: boundary rule on ghost cells
-  // (SpaceOperator::ApplyBoundaryConditions), cell kinds and ids.
+  // (1a) start copying plane p into its ring slot. Tensor path: one thread
+  // issues the plane's copy (all components) against the slot's mbarrier,
+  // after a proxy fence orders the slot's earlier generic accesses (every
+  // thread passed a barrier since) before the asynchronous write. Element
+  // path (periodic x or y): one cp.async per value from the image or
+  // wrapped position.
+  auto issue_plane = [&](int p) {
+    int sz;
+    bool farz = false;
+    const int kk = resolve_axis(p, g.nz, zper, sz, farz);
+    const int s = slot4(p);
+    if (use_tma) {
+      if (tid == 0) {
+        const unsigned bar = (unsigned)__cvta_generic_to_shared(&sm.bar[s]);
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(&sm.v[s][0][0][0]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TMA_BYTES) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+            "[%6];" ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(&a.tin)), "r"(i0 - 4), "r"(j0 - 2), "r"(kk),
+            "r"(0), "r"(bar)
+            : "memory");
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < LPT; r++) {
+        const int q = tid + r * NT;
+        if (q >= NLOAD) break;
+        const int ly = q / S::RX, lx = q - ly * S::RX;
+        const long long off = (long long)kk * g.plane + xyoff[r];
+#pragma unroll
+        for (int c = 0; c < 5; c++) cp_async_t(&M2C_VV(s, c, ly, lx), static_cast<const T*>(a.Pin[c]) + off);
+      }
+      cp_async_commit();
+    }
+    if (MULTI) {
+#pragma unroll
+      for (int r = 0; r < LPT; r++) {
+        const int q = tid + r * NT;
+        if (q >= NLOAD) break;
+        idreg[r] = a.id[(long long)kk * g.plane + xyoff[r]];
+      }
+    }
+  };
+
+  // (1b) wait for plane p, then a CTA barrier (which also keeps the plane's
+  // commit from overwriting ids and kinds the previous iteration's update
+  // still reads). Tensor path: every thread polls the slot's mbarrier
+  // (bounded; a copy that never lands is reported and the CTA stops).
+  auto wait_plane = [&](int p) -> bool {
+    if (!use_tma) {
+      cp_async_wait_all();
+      __syncthreads();
+      return true;
+    }
+    const int s = slot4(p);
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&sm.bar[s]);
+    const unsigned parity = (tma_phase >> s) & 1u;
+    unsigned ok = 0;
+    for (int it = 0; it < STAGE_TMA_POLLS && !ok; it++) {
+      asm volatile(
+          "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}"
+          : "=r"(ok)
+          : "r"(bar), "r"(parity)
+          : "memory");
+    }
+    tma_phase ^= 1u << s;
+    if (!ok) report(a.err, ERR_ITER_CAP, -1, where + 5);
+    __syncthreads();
+    return ok != 0;
+  };
+
+  // (1c) the landed plane: boundary rule on ghost cells
+  // (SpaceOperator::ApplyBoundaryConditions), cell kinds and ids. A ghost
+  // cell takes its image cell's value (the element path copied it there; the
+  // tensor path reads it from the neighbour in x or y, or finds it in place
+  // for a ghost plane in z), then the rule of its face.
   auto commit_plane = [&](int p) {
     const int s = slot4(p);
+    int sz;
+    bool farz = false;
+    resolve_axis(p, g.nz, zper, sz, farz);
 #pragma unroll
     for (int r = 0; r < LPT; r++) {
       const int q = tid + r * NT;
       if (q >= NLOAD) break;
       const int ly = q / S::RX, lx = q - ly * S::RX;
-      const uint8_t info = sm.rinfo[q];
-      const int gaxis = (info >> 1) & 3;
-      if (gaxis) {
-        const int axis = gaxis - 1, side = (info >> 3) & 1;
+      const int gx = xyinfo[r] & 3, gy = (xyinfo[r] >> 2) & 3;
+      const bool far = (xyinfo[r] & 16) || farz;
+      const int nghost = (gx != 0) + (gy != 0) + (sz >= 0);
+      const bool real = nghost == 0 && !far;
+      if (nghost == 1 && !far) {
+        const int axis = gx ? 0 : (gy ? 1 : 2);
+        const int side = gx ? gx - 1 : (gy ? gy - 1 : sz);
         const int bc = g.bc[2 * axis + side];
+        if (use_tma && axis < 2 && bc != BC_INLET && bc != BC_OUTLET) {
+          const int ix = axis == 0 ? lx + (side ? -1 : 1) : lx, iy = axis == 1 ? ly + (side ? -1 : 1) : ly;
+#pragma unroll
+          for (int c = 0; c < 5; c++) M2C_VV(s, c, ly, lx) = M2C_VV(s, c, iy, ix);
+        }
         if (bc == BC_INLET) {
 #pragma unroll
-          for (int c = 0; c < 5; c++) sm.v[s][c][ly][lx] = T(g.inlet[c]);
+          for (int c = 0; c < 5; c++) M2C_VV(s, c, ly, lx) = T(g.inlet[c]);
         } else if (bc == BC_OUTLET) {
 #pragma unroll
-          for (int c = 0; c < 5; c++) sm.v[s][c][ly][lx] = T(g.outlet[c]);
+          for (int c = 0; c < 5; c++) M2C_VV(s, c, ly, lx) = T(g.outlet[c]);
         } else if (bc == BC_STICKWALL) {
-          sm.v[s][1][ly][lx] = -sm.v[s][1][ly][lx];
-          sm.v[s][2][ly][lx] = -sm.v[s][2][ly][lx];
-          sm.v[s][3][ly][lx] = -sm.v[s][3][ly][lx];
+          M2C_VV(s, 1, ly, lx) = -M2C_VV(s, 1, ly, lx);
+          M2C_VV(s, 2, ly, lx) = -M2C_VV(s, 2, ly, lx);
+          M2C_VV(s, 3, ly, lx) = -M2C_VV(s, 3, ly, lx);
         } else {  // SYMMETRY / SLIPWALL: normal velocity flipped
-          sm.v[s][1 + axis][ly][lx] = -sm.v[s][1 + axis][ly][lx];
+          M2C_VV(s, 1 + axis, ly, lx) = -M2C_VV(s, 1 + axis, ly, lx);
         }
       }
-      sm.real[s][ly][lx] = info & 1;
+      sm.real[s][ly][lx] = real ? 1 : 0;
       sm.ids[s][ly][lx] = MULTI ? idreg[r] : 0;
     }
+    // order this thread's generic writes to the slot before the tensor copy
+    // that refills it four planes later
+    if (use_tma) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   };
 
   // Limited slopes in direction d of the real cell at loaded position
@@ -406,8 +520,8 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     }
 #pragma unroll
     for (int c = 0; c < 5; c++) {
-      const T vc = sm.v[s0][c][ly][lx];
-      T sl = limited_slope_c(limiter, A, B, K, alpha, vc - sm.v[sm1][c][lym][lxm], sm.v[sp1][c][lyp][lxp] - vc);
+      const T vc = M2C_VV(s0, c, ly, lx);
+      T sl = limited_slope_c(limiter, A, B, K, alpha, vc - M2C_VV(sm1, c, lym, lxm), M2C_VV(sp1, c, lyp, lxp) - vc);
       sd[c] = zero ? T(0) : sl;
     }
   };
@@ -444,8 +558,8 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     T qm[5], qp[5], dl[5], dr[5];
 #pragma unroll
     for (int c = 0; c < 5; c++) {
-      qm[c] = sm.v[sm1][c][lym][lxm];
-      qp[c] = sm.v[sp1][c][lyp][lxp];
+      qm[c] = M2C_VV(sm1, c, lym, lxm);
+      qp[c] = M2C_VV(sp1, c, lyp, lxp);
     }
     const bool uspace = rv != 2;
     if (uspace) {
@@ -506,7 +620,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       const Eos<T>& e = eos_of<T, MULTI>(a.s, id);
       T v[5], sx[5], sy[5], sz[5];
 #pragma unroll
-      for (int c = 0; c < 5; c++) v[c] = sm.v[s0][c][ly][lx];
+      for (int c = 0; c < 5; c++) v[c] = M2C_VV(s0, c, ly, lx);
       uint8_t m = 0;
       int err = ERR_NONE;
       bool cons = false;
@@ -571,7 +685,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     if (CONS && (mk & 0x40)) {  // conservative-variable face state
       T v[5], u[5], uf[5];
 #pragma unroll
-      for (int c = 0; c < 5; c++) v[c] = sm.v[s0][c][my + 1][mx + 1];
+      for (int c = 0; c < 5; c++) v[c] = M2C_VV(s0, c, my + 1, mx + 1);
       if (rev) {
 #pragma unroll
         for (int c = 0; c < 5; c++) out[c] = v[c];
@@ -589,7 +703,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     }
 #pragma unroll
     for (int c = 0; c < 5; c++) {
-      const T v = sm.v[s0][c][my + 1][mx + 1];
+      const T v = M2C_VV(s0, c, my + 1, mx + 1);
       const T sd = sm.sig[ms][d][c][my][mx];
       out[c] = rev ? v : (side ? v + T(0.5) * sd : v - T(0.5) * sd);
     }
@@ -614,13 +728,13 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     if (!rL) {  // low-side boundary face
       T gc[5];
 #pragma unroll
-      for (int c = 0; c < 5; c++) gc[c] = sm.v[sL][c][myL + 1][mxL + 1];
+      for (int c = 0; c < 5; c++) gc[c] = M2C_VV(sL, c, myL + 1, mxL + 1);
       ghost_face(g.bc[2 * d], d, VR, gc, eos_of<T, MULTI>(a.s, idL), VL);
     }
     if (!rR) {  // high-side boundary face
       T gc[5];
 #pragma unroll
-      for (int c = 0; c < 5; c++) gc[c] = sm.v[sR][c][myR + 1][mxR + 1];
+      for (int c = 0; c < 5; c++) gc[c] = M2C_VV(sR, c, myR + 1, mxR + 1);
       ghost_face(g.bc[2 * d + 1], d, VL, gc, eos_of<T, MULTI>(a.s, idR), VR);
     }
     int err = ERR_NONE;
@@ -632,8 +746,8 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       if (iv.mp_recon == 0) {  // constant reconstruction: cell-centred states
 #pragma unroll
         for (int c = 0; c < 5; c++) {
-          WL[c] = sm.v[sL][c][myL + 1][mxL + 1];
-          WR[c] = sm.v[sR][c][myR + 1][mxR + 1];
+          WL[c] = M2C_VV(sL, c, myL + 1, mxL + 1);
+          WR[c] = M2C_VV(sR, c, myR + 1, mxR + 1);
         }
       } else {
 #pragma unroll
@@ -729,23 +843,22 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     if (own) { dxi = g.dx[gi]; dyj = g.dy[gj]; }
 
     // pipeline prologue: planes kb-2 and kb-1 committed, plane kb in flight
+    // (a plane copy that never lands stops the CTA, all threads together)
+    tile_setup();
     __syncthreads();
     issue_plane(kb - 2);
-    cp_async_wait_all();
-    __syncthreads();
+    bool landed = wait_plane(kb - 2);
     commit_plane(kb - 2);
-    __syncthreads();
+    if (__syncthreads_or(!landed)) return;
     issue_plane(kb - 1);
-    cp_async_wait_all();
-    __syncthreads();
+    landed = wait_plane(kb - 1);
     commit_plane(kb - 1);
-    __syncthreads();
+    if (__syncthreads_or(!landed)) return;
     issue_plane(kb);
     for (int m = kb - 2; m < ke; m++) {
-      cp_async_wait_all();
-      __syncthreads();
+      landed = wait_plane(m + 2);
       commit_plane(m + 2);
-      __syncthreads();
+      if (__syncthreads_or(!landed)) return;
       if (m + 3 <= ke + 1) issue_plane(m + 3);  // in flight during the work below
       if (m >= kb && own) {  // the update's FP64 inputs of plane m into L1 while the faces are computed
         const long long offp = (long long)m * g.plane + (long long)gj * g.px + gi;
@@ -808,7 +921,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
             const int slot = a.iface.slot[off];
             T W[5];
 #pragma unroll
-            for (int c = 0; c < 5; c++) W[c] = sm.v[sc][c][ly][lx];
+            for (int c = 0; c < 5; c++) W[c] = M2C_VV(sc, c, ly, lx);
             for (int d = 0; d < 3; d++) {
               if (!ifc[d]) continue;
               const long long base = ((long long)slot * 3 + d) * 5;
