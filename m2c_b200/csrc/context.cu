@@ -375,6 +375,13 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
     }
     std::vector<double> Cm(A.size());
     for (size_t q = 0; q < A.size(); q++) Cm[q] = B[q] / (A[q] + 1.0);  // Reconstructor.h:97
+    bool uni = true;
+    for (size_t q = 1; q < A.size(); q++)
+      uni = uni && A[q] == A[0] && B[q] == B[0] && K[q] == K[0] && Cm[q] == Cm[0];
+    c->g.lu[a] = uni && !A.empty() ? 1 : 0;
+    if (!A.empty()) {
+      c->g.lA0[a] = A[0]; c->g.lB0[a] = B[0]; c->g.lK0[a] = K[0]; c->g.lC0[a] = Cm[0];
+    }
     upload_vec(&c->lA[a], A, c->stream, &st);
     upload_vec(&c->lB[a], B, c->stream, &st);
     upload_vec(&c->lK[a], K, c->stream, &st);
@@ -637,7 +644,11 @@ static m2cg_status check_device_error(m2cg_ctx* c) {
     cudaMemsetAsync(c->err, 0, sizeof(DevError), c->stream);
     m2cg_status st = e.code == ERR_STATE || e.code == ERR_SOUND || e.code == ERR_HLLC ? M2CG_ERR_STATE
                      : e.code == ERR_RIEMANN ? M2CG_ERR_RIEMANN
-                     : e.code == ERR_ITER_CAP ? M2CG_ERR_ITER_CAP : M2CG_ERR_STATE;
+                     : e.code == ERR_ITER_CAP ? M2CG_ERR_ITER_CAP
+                     : e.code == ERR_UNSUPPORTED ? M2CG_ERR_UNSUPPORTED : M2CG_ERR_STATE;
+    if (e.code == ERR_UNSUPPORTED)
+      return fail(st, "unresolved background cells with apply_failsafe_density Off need the level-set "
+                      "correction of unresolved cells, which is not supported");
     return fail(st, "device error code %d at cell %d (site %d)", e.code, e.cell, e.where);
   }
   return M2CG_OK;
@@ -713,7 +724,7 @@ extern "C" m2cg_status m2cg_update_states_after_interface_motion(m2cg_ctx* c, co
   CK(cudaGetLastError());
   const bool mixed = c->scheme.precision == M2CG_PREC_MIXED;
   st = multiphase_update_states(c->mp, c->stream, c->V[c->cur], mixed ? c->Vf[c->cur] : nullptr, c->id, c->err,
-                                use_rs != 0, unresolved);
+                                use_rs != 0, false, unresolved);
   if (st) return st;
   c->counters.kernel_launches += 5;
   st = compute_dtmin(c);

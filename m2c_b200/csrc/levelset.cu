@@ -475,7 +475,9 @@ struct ReinitBuf {
   double* sign;
   double* phibk;
   uint8_t* tag;
-  unsigned long long* red;  // [0] max residual bits, [1] max rel. change bits, [2] first-layer count, [3] done flag
+  unsigned long long* red;  // [0] max residual bits, [1] max rel. change bits, [2] first-layer count,
+                            // [3] converged on the residual (this iteration), [4] attempt finished,
+                            // [5] iterations of the attempt, [6] last max rel. change bits
 };
 
 static ReinitBuf carve(double* base, long long n) {
@@ -556,7 +558,7 @@ __device__ __forceinline__ double reinit_local(const Grid3& g, const LsGeom& geo
 // index division, rows of 32 consecutive cells per warp.
 __global__ void __launch_bounds__(256) k_reinit_stage(Grid3 g, LsGeom geo, ReinitBuf b, int stage, double cfl,
                                                       double tol, const double* in, double* phi, double* out) {
-  if (stage > 1 && b.red[3]) return;  // converged on the residual in stage 1
+  if (b.red[4] || (stage > 1 && b.red[3])) return;  // attempt finished, or converged on the residual in stage 1
   double maxres = 0.0, maxrel = 0.0;
   const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
   for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
@@ -612,8 +614,32 @@ __global__ void __launch_bounds__(256) k_reinit_stage(Grid3 g, LsGeom geo, Reini
 }
 
 __global__ void k_reinit_check(ReinitBuf b, double tol) {
+  if (b.red[4]) return;
   const double r = __longlong_as_double((long long)b.red[0]);
   b.red[3] = (r < tol) ? 1ull : 0ull;
+}
+
+// Start of an attempt: nothing to do without a first layer.
+__global__ void k_reinit_begin(ReinitBuf b) {
+  b.red[4] = b.red[2] == 0 ? 1ull : 0ull;
+  b.red[5] = 0;
+  b.red[0] = b.red[1] = b.red[3] = 0;
+}
+
+// End of a pseudo-time iteration (LevelSetReinitializer.cpp:~220-260): count
+// it, stop the attempt once the residual (checked before the update) or the
+// largest relative change of phi is below the tolerance, and clear the
+// reductions for the next iteration.
+__global__ void k_reinit_end(ReinitBuf b, double tol) {
+  if (b.red[4]) return;
+  b.red[5] += 1;
+  if (b.red[3]) {
+    b.red[4] = 1;
+  } else {
+    b.red[6] = b.red[1];
+    if (__longlong_as_double((long long)b.red[1]) < tol) b.red[4] = 1;
+  }
+  b.red[0] = b.red[1] = b.red[3] = 0;
 }
 
 static double bits_to_double(unsigned long long u) {
@@ -631,35 +657,29 @@ m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& 
   const int grid = grid1d(ni);
   // each CTA walks a column of planes (k = bz, bz + 64, ...)
   const dim3 grid3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 64 ? g.nz : 64), block3(32, 8);
-  cudaMemsetAsync(b.red, 0, 4 * sizeof(unsigned long long), s);
+  cudaMemsetAsync(b.red, 0, 8 * sizeof(unsigned long long), s);
   k_reinit_prep<<<grid, 256, 0, s>>>(g, geo, phi, b);
-  unsigned long long hred[4];
-  cudaMemcpyAsync(hred, b.red, sizeof hred, cudaMemcpyDeviceToHost, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
-  if (hred[2] == 0) return M2CG_OK;  // no interface: nothing to do
   const double tol = ls.reinit_tol;
   const int maxIts = ls.reinit_maxits;
-  int total = 0;
+  // Each attempt queues all its iterations at once; the iterations after
+  // convergence find the attempt finished on the device and return at once,
+  // so one read-back per attempt (not per iteration) decides on a retry.
   for (;;) {
     const double cfl = *cfl_state;
-    int iter;
-    double dphi_max = 0.0;
-    for (iter = 0; iter < maxIts; iter++) {
-      cudaMemsetAsync(b.red, 0, 2 * sizeof(unsigned long long), s);
-      cudaMemsetAsync(b.red + 3, 0, sizeof(unsigned long long), s);
+    k_reinit_begin<<<1, 1, 0, s>>>(b);
+    for (int iter = 0; iter < maxIts; iter++) {
       k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 1, cfl, tol, phi, phi, b.phi1);
       k_reinit_check<<<1, 1, 0, s>>>(b, tol);
       k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 2, cfl, tol, b.phi1, phi, b.phi2);
       k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 3, cfl, tol, b.phi2, phi, phi);
-      cudaMemcpyAsync(hred, b.red, sizeof hred, cudaMemcpyDeviceToHost, s);
-      if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
-      total++;
-      if (hred[3]) break;  // residual below the tolerance (checked before updating phi)
-      dphi_max = bits_to_double(hred[1]);
-      if (dphi_max < tol) break;
+      k_reinit_end<<<1, 1, 0, s>>>(b, tol);
     }
-    if (iterations) *iterations += total;
-    if (iter < maxIts) return M2CG_OK;
+    unsigned long long hred[8];
+    cudaMemcpyAsync(hred, b.red, sizeof hred, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
+    if (iterations) *iterations += (int)hred[5];
+    if (hred[4]) return M2CG_OK;  // converged (or no interface)
+    const double dphi_max = bits_to_double(hred[6]);
     if (dphi_max < 0.02) return M2CG_OK;
     if (cfl < 0.02) return M2CG_ERR_REINIT;
     *cfl_state = cfl / 1.5;

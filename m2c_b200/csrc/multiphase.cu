@@ -90,6 +90,10 @@ struct Multiphase {
   // host-side counters
   long long riemann_calls = 0, riemann_iterations = 0, riemann_errors = 0, unresolved = 0, reinit_calls = 0;
   long long riemann_evaluations = 0, failsafe_cells = 0, riemann_nontrivial = 0;
+  // per-run totals accumulated on the device at the end of every step (no
+  // host round trip per step): [0] calls, [1] iterations, [2] errors,
+  // [3] evaluations, [4] non-trivial calls, [5] unresolved, [6] failsafe cells
+  long long* totals = nullptr;
   uint8_t* mask = nullptr;       // [interior cells] unresolved-list membership, zero between updates
   double failsafe[MAXMAT] = {};  // MaterialModelData::failsafe_density
   double* reinit_buf = nullptr;  // reinitialisation work arrays
@@ -786,6 +790,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   }
   A((void**)&mp->blockcnt, mp->nblocks_scan * 4);
   A((void**)&mp->nchanged, 4 * 4);
+  A((void**)&mp->totals, 8 * sizeof(long long));
   A((void**)&mp->mask, ninterior);
   if (!ok) {
     multiphase_destroy(mp);
@@ -795,6 +800,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   cudaMemsetAsync(mp->counts, 0, 16 * 4, s);
   cudaMemsetAsync(mp->rsValid, 0, mp->cap_slots * 3, s);
   cudaMemsetAsync(mp->mask, 0, ninterior, s);
+  cudaMemsetAsync(mp->totals, 0, 8 * sizeof(long long), s);
   if (levelset_geom_create(s, g, ls, xc, dx, &mp->lsg) != M2CG_OK) {
     multiphase_destroy(mp);
     return M2CG_ERR_NOMEM;
@@ -816,6 +822,7 @@ void multiphase_destroy(Multiphase* mp) {
   cudaFree(mp->Vsm); cudaFree(mp->Vsp); cudaFree(mp->Vmid); cudaFree(mp->midid);
   cudaFree(mp->rsVsm); cudaFree(mp->rsVsp); cudaFree(mp->rsValid); cudaFree(mp->scratch);
   cudaFree(mp->changed); cudaFree(mp->blockcnt); cudaFree(mp->nchanged); cudaFree(mp->mask);
+  cudaFree(mp->totals);
   cudaFree(mp->reinit_buf);
   levelset_geom_destroy(&mp->lsg);
   delete mp;
@@ -931,16 +938,34 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
     mp->reinit_calls++;
     mp->reinit_iterations += its;
   }
-  m2cg_status st = multiphase_update_states(mp, s, Vnew, Vfnew, id, err, true, nullptr);
+  m2cg_status st = multiphase_update_states(mp, s, Vnew, Vfnew, id, err, true, true, nullptr);
   if (st) return st;
   if (counters) counters->kernel_launches += 8 + 3 * mp->scheme.rk_order;
   return M2CG_OK;
 }
 
+// End of a step's state update: add the step's counts to the run totals and
+// turn the two conditions the host used to check after the step into device
+// errors (read by the caller's next error check).
+__global__ void k_step_totals(const int* counts, const int* nchanged, long long* totals, DevError* err,
+                              int step_counts) {
+  if (step_counts) {
+    totals[0] += counts[5];
+    totals[1] += counts[4];
+    totals[2] += counts[3];
+    totals[3] += counts[6];
+    totals[4] += counts[7];
+    if (counts[2]) report(err, ERR_ITER_CAP, -1, 9);  // interface capacity exceeded
+  }
+  totals[5] += nchanged[1];
+  totals[6] += nchanged[3];
+  if (nchanged[2]) report(err, ERR_UNSUPPORTED, -1, 10);
+}
+
 uint8_t* multiphase_idn(Multiphase* mp) { return mp->idn; }
 
 m2cg_status multiphase_update_states(Multiphase* mp, cudaStream_t s, double* const* V, float* const* Vf, uint8_t* id,
-                                     DevError* err, bool use_rs, int* unresolved) {
+                                     DevError* err, bool use_rs, bool in_step, int* unresolved) {
   const Grid3& g = mp->g;
   const long long ninterior = (long long)g.nx * g.ny * g.nz;
   // ordered list of cells whose ID changed, then the sequential update
@@ -971,38 +996,34 @@ m2cg_status multiphase_update_states(Multiphase* mp, cudaStream_t s, double* con
   ua.mask = mp->mask;
   for (int m = 0; m < MAXMAT; m++) ua.failsafe_rho[m] = mp->failsafe[m];
   k_state_update<<<1, 32, 0, s>>>(ua);
+  // step counters into the device totals; interface-capacity overflow and
+  // the unsupported trapped-cell correction become device errors
+  // (only a step's own update counts its Riemann solves)
+  k_step_totals<<<1, 1, 0, s>>>(mp->counts, mp->nchanged, mp->totals, err, in_step ? 1 : 0);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
-  // step counters (one small read-back per step)
-  int hc[8], hn[4];
-  cudaMemcpyAsync(hc, mp->counts, sizeof hc, cudaMemcpyDeviceToHost, s);
+  if (in_step) return M2CG_OK;  // no host round trip inside a step
+  int hn[4];
   cudaMemcpyAsync(hn, mp->nchanged, sizeof hn, cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return M2CG_ERR_CUDA;
-  if (use_rs) {
-    mp->riemann_calls += hc[5];
-    mp->riemann_iterations += hc[4];
-    mp->riemann_errors += hc[3];
-    mp->riemann_evaluations += hc[6];
-    mp->riemann_nontrivial += hc[7];
-    if (hc[2]) return M2CG_ERR_ITER_CAP;  // interface capacity exceeded
-  }
-  mp->unresolved += hn[1];
-  mp->failsafe_cells += hn[3];
   if (unresolved) *unresolved = hn[1];
-  if (hn[2]) {
-    set_last_error("unresolved background cells with apply_failsafe_density Off need the level-set "
-                   "correction of unresolved cells, which is not supported");
-    return M2CG_ERR_UNSUPPORTED;
-  }
+  return M2CG_OK;
+}
+
+m2cg_status multiphase_read_totals(const Multiphase* mp, long long* t7) {
+  if (cudaMemcpy(t7, mp->totals, 7 * sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return M2CG_ERR_CUDA;
   return M2CG_OK;
 }
 
 void multiphase_counters(const Multiphase* mp, m2cg_counters* out) {
-  out->riemann_calls = mp->riemann_calls;
-  out->riemann_iterations = mp->riemann_iterations;
-  out->riemann_errors = mp->riemann_errors;
+  long long t[7] = {};
+  multiphase_read_totals(mp, t);
+  out->riemann_calls = t[0];
+  out->riemann_iterations = t[1];
+  out->riemann_errors = t[2];
   out->reinit_calls = mp->reinit_calls;
-  out->unresolved_cells = mp->unresolved;
-  out->riemann_evaluations = mp->riemann_evaluations;
-  out->failsafe_cells = mp->failsafe_cells;
-  out->riemann_nontrivial = mp->riemann_nontrivial;
+  out->unresolved_cells = t[5];
+  out->riemann_evaluations = t[3];
+  out->failsafe_cells = t[6];
+  out->riemann_nontrivial = t[4];
 }

@@ -33,6 +33,9 @@ void multiphase_counters(const Multiphase* mp, m2cg_counters* out);
 // The state update of cells whose ID differs from the step-start IDs
 // (multiphase_idn): Riemann-solution or extrapolation pass, FixUnresolvedNodes,
 // clip. use_rs: the stage-1 star states of the last step are valid for these IDs.
+// in_step: called at the end of a step (the step's counts go to the run
+// totals, no host round trip); otherwise *unresolved (may be NULL) receives
+// the cells handed to FixUnresolvedNodes after a read-back.
 m2cg_status multiphase_update_states(Multiphase* mp, cudaStream_t s, double* const* V, float* const* Vf, uint8_t* id,
-                                     m2c::DevError* err, bool use_rs, int* unresolved);
+                                     m2c::DevError* err, bool use_rs, bool in_step, int* unresolved);
 uint8_t* multiphase_idn(Multiphase* mp);

@@ -40,7 +40,8 @@ enum {
   ERR_SOUND = 9,      // c^2 < 0 in a flux or the CFL sweep (FluxFcnHLLC.h:118-130)
   ERR_HLLC = 10,      // NaN S* in HLLC (FluxFcnHLLC.h:235-241)
   ERR_RIEMANN = 4,
-  ERR_ITER_CAP = 6
+  ERR_ITER_CAP = 6,
+  ERR_UNSUPPORTED = 8  // a path the library does not implement was reached (state update)
 };
 
 // std::min / std::max semantics (not fmin/fmax): min(a,b) = (b<a)?b:a.

@@ -80,6 +80,11 @@ struct Grid3 {
   const double* lB[3];  // limiter coefficient B per axis index
   const int* lK[3];     // van Albada exponent per axis index
   const double* lC[3];  // generalized minmod B/(A+1) per axis index
+  // per axis: 1 if A, B, K and C are the same at every index (uniform
+  // meshes), which then stand in for the arrays
+  int lu[3];
+  double lA0[3], lB0[3], lC0[3];
+  int lK0[3];
 };
 
 struct SchemeK {
@@ -491,6 +496,28 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     if (use_tma) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   };
 
+  // Limiter coefficients (Reconstructor::Setup) of the cell at loaded
+  // position (lx, ly) of plane p along axis d: the axis' constants on a
+  // uniform axis, else its per-index arrays. The generalized minmod uses
+  // C = B/(A+1) only (carried in B).
+  auto limiter_coeffs = [&](int p, int lx, int ly, int d, T& A, T& B, int& K) {
+    if (g.lu[d]) {
+      if (limiter == LIM_VANALBADA) {
+        A = T(g.lA0[d]); B = T(g.lB0[d]); K = g.lK0[d];
+      } else {
+        A = T(0); B = T(g.lC0[d]);
+      }
+      return;
+    }
+    const int ix = d == 0 ? wrap_index(i0 + lx - 2, g.nx) : (d == 1 ? wrap_index(j0 + ly - 2, g.ny)
+                                                                    : wrap_index(p, g.nz));
+    if (limiter == LIM_VANALBADA) {
+      A = T(g.lA[d][ix]); B = T(g.lB[d][ix]); K = g.lK[d][ix];
+    } else {
+      A = T(0); B = T(g.lC[d][ix]);
+    }
+  };
+
   // Limited slopes in direction d of the real cell at loaded position
   // (lx, ly) of plane p (needs planes p-1, p, p+1 for d = 2).
   auto slopes = [&](int p, int lx, int ly, int d, T* sd) {
@@ -504,15 +531,9 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       for (int c = 0; c < 5; c++) sd[c] = T(0);
       return;
     }
-    const int ia = wrap_index(i0 + lx - 2, g.nx), ja = wrap_index(j0 + ly - 2, g.ny), ka = wrap_index(p, g.nz);
-    const int ix = d == 0 ? ia : (d == 1 ? ja : ka);
     T A, B;
     int K = 0;
-    if (limiter == LIM_VANALBADA) {
-      A = T(g.lA[d][ix]); B = T(g.lB[d][ix]); K = g.lK[d][ix];
-    } else {  // generalized minmod uses B/(A+1) only
-      A = T(0); B = T(g.lC[d][ix]);
-    }
+    limiter_coeffs(p, lx, ly, d, A, B, K);
     bool zero = false;
     if (slope_zero) {
       const uint8_t id = sm.ids[s0][ly][lx];
@@ -540,15 +561,9 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     if (d == 0) { lxm = lx - 1; lxp = lx + 1; }
     else if (d == 1) { lym = ly - 1; lyp = ly + 1; }
     else { sm1 = slot4(p - 1); sp1 = slot4(p + 1); }
-    const int ia = wrap_index(i0 + lx - 2, g.nx), ja = wrap_index(j0 + ly - 2, g.ny), ka = wrap_index(p, g.nz);
-    const int ix = d == 0 ? ia : (d == 1 ? ja : ka);
     T A, B;
     int K = 0;
-    if (limiter == LIM_VANALBADA) {
-      A = T(g.lA[d][ix]); B = T(g.lB[d][ix]); K = g.lK[d][ix];
-    } else {
-      A = T(0); B = T(g.lC[d][ix]);
-    }
+    limiter_coeffs(p, lx, ly, d, A, B, K);
     const uint8_t idm = sm.ids[sm1][lym][lxm], idp = sm.ids[sp1][lyp][lxp];
     bool zero = false;
     if (slope_zero) {
@@ -877,6 +892,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       // (4) residual + RK update of plane m
       const double dzk = g.dz[m];
       const double ax = dyj * dzk, ay = dxi * dzk, az = dxi * dyj;
+      const float axf = float(ax), ayf = float(ay), azf = float(az);
       const double vol = dxi * dyj * dzk;
       // Vec5D::operator/= multiplies by the reciprocal (Vector5D.h:172-181)
       const double inv_mvol = 1.0 / (-vol);
@@ -938,16 +954,25 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       for (int c = 0; c < 5; c++) {
         // low faces: the flux this cell sees as the right-hand cell
         // (SpaceOperator.cpp:2555-2556, 2683-2684, 2810-2811)
-        const double fl = double(ifc[0] ? F2[0][c] : sm.fx[c][fxl]);
-        const double gl = double(ifc[1] ? F2[1][c] : sm.fy[c][fyl]);
-        const double hl = double(ifc[2] ? F2[2][c] : sm.fz[zl][c][fzc]);
-        double f = 0.0;
-        f = f - fl * ax;
-        f = f - gl * ay;
-        f = f - hl * az;
-        f = f + double(sm.fx[c][fxl + 1]) * ax;
-        f = f + double(sm.fy[c][fyl + TX]) * ay;
-        f = f + double(sm.fz[zr][c][fzc]) * az;
+        const T fl = ifc[0] ? F2[0][c] : sm.fx[c][fxl];
+        const T gl = ifc[1] ? F2[1][c] : sm.fy[c][fyl];
+        const T hl = ifc[2] ? F2[2][c] : sm.fz[zl][c][fzc];
+        double f;
+        if constexpr (sizeof(T) == 8) {
+          // FP64: the reference's order, 0 - Fl A - Gl A - Hl A + Fr A + Gr A + Hr A
+          f = 0.0;
+          f = f - fl * ax;
+          f = f - gl * ay;
+          f = f - hl * az;
+          f = f + double(sm.fx[c][fxl + 1]) * ax;
+          f = f + double(sm.fy[c][fyl + TX]) * ay;
+          f = f + double(sm.fz[zr][c][fzc]) * az;
+        } else {
+          // mixed: FP32 accumulation of the flux differences (the difference
+          // of two nearby FP32 fluxes is exact), one conversion per component
+          f = double((sm.fx[c][fxl + 1] - fl) * axf + (sm.fy[c][fyl + TX] - gl) * ayf +
+                     (sm.fz[zr][c][fzc] - hl) * azf);
+        }
         const double R = f * inv_mvol;
         if (a.Ro[0]) a.Ro[c][off] = R;
         Unew[c] = Unew[c] + bdt * R;
