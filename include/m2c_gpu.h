@@ -386,6 +386,13 @@ m2cg_status m2cg_batch_time_steps(m2cg_batch* b, int nsteps, float* ms);
  * of the batch then starts from its proposal. The network must outlive the
  * batch's use of it. */
 m2cg_status m2cg_batch_set_mlp(m2cg_batch* b, const m2cg_mlp* m);
+/* Attach a trained network (NULL detaches) to a two-material context: every
+ * interface Riemann problem of its steps starts from the network's proposal
+ * (features of the stage states the solve uses; BF16 inference on the
+ * device, no host round trip). No reference counterpart. The network must
+ * outlive the context's use of it; the first attachment allocates per-face
+ * buffers (about 90 bytes per interface-face slot). */
+m2cg_status m2cg_set_mlp(m2cg_ctx* ctx, const m2cg_mlp* m);
 m2cg_status m2cg_batch_destroy(m2cg_batch* b);
 
 #ifdef __cplusplus

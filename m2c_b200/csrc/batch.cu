@@ -41,7 +41,7 @@ namespace m2c {
 
 void set_last_error(const char* msg);
 cudaError_t mlp_warm_device(const m2cg_mlp* m, cudaStream_t s, const float* X, const int* valid, const double* P,
-                            int n, float* y, double* warm);
+                            int n, float* y, double* warm, const int* ndev);
 
 constexpr int TUBE_IFACE_CAP = 8;        // interface faces tracked per tube
 constexpr int TUBE_RIEMANN_THREADS = 16384; // threads of the Riemann kernel (each owns path scratch)
@@ -699,7 +699,7 @@ static cudaError_t enqueue_step(m2cg_batch* b, int cur) {
     if (b->mlp) {
       const int nslot = b->ntubes * TUBE_IFACE_CAP;
       k_tube_features<<<(nslot + 255) / 256, 256, 0, b->stream>>>(A, S, b->fX, b->fP, b->fvalid);
-      mlp_warm_device(b->mlp, b->stream, b->fX, b->fvalid, b->fP, nslot, b->fy, b->fwarm);
+      mlp_warm_device(b->mlp, b->stream, b->fX, b->fvalid, b->fP, nslot, b->fy, b->fwarm, nullptr);
     }
     k_tube_riemann<<<TUBE_RIEMANN_THREADS / 64, 64, 0, b->stream>>>(A, S);
     k_tube_stage<<<b->stage_grid, b->stage_threads, smem, b->stream>>>(A, S);

@@ -1025,6 +1025,15 @@ extern "C" m2cg_status m2cg_profile_stages(m2cg_ctx* c, int nsteps, float* stage
   return M2CG_OK;
 }
 
+// Attach the learned warm start to the context's interface Riemann solves.
+extern "C" m2cg_status m2cg_set_mlp(m2cg_ctx* c, const m2cg_mlp* m) {
+  if (!c) return fail(M2CG_ERR_ARG, "null argument");
+  if (!c->mp) return fail(M2CG_ERR_ARG, "no level set: the context has no interface Riemann problems");
+  m2cg_status st = multiphase_set_mlp(c->mp, m);
+  if (st) return fail(st, "allocation of the warm-start buffers failed");
+  return M2CG_OK;
+}
+
 // Select the CUDA device for contexts created afterwards on this thread.
 extern "C" m2cg_status m2cg_set_device(int device) {
   CK(cudaSetDevice(device));

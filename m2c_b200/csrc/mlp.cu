@@ -251,8 +251,9 @@ __device__ void stage_weights(InferSmem& S, const float* params, const float* no
 // units (log(pstar / pac)), BF16 weights and activations, FP32 accumulation.
 // 8 warps per CTA, 16 rows per warp per iteration.
 __global__ void __launch_bounds__(256) k_mlp_infer(const float* params, const float* norm, const float* X,
-                                                   const int* valid, int n, float* yout) {
+                                                   const int* valid, int n, const int* ndev, float* yout) {
   __shared__ InferSmem S;
+  if (ndev && *ndev < n) n = *ndev;  // rows counted on the device (n is then the capacity)
   stage_weights(S, params, norm);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -314,7 +315,9 @@ __global__ void k_mlp_features_pairs(const Eos<double>* eos, int n, const double
   }
 }
 
-__global__ void k_mlp_to_pressure(const float* y, const double* P, const int* valid, int n, double* p) {
+__global__ void k_mlp_to_pressure(const float* y, const double* P, const int* valid, int n, const int* ndev,
+                                  double* p) {
+  if (ndev && *ndev < n) n = *ndev;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
     p[q] = valid[q] ? P[q] * exp((double)y[q]) : NAN;
 }
@@ -544,7 +547,7 @@ extern "C" m2cg_status m2cg_mlp_train(m2cg_mlp* m, const float* X, const float* 
 static cudaError_t infer_rows(m2cg_mlp* m, const float* dX, const int* dvalid, int n, float* dyout) {
   const int tiles = (n + 15) / 16;
   const int grid = std::max(1, std::min((tiles + 7) / 8, 148 * 4));
-  k_mlp_infer<<<grid, 256, 0, m->stream>>>(m->w, m->norm, dX, dvalid, n, dyout);
+  k_mlp_infer<<<grid, 256, 0, m->stream>>>(m->w, m->norm, dX, dvalid, n, nullptr, dyout);
   return cudaGetLastError();
 }
 
@@ -552,11 +555,11 @@ namespace m2c {
 // Device-side proposals for rows of raw features (used by the batched tubes):
 // warm[r] = P[r] exp(network(X[r])) where valid[r], else NaN.
 cudaError_t mlp_warm_device(const m2cg_mlp* m, cudaStream_t s, const float* X, const int* valid, const double* P,
-                            int n, float* y, double* warm) {
+                            int n, float* y, double* warm, const int* ndev) {
   const int tiles = (n + 15) / 16;
   const int grid = std::max(1, std::min((tiles + 7) / 8, 148 * 4));
-  k_mlp_infer<<<grid, 256, 0, s>>>(m->w, m->norm, X, valid, n, y);
-  k_mlp_to_pressure<<<(n + 255) / 256, 256, 0, s>>>(y, P, valid, n, warm);
+  k_mlp_infer<<<grid, 256, 0, s>>>(m->w, m->norm, X, valid, n, ndev, y);
+  k_mlp_to_pressure<<<std::max(1, std::min((n + 255) / 256, 148 * 8)), 256, 0, s>>>(y, P, valid, n, ndev, warm);
   return cudaGetLastError();
 }
 }  // namespace m2c
@@ -602,7 +605,7 @@ static m2cg_status pairs_common(m2cg_mlp* m, const m2cg_material* mats, int n, c
       if (valid_out) ck(cudaMemcpyAsync(valid_out, dvalid, nn * 4, cudaMemcpyDeviceToHost, s));
     } else if (mode == 1) {
       if (e == cudaSuccess) ck(infer_rows(m, dX, dvalid, n, dy));
-      if (e == cudaSuccess) k_mlp_to_pressure<<<grid, 256, 0, s>>>(dy, dP, dvalid, n, dp);
+      if (e == cudaSuccess) k_mlp_to_pressure<<<grid, 256, 0, s>>>(dy, dP, dvalid, n, nullptr, dp);
       ck(cudaGetLastError());
       ck(cudaMemcpyAsync(p_out, dp, nn * 8, cudaMemcpyDeviceToHost, s));
     }

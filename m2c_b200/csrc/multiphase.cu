@@ -30,9 +30,12 @@
 #include "levelset.h"
 #include "ls_device.cuh"
 #include "multiphase.h"
+#include "mlp.cuh"
 #include "riemann_batch.h"
 
 namespace m2c {
+cudaError_t mlp_warm_device(const m2cg_mlp* m, cudaStream_t s, const float* X, const int* valid, const double* P,
+                            int n, float* y, double* warm, const int* ndev);
 
 // Threads running Riemann problems at once (each owns an integration-path
 // scratch region of 2 x RIEMANN_PATH_CAP x 3 doubles).
@@ -94,6 +97,14 @@ struct Multiphase {
   // host round trip per step): [0] calls, [1] iterations, [2] errors,
   // [3] evaluations, [4] non-trivial calls, [5] unresolved, [6] failsafe cells
   long long* totals = nullptr;
+  // learned warm start (optional): per interface face the network's features,
+  // base pressure, validity, output and proposed star pressure
+  const m2cg_mlp* mlp = nullptr;
+  float* fX = nullptr;
+  double* fP = nullptr;
+  int* fvalid = nullptr;
+  float* fy = nullptr;
+  double* fwarm = nullptr;
   uint8_t* mask = nullptr;       // [interior cells] unresolved-list membership, zero between updates
   double failsafe[MAXMAT] = {};  // MaterialModelData::failsafe_density
   double* reinit_buf = nullptr;  // reinitialisation work arrays
@@ -201,6 +212,7 @@ struct IfaceRiemannArgs {
   int normal_mode;        // MultiPhaseData::riemann_normal
   const double* phi;      // phi^n (the reference's loose coupling uses the step's phi)
   LsGeom geo;
+  const double* warm;     // per face: proposed star pressure of the learned warm start, or NULL
 };
 
 // Groups: 4 wave patterns x IFACE_STRENGTHS rarefaction strengths; sizes in
@@ -306,7 +318,7 @@ __global__ void __launch_bounds__(128, M2C_IFACE_MINB) k_iface_riemann(IfaceRiem
     double Vs[5], Vsm[5], Vsp[5];
     int mid = 0;
     bool bad = false;
-    int r = rs.solve(dir, VL, idL, VR, idR, Vs, mid, Vsm, Vsp, NAN, bad);
+    int r = rs.solve(dir, VL, idL, VR, idR, Vs, mid, Vsm, Vsp, a.warm ? a.warm[f] : NAN, bad);
     a.eos[idL].clip(Vsm);
     a.eos[idR].clip(Vsp);
     const long long b = ((long long)s * 3 + d) * 5;
@@ -330,6 +342,29 @@ __global__ void __launch_bounds__(128, M2C_IFACE_MINB) k_iface_riemann(IfaceRiem
     atomicAdd(&a.counts[6], rs.evaluations);
     atomicAdd(&a.counts[5], 1);
     if (rs.evaluations > 0) atomicAdd(&a.counts[7], 1);  // not answered by the trivial branch
+  }
+}
+
+// Features of the learned warm start for every interface face of the stage:
+// the same left/right states and Riemann direction the solve will use.
+__global__ void k_iface_features(IfaceRiemannArgs a, float* X, double* P, int* valid) {
+  const Grid3& g = a.st.g;
+  long long nf = a.counts[1];
+  if (nf > a.cap_faces) nf = a.cap_faces;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+    const int q = a.faces[3 * f], d = a.faces[3 * f + 2];
+    int i, j, k;
+    cell_coords(g, q, i, j, k);
+    int ni, nj, nk;
+    low_neighbour(g, i, j, k, d, ni, nj, nk);
+    const long long offR = offset_of(g, i, j, k), offL = offset_of(g, ni, nj, nk);
+    const uint8_t idR = a.st.id[offR], idL = a.st.id[offL];
+    double VL[5], VR[5], dir[3], Pq = 0.0;
+    stage_state(a.st, a.eos, offL, idL, VL);
+    stage_state(a.st, a.eos, offR, idR, VR);
+    riemann_direction(a.normal_mode, g, a.geo, a.phi, i, j, k, d, idR, idL, dir);
+    valid[f] = mlp_features(a.eos[idL], a.eos[idR], VL, VR, dir, X + f * MLP_IN, &Pq) ? 1 : 0;
+    P[f] = Pq;
   }
 }
 
@@ -823,6 +858,7 @@ void multiphase_destroy(Multiphase* mp) {
   cudaFree(mp->rsVsm); cudaFree(mp->rsVsp); cudaFree(mp->rsValid); cudaFree(mp->scratch);
   cudaFree(mp->changed); cudaFree(mp->blockcnt); cudaFree(mp->nchanged); cudaFree(mp->mask);
   cudaFree(mp->totals);
+  cudaFree(mp->fX); cudaFree(mp->fP); cudaFree(mp->fvalid); cudaFree(mp->fy); cudaFree(mp->fwarm);
   cudaFree(mp->reinit_buf);
   levelset_geom_destroy(&mp->lsg);
   delete mp;
@@ -902,6 +938,12 @@ m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
   cudaMemsetAsync(mp->counts + IFACE_GROUP0, 0, 2 * IFACE_GROUPS * sizeof(int), s);
   k_iface_classify<<<148 * 8, 256, 0, s>>>(ra);
   k_iface_group<<<148 * 8, 256, 0, s>>>(ra);
+  if (mp->mlp) {
+    // the network's proposals for this stage's problems, counted on the device
+    k_iface_features<<<148 * 8, 256, 0, s>>>(ra, mp->fX, mp->fP, mp->fvalid);
+    mlp_warm_device(mp->mlp, s, mp->fX, mp->fvalid, mp->fP, (int)mp->cap_faces, mp->fy, mp->fwarm, &mp->counts[1]);
+    ra.warm = mp->fwarm;
+  }
   k_iface_riemann<<<mp->iface_blocks, 128, 0, s>>>(ra);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
   a.iface.slot = mp->slot;
@@ -1026,4 +1068,21 @@ void multiphase_counters(const Multiphase* mp, m2cg_counters* out) {
   out->riemann_evaluations = t[3];
   out->failsafe_cells = t[6];
   out->riemann_nontrivial = t[4];
+}
+
+m2cg_status multiphase_set_mlp(Multiphase* mp, const m2cg_mlp* m) {
+  if (m && !mp->fX) {
+    const size_t n = (size_t)mp->cap_faces;
+    if (cudaMalloc((void**)&mp->fX, n * MLP_IN * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&mp->fP, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&mp->fvalid, n * sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&mp->fy, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&mp->fwarm, n * sizeof(double)) != cudaSuccess) {
+      cudaFree(mp->fX); cudaFree(mp->fP); cudaFree(mp->fvalid); cudaFree(mp->fy); cudaFree(mp->fwarm);
+      mp->fX = nullptr; mp->fP = nullptr; mp->fvalid = nullptr; mp->fy = nullptr; mp->fwarm = nullptr;
+      return M2CG_ERR_NOMEM;
+    }
+  }
+  mp->mlp = m;
+  return M2CG_OK;
 }

@@ -30,6 +30,9 @@ m2cg_status multiphase_end_step(Multiphase* mp, cudaStream_t s, double* const* V
                                 float* const* Vfnew, uint8_t* id,
                                 const double* clock, m2c::DevError* err, m2cg_counters* counters);
 void multiphase_counters(const Multiphase* mp, m2cg_counters* out);
+// Attach (m != NULL) or detach the learned warm start of the interface
+// Riemann solves; allocates the per-face feature buffers on first use.
+m2cg_status multiphase_set_mlp(Multiphase* mp, const m2cg_mlp* m);
 // The state update of cells whose ID differs from the step-start IDs
 // (multiphase_idn): Riemann-solution or extrapolation pass, FixUnresolvedNodes,
 // clip. use_rs: the stage-1 star states of the last step are valid for these IDs.

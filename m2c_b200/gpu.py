@@ -76,6 +76,7 @@ def lib():
     L.m2cg_batch_time_steps.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
     L.m2cg_batch_destroy.argtypes = [vp]
     L.m2cg_batch_set_mlp.argtypes = [vp, vp]
+    L.m2cg_set_mlp.argtypes = [vp, vp]
     fp = C.POINTER(C.c_float)
     L.m2cg_mlp_create.argtypes = [C.c_ulonglong, C.POINTER(vp)]
     L.m2cg_mlp_destroy.argtypes = [vp]
@@ -96,6 +97,7 @@ def lib():
                  "m2cg_get_stream", "m2cg_profile_stages", "m2cg_batch_create", "m2cg_batch_run",
                  "m2cg_batch_download", "m2cg_batch_get_tuning", "m2cg_batch_get_counters",
                  "m2cg_batch_tube_errors", "m2cg_batch_time_steps", "m2cg_batch_destroy", "m2cg_batch_set_mlp",
+                 "m2cg_set_mlp",
                  "m2cg_mlp_create", "m2cg_mlp_destroy", "m2cg_mlp_get_params", "m2cg_mlp_set_params",
                  "m2cg_mlp_loss_grad", "m2cg_mlp_train", "m2cg_mlp_features_pairs", "m2cg_mlp_infer",
                  "m2cg_mlp_predict_pairs"):
@@ -237,6 +239,12 @@ class Solver:
                                                               int(bool(use_stored_riemann_solutions)),
                                                               C.byref(n)))
         return n.value
+
+    def set_mlp(self, mlp):
+        """Start every interface Riemann solve of the steps from the
+        network's proposal (None detaches; two materials only)."""
+        check(lib().m2cg_set_mlp(self.h, mlp.h if mlp is not None else None))
+        self._mlp = mlp  # keep it alive while attached
 
     def stream(self):
         p = C.c_void_p()

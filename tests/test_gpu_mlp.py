@@ -77,7 +77,10 @@ def test_warm_start_saves_evaluations(gpu, trained):
     print(f"\nwarm start: evaluations {ev_c:.3f} -> {ev_h:.3f} ({ev_c / ev_h:.2f}x), "
           f"secant iterations {it_c:.3f} -> {it_h:.3f}; |log(p/p*)| median {np.median(rel):.2e} "
           f"p90 {np.percentile(rel, 90):.2e}; |dp*|/P p99 {np.percentile(dp, 99):.2e} max {dp.max():.2e}")
-    assert ev_h < ev_c
+    # measured on this network and these problems: about 1.2x fewer
+    # evaluations and 1.3x fewer secant iterations
+    assert ev_c / ev_h >= 1.1, ev_c / ev_h
+    assert it_c / it_h >= 1.15, it_c / it_h
     # the solver decides: both solves pass its stopping test (velocity
     # mismatch below tol_main x max sound speed, or a bracket narrower than
     # tol_main x pressure scale), so their star velocities agree within
@@ -113,3 +116,30 @@ def test_batch_with_warm_start_matches_cold(gpu, trained):
         assert (np.abs(Vh[t] - Vc[t]).max(axis=0) <= 1e-3 * scale + 1e-9).all(), t
     assert np.allclose(th, tc, rtol=1e-3)
     print(f"\ntubes: evaluations {cnt[0]['riemann_evaluations']} -> {cnt[1]['riemann_evaluations']}")
+
+
+def test_bubble_with_warm_start_matches_cold(gpu, trained):
+    """m2cg_set_mlp on a two-material context: the interface Riemann
+    problems of every stage start from the network's proposals, the solver
+    still decides, so the bubble's steps agree with the cold run to the
+    solver's tolerance and the material IDs are identical."""
+    net, _ = trained
+    outs, cnt = [], []
+    for use in (False, True):
+        g, s, mats, ls, V, ID, PHI = cases.bubble_case(24, reinit_frequency=-1, shock_front="contact",
+                                                       nbubbles=1, radius=4.0e-3)
+        sol = gpu.Solver(g, s, mats, ls)
+        sol.upload(V, ID, PHI)
+        if use:
+            sol.set_mlp(net)
+        sol.run(6)
+        outs.append(sol.download())
+        cnt.append(sol.counters())
+        sol.close()
+    (Vc, IDc, Pc), (Vh, IDh, Ph) = outs
+    assert np.array_equal(IDc, IDh)
+    scale = np.abs(Vc[1:-1, 1:-1, 1:-1]).reshape(-1, 5).max(axis=0)
+    assert (np.abs(Vh - Vc)[1:-1, 1:-1, 1:-1].reshape(-1, 5).max(axis=0) <= 1e-3 * scale).all()
+    assert cnt[1]["riemann_nontrivial"] > 0
+    print(f"\nbubble: star-state evaluations {cnt[0]['riemann_evaluations']} -> {cnt[1]['riemann_evaluations']}, "
+          f"secant iterations {cnt[0]['riemann_iterations']} -> {cnt[1]['riemann_iterations']}")
