@@ -518,7 +518,19 @@ def extra_warm_start(net, n=100_000):
     cl = np.sqrt(g[0::2] * (VL[:, 4] + pc[0::2]) / VL[:, 0])
     cr = np.sqrt(g[1::2] * (VR[:, 4] + pc[1::2]) / VR[:, 0])
     du = (np.abs(hot["Vsm"][:, 1] - cold["Vsm"][:, 1]) / np.maximum(cl, cr))[both]
+    # what a proposal of a given accuracy would save: the cold solution's p*
+    # perturbed by a log-normal error of width eps, through the same solver
+    curve = {}
+    okc = (cold["err"] == 0) & (cold["Vsm"][:, 4] > 0)
+    rng = np.random.default_rng(5)
+    for eps in (0.0, 1e-5, 1e-4, 1e-3, 6e-3):
+        prop = np.where(okc, cold["Vsm"][:, 4] * np.exp(eps * rng.normal(size=n)), np.nan)
+        r = warmstart.solve(s, mats, VL, VR, dirs, warm=prop)
+        m = okc & (r["err"] == 0)
+        curve[f"{eps:g}"] = {"iteration_ratio": float(cold["iters"][m].mean() / r["iters"][m].mean()),
+                             "evaluation_ratio": float(cold["evals"][m].mean() / r["evals"][m].mean())}
     return {"problems": n, "solved_both": int(both.sum()),
+            "proposal_error_vs_gain": curve,
             "evaluations_cold": float(cold["evals"][both].mean()), "evaluations_warm": float(hot["evals"][both].mean()),
             "evaluation_ratio": float(cold["evals"][both].mean() / hot["evals"][both].mean()),
             "iterations_cold": float(cold["iters"][both].mean()), "iterations_warm": float(hot["iters"][both].mean()),
