@@ -355,7 +355,11 @@ typedef struct m2cg_batch m2cg_batch;
 typedef struct {
   int cells_per_block;   /* cells handled by one CTA per work item; 0 = autotune */
   int threads_per_block; /* 0 = autotune */
-  int use_graph;         /* capture the step loop in a CUDA graph */
+  int use_graph;         /* launch mode: 0 kernels per phase, launched one by one; 1 the same
+                            captured in CUDA graphs and replayed; 2 one persistent launch per
+                            run, each CTA advancing whole tubes through all their steps (tubes
+                            are independent, so no CTA waits on another); -1 measure 1 and 2
+                            and take the faster */
 } m2cg_batch_tuning;
 
 /* ntubes tubes; tube t has len[t] cells on [0, 1] (cell width 1/len[t]),

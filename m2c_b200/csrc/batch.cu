@@ -95,10 +95,7 @@ __device__ __forceinline__ void tube_fail(const TubeArgs& A, int t, int code, in
 
 // SpaceOperator::ComputeTimeStepSize per tube (dy = dz = 1), the ID snapshot,
 // and the ordered list of interface faces (ID differs across the face).
-__global__ void k_tube_begin(TubeArgs A, int cur) {
-  const int lane = threadIdx.x & 31;
-  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (t >= A.ntubes) return;
+__device__ void tube_begin(const TubeArgs& A, int t, int cur, int lane) {
   const long long o = A.off[t];
   const int n = (int)(A.off[t + 1] - o);
   const double h = 1.0 / n;
@@ -141,6 +138,13 @@ __global__ void k_tube_begin(TubeArgs A, int cur) {
   }
 }
 
+__global__ void k_tube_begin(TubeArgs A, int cur) {
+  const int lane = threadIdx.x & 31;
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t >= A.ntubes) return;
+  tube_begin(A, t, cur, lane);
+}
+
 // Primitive state of a real cell at this stage: V^n (stage 1) or clip(C2P(U_s)).
 __device__ __forceinline__ void tube_state(const TubeArgs& A, const TubeStage& S, const Eos<double>& e, long long q,
                                            double* V) {
@@ -157,6 +161,45 @@ __device__ __forceinline__ void tube_state(const TubeArgs& A, const TubeStage& S
 // Exact Riemann problem at every interface face of every tube
 // (SpaceOperator.cpp:2499-2523: MESH normal, cell-centred states, star
 // states clipped with each side's EOS; stage-1 results kept).
+__device__ void tube_riemann(const TubeArgs& A, const TubeStage& S, int t, int k, RiemannSolver& rs) {
+  const long long w = (long long)t * TUBE_IFACE_CAP + k;
+  const long long o = A.off[t];
+  const int i = A.iface[w];
+  const uint8_t idL = A.id[o + i - 1], idR = A.id[o + i];
+  const Eos<double>* eos = A.eos + 2 * t;
+  double VL[5], VR[5];
+  tube_state(A, S, eos[idL], o + i - 1, VL);
+  tube_state(A, S, eos[idR], o + i, VR);
+  const double dir[3] = {1.0, 0.0, 0.0};
+  double Vs[5], Vsm[5], Vsp[5];
+  int mid = 0;
+  bool bad = false;
+  rs.eos = eos;
+  const double warm = A.warm ? A.warm[w] : NAN;
+  const int r = rs.solve(dir, VL, idL, VR, idR, Vs, mid, Vsm, Vsp, warm, bad);
+  eos[idL].clip(Vsm);
+  eos[idR].clip(Vsp);
+  for (int c = 0; c < 5; c++) {
+    A.Vsm[w * 5 + c] = Vsm[c];
+    A.Vsp[w * 5 + c] = Vsp[c];
+    A.Vmid[w * 5 + c] = Vs[c];
+  }
+  A.midid[w] = mid;
+  if (S.stage == 1) {
+    for (int c = 0; c < 5; c++) {
+      A.rsVsm[w * 5 + c] = Vsm[c];
+      A.rsVsp[w * 5 + c] = Vsp[c];
+    }
+    A.rsValid[w] = (r == RIEM_OK) ? 1 : 0;
+  }
+  atomicAdd(&A.cnt[0], 1ull);
+  atomicAdd(&A.cnt[1], (unsigned long long)rs.iterations);
+  atomicAdd(&A.cnt[5], (unsigned long long)rs.evaluations);
+  if (r != RIEM_OK) atomicAdd(&A.cnt[2], 1ull);
+  if (r & RIEM_PATH_OVERFLOW) tube_fail(A, t, ERR_ITER_CAP, (int)(o + i), 7);
+  if (bad) tube_fail(A, t, ERR_STATE, (int)(o + i), 8);
+}
+
 __global__ void k_tube_riemann(TubeArgs A, TubeStage S) {
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
@@ -168,45 +211,7 @@ __global__ void k_tube_riemann(TubeArgs A, TubeStage S) {
   rs.path3.cap = RIEMANN_PATH_CAP;
   // one thread per tube (tubes rarely hold more than one interface face)
   for (long long tt = tid; tt < A.ntubes; tt += nth)
-  for (int k = 0; k < A.nif[tt]; k++) {
-    const int t = (int)tt;
-    const long long w = tt * TUBE_IFACE_CAP + k;
-    const long long o = A.off[t];
-    const int i = A.iface[w];
-    const uint8_t idL = A.id[o + i - 1], idR = A.id[o + i];
-    const Eos<double>* eos = A.eos + 2 * t;
-    double VL[5], VR[5];
-    tube_state(A, S, eos[idL], o + i - 1, VL);
-    tube_state(A, S, eos[idR], o + i, VR);
-    const double dir[3] = {1.0, 0.0, 0.0};
-    double Vs[5], Vsm[5], Vsp[5];
-    int mid = 0;
-    bool bad = false;
-    rs.eos = eos;
-    const double warm = A.warm ? A.warm[w] : NAN;
-    const int r = rs.solve(dir, VL, idL, VR, idR, Vs, mid, Vsm, Vsp, warm, bad);
-    eos[idL].clip(Vsm);
-    eos[idR].clip(Vsp);
-    for (int c = 0; c < 5; c++) {
-      A.Vsm[w * 5 + c] = Vsm[c];
-      A.Vsp[w * 5 + c] = Vsp[c];
-      A.Vmid[w * 5 + c] = Vs[c];
-    }
-    A.midid[w] = mid;
-    if (S.stage == 1) {
-      for (int c = 0; c < 5; c++) {
-        A.rsVsm[w * 5 + c] = Vsm[c];
-        A.rsVsp[w * 5 + c] = Vsp[c];
-      }
-      A.rsValid[w] = (r == RIEM_OK) ? 1 : 0;
-    }
-    atomicAdd(&A.cnt[0], 1ull);
-    atomicAdd(&A.cnt[1], (unsigned long long)rs.iterations);
-    atomicAdd(&A.cnt[5], (unsigned long long)rs.evaluations);
-    if (r != RIEM_OK) atomicAdd(&A.cnt[2], 1ull);
-    if (r & RIEM_PATH_OVERFLOW) tube_fail(A, t, ERR_ITER_CAP, (int)(o + i), 7);
-    if (bad) tube_fail(A, t, ERR_STATE, (int)(o + i), 8);
-  }
+    for (int k = 0; k < A.nif[tt]; k++) tube_riemann(A, S, (int)tt, k, rs);
 }
 
 // Features of every interface problem of this stage (the states the Riemann
@@ -274,10 +279,11 @@ __device__ __forceinline__ double tube_x(int i, int n, double h) {
   return 0.5 * h + i * h;
 }
 
-__global__ void k_tube_stage(const __grid_constant__ TubeArgs A, const TubeStage S) {
-  extern __shared__ __align__(16) unsigned char tube_smem_raw[];
+// One work item of a stage: cells c0 .. c0+cpb-1 of tube t (all threads of
+// the CTA; barriers inside).
+__device__ __forceinline__ void tube_stage_item(const TubeArgs& A, const TubeStage& S, const TubeSmem& sm, int t,
+                                                int c0) {
   const int cpb = A.cpb;
-  TubeSmem sm = tube_smem(tube_smem_raw, cpb);
   const int NT = blockDim.x, tid = threadIdx.x;
   const int ld = cpb + 4;
   const int where = S.stage * 16;
@@ -286,210 +292,214 @@ __global__ void k_tube_stage(const __grid_constant__ TubeArgs A, const TubeStage
   const double* phin = A.phi[S.cur];
   const double* phin_stage = S.stage == 1 ? phin : A.phis[(S.stage - 2) & 1];
   double* phout = S.final_stage ? A.phi[1 - S.cur] : A.phis[(S.stage - 1) & 1];
-
-  for (int item = blockIdx.x; item < A.nitems; item += gridDim.x) {
-    const int2 it = A.items[item];
-    const int t = it.x, c0 = it.y;
-    const long long o = A.off[t];
-    const int n = (int)(A.off[t + 1] - o);
-    const int ce = min(c0 + cpb, n);
-    const Eos<double>* eos = A.eos + 2 * t;
-    const double dt = A.clock[2 * t + 1];
-    const double bdt = S.bdt_coef * dt;
-    const bool us_clip = S.stage > 1 && A.clip[4 * t + S.stage - 2];
-    const double h = 1.0 / n;
-    __syncthreads();
-    // load cells c0-2 .. c0+cpb+1 (ghost rules: INLET/OUTLET states, phi by ZERO_NEUMANN)
-    for (int j = tid; j < ld; j += NT) {
-      const int i = c0 - 2 + j;
-      double V[5];
-      uint8_t id = 0, real = 0;
-      double ph = 0.0;
-      if (i >= 0 && i < n) {
-        id = A.id[o + i];
-        tube_state(A, S, eos[id], o + i, V);
-        ph = phin_stage[o + i];
-        real = 1;
-      } else if (i == -1 || i == n) {
-        const int img = i < 0 ? 0 : n - 1;
-        id = A.id[o + img];
-        const double* b = i < 0 ? A.bcl + 5 * t : A.bcr + 5 * t;
-        for (int c = 0; c < 5; c++) V[c] = b[c];
-        ph = phin_stage[o + img];
+  const long long o = A.off[t];
+  const int n = (int)(A.off[t + 1] - o);
+  const int ce = min(c0 + cpb, n);
+  const Eos<double>* eos = A.eos + 2 * t;
+  const double dt = A.clock[2 * t + 1];
+  const double bdt = S.bdt_coef * dt;
+  const bool us_clip = S.stage > 1 && A.clip[4 * t + S.stage - 2];
+  const double h = 1.0 / n;
+  __syncthreads();
+  // load cells c0-2 .. c0+cpb+1 (ghost rules: INLET/OUTLET states, phi by ZERO_NEUMANN)
+  for (int j = tid; j < ld; j += NT) {
+    const int i = c0 - 2 + j;
+    double V[5];
+    uint8_t id = 0, real = 0;
+    double ph = 0.0;
+    if (i >= 0 && i < n) {
+      id = A.id[o + i];
+      tube_state(A, S, eos[id], o + i, V);
+      ph = phin_stage[o + i];
+      real = 1;
+    } else if (i == -1 || i == n) {
+      const int img = i < 0 ? 0 : n - 1;
+      id = A.id[o + img];
+      const double* b = i < 0 ? A.bcl + 5 * t : A.bcr + 5 * t;
+      for (int c = 0; c < 5; c++) V[c] = b[c];
+      ph = phin_stage[o + img];
+    } else {
+      for (int c = 0; c < 5; c++) V[c] = 0.0;
+    }
+    for (int c = 0; c < 5; c++) sm.v[c][j] = V[c];
+    sm.ids[j] = id;
+    sm.real[j] = real;
+    sm.ph[j] = ph;
+  }
+  __syncthreads();
+  // slopes and revert chain of real cells c0-1 .. c0+cpb
+  for (int j = 1 + tid; j < ld - 1; j += NT) {
+    if (!sm.real[j]) { sm.mask[j] = 0; continue; }
+    const uint8_t id = sm.ids[j];
+    const Eos<double>& e = eos[id];
+    const bool zx = A.slope_zero && (id != sm.ids[j - 1] || id != sm.ids[j + 1]);
+    double v[5], s[5];
+    for (int c = 0; c < 5; c++) {
+      const double vc = sm.v[c][j];
+      v[c] = vc;
+      s[c] = A.rec_linear ? limited_slope_c(A.limiter, A.limA, A.limiter == LIM_GENMINMOD ? A.limC : A.limB, A.vak,
+                                            A.alpha, vc - sm.v[c][j - 1], sm.v[c][j + 1] - vc)
+                          : 0.0;
+      if (zx) s[c] = 0.0;
+      sm.sg[c][j] = s[c];
+    }
+    // Reconstructor.cpp:719-775 and SpaceOperator.cpp:3240-3277, faces l, r
+    uint8_t m = 0;
+    bool chain = false;
+    for (int q = 0; q < 2; q++) {
+      double f[5];
+      for (int c = 0; c < 5; c++) f[c] = q ? v[c] + 0.5 * s[c] : v[c] - 0.5 * s[c];
+      const bool bad = e.bad(f);
+      bool rev = false;
+      if (!chain && bad) { rev = true; chain = true; }
+      if (!rev && e.needs_clip(f)) rev = true;
+      if (rev) m |= uint8_t(1u << q);
+      else if (bad) tube_fail(A, t, ERR_STATE, (int)(o + c0 - 2 + j), where + 1);
+    }
+    sm.mask[j] = m;
+  }
+  __syncthreads();
+  // faces c0-1/2 .. ce-1/2 (face f: between cells c0+f-1 and c0+f)
+  for (int f = tid; f <= ce - c0; f += NT) {
+    const int jL = f + 1, jR = f + 2;
+    const bool rL = sm.real[jL], rR = sm.real[jR];
+    const uint8_t idL = sm.ids[jL], idR = sm.ids[jR];
+    double VL[5], VR[5], F[5], F2[5];
+    if (rL) {
+      const bool rev = sm.mask[jL] & 2;
+      for (int c = 0; c < 5; c++) VL[c] = rev ? sm.v[c][jL] : sm.v[c][jL] + 0.5 * sm.sg[c][jL];
+    }
+    if (rR) {
+      const bool rev = sm.mask[jR] & 1;
+      for (int c = 0; c < 5; c++) VR[c] = rev ? sm.v[c][jR] : sm.v[c][jR] - 0.5 * sm.sg[c][jR];
+    }
+    if (!rL) {  // INLET ghost face (Reconstructor.cpp:822-833 + clip check)
+      double gc[5];
+      for (int c = 0; c < 5; c++) gc[c] = sm.v[c][jL];
+      ghost_face(BC_INLET, 0, VR, gc, eos[idL], VL);
+    }
+    if (!rR) {  // OUTLET ghost face
+      double gc[5];
+      for (int c = 0; c < 5; c++) gc[c] = sm.v[c][jR];
+      ghost_face(BC_OUTLET, 0, VL, gc, eos[idR], VR);
+    }
+    int err = ERR_NONE;
+    if (rL && rR && idL != idR) {
+      // material interface (SpaceOperator.cpp:2486-2542)
+      double WL[5], WR[5];
+      for (int c = 0; c < 5; c++) { WL[c] = sm.v[c][jL]; WR[c] = sm.v[c][jR]; }
+      if (A.mp_flux == 2) {
+        err = flux_llf2(eos[idL], eos[idR], 0, WL, WR, F);
+        for (int c = 0; c < 5; c++) F2[c] = F[c];
       } else {
-        for (int c = 0; c < 5; c++) V[c] = 0.0;
-      }
-      for (int c = 0; c < 5; c++) sm.v[c][j] = V[c];
-      sm.ids[j] = id;
-      sm.real[j] = real;
-      sm.ph[j] = ph;
-    }
-    __syncthreads();
-    // slopes and revert chain of real cells c0-1 .. c0+cpb
-    for (int j = 1 + tid; j < ld - 1; j += NT) {
-      if (!sm.real[j]) { sm.mask[j] = 0; continue; }
-      const uint8_t id = sm.ids[j];
-      const Eos<double>& e = eos[id];
-      const bool zx = A.slope_zero && (id != sm.ids[j - 1] || id != sm.ids[j + 1]);
-      double v[5], s[5];
-      for (int c = 0; c < 5; c++) {
-        const double vc = sm.v[c][j];
-        v[c] = vc;
-        s[c] = A.rec_linear ? limited_slope_c(A.limiter, A.limA, A.limiter == LIM_GENMINMOD ? A.limC : A.limB, A.vak,
-                                              A.alpha, vc - sm.v[c][j - 1], sm.v[c][j + 1] - vc)
-                            : 0.0;
-        if (zx) s[c] = 0.0;
-        sm.sg[c][j] = s[c];
-      }
-      // Reconstructor.cpp:719-775 and SpaceOperator.cpp:3240-3277, faces l, r
-      uint8_t m = 0;
-      bool chain = false;
-      for (int q = 0; q < 2; q++) {
-        double f[5];
-        for (int c = 0; c < 5; c++) f[c] = q ? v[c] + 0.5 * s[c] : v[c] - 0.5 * s[c];
-        const bool bad = e.bad(f);
-        bool rev = false;
-        if (!chain && bad) { rev = true; chain = true; }
-        if (!rev && e.needs_clip(f)) rev = true;
-        if (rev) m |= uint8_t(1u << q);
-        else if (bad) tube_fail(A, t, ERR_STATE, (int)(o + c0 - 2 + j), where + 1);
-      }
-      sm.mask[j] = m;
-    }
-    __syncthreads();
-    // faces c0-1/2 .. ce-1/2 (face f: between cells c0+f-1 and c0+f)
-    for (int f = tid; f <= ce - c0; f += NT) {
-      const int jL = f + 1, jR = f + 2;
-      const bool rL = sm.real[jL], rR = sm.real[jR];
-      const uint8_t idL = sm.ids[jL], idR = sm.ids[jR];
-      double VL[5], VR[5], F[5], F2[5];
-      if (rL) {
-        const bool rev = sm.mask[jL] & 2;
-        for (int c = 0; c < 5; c++) VL[c] = rev ? sm.v[c][jL] : sm.v[c][jL] + 0.5 * sm.sg[c][jL];
-      }
-      if (rR) {
-        const bool rev = sm.mask[jR] & 1;
-        for (int c = 0; c < 5; c++) VR[c] = rev ? sm.v[c][jR] : sm.v[c][jR] - 0.5 * sm.sg[c][jR];
-      }
-      if (!rL) {  // INLET ghost face (Reconstructor.cpp:822-833 + clip check)
-        double gc[5];
-        for (int c = 0; c < 5; c++) gc[c] = sm.v[c][jL];
-        ghost_face(BC_INLET, 0, VR, gc, eos[idL], VL);
-      }
-      if (!rR) {  // OUTLET ghost face
-        double gc[5];
-        for (int c = 0; c < 5; c++) gc[c] = sm.v[c][jR];
-        ghost_face(BC_OUTLET, 0, VL, gc, eos[idR], VR);
-      }
-      int err = ERR_NONE;
-      if (rL && rR && idL != idR) {
-        // material interface (SpaceOperator.cpp:2486-2542)
-        double WL[5], WR[5];
-        for (int c = 0; c < 5; c++) { WL[c] = sm.v[c][jL]; WR[c] = sm.v[c][jR]; }
-        if (A.mp_flux == 2) {
-          err = flux_llf2(eos[idL], eos[idR], 0, WL, WR, F);
-          for (int c = 0; c < 5; c++) F2[c] = F[c];
+        const int gi = c0 + f;  // tube-local index of the right cell
+        int k = -1;
+        const int nf = A.nif[t];
+        for (int q = 0; q < nf; q++)
+          if (A.iface[t * TUBE_IFACE_CAP + q] == gi) k = q;
+        if (k < 0) {
+          tube_fail(A, t, ERR_STATE, (int)(o + gi), where + 5);
+          for (int c = 0; c < 5; c++) F[c] = F2[c] = 0.0;
         } else {
-          const int gi = c0 + f;  // tube-local index of the right cell
-          int k = -1;
-          const int nf = A.nif[t];
-          for (int q = 0; q < nf; q++)
-            if (A.iface[t * TUBE_IFACE_CAP + q] == gi) k = q;
-          if (k < 0) {
-            tube_fail(A, t, ERR_STATE, (int)(o + gi), where + 5);
-            for (int c = 0; c < 5; c++) F[c] = F2[c] = 0.0;
+          const long long b = ((long long)t * TUBE_IFACE_CAP + k) * 5;
+          if (A.mp_flux == 0) {
+            double Vm[5];
+            for (int c = 0; c < 5; c++) Vm[c] = A.Vmid[b + c];
+            phys_flux(eos[A.midid[t * TUBE_IFACE_CAP + k]], 0, Vm, F);
+            for (int c = 0; c < 5; c++) F2[c] = F[c];
           } else {
-            const long long b = ((long long)t * TUBE_IFACE_CAP + k) * 5;
-            if (A.mp_flux == 0) {
-              double Vm[5];
-              for (int c = 0; c < 5; c++) Vm[c] = A.Vmid[b + c];
-              phys_flux(eos[A.midid[t * TUBE_IFACE_CAP + k]], 0, Vm, F);
-              for (int c = 0; c < 5; c++) F2[c] = F[c];
-            } else {
-              double Sm[5], Sp[5];
-              for (int c = 0; c < 5; c++) { Sm[c] = A.Vsm[b + c]; Sp[c] = A.Vsp[b + c]; }
-              err = num_flux(A.flux, eos[idL], 0, WL, Sm, A.delta, F);
-              if (!err) err = num_flux(A.flux, eos[idR], 0, Sp, WR, A.delta, F2);
-            }
+            double Sm[5], Sp[5];
+            for (int c = 0; c < 5; c++) { Sm[c] = A.Vsm[b + c]; Sp[c] = A.Vsp[b + c]; }
+            err = num_flux(A.flux, eos[idL], 0, WL, Sm, A.delta, F);
+            if (!err) err = num_flux(A.flux, eos[idR], 0, Sp, WR, A.delta, F2);
           }
         }
-      } else {
-        err = num_flux(A.flux, eos[rR ? idR : idL], 0, VL, VR, A.delta, F);
-        for (int c = 0; c < 5; c++) F2[c] = F[c];
       }
-      if (err) tube_fail(A, t, err, (int)(o + c0 + f), where + 2);
-      for (int c = 0; c < 5; c++) { sm.F[c][f] = F[c]; sm.F2[c][f] = F2[c]; }
+    } else {
+      err = num_flux(A.flux, eos[rR ? idR : idL], 0, VL, VR, A.delta, F);
+      for (int c = 0; c < 5; c++) F2[c] = F[c];
     }
-    __syncthreads();
-    // residual, RK update, C2P/clip/check; level-set stage
-    for (int i = c0 + tid; i < ce; i += NT) {
-      const int f = i - c0, j = f + 2;
-      const long long q = o + i;
-      const uint8_t id = sm.ids[j];
-      const Eos<double>& e = eos[id];
-      double Vn[5], Un[5], Unew[5];
-      for (int c = 0; c < 5; c++) Vn[c] = A.V[S.cur][c][q];
-      e.p2c(Vn, Un);
-      double u_ls;
-      if (S.stage == 1) {
-        for (int c = 0; c < 5; c++) Unew[c] = Un[c];
-        u_ls = Vn[1];
-      } else {
-        double Usv[5];
-        for (int c = 0; c < 5; c++) Usv[c] = Us[c][q];
-        const double inv = 1.0 / Usv[0];
-        u_ls = Usv[1] * inv;
-        if (us_clip) {
-          double Vs[5];
-          e.c2p(Usv, Vs);
-          e.clip(Vs);
-          e.p2c(Vs, Usv);
-        }
-        for (int c = 0; c < 5; c++) Unew[c] = S.a_prev * Usv[c] + S.a_un * Un[c];
+    if (err) tube_fail(A, t, err, (int)(o + c0 + f), where + 2);
+    for (int c = 0; c < 5; c++) { sm.F[c][f] = F[c]; sm.F2[c][f] = F2[c]; }
+  }
+  __syncthreads();
+  // residual, RK update, C2P/clip/check; level-set stage
+  for (int i = c0 + tid; i < ce; i += NT) {
+    const int f = i - c0, j = f + 2;
+    const long long q = o + i;
+    const uint8_t id = sm.ids[j];
+    const Eos<double>& e = eos[id];
+    double Vn[5], Un[5], Unew[5];
+    for (int c = 0; c < 5; c++) Vn[c] = A.V[S.cur][c][q];
+    e.p2c(Vn, Un);
+    double u_ls;
+    if (S.stage == 1) {
+      for (int c = 0; c < 5; c++) Unew[c] = Un[c];
+      u_ls = Vn[1];
+    } else {
+      double Usv[5];
+      for (int c = 0; c < 5; c++) Usv[c] = Us[c][q];
+      const double inv = 1.0 / Usv[0];
+      u_ls = Usv[1] * inv;
+      if (us_clip) {
+        double Vs[5];
+        e.c2p(Usv, Vs);
+        e.clip(Vs);
+        e.p2c(Vs, Usv);
       }
-      // residual in the reference's summation order; the y and z faces of a
-      // one-cell-wide grid add exact zeros (SpaceOperator.cpp:3351-3409)
-      const double vol = h * 1.0 * 1.0;
-      const double ax = 1.0 * 1.0;
-      const double inv_mvol = 1.0 / (-vol);
-      for (int c = 0; c < 5; c++) {
-        double fs = 0.0;
-        fs = fs - sm.F2[c][f] * ax;
-        fs = fs + sm.F[c][f + 1] * ax;
-        const double R = fs * inv_mvol;
-        Unew[c] = Unew[c] + bdt * R;
-      }
-      double V[5];
-      e.c2p(Unew, V);
-      if (e.clip(V)) atomicOr(&A.clip[4 * t + S.stage - 1], 1);
-      if (e.bad(V)) tube_fail(A, t, ERR_STATE, (int)q, where + 3);
-      if (S.final_stage) {
-        for (int c = 0; c < 5; c++) A.V[1 - S.cur][c][q] = V[c];
-      } else {
-        for (int c = 0; c < 5; c++) Uo[c][q] = Unew[c];
-      }
-      // level set: -(u dphi/dx) with FD3 (LevelSetOperator.cpp:1066-1140)
-      const double xi = tube_x(i, n, h);
-      const double pc = sm.ph[j];
-      double lo, hi;
-      if (i - 2 >= -1) {
-        double cf[4];
-        taylor4(tube_x(i - 2, n, h) - xi, tube_x(i - 1, n, h) - xi, 0.0, tube_x(i + 1, n, h) - xi, cf);
-        lo = fd4(cf, sm.ph[j - 2], sm.ph[j - 1], pc, sm.ph[j + 1]);
-      } else {
-        lo = (pc - sm.ph[j - 1]) / (xi - tube_x(i - 1, n, h));
-      }
-      if (i + 2 <= n) {
-        double cf[4];
-        taylor4(tube_x(i - 1, n, h) - xi, 0.0, tube_x(i + 1, n, h) - xi, tube_x(i + 2, n, h) - xi, cf);
-        hi = fd4(cf, sm.ph[j - 1], pc, sm.ph[j + 1], sm.ph[j + 2]);
-      } else {
-        hi = (sm.ph[j + 1] - pc) / (tube_x(i + 1, n, h) - xi);
-      }
-      const double rphi = ((u_ls >= 0 ? lo * u_ls : hi * u_ls) + 0.0 + 0.0) * -1.0;
-      const double base = S.stage == 1 ? phin[q] : S.a_prev * phin_stage[q] + S.a_un * phin[q];
-      phout[q] = base + bdt * rphi;
+      for (int c = 0; c < 5; c++) Unew[c] = S.a_prev * Usv[c] + S.a_un * Un[c];
     }
+    // residual in the reference's summation order; the y and z faces of a
+    // one-cell-wide grid add exact zeros (SpaceOperator.cpp:3351-3409)
+    const double vol = h * 1.0 * 1.0;
+    const double ax = 1.0 * 1.0;
+    const double inv_mvol = 1.0 / (-vol);
+    for (int c = 0; c < 5; c++) {
+      double fs = 0.0;
+      fs = fs - sm.F2[c][f] * ax;
+      fs = fs + sm.F[c][f + 1] * ax;
+      const double R = fs * inv_mvol;
+      Unew[c] = Unew[c] + bdt * R;
+    }
+    double V[5];
+    e.c2p(Unew, V);
+    if (e.clip(V)) atomicOr(&A.clip[4 * t + S.stage - 1], 1);
+    if (e.bad(V)) tube_fail(A, t, ERR_STATE, (int)q, where + 3);
+    if (S.final_stage) {
+      for (int c = 0; c < 5; c++) A.V[1 - S.cur][c][q] = V[c];
+    } else {
+      for (int c = 0; c < 5; c++) Uo[c][q] = Unew[c];
+    }
+    // level set: -(u dphi/dx) with FD3 (LevelSetOperator.cpp:1066-1140)
+    const double xi = tube_x(i, n, h);
+    const double pc = sm.ph[j];
+    double lo, hi;
+    if (i - 2 >= -1) {
+      double cf[4];
+      taylor4(tube_x(i - 2, n, h) - xi, tube_x(i - 1, n, h) - xi, 0.0, tube_x(i + 1, n, h) - xi, cf);
+      lo = fd4(cf, sm.ph[j - 2], sm.ph[j - 1], pc, sm.ph[j + 1]);
+    } else {
+      lo = (pc - sm.ph[j - 1]) / (xi - tube_x(i - 1, n, h));
+    }
+    if (i + 2 <= n) {
+      double cf[4];
+      taylor4(tube_x(i - 1, n, h) - xi, 0.0, tube_x(i + 1, n, h) - xi, tube_x(i + 2, n, h) - xi, cf);
+      hi = fd4(cf, sm.ph[j - 1], pc, sm.ph[j + 1], sm.ph[j + 2]);
+    } else {
+      hi = (sm.ph[j + 1] - pc) / (tube_x(i + 1, n, h) - xi);
+    }
+    const double rphi = ((u_ls >= 0 ? lo * u_ls : hi * u_ls) + 0.0 + 0.0) * -1.0;
+    const double base = S.stage == 1 ? phin[q] : S.a_prev * phin_stage[q] + S.a_un * phin[q];
+    phout[q] = base + bdt * rphi;
+  }
+}
+
+__global__ void k_tube_stage(const __grid_constant__ TubeArgs A, const TubeStage S) {
+  extern __shared__ __align__(16) unsigned char tube_smem_raw[];
+  const TubeSmem sm = tube_smem(tube_smem_raw, A.cpb);
+  for (int item = blockIdx.x; item < A.nitems; item += gridDim.x) {
+    const int2 it = A.items[item];
+    tube_stage_item(A, S, sm, it.x, it.y);
   }
 }
 
@@ -546,10 +556,7 @@ __device__ int tube_local_update(const TubeArgs& A, double* const* V, int t, lon
 
 // Material ID from the sign change of phi and the ordered update of cells
 // whose ID changed (MultiPhaseOperator.cpp:127-332, 824-1027); one warp per tube.
-__global__ void k_tube_end(TubeArgs A, int cur_new) {
-  const int lane = threadIdx.x & 31;
-  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (t >= A.ntubes) return;
+__device__ void tube_end(const TubeArgs& A, int t, int cur_new, int lane) {
   const long long o = A.off[t];
   const int n = (int)(A.off[t + 1] - o);
   const double* phnew = A.phi[cur_new];
@@ -591,6 +598,72 @@ __global__ void k_tube_end(TubeArgs A, int cur_new) {
   if (lane == 0 && unresolved) atomicAdd(&A.cnt[3], (unsigned long long)unresolved);
 }
 
+__global__ void k_tube_end(TubeArgs A, int cur_new) {
+  const int lane = threadIdx.x & 31;
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t >= A.ntubes) return;
+  tube_end(A, t, cur_new, lane);
+}
+
+// The whole run in one persistent launch: tubes are independent (each has
+// its own CFL time step), so a CTA takes the next tube from a work counter
+// (tubes ordered longest first) and advances it by nsteps complete steps on
+// its own: warp 0 computes the time step and the interface faces, the
+// interface Riemann problems are solved by one thread each, every thread
+// works on the stage's cell chunks, and warp 0 makes the ID and ordered state
+// update; CTA barriers order the phases. No CTA waits on another. A slow
+// interface solve delays only its own tube.
+__global__ void __launch_bounds__(128) k_tube_run(const __grid_constant__ TubeArgs A, int nsteps, int cur0,
+                                                  int* next, const int* order) {
+  extern __shared__ __align__(16) unsigned char tube_smem_raw[];
+  const TubeSmem sm = tube_smem(tube_smem_raw, A.cpb);
+  __shared__ int tube;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  RiemannSolver rs;
+  rs.P = A.P;
+  if (threadIdx.x < TUBE_IFACE_CAP) {
+    rs.path1.pt = A.scratch + ((long long)blockIdx.x * TUBE_IFACE_CAP + threadIdx.x) * 2 * 3 * RIEMANN_PATH_CAP;
+    rs.path1.cap = RIEMANN_PATH_CAP;
+    rs.path3.pt = rs.path1.pt + 3 * RIEMANN_PATH_CAP;
+    rs.path3.cap = RIEMANN_PATH_CAP;
+  }
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int w = atomicAdd(next, 1);
+      tube = w < A.ntubes ? order[w] : -1;
+    }
+    __syncthreads();
+    const int t = tube;
+    if (t < 0) return;
+    const int n = (int)(A.off[t + 1] - A.off[t]);
+    int cur = cur0;
+    for (int step = 0; step < nsteps; step++) {
+      if (warp == 0) tube_begin(A, t, cur, lane);
+      __syncthreads();
+      for (int st = 1; st <= A.rk; st++) {
+        TubeStage S;
+        S.stage = st;
+        S.final_stage = st == A.rk;
+        S.cur = cur;
+        S.a_prev = 0.0; S.a_un = 1.0; S.bdt_coef = 1.0;
+        if (st > 1) {
+          if (A.rk == 2) { S.a_prev = 0.5; S.a_un = 0.5; S.bdt_coef = 0.5; }
+          else if (st == 2) { S.a_prev = 0.25; S.a_un = 0.75; S.bdt_coef = 0.25; }
+          else { S.a_prev = 2.0 / 3.0; S.a_un = 1.0 / 3.0; S.bdt_coef = 2.0 / 3.0; }
+        }
+        if ((int)threadIdx.x < A.nif[t]) tube_riemann(A, S, t, threadIdx.x, rs);
+        __syncthreads();
+        for (int c0 = 0; c0 < n; c0 += A.cpb) tube_stage_item(A, S, sm, t, c0);
+        __syncthreads();
+      }
+      if (warp == 0) tube_end(A, t, 1 - cur, lane);
+      __syncthreads();
+      cur = 1 - cur;
+    }
+  }
+}
+
 }  // namespace m2c
 
 using namespace m2c;
@@ -624,6 +697,11 @@ struct m2cg_batch {
   int* fvalid = nullptr;
   float* fy = nullptr;
   double* fwarm = nullptr;
+  // one persistent launch per run (use_graph == 2): tubes longest first, the
+  // work counter, and the grid
+  int* run_order = nullptr;
+  int* run_next = nullptr;
+  int run_grid = 0;
 };
 
 static m2cg_status bfail(m2cg_status st, const char* msg) {
@@ -681,6 +759,32 @@ static cudaError_t configure_stage(m2cg_batch* b, int threads, int cpb) {
   b->tuning.cells_per_block = cpb;
   b->tuning.threads_per_block = threads;
   return cudaSuccess;
+}
+
+// The persistent whole-run kernel's grid for the current cells_per_block:
+// resident CTAs of 128 threads, at most one per tube and at most the
+// Riemann scratch's CTA slots.
+static cudaError_t configure_run(m2cg_batch* b) {
+  const size_t smem = tube_smem_bytes(b->A.cpb);
+  cudaError_t e = cudaFuncSetAttribute(k_tube_run, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, nsm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tube_run, 128, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+  b->run_grid = std::min(std::min(per_sm * nsm, b->ntubes), TUBE_RIEMANN_THREADS / TUBE_IFACE_CAP);
+  return cudaSuccess;
+}
+
+// nsteps steps of every tube in one launch of the persistent kernel.
+static cudaError_t enqueue_run(m2cg_batch* b, int nsteps) {
+  cudaError_t e = cudaMemsetAsync(b->run_next, 0, sizeof(int), b->stream);
+  if (e != cudaSuccess) return e;
+  k_tube_run<<<b->run_grid, 128, tube_smem_bytes(b->A.cpb), b->stream>>>(b->A, nsteps, b->cur, b->run_next,
+                                                                         b->run_order);
+  b->cur ^= nsteps & 1;
+  return cudaGetLastError();
 }
 
 // Queue one step starting from state parity `cur`.
@@ -759,51 +863,65 @@ static cudaError_t reset_state(m2cg_batch* b) {
   return e;
 }
 
-// Measured choice of (threads_per_block, cells_per_block): each candidate
-// advances a copy of the initial state by a few steps, the fastest wins, and
-// the state is restored afterwards.
-static cudaError_t autotune(m2cg_batch* b, int fix_threads, int fix_cpb) {
-  const int cand[][2] = {{128, 128}, {128, 256}, {256, 256}, {256, 512}, {128, 512}, {512, 512},
-                         {256, 1024}, {512, 1024}, {64, 128}, {256, 128}};
+// Measured choice of (threads_per_block, cells_per_block, launch mode): each
+// candidate advances a copy of the initial state by a few steps, the fastest
+// wins, and the state is restored afterwards. Modes: 1 = the step sequence as
+// kernels per phase (graph-replayed), 2 = one persistent launch per run
+// (128 threads). fix_mode 0 tries both.
+static cudaError_t autotune(m2cg_batch* b, int fix_threads, int fix_cpb, int fix_mode) {
+  const int cand[][3] = {{128, 128, 1}, {128, 256, 1}, {256, 256, 1}, {256, 512, 1}, {128, 512, 1}, {512, 512, 1},
+                         {256, 1024, 1}, {512, 1024, 1}, {64, 128, 1}, {256, 128, 1},
+                         {128, 256, 2}, {128, 512, 2}, {128, 1024, 2}};
   int maxsm = 0;
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
   float best = 1e30f;
-  int bt = 0, bc = 0;
+  int bt = 0, bc = 0, bm = 0;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaError_t err = cudaSuccess;
   for (auto& c : cand) {
-    const int th = fix_threads ? fix_threads : c[0], cpb = fix_cpb ? fix_cpb : c[1];
+    const int mode = c[2];
+    if (fix_mode && (fix_mode == 2) != (mode == 2)) continue;
+    if (mode == 2 && fix_threads && fix_threads != 128) continue;
+    const int th = mode == 2 ? 128 : (fix_threads ? fix_threads : c[0]), cpb = fix_cpb ? fix_cpb : c[1];
     if (tube_smem_bytes(cpb) > (size_t)maxsm) continue;
-    if (configure_stage(b, th, cpb) != cudaSuccess) {
+    if (configure_stage(b, th, cpb) != cudaSuccess || (mode == 2 && configure_run(b) != cudaSuccess)) {
       cudaGetLastError();
       continue;
     }
     err = reset_state(b);
     if (err != cudaSuccess) break;
-    int cur = 0;
-    enqueue_step(b, cur);  // warm-up
-    cur = 1 - cur;
-    cudaEventRecord(e0, b->stream);
-    for (int k = 0; k < 2; k++) {
-      enqueue_step(b, cur);
+    if (mode == 2) {
+      enqueue_run(b, 1);  // warm-up
+      cudaEventRecord(e0, b->stream);
+      enqueue_run(b, 2);
+    } else {
+      int cur = 0;
+      enqueue_step(b, cur);  // warm-up
       cur = 1 - cur;
+      cudaEventRecord(e0, b->stream);
+      for (int k = 0; k < 2; k++) {
+        enqueue_step(b, cur);
+        cur = 1 - cur;
+      }
     }
     cudaEventRecord(e1, b->stream);
     err = cudaEventSynchronize(e1);
     if (err != cudaSuccess) break;
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best) { best = ms; bt = th; bc = cpb; }
-    if (fix_threads && fix_cpb) break;
+    if (ms < best) { best = ms; bt = th; bc = cpb; bm = mode; }
+    if (fix_threads && fix_cpb && fix_mode) break;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (err != cudaSuccess) return err;
   if (!bt) return cudaErrorInvalidConfiguration;
   err = configure_stage(b, bt, bc);
+  if (err == cudaSuccess && bm == 2) err = configure_run(b);
   if (err == cudaSuccess) err = reset_state(b);
+  if (bm == 2) b->tuning.use_graph = 2;
   return err;
 }
 
@@ -946,11 +1064,25 @@ extern "C" m2cg_status m2cg_batch_create(const m2cg_scheme* scheme, int ntubes, 
     m2cg_batch_destroy(b);
     return bfail(M2CG_ERR_CUDA, cudaGetErrorString(e));
   }
+  // the persistent kernel's tube order (longest first) and work counter
+  {
+    std::vector<int> ord(T);
+    for (int t = 0; t < T; t++) ord[t] = t;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return len[x] > len[y]; });
+    b->run_order = (int*)alloc(sizeof(int) * T);
+    b->run_next = (int*)alloc(sizeof(int));
+    if (!ok) e = cudaErrorMemoryAllocation;
+    if (e == cudaSuccess) e = cudaMemcpy(b->run_order, ord.data(), sizeof(int) * T, cudaMemcpyHostToDevice);
+  }
   const int fix_t = tuning ? tuning->threads_per_block : 0;
   const int fix_c = tuning ? tuning->cells_per_block : 0;
-  b->tuning.use_graph = tuning ? tuning->use_graph : 1;
-  e = autotune(b, fix_t, fix_c);
-  if (e == cudaSuccess && b->tuning.use_graph) e = build_graphs(b);
+  // use_graph: 0 kernels per phase launched directly, 1 the same captured in
+  // graphs, 2 one persistent launch per run; without a tuning both 1 and 2
+  // are measured
+  const int mode = tuning ? tuning->use_graph : -1;
+  b->tuning.use_graph = mode < 0 ? 1 : mode;
+  if (e == cudaSuccess) e = autotune(b, fix_t, fix_c, mode < 0 ? 0 : (mode == 2 ? 2 : 1));
+  if (e == cudaSuccess && b->tuning.use_graph == 1) e = build_graphs(b);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) {
     char msg[200];
@@ -981,7 +1113,9 @@ extern "C" m2cg_status m2cg_batch_run(m2cg_batch* b, int nsteps) {
   if (!b || nsteps < 0) return bfail(M2CG_ERR_ARG, "bad argument");
   int left = nsteps;
   cudaError_t e = cudaSuccess;
-  if (b->tuning.use_graph) {
+  if (b->tuning.use_graph == 2) {
+    if (nsteps > 0) e = enqueue_run(b, nsteps);
+  } else if (b->tuning.use_graph) {
     if (left > 0 && b->cur == 1) {
       e = cudaGraphLaunch(b->graph[1], b->stream);
       b->cur = 0;
@@ -1004,7 +1138,7 @@ extern "C" m2cg_status m2cg_batch_run(m2cg_batch* b, int nsteps) {
   }
   if (e != cudaSuccess) return bfail(M2CG_ERR_CUDA, cudaGetErrorString(e));
   b->steps += nsteps;
-  b->launches += (long long)nsteps * (2 + (b->mlp ? 5 : 2) * b->scheme.rk_order);
+  b->launches += b->tuning.use_graph == 2 ? 1 : (long long)nsteps * (2 + (b->mlp ? 5 : 2) * b->scheme.rk_order);
   return batch_check(b);
 }
 
@@ -1075,7 +1209,9 @@ extern "C" m2cg_status m2cg_batch_time_steps(m2cg_batch* b, int nsteps, float* m
   // same launch sequence as m2cg_batch_run, without the per-call error check
   int left = nsteps;
   cudaError_t e = cudaSuccess;
-  if (b->tuning.use_graph) {
+  if (b->tuning.use_graph == 2) {
+    if (nsteps > 0) e = enqueue_run(b, nsteps);
+  } else if (b->tuning.use_graph) {
     if (left > 0 && b->cur == 1) { e = cudaGraphLaunch(b->graph[1], b->stream); b->cur = 0; left--; }
     while (e == cudaSuccess && left >= 2) { e = cudaGraphLaunch(b->graph[2], b->stream); left -= 2; }
     if (e == cudaSuccess && left == 1) { e = cudaGraphLaunch(b->graph[0], b->stream); b->cur = 1; }
@@ -1089,7 +1225,7 @@ extern "C" m2cg_status m2cg_batch_time_steps(m2cg_batch* b, int nsteps, float* m
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->steps += nsteps;
-  b->launches += (long long)nsteps * (2 + (b->mlp ? 5 : 2) * b->scheme.rk_order);
+  b->launches += b->tuning.use_graph == 2 ? 1 : (long long)nsteps * (2 + (b->mlp ? 5 : 2) * b->scheme.rk_order);
   if (st) return st;
   return batch_check(b);
 }
@@ -1108,7 +1244,14 @@ extern "C" m2cg_status m2cg_batch_set_mlp(m2cg_batch* b, const m2cg_mlp* m) {
   }
   b->mlp = m;
   b->A.warm = m ? b->fwarm : nullptr;
-  if (b->tuning.use_graph) {
+  // the network's inference runs over all tubes between phases, which the
+  // persistent whole-run kernel does not have: use the graph-replayed steps
+  if (m && b->tuning.use_graph == 2) {
+    cudaError_t e = configure_stage(b, 128, b->A.cpb);
+    if (e != cudaSuccess) return bfail(M2CG_ERR_CUDA, cudaGetErrorString(e));
+    b->tuning.use_graph = 1;
+  }
+  if (b->tuning.use_graph == 1) {
     cudaError_t e = build_graphs(b);
     if (e != cudaSuccess) return bfail(M2CG_ERR_CUDA, cudaGetErrorString(e));
   }

@@ -270,7 +270,7 @@ class Batch:
     INLET/OUTLET ghosts holding those states. Each tube is what one reference
     run of the same setup computes (TimeIntegratorRK2/RK3, MultiPhaseOperator)."""
 
-    def __init__(self, s, lens, mats, VL, VR, cells_per_block=0, threads_per_block=0, use_graph=1):
+    def __init__(self, s, lens, mats, VL, VR, cells_per_block=0, threads_per_block=0, use_graph=-1):
         L = lib()
         self.lens = np.ascontiguousarray(lens, np.int32)
         self.ntubes = len(self.lens)

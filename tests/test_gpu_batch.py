@@ -90,12 +90,15 @@ def test_batch_matches_3d_path(gpu):
 
 
 def test_batch_tunings_agree(gpu):
-    """Autotuned, fixed-shape, graph and direct-launch runs give the same bits."""
+    """Autotuned, fixed-shape, graph, direct-launch and persistent whole-run
+    (one launch advancing each tube through all its steps) runs give the
+    same bits."""
     lens, mats, VL, VR = _batch_case(seed=9)
     s = cases.tube_scheme()
     outs = []
     for kw in (dict(), dict(cells_per_block=128, threads_per_block=128), dict(cells_per_block=512,
-               threads_per_block=256, use_graph=0)):
+               threads_per_block=256, use_graph=0), dict(cells_per_block=256, threads_per_block=128, use_graph=2),
+               dict(cells_per_block=1024, threads_per_block=128, use_graph=2)):
         b = gpu.Batch(s, lens, mats, VL, VR, **kw)
         b.run(7)  # odd count: exercises the single-step graph
         b.run(4)
