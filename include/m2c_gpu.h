@@ -133,7 +133,9 @@ typedef struct {
   int reinit_maxits;
   double reinit_cfl;
   double reinit_tol;
-  int reinit_first_layer; /* 0 FIXED (only FIXED is implemented) */
+  int reinit_first_layer; /* firstLayerTreatment: 0 FIXED, 1 CONSTRAINED1 (CR-1), 2 CONSTRAINED2
+                             (CR-2), 3 ITERATIVE_CONSTRAINED1 (HCR-1), 4 ITERATIVE_CONSTRAINED2
+                             (HCR-2) */
   int solver;             /* M2CG_LS_FINITE_DIFFERENCE (default) or M2CG_LS_FINITE_VOLUME */
   int flux;               /* finite volume: M2CG_LSFLUX_*, default ROE */
   double delta;           /* finite volume: entropy-fix coefficient of the ROE flux (0.2) */

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -461,7 +462,11 @@ void levelset_pack(cudaStream_t s, const Grid3& g, const LsGeom& geo, const doub
 
 // --------------------------------------------------------------------------
 // Reinitialisation (LevelSetReinitializer::ReinitializeFullDomain,
-// LevelSetReinitializer.cpp:74-171) with the FIXED first-layer treatment:
+// LevelSetReinitializer.cpp:74-171) with every first-layer treatment: FIXED,
+// CONSTRAINED1/2 (CR-1/2: the first layer reset once from |grad phi| and a
+// curvature-selected correction set, 643-865) and ITERATIVE_CONSTRAINED1/2
+// (HCR-1/2: the first layer left free and pulled back after every
+// iteration, 1357-1450). The FIXED sequence:
 //   tag the first layer (a face neighbour with phi*phi_nb <= 0, 297-428),
 //   smoothed sign S = phi / sqrt(phi^2 + min(dx,dy,dz)^2) (594-615),
 //   pseudo-time SSP-RK3 of R = -dt S (|grad phi|_Godunov - 1) with the first
@@ -469,30 +474,40 @@ void levelset_pack(cudaStream_t s, const Grid3& g, const LsGeom& geo, const doub
 //   relative change drops below the tolerance; on failure the CFL number is
 //   divided by 1.5 and the iteration restarts from the saved phi (154-169).
 // --------------------------------------------------------------------------
+// first-layer treatments (LevelSetReinitializationData::FirstLayerTreatment)
+enum { FL_FIXED = 0, FL_CR1 = 1, FL_CR2 = 2, FL_HCR1 = 3, FL_HCR2 = 4 };
+
 struct ReinitBuf {
   double* phi1;
   double* phi2;
   double* sign;
   double* phibk;
+  double* fc;               // [n] first-layer corrections (treatments other than FIXED)
+  double* nrm[3];           // [n] unit normals (CR-1/2)
   uint8_t* tag;
   unsigned long long* red;  // [0] max residual bits, [1] max rel. change bits, [2] first-layer count,
                             // [3] converged on the residual (this iteration), [4] attempt finished,
                             // [5] iterations of the attempt, [6] last max rel. change bits
 };
 
-static ReinitBuf carve(double* base, long long n) {
+static int reinit_arrays(int first_layer) { return first_layer == FL_FIXED ? 4 : 8; }
+
+static ReinitBuf carve(double* base, long long n, int first_layer) {
   ReinitBuf b;
+  const int na = reinit_arrays(first_layer);
   b.phi1 = base;
   b.phi2 = base + n;
   b.sign = base + 2 * n;
   b.phibk = base + 3 * n;
-  b.red = (unsigned long long*)(base + 4 * n);
-  b.tag = (uint8_t*)(base + 4 * n + 8);
+  b.fc = na > 4 ? base + 4 * n : nullptr;
+  for (int a = 0; a < 3; a++) b.nrm[a] = na > 4 ? base + (5 + a) * n : nullptr;
+  b.red = (unsigned long long*)(base + na * n);
+  b.tag = (uint8_t*)(base + na * n + 8);
   return b;
 }
 
-m2cg_status reinit_alloc(long long ncell, double** buf) {
-  size_t bytes = (size_t)(4 * ncell + 8) * 8 + (size_t)ncell + 64;
+m2cg_status reinit_alloc(long long ncell, int first_layer, double** buf) {
+  size_t bytes = (size_t)(reinit_arrays(first_layer) * ncell + 8) * 8 + (size_t)ncell + 64;
   if (cudaMalloc((void**)buf, bytes) != cudaSuccess) return M2CG_ERR_NOMEM;
   return M2CG_OK;
 }
@@ -557,14 +572,16 @@ __device__ __forceinline__ double reinit_local(const Grid3& g, const LsGeom& geo
 // Thread (x, y) of CTA (bx, by, bz) owns cell (32 bx + x, 8 by + y, bz): no
 // index division, rows of 32 consecutive cells per warp.
 __global__ void __launch_bounds__(256) k_reinit_stage(Grid3 g, LsGeom geo, ReinitBuf b, int stage, double cfl,
-                                                      double tol, const double* in, double* phi, double* out) {
+                                                      double tol, const double* in, double* phi, double* out,
+                                                      int fix_first) {
   if (b.red[4] || (stage > 1 && b.red[3])) return;  // attempt finished, or converged on the residual in stage 1
   double maxres = 0.0, maxrel = 0.0;
   const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
   for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
     const long long off = loff(g, i, j, k);
     double R = 0.0;
-    if (!b.tag[off]) {
+    const bool tagged = b.tag[off] != 0;
+    if (!tagged || !fix_first) {  // the first layer is held fixed except under HCR-1/2 (967-985)
       const double dx = smin(g.dx[i], smin(g.dy[j], g.dz[k]));
       const double dt = cfl * dx;
       double lr;
@@ -573,7 +590,7 @@ __global__ void __launch_bounds__(256) k_reinit_stage(Grid3 g, LsGeom geo, Reini
         R = -dt * b.sign[off] * lr;
       else
         R = -dt * b.sign[off] * lr / fabs(lr);
-      maxres = smax(maxres, fabs(lr));
+      if (!tagged) maxres = smax(maxres, fabs(lr));  // the max residual leaves out the first layer
     }
     if (stage == 1) {
       out[off] = in[off] + R;
@@ -585,9 +602,13 @@ __global__ void __launch_bounds__(256) k_reinit_stage(Grid3 g, LsGeom geo, Reini
       double t = 1.0 / 3.0 * old + 2.0 / 3.0 * in[off];
       const double nw = t + 2.0 / 3.0 * R;
       phi[off] = nw;
-      double le = fabs(nw - old);
-      if (nw != 0) le /= fabs(nw);
-      maxrel = smax(maxrel, le);
+      if (tagged && !fix_first) {
+        out[off] = old;  // HCR: the first layer's change is measured after its correction
+      } else {
+        double le = fabs(nw - old);
+        if (nw != 0) le /= fabs(nw);
+        maxrel = smax(maxrel, le);
+      }
     }
   }
   // maxima over the CTA (warp shuffles, then its 8 warps), one atomic per CTA:
@@ -642,6 +663,283 @@ __global__ void k_reinit_end(ReinitBuf b, double tol) {
   b.red[0] = b.red[1] = b.red[3] = 0;
 }
 
+// ---- first-layer treatments (LevelSetReinitializer.cpp:297-428, 643-952, 1129-1241, 1357-1450) ----
+
+// LevelSetReinitializer::CentralDifferenceLocal (LevelSetReinitializer.h:123-128)
+__device__ __forceinline__ double central_local(double p0, double p1, double p2, double x0, double x1, double x2) {
+  const double c0 = -(x2 - x1) / ((x1 - x0) * (x2 - x0));
+  const double c1 = 1.0 / (x1 - x0) - 1.0 / (x2 - x1);
+  const double c2 = (x1 - x0) / ((x2 - x0) * (x2 - x1));
+  return c0 * p0 + c1 * p1 + c2 * p2;
+}
+
+// Tag of node c (interior: the tag array; face ghost: the reference tags its
+// ghost layer with the same test, TagFirstLayerNodes 309-372, where the
+// unpopulated edge ghosts it reaches read as zero).
+__device__ double fl_tag(const Grid3& g, const LsGeom& geo, const double* phi0, const ReinitBuf& b, int i, int j,
+                         int k) {
+  const int c[3] = {i, j, k}, n[3] = {g.nx, g.ny, g.nz};
+  int out = 0;
+  for (int a = 0; a < 3; a++) out += (c[a] < 0 || c[a] >= n[a]) && g.bc[2 * a] != BC_PERIODIC;
+  if (out == 0) return b.tag[loff(g, (i + g.nx) % g.nx, (j + g.ny) % g.ny, (k + g.nz) % g.nz)];
+  if (out > 1) return 0.0;
+  const double p = phi_at(g, geo, phi0, i, j, k);
+  for (int q = 0; q < 6; q++) {
+    int d[3] = {i, j, k};
+    d[q >> 1] += (q & 1) ? 1 : -1;
+    int dout = 0, beyond = 0;
+    for (int a = 0; a < 3; a++) {
+      const bool o = (d[a] < 0 || d[a] >= n[a]) && g.bc[2 * a] != BC_PERIODIC;
+      dout += o;
+      beyond += d[a] < -1 || d[a] > n[a];
+    }
+    if (beyond) continue;                      // outside the ghosted range
+    const double pn = dout > 1 ? 0.0 : phi_at(g, geo, phi0, d[0], d[1], d[2]);
+    if (p * pn <= 0) return 1.0;
+  }
+  return 0.0;
+}
+
+// DifferentiateInFirstLayer (899-951): one-sided, central or zero derivative
+// at a first-layer node from the tagged neighbours.
+__device__ double fl_diff(double x0, double x1, double x2, double tag0, double tag2, double phi0, double phi1,
+                          double phi2, double phi00, double phi3, double eps) {
+  bool u0 = tag0 != 0, u2 = tag2 != 0;
+  if (!u0 && !u2) return 0.0;
+  const double dphi0 = phi1 - phi0, dphi1 = phi2 - phi1;
+  const bool condB = dphi0 * dphi1 < 0 || phi0 * phi00 < 0 || phi2 * phi3 < 0;
+  if (condB) {
+    if (u0 && (phi0 * phi2 < 0) && fabs(dphi0 + eps) < fabs(dphi1)) u0 = false;
+    if (u2 && (phi0 * phi2 < 0) && fabs(dphi1 + eps) < fabs(dphi0)) u2 = false;
+  }
+  if (!u0 && !u2) return 0.0;
+  if (u0) return u2 ? central_local(phi0, phi1, phi2, x0, x1, x2) : (phi1 - phi0) / (x1 - x0);
+  return (phi2 - phi1) / (x2 - x1);
+}
+
+// CR-1/2 step 1 (ReinitializeFirstLayerNodes 660-706): phi = phig / |grad phig|
+// at every first-layer node, its unit normal kept. phig (b.phi2) is the level
+// set at the start of the reinitialisation.
+__global__ void k_fl_rescale(Grid3 g, LsGeom geo, ReinitBuf b, double* phi) {
+  const double* pg = b.phi2;
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
+    const long long off = loff(g, i, j, k);
+    if (!b.tag[off]) continue;
+    const double* X = geo.xg[0];
+    const double* Y = geo.xg[1];
+    const double* Z = geo.xg[2];
+    auto P = [&](int a, int bb, int c) { return phi_at(g, geo, pg, a, bb, c); };
+    auto Tg = [&](int a, int bb, int c) { return fl_tag(g, geo, pg, b, a, bb, c); };
+    double gr[3];
+    gr[0] = fl_diff(X[i], X[i + 1], X[i + 2], Tg(i - 1, j, k), Tg(i + 1, j, k), P(i - 1, j, k), pg[off],
+                    P(i + 1, j, k), i - 2 >= -1 ? P(i - 2, j, k) : P(i - 1, j, k),
+                    i + 2 <= g.nx ? P(i + 2, j, k) : P(i + 1, j, k), 1.0e-3 * g.dx[i]);
+    // (the reference reads j+2 in both branches of its y test; beyond the
+    // ghost layer that is the ghost here)
+    gr[1] = fl_diff(Y[j], Y[j + 1], Y[j + 2], Tg(i, j - 1, k), Tg(i, j + 1, k), P(i, j - 1, k), pg[off],
+                    P(i, j + 1, k), j - 2 >= -1 ? P(i, j - 2, k) : P(i, j - 1, k),
+                    P(i, j + 2 <= g.ny ? j + 2 : g.ny, k), 1.0e-3 * g.dy[j]);
+    gr[2] = fl_diff(Z[k], Z[k + 1], Z[k + 2], Tg(i, j, k - 1), Tg(i, j, k + 1), P(i, j, k - 1), pg[off],
+                    P(i, j, k + 1), k - 2 >= -1 ? P(i, j, k - 2) : P(i, j, k - 1),
+                    k + 2 <= g.nz ? P(i, j, k + 2) : P(i, j, k + 1), 1.0e-3 * g.dz[k]);
+    const double nrm = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+    for (int a = 0; a < 3; a++) b.nrm[a][off] = gr[a] / nrm;
+    phi[off] = nrm == 0 ? pg[off] : pg[off] / nrm;
+  }
+}
+
+// CR-1/2: unit normal of phi beyond the first layer
+// (ComputeNormalDirectionBeyondFirstLayer 1209-1230); the domain's ghost
+// layer still holds the values of the level set before the rescaling.
+__global__ void k_fl_normal(Grid3 g, LsGeom geo, ReinitBuf b, const double* phi) {
+  const double* pg = b.phi2;
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
+    const long long off = loff(g, i, j, k);
+    if (b.tag[off]) continue;
+    auto P = [&](int a, int bb, int c) {
+      const bool in = a >= 0 && a < g.nx && bb >= 0 && bb < g.ny && c >= 0 && c < g.nz;
+      return in ? phi[loff(g, a, bb, c)] : phi_at(g, geo, pg, a, bb, c);
+    };
+    const double* X = geo.xg[0];
+    const double* Y = geo.xg[1];
+    const double* Z = geo.xg[2];
+    double v[3];
+    v[0] = central_local(P(i - 1, j, k), phi[off], P(i + 1, j, k), X[i], X[i + 1], X[i + 2]);
+    v[1] = central_local(P(i, j - 1, k), phi[off], P(i, j + 1, k), Y[j], Y[j + 1], Y[j + 2]);
+    v[2] = central_local(P(i, j, k - 1), phi[off], P(i, j, k + 1), Z[k], Z[k + 1], Z[k + 2]);
+    const double m = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (m != 0.0) {
+      const double inv = 1.0 / m;  // Vec3D::operator/=
+      for (int a = 0; a < 3; a++) v[a] *= inv;
+    }
+    for (int a = 0; a < 3; a++) b.nrm[a][off] = v[a];
+  }
+}
+
+// The opposite-side neighbours S of a first-layer node (TagFirstLayerNodes
+// 376-414, from the level set at the start: phig * phig_nb < 0).
+__device__ __forceinline__ int fl_set(const Grid3& g, const LsGeom& geo, const double* pg, int i, int j, int k,
+                                      double* nb) {
+  const double p = pg[loff(g, i, j, k)];
+  int s = 0;
+  for (int q = 0; q < 6; q++) {
+    int d[3] = {i, j, k};
+    d[q >> 1] += (q & 1) ? 1 : -1;
+    nb[q] = phi_at(g, geo, pg, d[0], d[1], d[2]);
+    if (p * nb[q] < 0) s |= 1 << q;
+  }
+  return s;
+}
+
+// CR-1/2 steps 2-3 (721-841): curvature of the normal field selects the
+// correction set; its nodes get the averaged ratio of the rescaled to the
+// original level set of their opposite-side neighbours. Writes the new value
+// (or DBL_MAX: unchanged) into fc; k_fl_apply copies it.
+__global__ void k_fl_correct(Grid3 g, LsGeom geo, ReinitBuf b, const double* phi, int mode) {
+  const double* pg = b.phi2;
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
+    const long long off = loff(g, i, j, k);
+    if (!b.tag[off]) continue;
+    const double* X = geo.xg[0];
+    const double* Y = geo.xg[1];
+    const double* Z = geo.xg[2];
+    const int c[3] = {i, j, k}, n[3] = {g.nx, g.ny, g.nz};
+    const double* xs[3] = {X, Y, Z};
+    double curv = 0.0;
+    for (int a = 0; a < 3; a++) {
+      int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+      lo[a]--; hi[a]++;
+      const double* N = b.nrm[a];
+      const double* x = xs[a];
+      const bool hl = c[a] - 1 >= 0, hh = c[a] + 1 < n[a];
+      double ca;
+      if (hl && hh)
+        ca = central_local(N[loff(g, lo[0], lo[1], lo[2])], N[off], N[loff(g, hi[0], hi[1], hi[2])], x[c[a]],
+                           x[c[a] + 1], x[c[a] + 2]);
+      else if (hl)
+        ca = (N[off] - N[loff(g, lo[0], lo[1], lo[2])]) / (x[c[a] + 1] - x[c[a]]);
+      else if (hh)
+        ca = (N[loff(g, hi[0], hi[1], hi[2])] - N[off]) / (x[c[a] + 2] - x[c[a] + 1]);
+      else
+        ca = 0.0;
+      curv = a == 0 ? ca : curv + ca;
+    }
+    const double p0 = pg[off];
+    if (!(curv * p0 < 0 || (curv == 0.0 && p0 < 0))) {
+      b.fc[off] = DBL_MAX;
+      continue;
+    }
+    double nbg[6];
+    const int sset = fl_set(g, geo, pg, i, j, k, nbg);
+    auto Pc = [&](int q) {  // the rescaled level set at neighbour q (ghosts: not rescaled)
+      int d[3] = {i, j, k};
+      d[q >> 1] += (q & 1) ? 1 : -1;
+      const bool in = d[0] >= 0 && d[0] < g.nx && d[1] >= 0 && d[1] < g.ny && d[2] >= 0 && d[2] < g.nz;
+      return in ? phi[loff(g, d[0], d[1], d[2])] : phi_at(g, geo, pg, d[0], d[1], d[2]);
+    };
+    double f = 0.0;
+    if (mode == FL_CR1) {
+      double sum = 0.0;
+      int ns = 0;
+      for (int q = 0; q < 6; q++)
+        if (sset & (1 << q)) { sum += Pc(q) / nbg[q]; ns++; }
+      f = ns != 0 ? p0 * sum / (double)ns : 0.0;
+    } else {
+      double s1 = 0.0, s2 = 0.0;
+      for (int q = 0; q < 6; q++)
+        if (sset & (1 << q)) { s1 += Pc(q); s2 += nbg[q]; }
+      f = s2 != 0 ? p0 * s1 / s2 : 0.0;
+    }
+    b.fc[off] = f;
+  }
+}
+
+__global__ void k_fl_apply(Grid3 g, ReinitBuf b, double* phi) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
+    const long long off = loff(g, i, j, k);
+    if (b.tag[off] && b.fc[off] != DBL_MAX) phi[off] = b.fc[off];
+  }
+}
+
+// HCR-1/2 (ApplyCorrectionToFirstLayerNodes 1357-1450), after every
+// iteration: a first-layer node all of whose opposite-side neighbours are
+// still on the other side is pulled towards the value the original ratios
+// give: F = (sum r_a phi_a / |S| - phi) (HCR-1) or (r0 sum phi_a - phi)
+// (HCR-2), over max(dx,dy,dz); then phi += dt beta F (beta 1/2), with the
+// relative change of these nodes joining the iteration's maximum.
+__global__ void k_hcr_force(Grid3 g, LsGeom geo, ReinitBuf b, const double* phi, int mode) {
+  if (b.red[4] || b.red[3]) return;
+  const double* pg = b.phibk;  // the level set at the start (HCR has no rescaling step)
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
+    const long long off = loff(g, i, j, k);
+    if (!b.tag[off]) continue;
+    double nbg[6];
+    const int sset = fl_set(g, geo, pg, i, j, k, nbg);
+    const double p = phi[off], p0g = pg[off];
+    double cur[6];
+    bool in_c = true;
+    int ns = 0;
+    double sumg = 0.0;
+    for (int q = 0; q < 6; q++) {
+      int d[3] = {i, j, k};
+      d[q >> 1] += (q & 1) ? 1 : -1;
+      cur[q] = phi_at(g, geo, phi, d[0], d[1], d[2]);
+      if (sset & (1 << q)) {
+        ns++;
+        sumg += nbg[q];
+        if (p * cur[q] >= 0) in_c = false;
+      }
+    }
+    double f = 0.0;
+    if (in_c) {
+      if (mode == FL_HCR1) {
+        double sum = 0.0;
+        for (int q = 0; q < 6; q++)
+          if (sset & (1 << q)) sum += (p0g / nbg[q]) * cur[q];
+        f = ns != 0 ? sum / (double)ns - p : 0.0 - p;
+      } else {
+        const double r0 = sumg != 0 ? p0g / sumg : 0.0;
+        double sum = 0.0;
+        for (int q = 0; q < 6; q++)
+          if (sset & (1 << q)) sum += cur[q];
+        f = r0 * sum - p;
+      }
+      f /= smax(g.dx[i], smax(g.dy[j], g.dz[k]));
+    }
+    b.fc[off] = f;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_hcr_apply(Grid3 g, ReinitBuf b, double* phi, double cfl) {
+  if (b.red[4] || b.red[3]) return;
+  double maxrel = 0.0;
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
+  for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
+    const long long off = loff(g, i, j, k);
+    if (!b.tag[off]) continue;
+    const double dt = cfl * smin(g.dx[i], smin(g.dy[j], g.dz[k]));
+    const double nw = phi[off] + dt * 0.5 * b.fc[off];
+    phi[off] = nw;
+    const double old = b.phi1[off];  // the value at the start of the iteration (kept by stage 3)
+    double le = fabs(nw - old);
+    if (nw != 0) le /= fabs(nw);
+    maxrel = smax(maxrel, le);
+  }
+  for (int o = 16; o > 0; o >>= 1) maxrel = smax(maxrel, __shfl_xor_sync(0xffffffffu, maxrel, o));
+  __shared__ double wrel[8];
+  if (threadIdx.x == 0) wrel[threadIdx.y] = maxrel;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int w = 1; w < 8; w++) maxrel = smax(maxrel, wrel[w]);
+    if (maxrel > 0) atomicMax(&b.red[1], (unsigned long long)__double_as_longlong(maxrel));
+  }
+}
+
 static double bits_to_double(unsigned long long u) {
   double d;
   memcpy(&d, &u, 8);
@@ -652,13 +950,26 @@ m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& 
                                   double* phi, double* buf, DevError* err, double* cfl_state, int* iterations) {
   (void)err;
   const long long n = g.plane * g.nz;
-  ReinitBuf b = carve(buf, n);
+  const int fl = ls.reinit_first_layer;
+  ReinitBuf b = carve(buf, n, fl);
   const long long ni = (long long)g.nx * g.ny * g.nz;
   const int grid = grid1d(ni);
   // each CTA walks a column of planes (k = bz, bz + 64, ...)
   const dim3 grid3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 64 ? g.nz : 64), block3(32, 8);
   cudaMemsetAsync(b.red, 0, 8 * sizeof(unsigned long long), s);
   k_reinit_prep<<<grid, 256, 0, s>>>(g, geo, phi, b);
+  if (fl == FL_CR1 || fl == FL_CR2) {
+    // ReinitializeFullDomain step 2 (86-92): rescale and correct the first
+    // layer once (phig = the level set at the start, kept in phi2), then the
+    // retry backup is the corrected level set (96)
+    cudaMemcpyAsync(b.phi2, phi, n * 8, cudaMemcpyDeviceToDevice, s);
+    k_fl_rescale<<<grid3, block3, 0, s>>>(g, geo, b, phi);
+    k_fl_normal<<<grid3, block3, 0, s>>>(g, geo, b, phi);
+    k_fl_correct<<<grid3, block3, 0, s>>>(g, geo, b, phi, fl);
+    k_fl_apply<<<grid3, block3, 0, s>>>(g, b, phi);
+    cudaMemcpyAsync(b.phibk, phi, n * 8, cudaMemcpyDeviceToDevice, s);
+  }
+  const int fix_first = fl == FL_HCR1 || fl == FL_HCR2 ? 0 : 1;
   const double tol = ls.reinit_tol;
   const int maxIts = ls.reinit_maxits;
   // Each attempt queues all its iterations at once; the iterations after
@@ -668,10 +979,14 @@ m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& 
     const double cfl = *cfl_state;
     k_reinit_begin<<<1, 1, 0, s>>>(b);
     for (int iter = 0; iter < maxIts; iter++) {
-      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 1, cfl, tol, phi, phi, b.phi1);
+      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 1, cfl, tol, phi, phi, b.phi1, fix_first);
       k_reinit_check<<<1, 1, 0, s>>>(b, tol);
-      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 2, cfl, tol, b.phi1, phi, b.phi2);
-      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 3, cfl, tol, b.phi2, phi, phi);
+      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 2, cfl, tol, b.phi1, phi, b.phi2, fix_first);
+      k_reinit_stage<<<grid3, block3, 0, s>>>(g, geo, b, 3, cfl, tol, b.phi2, phi, b.phi1, fix_first);
+      if (!fix_first) {  // HCR-1/2 after every iteration (142, 1357-1450)
+        k_hcr_force<<<grid3, block3, 0, s>>>(g, geo, b, phi, fl);
+        k_hcr_apply<<<grid3, block3, 0, s>>>(g, b, phi, cfl);
+      }
       k_reinit_end<<<1, 1, 0, s>>>(b, tol);
     }
     unsigned long long hred[8];

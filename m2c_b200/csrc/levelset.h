@@ -42,7 +42,9 @@ void levelset_pack(cudaStream_t s, const Grid3& g, const LsGeom& geo, const doub
 // (stage 1: out = phi_n + dt*R).
 m2cg_status levelset_stage(cudaStream_t s, const Grid3& g, const SchemeK& sk, const LsGeom& geo, const StageArgs& a,
                            const double* in, const double* phin, double* out);
-m2cg_status reinit_alloc(long long ncell, double** buf);
+// first_layer: LevelSetReinitializationData::firstLayerTreatment (the
+// treatments other than FIXED need per-cell correction and normal arrays).
+m2cg_status reinit_alloc(long long ncell, int first_layer, double** buf);
 // cfl_state: the pseudo-time CFL number, reduced in place on a failed attempt
 // and kept for later calls (as LevelSetReinitializer::cfl is).
 m2cg_status levelset_reinitialize(cudaStream_t s, const Grid3& g, const LsGeom& geo, const m2cg_levelset& ls,

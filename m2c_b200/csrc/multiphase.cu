@@ -771,7 +771,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   if (scheme.mp_recon != 0) return M2CG_ERR_UNSUPPORTED;  // interface Riemann inputs: constant recon
   if (scheme.mp_phasechange_type != 0 && scheme.mp_phasechange_type != 1) return M2CG_ERR_UNSUPPORTED;
   if (ls.material_id != 1) return M2CG_ERR_UNSUPPORTED;
-  if (ls.reinit_first_layer != 0) return M2CG_ERR_UNSUPPORTED;
+  if (ls.reinit_first_layer < 0 || ls.reinit_first_layer > 4) return M2CG_ERR_ARG;
   if (ls.solver != M2CG_LS_FINITE_VOLUME && ls.solver != M2CG_LS_FINITE_DIFFERENCE) return M2CG_ERR_ARG;
   if (ls.solver == M2CG_LS_FINITE_VOLUME &&
       (ls.flux < 0 || ls.flux > 2 || ls.rec_type < 0 || ls.rec_type > 1 || ls.limiter < 0 || ls.limiter > 2))
@@ -840,7 +840,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
     multiphase_destroy(mp);
     return M2CG_ERR_NOMEM;
   }
-  if (ls.reinit_frequency > 0 && reinit_alloc(mp->ncell, &mp->reinit_buf) != M2CG_OK) {
+  if (ls.reinit_frequency > 0 && reinit_alloc(mp->ncell, ls.reinit_first_layer, &mp->reinit_buf) != M2CG_OK) {
     multiphase_destroy(mp);
     return M2CG_ERR_NOMEM;
   }

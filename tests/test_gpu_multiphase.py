@@ -336,3 +336,31 @@ def test_bubble_on_stretched_mesh_matches_reference(gpu, ref):
     assert np.array_equal(inner(IDg), inner(IDr))
     assert rel_err(inner(Vg), inner(Vr)) <= TOL
     assert rel_err(inner(Pg), inner(Pr), axis_last=False) <= TOL
+
+
+@pytest.mark.parametrize("first_layer", [1, 2, 3, 4])
+def test_reinitialisation_first_layer_treatments_match_reference(gpu, ref, first_layer):
+    """LevelSetReinitializationData::firstLayerTreatment CONSTRAINED1/2 (CR-1/2:
+    the first layer rescaled by |grad phi| and corrected on a curvature-chosen
+    set before the iterations, LevelSetReinitializer.cpp:643-865) and
+    ITERATIVE_CONSTRAINED1/2 (HCR-1/2: the first layer left free and pulled
+    back after every iteration, 1357-1450), through steps of the bubble with a
+    reinitialisation every 2 steps."""
+    g, s, mats, ls, V, ID, PHI = cases.bubble_case(24, reinit_frequency=2)
+    ls.reinit_first_layer = first_layer
+    sol, rc = make(gpu, ref, g, s, mats, ls, V, ID, PHI)
+    for _ in range(6):
+        sol.run(1)
+        rc.run(1)
+    Vg, IDg, Pg = sol.download()
+    Vr, IDr, Pr = rc.get_state()
+    assert np.array_equal(inner(IDg), inner(IDr))
+    assert rel_err(inner(Vg), inner(Vr)) <= TOL
+    assert rel_err(inner(Pg), inner(Pr), axis_last=False) <= TOL
+    assert sol.counters()["reinit_calls"] == 3
+    # the treatment changes the level set (against FIXED)
+    g2, s2, mats2, ls2, V2, ID2, PHI2 = cases.bubble_case(24, reinit_frequency=2)
+    other = gpu.Solver(g2, s2, mats2, ls2)
+    other.upload(V2, ID2, PHI2)
+    other.run(6)
+    assert np.abs(inner(other.download()[2]) - inner(Pg)).max() > 0
