@@ -278,6 +278,10 @@ static m2cg_status check_scheme(const m2cg_scheme* s, const m2cg_material* mats,
   if (s->rec_var < M2CG_RECVAR_PRIMITIVE || s->rec_var > M2CG_RECVAR_CONS_CHAR)
     return fail(M2CG_ERR_ARG, "unknown reconstruction variable type %d", s->rec_var);
   if (s->rk_order < 1 || s->rk_order > 3) return fail(M2CG_ERR_ARG, "rk_order must be 1, 2 or 3");
+  // SpaceOperator.cpp:78-83: the LLF interface flux stores no star states
+  if (nmat > 1 && s->mp_flux == M2CG_MPFLUX_LLF && s->mp_phasechange_type == 0)
+    return fail(M2CG_ERR_ARG, "MultiPhase::Flux = LocalLaxFriedrichs is incompatible with PhaseChange = "
+                              "RiemannSolution");
   for (int m = 0; m < nmat; m++)
     if (mats[m].eos != M2CG_EOS_SG && mats[m].eos != M2CG_EOS_NASG)
       return fail(M2CG_ERR_UNSUPPORTED, "material %d: only stiffened gas and NASG are supported", m);
