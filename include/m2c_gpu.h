@@ -245,6 +245,25 @@ m2cg_status m2cg_profile_stages(m2cg_ctx* ctx, int nsteps, float* stage_ms, int*
  * own work after the library's. */
 m2cg_status m2cg_get_stream(const m2cg_ctx* ctx, void** stream);
 
+/* Probes (ProbeOutput::SetupInterpolation / InterpolateSolutionAtProbe,
+ * ProbeOutput.cpp:219-340, 636-673): the primitive state at n fixed points
+ * xyz [n][3], interpolated trilinearly from the cell centres and the ghost
+ * layer the boundary rule fills, exactly as the reference does (invalid edge
+ * ghosts replaced by the average of the valid corners). m2cg_run and
+ * m2cg_advance sample them on the device after every `every`-th step
+ * (0: only on m2cg_sample_probes) into a device buffer of `capacity`
+ * records, with no host round trip; a record is t, the step count, then
+ * rho, u, v, w, p of each probe (2 + 5n doubles). A probe outside the
+ * ghosted mesh is M2CG_ERR_ARG, as the reference aborts. The device record
+ * buffer and the sampling schedule have no reference counterpart (the
+ * reference writes a text line per sample). */
+m2cg_status m2cg_set_probes(m2cg_ctx* ctx, int n, const double* xyz, int every, int capacity);
+m2cg_status m2cg_sample_probes(m2cg_ctx* ctx);
+/* Copy the records taken since the last read into `records` (room for the
+ * capacity given to m2cg_set_probes; NULL drops them), their number into
+ * *nrec, and empty the buffer. */
+m2cg_status m2cg_read_probes(m2cg_ctx* ctx, double* records, int* nrec);
+
 /* Text of the last error on this thread (never NULL). */
 const char* m2cg_last_error(void);
 

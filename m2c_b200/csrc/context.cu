@@ -165,7 +165,13 @@ struct m2cg_ctx {
   bool rs_valid = false;  // the multiphase star states stored by the last step match the resident state
   m2cg_counters counters = {};
   Multiphase* mp = nullptr;  // two-material machinery (nullptr for one material)
-  // optional per-stage event timing (benchmark roofline)
+  // probes (ProbeOutput): per probe the lower node (i, j, k), the trilinear
+  // coordinates and the valid-corner mask; records sampled on the device
+  int nprobe = 0, probe_every = 0, probe_cap = 0, probe_count = 0;
+  int* probe_ijk = nullptr;        // [n][4]: i, j, k, valid mask
+  double* probe_xi = nullptr;      // [n][3]
+  double* probe_rec = nullptr;     // [cap][2 + 5n]: t, step, V of each probe
+    // optional per-stage event timing (benchmark roofline)
   bool profile = false;
   std::vector<cudaEvent_t> ev;  // pairs (before, after) per stage launch
 };
@@ -466,6 +472,7 @@ extern "C" m2cg_status m2cg_destroy(m2cg_ctx* c) {
   for (int a = 0; a < 3; a++) { cudaFree(c->lA[a]); cudaFree(c->lB[a]); cudaFree(c->lK[a]); cudaFree(c->lC[a]); }
   cudaFree(c->clock); cudaFree(c->dtmin); cudaFree(c->clipflags); cudaFree(c->err);
   cudaFree(c->stage_buf);
+  cudaFree(c->probe_ijk); cudaFree(c->probe_xi); cudaFree(c->probe_rec);
   if (c->mp) multiphase_destroy(c->mp);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -639,6 +646,8 @@ static int grid1d(long long n) {
   if (b < 1) b = 1;
   return (int)b;
 }
+
+static m2cg_status sample_probes(m2cg_ctx* c);
 
 static m2cg_status check_device_error(m2cg_ctx* c) {
   DevError e;
@@ -876,6 +885,10 @@ extern "C" m2cg_status m2cg_advance(m2cg_ctx* c, double t_new, double dt, int ti
   if (c->mp) multiphase_set_step(c->mp, time_step);
   m2cg_status st = rk_step(c, true);
   if (st) return st;
+  if (c->nprobe && c->probe_every > 0 && c->counters.steps % c->probe_every == 0) {
+    st = sample_probes(c);
+    if (st) return st;
+  }
   return check_device_error(c);
 }
 
@@ -898,6 +911,10 @@ static m2cg_status run_steps(m2cg_ctx* c, int nsteps, double t_max, double t0, d
     if (c->mp) multiphase_set_step(c->mp, -1);
     m2cg_status st = rk_step(c, true);
     if (st) return st;
+    if (c->nprobe && c->probe_every > 0 && c->counters.steps % c->probe_every == 0) {
+      st = sample_probes(c);
+      if (st) return st;
+    }
     n++;
     if (finite) {
       CK(cudaMemcpyAsync(&tnow, c->clock, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1026,6 +1043,170 @@ extern "C" m2cg_status m2cg_profile_stages(m2cg_ctx* c, int nsteps, float* stage
   if (stage_launches) *stage_launches = (int)(c->ev.size() / 2);
   if (step_ms) *step_ms = total;
   c->ev.clear();
+  return M2CG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Probes (ProbeOutput::SetupInterpolation / InterpolateSolutionAtProbe,
+// ProbeOutput.cpp:219-340, 636-673)
+// ---------------------------------------------------------------------------
+struct V5 {
+  double* p[5];
+};
+
+// Node value of component p at (i, j, k), interior or face ghost (the
+// boundary rule of ApplyBoundaryConditions, as written into the ghosted
+// host layout by m2cg_download_state).
+__device__ double node_value(const Grid3& g, double* const* V, int i, int j, int k, int p) {
+  int out[3] = {i < 0 ? 0 : i >= g.nx ? 1 : -1, j < 0 ? 0 : j >= g.ny ? 1 : -1, k < 0 ? 0 : k >= g.nz ? 1 : -1};
+  int ii = i < 0 ? 0 : i >= g.nx ? g.nx - 1 : i;
+  int jj = j < 0 ? 0 : j >= g.ny ? g.ny - 1 : j;
+  int kk = k < 0 ? 0 : k >= g.nz ? g.nz - 1 : k;
+  int axis = out[0] >= 0 ? 0 : out[1] >= 0 ? 1 : out[2] >= 0 ? 2 : -1;
+  if (axis >= 0 && g.bc[2 * axis] == BC_PERIODIC) {
+    const int c3[3] = {i, j, k}, n3[3] = {g.nx, g.ny, g.nz};
+    const int w = (c3[axis] + n3[axis]) % n3[axis];
+    if (axis == 0) ii = w; else if (axis == 1) jj = w; else kk = w;
+    axis = -1;
+  }
+  double v = V[p][(long long)kk * g.plane + (long long)jj * g.px + ii];
+  if (axis >= 0) {
+    const int bc = g.bc[2 * axis + out[axis]];
+    if (bc == BC_INLET) v = g.inlet[p];
+    else if (bc == BC_OUTLET) v = g.outlet[p];
+    else if (bc == BC_STICKWALL) v = (p >= 1 && p <= 3) ? -v : v;
+    else if (p == axis + 1) v = -v;
+  }
+  return v;
+}
+
+// One record: every component of every probe; invalid corners count as
+// zero, and with fewer than 8 valid corners they take the average of the
+// others (636-669); then the trilinear interpolation of
+// MathTools::trilinear_interpolation (the local-coordinate form).
+__global__ void k_sample_probes(Grid3 g, V5 V, const int* ijk, const double* xi, int n, const double* clock,
+                                double step, double* rec) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q == 0) {
+    rec[0] = clock[0];
+    rec[1] = step;
+  }
+  if (q >= 5 * n) return;
+  const int pr = q / 5, p = q - 5 * pr;
+  const int i = ijk[4 * pr], j = ijk[4 * pr + 1], k = ijk[4 * pr + 2], valid = ijk[4 * pr + 3];
+  double c[8];
+  int nv = 0;
+  for (int a = 0; a < 8; a++) {  // c000, c100, c010, c110, c001, c101, c011, c111
+    const bool ok = (valid >> a) & 1;
+    c[a] = ok ? node_value(g, V.p, i + (a & 1), j + ((a >> 1) & 1), k + ((a >> 2) & 1), p) : 0.0;
+    nv += ok;
+  }
+  if (nv < 8) {
+    const double avg = (c[0] + c[1] + c[2] + c[3] + c[4] + c[5] + c[6] + c[7]) / nv;
+    for (int a = 0; a < 8; a++)
+      if (!((valid >> a) & 1)) c[a] = avg;
+  }
+  const double* x = xi + 3 * pr;
+  const double c00 = c[0] * (1.0 - x[0]) + c[1] * x[0];
+  const double c01 = c[4] * (1.0 - x[0]) + c[5] * x[0];
+  const double c10 = c[2] * (1.0 - x[0]) + c[3] * x[0];
+  const double c11 = c[6] * (1.0 - x[0]) + c[7] * x[0];
+  const double c0 = c00 * (1.0 - x[1]) + c10 * x[1];
+  const double c1 = c01 * (1.0 - x[1]) + c11 * x[1];
+  rec[2 + q] = c0 * (1.0 - x[2]) + c1 * x[2];
+}
+
+static m2cg_status sample_probes(m2cg_ctx* c) {
+  if (!c->nprobe) return M2CG_OK;
+  if (c->probe_count >= c->probe_cap) return fail(M2CG_ERR_ARG, "probe record buffer full (read it with m2cg_read_probes)");
+  V5 v;
+  for (int p = 0; p < 5; p++) v.p[p] = c->V[c->cur][p];
+  double* rec = c->probe_rec + (size_t)c->probe_count * (2 + 5 * c->nprobe);
+  k_sample_probes<<<(5 * c->nprobe + 127) / 128, 128, 0, c->stream>>>(c->g, v, c->probe_ijk, c->probe_xi, c->nprobe,
+                                                                      c->clock, (double)c->counters.steps, rec);
+  c->counters.kernel_launches += 1;
+  c->probe_count++;
+  CK(cudaGetLastError());
+  return M2CG_OK;
+}
+
+extern "C" m2cg_status m2cg_set_probes(m2cg_ctx* c, int n, const double* xyz, int every, int capacity) {
+  if (!c || n < 0 || (n > 0 && (!xyz || capacity < 1))) return fail(M2CG_ERR_ARG, "bad probe arguments");
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->probe_ijk); cudaFree(c->probe_xi); cudaFree(c->probe_rec);
+  c->probe_ijk = nullptr; c->probe_xi = nullptr; c->probe_rec = nullptr;
+  c->nprobe = 0;
+  c->probe_count = 0;
+  if (n == 0) return M2CG_OK;
+  // ghosted coordinates (SpaceOperator::PopulateGhostBoundaryCoordinates: x_0 - dx_0, x_{N-1} + dx_{N-1})
+  const std::vector<double>* xc[3] = {&c->hxc, &c->hyc, &c->hzc};
+  const std::vector<double>* dx[3] = {&c->hdx, &c->hdy, &c->hdz};
+  const int N[3] = {c->nx, c->ny, c->nz};
+  std::vector<double> X[3];
+  for (int a = 0; a < 3; a++) {
+    X[a].resize(N[a] + 2);
+    X[a][0] = (*xc[a])[0] - (*dx[a])[0];
+    for (int q = 0; q < N[a]; q++) X[a][q + 1] = (*xc[a])[q];
+    X[a][N[a] + 1] = (*xc[a])[N[a] - 1] + (*dx[a])[N[a] - 1];
+  }
+  auto crd = [&](int a, int idx) { return X[a][idx + 1]; };
+  // SpaceVariable3D::OutsidePhysicalDomainAndUnpopulated (SpaceVariable.h:150-159), with its test of
+  // j (not i) against NX on the x axis kept: a node outside in more than one count is not populated
+  auto unpopulated = [&](int i, int j, int k) {
+    int count = 0;
+    if (i < 0 || j >= N[0]) count++;
+    if (j < 0 || j >= N[1]) count++;
+    if (k < 0 || k >= N[2]) count++;
+    return count > 1;
+  };
+  std::vector<int> ijk(4 * (size_t)n);
+  std::vector<double> xi(3 * (size_t)n);
+  for (int q = 0; q < n; q++) {
+    int id3[3];
+    for (int a = 0; a < 3; a++) {
+      const double pa = xyz[3 * q + a];
+      if (pa < crd(a, -1) || pa >= crd(a, N[a])) return fail(M2CG_ERR_ARG, "cannot locate probe node %d in the domain", q);
+      int found = -2;
+      for (int i = -2; i < N[a]; i++)
+        if (pa < crd(a, i + 1)) { found = i; break; }
+      id3[a] = found;
+      xi[3 * q + a] = (pa - crd(a, found)) / (crd(a, found + 1) - crd(a, found));
+    }
+    int mask = 0, nv = 0;
+    for (int b = 0; b < 8; b++) {
+      const bool ok = !unpopulated(id3[0] + (b & 1), id3[1] + ((b >> 1) & 1), id3[2] + ((b >> 2) & 1));
+      mask |= ok ? (1 << b) : 0;
+      nv += ok;
+    }
+    if (nv == 0) return fail(M2CG_ERR_ARG, "probe node %d is too close to the edges of the domain boundary", q);
+    ijk[4 * q] = id3[0]; ijk[4 * q + 1] = id3[1]; ijk[4 * q + 2] = id3[2]; ijk[4 * q + 3] = mask;
+  }
+  const size_t rec = (size_t)capacity * (2 + 5 * (size_t)n) * sizeof(double);
+  if (cudaMalloc((void**)&c->probe_ijk, ijk.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&c->probe_xi, xi.size() * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&c->probe_rec, rec) != cudaSuccess)
+    return fail(M2CG_ERR_NOMEM, "probe buffers: allocation failed");
+  CK(cudaMemcpy(c->probe_ijk, ijk.data(), ijk.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->probe_xi, xi.data(), xi.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c->nprobe = n;
+  c->probe_every = every;
+  c->probe_cap = capacity;
+  return M2CG_OK;
+}
+
+extern "C" m2cg_status m2cg_sample_probes(m2cg_ctx* c) {
+  if (!c) return fail(M2CG_ERR_ARG, "null argument");
+  return sample_probes(c);
+}
+
+extern "C" m2cg_status m2cg_read_probes(m2cg_ctx* c, double* records, int* nrec) {
+  if (!c || !nrec) return fail(M2CG_ERR_ARG, "null argument");
+  *nrec = c->probe_count;
+  if (c->probe_count && records)
+    CK(cudaMemcpyAsync(records, c->probe_rec, (size_t)c->probe_count * (2 + 5 * c->nprobe) * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->probe_count = 0;
   return M2CG_OK;
 }
 

@@ -77,6 +77,9 @@ def lib():
     L.m2cg_batch_destroy.argtypes = [vp]
     L.m2cg_batch_set_mlp.argtypes = [vp, vp]
     L.m2cg_set_mlp.argtypes = [vp, vp]
+    L.m2cg_set_probes.argtypes = [vp, C.c_int, dp, C.c_int, C.c_int]
+    L.m2cg_sample_probes.argtypes = [vp]
+    L.m2cg_read_probes.argtypes = [vp, dp, ip]
     fp = C.POINTER(C.c_float)
     L.m2cg_mlp_create.argtypes = [C.c_ulonglong, C.POINTER(vp)]
     L.m2cg_mlp_destroy.argtypes = [vp]
@@ -97,7 +100,7 @@ def lib():
                  "m2cg_get_stream", "m2cg_profile_stages", "m2cg_batch_create", "m2cg_batch_run",
                  "m2cg_batch_download", "m2cg_batch_get_tuning", "m2cg_batch_get_counters",
                  "m2cg_batch_tube_errors", "m2cg_batch_time_steps", "m2cg_batch_destroy", "m2cg_batch_set_mlp",
-                 "m2cg_set_mlp",
+                 "m2cg_set_mlp", "m2cg_set_probes", "m2cg_sample_probes", "m2cg_read_probes",
                  "m2cg_mlp_create", "m2cg_mlp_destroy", "m2cg_mlp_get_params", "m2cg_mlp_set_params",
                  "m2cg_mlp_loss_grad", "m2cg_mlp_train", "m2cg_mlp_features_pairs", "m2cg_mlp_infer",
                  "m2cg_mlp_predict_pairs"):
@@ -239,6 +242,25 @@ class Solver:
                                                               int(bool(use_stored_riemann_solutions)),
                                                               C.byref(n)))
         return n.value
+
+    def set_probes(self, xyz, every=1, capacity=1024):
+        """Sample the primitive state at the points xyz [n][3] on the device
+        after every `every`-th step (ProbeOutput's interpolation)."""
+        self._probe_xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        self._probe_cap = capacity
+        check(lib().m2cg_set_probes(self.h, len(self._probe_xyz), abi.dptr(self._probe_xyz), every, capacity))
+
+    def sample_probes(self):
+        check(lib().m2cg_sample_probes(self.h))
+
+    def read_probes(self):
+        """Records since the last read, [nrec][2 + 5n]: t, step, then rho, u,
+        v, w, p of each probe."""
+        n = len(self._probe_xyz)
+        out = np.empty((self._probe_cap, 2 + 5 * n))
+        cnt = C.c_int()
+        check(lib().m2cg_read_probes(self.h, abi.dptr(out), C.byref(cnt)))
+        return out[:cnt.value]
 
     def set_mlp(self, mlp):
         """Start every interface Riemann solve of the steps from the

@@ -206,3 +206,36 @@ def test_stretched_mesh_matches_reference(gpu, ref, limiter):
     Vg, _, _ = sol.download()
     Vr, _, _ = rc.get_state()
     assert rel_err(inner(Vg), inner(Vr)) <= FP64_TOL
+
+
+def test_probes_match_reference_interpolation(gpu):
+    """m2cg_set_probes: device samples of the state at fixed points after
+    every step equal the reference's probe interpolation (ProbeOutput.cpp:
+    219-340, 636-673, restated in oracle/probe_ref.py) applied to the
+    downloaded ghosted state, bit for bit; points near the walls use the
+    ghost layer, and the ones whose cell touches an edge ghost the reference
+    leaves unpopulated use its averaging rule."""
+    from oracle import probe_ref
+    bc = (abi.BC_INLET, abi.BC_OUTLET, abi.BC_SLIPWALL, abi.BC_SYMMETRY, abi.BC_STICKWALL, abi.BC_SYMMETRY)
+    g, s, mats, V = cases.random_box(17, 11, 9, seed=5, bc=bc, mesh=cases.stretch)
+    xc, yc, zc = abi.cell_centres(g)
+    mesh = getattr(g, "_mesh", {})
+    widths = [mesh[a][1] for a in range(3)]
+    coords = [probe_ref.ghosted_coords(c, w) for c, w in zip((xc, yc, zc), widths)]
+    rng = np.random.default_rng(3)
+    pts = [[rng.uniform(coords[a][0], coords[a][-1] - 1e-12) for a in range(3)] for _ in range(40)]
+    pts += [[coords[0][0], coords[1][1], coords[2][5]], [coords[0][-2], coords[1][-2], coords[2][-2]],
+            [0.5 * (coords[0][0] + coords[0][1]), 0.5 * (coords[1][-2] + coords[1][-1]), coords[2][3]]]
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    sol.set_probes(pts, every=2, capacity=8)
+    sol.sample_probes()
+    sol.run(4)
+    rec = sol.read_probes()
+    assert rec.shape == (3, 2 + 5 * len(pts))
+    assert list(rec[:, 1]) == [0.0, 2.0, 4.0]
+    Vd, _, _ = sol.download()
+    setup = probe_ref.setup(pts, coords, (g.nx, g.ny, g.nz))
+    want = np.array([[probe_ref.interpolate(Vd, e, c) for c in range(5)] for e in setup]).ravel()
+    assert np.array_equal(rec[-1, 2:], want), np.abs(rec[-1, 2:] - want).max()
+    assert len(sol.read_probes()) == 0
