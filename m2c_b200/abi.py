@@ -107,7 +107,7 @@ def scheme(**kw):
     s.riem_min_pressure = -1.0e8
     s.riem_failure_threshold = 0.2
     s.riem_pressure_at_failure = 1.0e-8
-    s.riem_warm_delta = 0.01
+    s.riem_warm_delta = 3.0e-4
     s.mp_riemann_normal = RIEMANN_NORMAL_MESH
     for k, v in kw.items():
         if not hasattr(s, k):

@@ -77,10 +77,10 @@ def test_warm_start_saves_evaluations(gpu, trained):
     print(f"\nwarm start: evaluations {ev_c:.3f} -> {ev_h:.3f} ({ev_c / ev_h:.2f}x), "
           f"secant iterations {it_c:.3f} -> {it_h:.3f}; |log(p/p*)| median {np.median(rel):.2e} "
           f"p90 {np.percentile(rel, 90):.2e}; |dp*|/P p99 {np.percentile(dp, 99):.2e} max {dp.max():.2e}")
-    # measured on this network and these problems: about 1.2x fewer
-    # evaluations and 1.3x fewer secant iterations
-    assert ev_c / ev_h >= 1.1, ev_c / ev_h
-    assert it_c / it_h >= 1.15, it_c / it_h
+    # the north star's measure is secant iterations (>= 2x); star-state
+    # evaluations, the work itself, fall by less (measured ~1.3x)
+    assert it_c / it_h >= 2.0, it_c / it_h
+    assert ev_c / ev_h >= 1.15, ev_c / ev_h
     # the solver decides: both solves pass its stopping test (velocity
     # mismatch below tol_main x max sound speed, or a bracket narrower than
     # tol_main x pressure scale), so their star velocities agree within
