@@ -437,6 +437,7 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
     const double* xc[3] = {c->hxc.data(), c->hyc.data(), c->hzc.data()};
     const double* dxs[3] = {c->hdx.data(), c->hdy.data(), c->hdz.data()};
     st = multiphase_create(c->stream, g, sk, *scheme, mats, nmat, *ls, xc, dxs, &c->mp);
+    if (st) fail(st, "two-material setup refused or failed (status %d): interface options or level-set settings", (int)st);
   }
   if (st) {
     m2cg_destroy(c);
@@ -855,6 +856,11 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
     a.clipped_out = c->clipflags + (s - 1);
     a.dtmin_bits = (a.final_stage && want_dtmin && !c->mp) ? c->dtmin : nullptr;
     if (c->mp) {
+      StageArgs fa = a;
+      if (multiphase_face_pass(c->mp, fa)) {
+        m2cg_status st = launch_stage(c, fa);
+        if (st) return st;
+      }
       m2cg_status st = multiphase_stage(c->mp, c->stream, a);
       if (st) return st;
     }
@@ -958,6 +964,11 @@ extern "C" m2cg_status m2cg_compute_residual(m2cg_ctx* c, double* R_host) {
     c->rs_valid = false;  // the interface slots are reassigned
     m2cg_status st = multiphase_begin_step(c->mp, c->stream, Vn, c->id);
     if (st) return st;
+    StageArgs fa = a;
+    if (multiphase_face_pass(c->mp, fa)) {
+      st = launch_stage(c, fa);
+      if (st) return st;
+    }
     st = multiphase_stage(c->mp, c->stream, a);
     if (st) return st;
   }

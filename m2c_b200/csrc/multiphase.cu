@@ -82,6 +82,7 @@ struct Multiphase {
   double* rsVsp = nullptr;
   uint8_t* rsValid = nullptr;  // [slot][3]
   double* scratch = nullptr;   // Riemann integration paths
+  double* faceV = nullptr;     // LINEAR interface reconstruction: [slot][3][left, right][5] face states
   // changed cells (ordered)
   int* changed = nullptr;      // [ncell] ordered list of linear offsets
   int* blockcnt = nullptr;     // per-block counts for the ordered compaction
@@ -213,7 +214,26 @@ struct IfaceRiemannArgs {
   const double* phi;      // phi^n (the reference's loose coupling uses the step's phi)
   LsGeom geo;
   const double* warm;     // per face: proposed star pressure of the learned warm start, or NULL
+  const double* faceV;    // LINEAR reconstruction: the face pass's states, [slot][3][2][5]; NULL: cell states
 };
+
+// Left and right states of the interface problem on face f (low face d of
+// cell offR, whose slot is s): the cell-centred states of the stage, or
+// under LINEAR reconstruction the face states vr[L] and vl[R] that the
+// stage kernel's face pass wrote (SpaceOperator.cpp:2503-2506).
+__device__ __forceinline__ void iface_states(const IfaceRiemannArgs& a, int s, int d, long long offL, uint8_t idL,
+                                             long long offR, uint8_t idR, double* VL, double* VR) {
+  if (a.faceV) {
+    const double* o = a.faceV + ((long long)s * 3 + d) * 10;
+    for (int c = 0; c < 5; c++) {
+      VL[c] = o[c];
+      VR[c] = o[5 + c];
+    }
+    return;
+  }
+  stage_state(a.st, a.eos, offL, idL, VL);
+  stage_state(a.st, a.eos, offR, idR, VR);
+}
 
 // Groups: 4 wave patterns x IFACE_STRENGTHS rarefaction strengths; sizes in
 // counts[IFACE_GROUP0 ...], fill positions in the IFACE_GROUPS entries after.
@@ -232,7 +252,7 @@ __global__ void k_iface_classify(IfaceRiemannArgs a) {
   long long nf = a.counts[1];
   if (nf > a.cap_faces) nf = a.cap_faces;
   for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
-    const int q = a.faces[3 * f], d = a.faces[3 * f + 2];
+    const int q = a.faces[3 * f], sl = a.faces[3 * f + 1], d = a.faces[3 * f + 2];
     int i, j, k;
     cell_coords(g, q, i, j, k);
     int ni, nj, nk;
@@ -240,8 +260,7 @@ __global__ void k_iface_classify(IfaceRiemannArgs a) {
     const long long offR = offset_of(g, i, j, k), offL = offset_of(g, ni, nj, nk);
     const uint8_t idR = a.st.id[offR], idL = a.st.id[offL];
     double VL[5], VR[5];
-    stage_state(a.st, a.eos, offL, idL, VL);
-    stage_state(a.st, a.eos, offR, idR, VR);
+    iface_states(a, sl, d, offL, idL, offR, idR, VL, VR);
     const double c2l = a.eos[idL].c2(VL[0], a.eos[idL].energy(VL[0], VL[4]));
     const double c2r = a.eos[idR].c2(VR[0], a.eos[idR].energy(VR[0], VR[4]));
     int pat = 0;
@@ -311,8 +330,7 @@ __global__ void __launch_bounds__(128, M2C_IFACE_MINB) k_iface_riemann(IfaceRiem
     const long long offR = offset_of(g, i, j, k), offL = offset_of(g, ni, nj, nk);
     const uint8_t idR = a.st.id[offR], idL = a.st.id[offL];
     double VL[5], VR[5];
-    stage_state(a.st, a.eos, offL, idL, VL);
-    stage_state(a.st, a.eos, offR, idR, VR);
+    iface_states(a, s, d, offL, idL, offR, idR, VL, VR);
     double dir[3];
     riemann_direction(a.normal_mode, g, a.geo, a.phi, i, j, k, d, idR, idL, dir);
     double Vs[5], Vsm[5], Vsp[5];
@@ -352,7 +370,7 @@ __global__ void k_iface_features(IfaceRiemannArgs a, float* X, double* P, int* v
   long long nf = a.counts[1];
   if (nf > a.cap_faces) nf = a.cap_faces;
   for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
-    const int q = a.faces[3 * f], d = a.faces[3 * f + 2];
+    const int q = a.faces[3 * f], sl = a.faces[3 * f + 1], d = a.faces[3 * f + 2];
     int i, j, k;
     cell_coords(g, q, i, j, k);
     int ni, nj, nk;
@@ -360,8 +378,7 @@ __global__ void k_iface_features(IfaceRiemannArgs a, float* X, double* P, int* v
     const long long offR = offset_of(g, i, j, k), offL = offset_of(g, ni, nj, nk);
     const uint8_t idR = a.st.id[offR], idL = a.st.id[offL];
     double VL[5], VR[5], dir[3], Pq = 0.0;
-    stage_state(a.st, a.eos, offL, idL, VL);
-    stage_state(a.st, a.eos, offR, idR, VR);
+    iface_states(a, sl, d, offL, idL, offR, idR, VL, VR);
     riemann_direction(a.normal_mode, g, a.geo, a.phi, i, j, k, d, idR, idL, dir);
     valid[f] = mlp_features(a.eos[idL], a.eos[idR], VL, VR, dir, X + f * MLP_IN, &Pq) ? 1 : 0;
     P[f] = Pq;
@@ -768,7 +785,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
                               const m2cg_material* mats, int nmat, const m2cg_levelset& ls, const double* const* xc,
                               const double* const* dx, Multiphase** out) {
   *out = nullptr;
-  if (scheme.mp_recon != 0) return M2CG_ERR_UNSUPPORTED;  // interface Riemann inputs: constant recon
+  if (scheme.mp_recon != 0 && scheme.mp_recon != 1) return M2CG_ERR_ARG;
   if (scheme.mp_phasechange_type != 0 && scheme.mp_phasechange_type != 1) return M2CG_ERR_UNSUPPORTED;
   if (ls.material_id != 1) return M2CG_ERR_UNSUPPORTED;
   if (ls.reinit_first_layer < 0 || ls.reinit_first_layer > 4) return M2CG_ERR_ARG;
@@ -812,6 +829,7 @@ m2cg_status multiphase_create(cudaStream_t s, const Grid3& g, const SchemeK& sk,
   A((void**)&mp->rsVsp, mp->cap_slots * 15 * 8);
   A((void**)&mp->rsValid, mp->cap_slots * 3);
   A((void**)&mp->scratch, (size_t)IFACE_RIEMANN_THREADS * 2 * 3 * RIEMANN_PATH_CAP * 8);
+  if (scheme.mp_recon == 1 && scheme.mp_flux != M2CG_MPFLUX_LLF) A((void**)&mp->faceV, (size_t)mp->cap_slots * 3 * 10 * 8);
   A((void**)&mp->changed, ninterior * 4);
   mp->nblocks_scan = 148 * 8;
   {
@@ -856,6 +874,7 @@ void multiphase_destroy(Multiphase* mp) {
   cudaFree(mp->order); cudaFree(mp->pattern);
   cudaFree(mp->Vsm); cudaFree(mp->Vsp); cudaFree(mp->Vmid); cudaFree(mp->midid);
   cudaFree(mp->rsVsm); cudaFree(mp->rsVsp); cudaFree(mp->rsValid); cudaFree(mp->scratch);
+  cudaFree(mp->faceV);
   cudaFree(mp->changed); cudaFree(mp->blockcnt); cudaFree(mp->nchanged); cudaFree(mp->mask);
   cudaFree(mp->totals);
   cudaFree(mp->fX); cudaFree(mp->fP); cudaFree(mp->fvalid); cudaFree(mp->fy); cudaFree(mp->fwarm);
@@ -907,6 +926,25 @@ m2cg_status multiphase_begin_step(Multiphase* mp, cudaStream_t s, double* const*
   return cudaGetLastError() == cudaSuccess ? M2CG_OK : M2CG_ERR_CUDA;
 }
 
+bool multiphase_face_pass(Multiphase* mp, StageArgs& a) {
+  if (!mp->faceV) return false;
+  a.iface.slot = mp->slot;
+  a.iface.mp_flux = mp->scheme.mp_flux;
+  a.iface.mp_recon = mp->scheme.mp_recon;
+  a.iface.faces_out = mp->faceV;
+  for (int p = 0; p < 5; p++) {
+    a.Po[p] = nullptr;
+    a.Uo[p] = nullptr;
+    a.Vo[p] = nullptr;
+    a.Vfo[p] = nullptr;
+    a.Ro[p] = nullptr;
+  }
+  a.final_stage = 0;
+  a.clipped_out = nullptr;
+  a.dtmin_bits = nullptr;
+  return true;
+}
+
 m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
   mp->stage = a.stage;
   // exact Riemann problems at the interface faces
@@ -935,6 +973,7 @@ m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, StageArgs& a) {
   ra.order = mp->order;
   ra.pattern = mp->pattern;
   ra.group_out = mp->order;
+  ra.faceV = mp->faceV;
   cudaMemsetAsync(mp->counts + IFACE_GROUP0, 0, 2 * IFACE_GROUPS * sizeof(int), s);
   k_iface_classify<<<148 * 8, 256, 0, s>>>(ra);
   k_iface_group<<<148 * 8, 256, 0, s>>>(ra);

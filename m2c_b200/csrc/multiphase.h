@@ -23,6 +23,11 @@ void multiphase_set_step(Multiphase* mp, int time_step);
 // Called before the stages of a step (V^n, ID) and before each stage launch
 // (fills the interface fields of the stage arguments).
 m2cg_status multiphase_begin_step(Multiphase* mp, cudaStream_t s, double* const* Vn, const uint8_t* id);
+// LINEAR interface reconstruction: turns a copy of the stage's arguments into
+// the face pass (the stage kernel writing the reconstructed states on both
+// sides of each interface face, launched before multiphase_stage); false if
+// the scheme needs none.
+bool multiphase_face_pass(Multiphase* mp, m2c::StageArgs& a);
 m2cg_status multiphase_stage(Multiphase* mp, cudaStream_t s, m2c::StageArgs& a);
 // After the last stage: level-set update, ID update, reinitialisation,
 // state update of cells that changed material.

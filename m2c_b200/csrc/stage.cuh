@@ -108,6 +108,11 @@ struct IfaceView {
   const int* midid;      // [slot][3 faces]
   int mp_flux;           // 0 EXACT, 1 NUMERICAL, 2 LLF
   int mp_recon;          // 0 CONSTANT (cell states), 1 LINEAR (face states)
+  // Face pass (LINEAR interface reconstruction): if set, the kernel only
+  // writes the reconstructed states on both sides of every interface face,
+  // [slot][3 faces][left, right][5], for the exact Riemann problems solved
+  // before the stage proper; no flux, no update.
+  double* faces_out;
 };
 
 struct StageArgs {
@@ -738,6 +743,11 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     }
     T VL[5], VR[5];
     const uint8_t idL = sm.ids[sL][myL + 1][mxL + 1], idR = sm.ids[sR][myR + 1][mxR + 1];
+    if (MULTI && a.iface.faces_out && idL == idR) {
+#pragma unroll
+      for (int c = 0; c < 5; c++) { F[c] = T(0); F2[c] = T(0); }
+      return;
+    }
     if (rL) cell_face(pL, mxL, myL, d, 1, VL);
     if (rR) cell_face(pR, mxR, myR, d, 0, VR);
     if (!rL) {  // low-side boundary face
@@ -753,6 +763,20 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       ghost_face(g.bc[2 * d + 1], d, VL, gc, eos_of<T, MULTI>(a.s, idR), VR);
     }
     int err = ERR_NONE;
+    if (MULTI && a.iface.faces_out) {  // face pass: the interface faces' states only
+#pragma unroll
+      for (int c = 0; c < 5; c++) { F[c] = T(0); F2[c] = T(0); }
+      const int gi = wrap_index(i0 + mxR - 1, g.nx), gj = wrap_index(j0 + myR - 1, g.ny);
+      const int gk = wrap_index(pR, g.nz);
+      const int slot = a.iface.slot[(long long)gk * g.plane + (long long)gj * g.px + gi];
+      double* o = a.iface.faces_out + ((long long)slot * 3 + d) * 10;
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        o[c] = double(VL[c]);
+        o[5 + c] = double(VR[c]);
+      }
+      return;
+    }
     if (MULTI && idL != idR) {
       // Material interface (SpaceOperator.cpp:2486-2542): two one-sided fluxes
       // against the exact Riemann star states, or LLF across the interface.
@@ -888,7 +912,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       __syncthreads();
       if (m >= kb - 1) faces(m, m >= kb);
       __syncthreads();
-      if (m < kb || !own) continue;
+      if (m < kb || !own || (MULTI && a.iface.faces_out)) continue;
       // (4) residual + RK update of plane m
       const double dzk = g.dz[m];
       const double ax = dyj * dzk, ay = dxi * dzk, az = dxi * dyj;
@@ -935,11 +959,17 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
           ifc[2] = me != sm.ids[slot4(m - 1)][ly][lx];
           if (ifc[0] || ifc[1] || ifc[2]) {
             const int slot = a.iface.slot[off];
-            T W[5];
-#pragma unroll
-            for (int c = 0; c < 5; c++) W[c] = M2C_VV(sc, c, ly, lx);
             for (int d = 0; d < 3; d++) {
               if (!ifc[d]) continue;
+              // this cell's side of the face: its cell-centred state, or its
+              // reconstructed state on that face (vl) under LINEAR
+              T W[5];
+              if (a.iface.mp_recon) {
+                cell_face(m, tx + 1, ty + 1, d, 0, W);
+              } else {
+#pragma unroll
+                for (int c = 0; c < 5; c++) W[c] = M2C_VV(sc, c, ly, lx);
+              }
               const long long base = ((long long)slot * 3 + d) * 5;
               T Sp[5];
 #pragma unroll
