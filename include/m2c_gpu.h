@@ -110,7 +110,7 @@ typedef struct {
   double riem_tol_main, riem_tol_shock, riem_tol_rarefaction;
   double riem_min_pressure, riem_failure_threshold, riem_pressure_at_failure;
   /* Warm start of the exact Riemann solve (no reference counterpart): the
-   * bracket tried around a proposed star pressure p is [p(1-d), p(1+d)]
+   * bracket tried around a proposed star pressure p is [p - d|p|, p + d|p|]
    * (default 3e-4: with proposals a few tenths of a percent off, the root is
    * usually bracketed at once or after the search's first expansions, and one
    * secant iteration meets the stopping test). */
@@ -118,6 +118,12 @@ typedef struct {
   /* MultiPhaseData::riemann_normal: direction of the interface Riemann
    * problem, 0 LEVEL_SET (gradient of phi), 1 MESH (face normal), 2 AVERAGE */
   int mp_riemann_normal;
+  /* Warm-start gate (no reference counterpart): a proposal p is ignored, and
+   * the acoustic starting points kept, where |log((p + S) / (pac + S))| <=
+   * gate, S = min(pinf_l, pinf_r): near-acoustic problems, which the acoustic
+   * estimate already starts within the network's own error. 0 (default):
+   * every proposal departing by more than riem_warm_delta is used. */
+  double riem_warm_gate;
 } m2cg_scheme;
 
 /* One level set (LevelSetSchemeData, IoData.h:653-679; reinit
@@ -334,10 +340,12 @@ m2cg_status m2cg_riemann_batch_noalloc(const m2cg_scheme* scheme, const m2cg_mat
 /* ---------------------------------------------------------------------------
  * Learned warm start for the interface Riemann solve (no counterpart in the
  * reference). A 16 -> 64 -> 64 -> 64 -> 1 tanh MLP maps dimensionless
- * features of a problem to log(pstar / pac), pac the acoustic estimate the
+ * features of a problem to log((pstar + S) / B), S = min(pinf_l, pinf_r) and
+ * B = max(pac + S, 1e-3 (max(|pl|, |pr|) + S)), pac the acoustic estimate the
  * solver's bracket search starts from; where the proposal p departs from pac
- * by more than riem_warm_delta, p(1 -+ riem_warm_delta) replaces the
- * acoustic starting points of that search. The solver's own iteration and stopping test are
+ * by more than riem_warm_delta (and passes riem_warm_gate),
+ * p -+ riem_warm_delta |p| replaces the acoustic starting points of that
+ * search. The solver's own iteration and stopping test are
  * unchanged, so results agree with the cold solve within tol_main.
  * Training runs on the GPU (FP32 forward + backward kernels, Adam);
  * inference runs BF16 on tensor cores with FP32 accumulation.
@@ -362,9 +370,10 @@ m2cg_status m2cg_mlp_loss_grad(m2cg_mlp* m, const float* Xn, const float* yn, in
 m2cg_status m2cg_mlp_train(m2cg_mlp* m, const float* X, const float* y, int n, int steps, int batch,
                            float lr, unsigned long long seed, float* final_loss);
 /* Features of problems with per-pair materials (as m2cg_riemann_batch_pairs):
- * X [n][16], base pressure pac [n], valid [n] (0 where no proposal can be made). */
+ * X [n][16], scale [n][2] = (base B, shift S) of the target log((p* + S) / B),
+ * valid [n] (0 where no proposal can be made). */
 m2cg_status m2cg_mlp_features_pairs(const m2cg_material* mats, int n, const double* VL,
-                                    const double* VR, const double* dir, float* X, double* P, int* valid);
+                                    const double* VR, const double* dir, float* X, double* scale, int* valid);
 /* Network output (target units) for raw feature rows, BF16 tensor cores. */
 m2cg_status m2cg_mlp_infer(m2cg_mlp* m, const float* X, const int* valid, int n, float* y);
 /* Proposed star pressures for per-pair problems (NaN where none). */

@@ -62,7 +62,7 @@ class Scheme(C.Structure):
         ("riem_tol_main", C.c_double), ("riem_tol_shock", C.c_double), ("riem_tol_rarefaction", C.c_double),
         ("riem_min_pressure", C.c_double), ("riem_failure_threshold", C.c_double),
         ("riem_pressure_at_failure", C.c_double), ("riem_warm_delta", C.c_double),
-        ("mp_riemann_normal", C.c_int),
+        ("mp_riemann_normal", C.c_int), ("riem_warm_gate", C.c_double),
     ]
 
 

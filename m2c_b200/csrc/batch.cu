@@ -232,9 +232,10 @@ __global__ void k_tube_features(TubeArgs A, TubeStage S, float* X, double* P, in
       tube_state(A, S, eos[idL], o + i - 1, VL);
       tube_state(A, S, eos[idR], o + i, VR);
       const double dir[3] = {1.0, 0.0, 0.0};
-      double Pq = 0.0;
-      ok = mlp_features(eos[idL], eos[idR], VL, VR, dir, X + w * MLP_IN, &Pq) ? 1 : 0;
-      P[w] = Pq;
+      double Pq[2] = {0.0, 0.0};
+      ok = mlp_features(eos[idL], eos[idR], VL, VR, dir, X + w * MLP_IN, Pq) ? 1 : 0;
+      P[2 * w] = Pq[0];
+      P[2 * w + 1] = Pq[1];
     }
     valid[w] = ok;
   }
@@ -449,15 +450,35 @@ __device__ __forceinline__ void tube_stage_item(const TubeArgs& A, const TubeSta
       }
       for (int c = 0; c < 5; c++) Unew[c] = S.a_prev * Usv[c] + S.a_un * Un[c];
     }
-    // residual in the reference's summation order; the y and z faces of a
-    // one-cell-wide grid add exact zeros (SpaceOperator.cpp:3351-3409)
+    // y and z faces of the one-cell-wide grid: SYMMETRY ghosts (the cell
+    // with its normal velocity negated), zero transverse slopes (the limiter
+    // sees differences of opposite sign or zero), so the face states are
+    // the cell's own state against its mirror image
+    // (SpaceOperator::ComputeAdvectionFluxes, Reconstructor.cpp:822-875).
+    // Their fluxes are not exactly zero in general (the star-state
+    // arithmetic rounds), so they are formed and summed as the reference
+    // sums them.
+    double Vc[5], M[5], G[4][5];
+    for (int c = 0; c < 5; c++) Vc[c] = sm.v[c][j];
+    for (int dd = 1; dd < 3; dd++) {
+      for (int c = 0; c < 5; c++) M[c] = Vc[c];
+      M[1 + dd] = -M[1 + dd];
+      int e2 = num_flux(A.flux, e, dd, M, Vc, A.delta, G[2 * (dd - 1)]);        // low face: ghost | cell
+      if (!e2) e2 = num_flux(A.flux, e, dd, Vc, M, A.delta, G[2 * (dd - 1) + 1]);  // high face: cell | ghost
+      if (e2) tube_fail(A, t, e2, (int)q, where + 2);
+    }
+    // residual in the reference's summation order (SpaceOperator.cpp:3351-3409)
     const double vol = h * 1.0 * 1.0;
-    const double ax = 1.0 * 1.0;
+    const double ax = 1.0 * 1.0, ay = h * 1.0, az = h * 1.0;
     const double inv_mvol = 1.0 / (-vol);
     for (int c = 0; c < 5; c++) {
       double fs = 0.0;
       fs = fs - sm.F2[c][f] * ax;
+      fs = fs - G[0][c] * ay;
+      fs = fs - G[2][c] * az;
       fs = fs + sm.F[c][f + 1] * ax;
+      fs = fs + G[1][c] * ay;
+      fs = fs + G[3][c] * az;
       const double R = fs * inv_mvol;
       Unew[c] = Unew[c] + bdt * R;
     }
@@ -1236,7 +1257,7 @@ extern "C" m2cg_status m2cg_batch_set_mlp(m2cg_batch* b, const m2cg_mlp* m) {
   const size_t nslot = (size_t)b->ntubes * TUBE_IFACE_CAP;
   if (m && !b->fX) {
     if (cudaMalloc((void**)&b->fX, nslot * MLP_IN * sizeof(float)) != cudaSuccess ||
-        cudaMalloc((void**)&b->fP, nslot * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&b->fP, 2 * nslot * sizeof(double)) != cudaSuccess ||
         cudaMalloc((void**)&b->fvalid, nslot * sizeof(int)) != cudaSuccess ||
         cudaMalloc((void**)&b->fy, nslot * sizeof(float)) != cudaSuccess ||
         cudaMalloc((void**)&b->fwarm, nslot * sizeof(double)) != cudaSuccess)

@@ -83,6 +83,7 @@ extern "C" void m2cg_default_scheme(m2cg_scheme* s) {
   s->riem_min_pressure = -1.0e8;
   s->riem_failure_threshold = 0.2;
   s->riem_pressure_at_failure = 1.0e-8;
+  s->riem_warm_gate = 0.0;
   s->riem_warm_delta = 3.0e-4;  // measured: the narrowest bracket that keeps the evaluations low
   s->mp_riemann_normal = 1;  // MultiPhaseData::MESH (IoData.cpp:1408)
 }

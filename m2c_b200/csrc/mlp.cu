@@ -308,9 +308,10 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const float* params, const fl
 __global__ void k_mlp_features_pairs(const Eos<double>* eos, int n, const double* VL, const double* VR,
                                      const double* dir, float* X, double* P, int* valid) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    double Pq = 0.0;
-    const bool ok = mlp_features(eos[2 * q], eos[2 * q + 1], VL + 5 * q, VR + 5 * q, dir + 3 * q, X + (long long)q * MLP_IN, &Pq);
-    P[q] = Pq;
+    double sc[2] = {0.0, 0.0};
+    const bool ok = mlp_features(eos[2 * q], eos[2 * q + 1], VL + 5 * q, VR + 5 * q, dir + 3 * q, X + (long long)q * MLP_IN, sc);
+    P[2 * q] = sc[0];
+    P[2 * q + 1] = sc[1];
     valid[q] = ok ? 1 : 0;
   }
 }
@@ -319,7 +320,7 @@ __global__ void k_mlp_to_pressure(const float* y, const double* P, const int* va
                                   double* p) {
   if (ndev && *ndev < n) n = *ndev;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
-    p[q] = valid[q] ? P[q] * exp((double)y[q]) : NAN;
+    p[q] = valid[q] ? P[2 * q] * exp((double)y[q]) - P[2 * q + 1] : NAN;
 }
 
 }  // namespace m2c
@@ -553,7 +554,7 @@ static cudaError_t infer_rows(m2cg_mlp* m, const float* dX, const int* dvalid, i
 
 namespace m2c {
 // Device-side proposals for rows of raw features (used by the batched tubes):
-// warm[r] = P[r] exp(network(X[r])) where valid[r], else NaN.
+// warm[r] = P[2r] exp(network(X[r])) - P[2r+1] where valid[r], else NaN.
 cudaError_t mlp_warm_device(const m2cg_mlp* m, cudaStream_t s, const float* X, const int* valid, const double* P,
                             int n, float* y, double* warm, const int* ndev) {
   const int tiles = (n + 15) / 16;
@@ -585,7 +586,7 @@ static m2cg_status pairs_common(m2cg_mlp* m, const m2cg_material* mats, int n, c
   m2cg_status st = M2CG_OK;
   if (cudaMalloc((void**)&deos, heos.size() * sizeof(Eos<double>)) != cudaSuccess ||
       cudaMalloc((void**)&dVL, nn * 40) != cudaSuccess || cudaMalloc((void**)&dVR, nn * 40) != cudaSuccess ||
-      cudaMalloc((void**)&ddir, nn * 24) != cudaSuccess || cudaMalloc((void**)&dP, nn * 8) != cudaSuccess ||
+      cudaMalloc((void**)&ddir, nn * 24) != cudaSuccess || cudaMalloc((void**)&dP, nn * 16) != cudaSuccess ||
       cudaMalloc((void**)&dp, nn * 8) != cudaSuccess || cudaMalloc((void**)&dX, nn * MLP_IN * 4) != cudaSuccess ||
       cudaMalloc((void**)&dy, nn * 4) != cudaSuccess || cudaMalloc((void**)&dvalid, nn * 4) != cudaSuccess)
     st = mfail(M2CG_ERR_NOMEM, "allocation failed");
@@ -601,7 +602,7 @@ static m2cg_status pairs_common(m2cg_mlp* m, const m2cg_material* mats, int n, c
     ck(cudaGetLastError());
     if (mode == 0) {
       if (X_out) ck(cudaMemcpyAsync(X_out, dX, nn * MLP_IN * 4, cudaMemcpyDeviceToHost, s));
-      if (P_out) ck(cudaMemcpyAsync(P_out, dP, nn * 8, cudaMemcpyDeviceToHost, s));
+      if (P_out) ck(cudaMemcpyAsync(P_out, dP, nn * 16, cudaMemcpyDeviceToHost, s));
       if (valid_out) ck(cudaMemcpyAsync(valid_out, dvalid, nn * 4, cudaMemcpyDeviceToHost, s));
     } else if (mode == 1) {
       if (e == cudaSuccess) ck(infer_rows(m, dX, dvalid, n, dy));

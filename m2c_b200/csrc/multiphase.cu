@@ -377,11 +377,12 @@ __global__ void k_iface_features(IfaceRiemannArgs a, float* X, double* P, int* v
     low_neighbour(g, i, j, k, d, ni, nj, nk);
     const long long offR = offset_of(g, i, j, k), offL = offset_of(g, ni, nj, nk);
     const uint8_t idR = a.st.id[offR], idL = a.st.id[offL];
-    double VL[5], VR[5], dir[3], Pq = 0.0;
+    double VL[5], VR[5], dir[3], Pq[2] = {0.0, 0.0};
     iface_states(a, sl, d, offL, idL, offR, idR, VL, VR);
     riemann_direction(a.normal_mode, g, a.geo, a.phi, i, j, k, d, idR, idL, dir);
-    valid[f] = mlp_features(a.eos[idL], a.eos[idR], VL, VR, dir, X + f * MLP_IN, &Pq) ? 1 : 0;
-    P[f] = Pq;
+    valid[f] = mlp_features(a.eos[idL], a.eos[idR], VL, VR, dir, X + f * MLP_IN, Pq) ? 1 : 0;
+    P[2 * f] = Pq[0];
+    P[2 * f + 1] = Pq[1];
   }
 }
 
@@ -1113,7 +1114,7 @@ m2cg_status multiphase_set_mlp(Multiphase* mp, const m2cg_mlp* m) {
   if (m && !mp->fX) {
     const size_t n = (size_t)mp->cap_faces;
     if (cudaMalloc((void**)&mp->fX, n * MLP_IN * sizeof(float)) != cudaSuccess ||
-        cudaMalloc((void**)&mp->fP, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&mp->fP, 2 * n * sizeof(double)) != cudaSuccess ||
         cudaMalloc((void**)&mp->fvalid, n * sizeof(int)) != cudaSuccess ||
         cudaMalloc((void**)&mp->fy, n * sizeof(float)) != cudaSuccess ||
         cudaMalloc((void**)&mp->fwarm, n * sizeof(double)) != cudaSuccess) {

@@ -62,6 +62,7 @@ RiemannParams riemann_params(const m2cg_scheme& s) {
   P.failure_threshold = s.riem_failure_threshold;
   P.pressure_at_failure = s.riem_pressure_at_failure;
   P.warm_delta = s.riem_warm_delta;
+  P.warm_gate = s.riem_warm_gate;
   return P;
 }
 

@@ -53,6 +53,7 @@ struct RiemannParams {
   int maxIts_main, maxIts_bracket, maxIts_shock, numSteps_rarefaction;
   double tol_main, tol_shock, tol_rarefaction, min_pressure, failure_threshold, pressure_at_failure;
   double warm_delta;  // half-width of the warm-start bracket, relative to the proposed star pressure
+  double warm_gate;   // proposals within this shifted log distance of the acoustic estimate are ignored
 };
 
 // result flags
@@ -547,13 +548,26 @@ struct RiemannSolver {
     // the acoustic (linearised) estimate the reference starts from
     const double Cl0 = rhol * cl, Cr0 = rhor * cr;
     const double pac = (Cr0 * pl + Cl0 * pr + Cl0 * Cr0 * (ul - ur)) / (Cl0 + Cr0);
-    if (isfinite(warm) && warm > 0.0 && P.warm_delta > 0.0 && !(fabs(warm - pac) <= P.warm_delta * fabs(pac))) {
+    bool use_warm =
+        isfinite(warm) && warm != 0.0 && P.warm_delta > 0.0 && !(fabs(warm - pac) <= P.warm_delta * fabs(pac));
+    if (use_warm && P.warm_gate > 0.0) {
+      // near-acoustic problem: the acoustic estimate starts as close as the
+      // proposal would (distance measured with pressures shifted by the
+      // smaller stiffness, the scale of the stopping test)
+      const double sh = fmin(fabs(eos[idl].pstiff), fabs(eos[idr].pstiff));
+      const double qa = pac + sh, qw = warm + sh;
+      if (qa > 0.0 && qw > 0.0 && fabs(log(qw / qa)) <= P.warm_gate) use_warm = false;
+    }
+    if (use_warm) {
       // warm start: a proposal departing from the acoustic estimate by more
-      // than the bracket width supplies the two points warm (1 -+ d) in place
-      // of the acoustic estimates, when both are feasible; FindInitialInterval
-      // then expands them as it would expand the acoustic pair
-      p0 = warm * (1.0 - P.warm_delta);
-      p1 = warm * (1.0 + P.warm_delta);
+      // than the bracket width supplies the two points warm -+ d |warm| in
+      // place of the acoustic estimates (p0 < p1, also for a negative
+      // proposal on a stiffened gas), when both are feasible;
+      // FindInitialInterval then expands them as it would expand the
+      // acoustic pair
+      const double half = P.warm_delta * fabs(warm);
+      p0 = warm - half;
+      p1 = warm + half;
       if (rho_u_star(1, path1, rhol, ul, pl, p0, idl, rhol, (p0 > pl) ? rhol * 1.1 : rhol * 0.9, rhol0, ul0, nullptr,
                      nullptr) &&
           rho_u_star(3, path3, rhor, ur, pr, p0, idr, rhor, (p0 > pr) ? rhor * 1.1 : rhor * 0.9, rhor0, ur0, nullptr,
@@ -779,7 +793,7 @@ struct RiemannSolver {
   }
 
   // ComputeRiemannSolution (59-342).
-  // Warm start (no counterpart in the reference): a finite positive warm_p
+  // Warm start (no counterpart in the reference): a finite non-zero warm_p
   // supplies the two starting points of the bracket search (see
   // feasible_points); the bracket expansion, the safeguarded secant loop and
   // its stopping test are the reference's, so a warm-started solve converges

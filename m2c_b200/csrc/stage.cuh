@@ -221,35 +221,6 @@ __device__ __forceinline__ const Eos<T>& eos_of(const SchemeK& s, int id) {
   return EosPick<T>::get(s, MULTI ? (id < s.nmat ? id : 0) : 0);
 }
 
-// Reconstructed face states of one real cell and the revert mask
-// (bit 0 l, 1 r, 2 b, 3 t, 4 k, 5 f). Returns ERR_NONE or ERR_STATE.
-template <typename T>
-__device__ __forceinline__ int cell_faces(const Eos<T>& e, const T* v, const T* sx, const T* sy, const T* sz,
-                                          uint8_t& mask) {
-  uint8_t m = 0;
-  bool chain_done = false;
-  int err = ERR_NONE;
-  // faces in the reference's order l, r, b, t, k, f
-#pragma unroll
-  for (int q = 0; q < 6; q++) {
-    const T* s = q < 2 ? sx : (q < 4 ? sy : sz);
-    T f[5];
-#pragma unroll
-    for (int p = 0; p < 5; p++) f[p] = (q & 1) ? v[p] + T(0.5) * s[p] : v[p] - T(0.5) * s[p];
-    const bool bad = e.bad(f);
-    bool reverted = false;
-    // Reconstructor.cpp:719-775: only the first non-physical face is reverted.
-    if (!chain_done && bad) { reverted = true; chain_done = true; }
-    // SpaceOperator.cpp:3240-3273: a face needing clipping reverts to the cell value.
-    if (!reverted && e.needs_clip(f)) reverted = true;
-    if (reverted) m |= uint8_t(1u << q);
-    // SpaceOperator.cpp:3275-3277: a face still non-physical is fatal.
-    else if (bad) err = ERR_STATE;
-  }
-  mask = m;
-  return err;
-}
-
 // Boundary face state built from the interior neighbour's face state
 // (Reconstructor.cpp:822-875) followed by the clip check of
 // CheckReconstructedStates on the ghost's inward face (3279-3318).
@@ -625,74 +596,104 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     return ok;
   };
 
-  // (2) slopes and revert mask of plane p
-  auto mask_plane = [&](int p) {
+  // (2) slopes and revert bits of the real cell at mask-region (mx, my) of
+  // plane p. A cell of the tile (own) gets all three directions; a halo cell
+  // only the direction dh (0: x, 1: y) across which the tile's faces read it
+  // (x-halo cells feed only the tile's x faces, y-halo cells its y faces).
+  // Its revert bits then follow the revert rule below for that direction's
+  // two faces alone; the rule differs from the full cell's only where two
+  // faces are non-physical, which the cell's own tile reports as an error.
+  // Revert bits: bit 2d + side (0 minus face, 1 plus face), 0x40 for a
+  // conservative-variable face state.
+  auto mask_cell = [&](int p, int mx, int my, bool own, int dh) {
     const int s0 = slot4(p), ms = p & 1;
-    const int ka = wrap_index(p, g.nz);
-    for (int q = tid; q < S::MY * S::MX; q += NT) {
-      const int my = q / S::MX, mx = q - my * S::MX;
-      const int ly = my + 1, lx = mx + 1;  // position in the loaded region
-      if (!sm.real[s0][ly][lx]) {
-        sm.mask[ms][my][mx] = 0;
-        continue;
-      }
-      const uint8_t id = sm.ids[s0][ly][lx];
-      const Eos<T>& e = eos_of<T, MULTI>(a.s, id);
-      T v[5], sx[5], sy[5], sz[5];
+    const int ly = my + 1, lx = mx + 1;  // position in the loaded region
+    if (!sm.real[s0][ly][lx]) {
+      sm.mask[ms][my][mx] = 0;
+      return;
+    }
+    const uint8_t id = sm.ids[s0][ly][lx];
+    const Eos<T>& e = eos_of<T, MULTI>(a.s, id);
+    T v[5];
 #pragma unroll
-      for (int c = 0; c < 5; c++) v[c] = M2C_VV(s0, c, ly, lx);
-      uint8_t m = 0;
-      int err = ERR_NONE;
-      bool cons = false;
-      if (CONS && rec_linear) {
-        // non-primitive variables; any non-physical face sends the cell back
-        // to primitive variables (the RETRY of Reconstructor.cpp:719-775)
-        const int rv = a.s.rec_var;
-        const bool uspace = rv != 2;
-        T u[5];
-        e.p2c(v, u);
-        bool okb = nonprim_slopes(p, lx, ly, 0, rv, e, v, u, sx);
-        okb = nonprim_slopes(p, lx, ly, 1, rv, e, v, u, sy) && okb;
-        okb = nonprim_slopes(p, lx, ly, 2, rv, e, v, u, sz) && okb;
-        if (!okb) err = ERR_SOUND;
-        cons = true;
-        uint8_t clipm = 0;
+    for (int c = 0; c < 5; c++) v[c] = M2C_VV(s0, c, ly, lx);
+    uint8_t m = 0;
+    int err = ERR_NONE;
+    bool cons = false;
+    if (CONS && rec_linear) {
+      // non-primitive variables; any non-physical face sends the cell back
+      // to primitive variables (the RETRY of Reconstructor.cpp:719-775).
+      // Halo cells take this path whole (the tile's cells and its halo ring).
+      T sx[5], sy[5], sz[5];
+      const int rv = a.s.rec_var;
+      const bool uspace = rv != 2;
+      T u[5];
+      e.p2c(v, u);
+      bool okb = nonprim_slopes(p, lx, ly, 0, rv, e, v, u, sx);
+      okb = nonprim_slopes(p, lx, ly, 1, rv, e, v, u, sy) && okb;
+      okb = nonprim_slopes(p, lx, ly, 2, rv, e, v, u, sz) && okb;
+      if (!okb) err = ERR_SOUND;
+      cons = true;
+      uint8_t clipm = 0;
 #pragma unroll
-        for (int q = 0; q < 6; q++) {
-          const T* sg = q < 2 ? sx : (q < 4 ? sy : sz);
-          T f[5];
-          if (uspace) {
-            T uf[5];
+      for (int q = 0; q < 6; q++) {
+        const T* sg = q < 2 ? sx : (q < 4 ? sy : sz);
+        T f[5];
+        if (uspace) {
+          T uf[5];
 #pragma unroll
-            for (int c = 0; c < 5; c++) uf[c] = (q & 1) ? u[c] + T(0.5) * sg[c] : u[c] - T(0.5) * sg[c];
-            e.c2p(uf, f);
-          } else {
+          for (int c = 0; c < 5; c++) uf[c] = (q & 1) ? u[c] + T(0.5) * sg[c] : u[c] - T(0.5) * sg[c];
+          e.c2p(uf, f);
+        } else {
 #pragma unroll
-            for (int c = 0; c < 5; c++) f[c] = (q & 1) ? v[c] + T(0.5) * sg[c] : v[c] - T(0.5) * sg[c];
-          }
-          if (e.bad(f)) cons = false;
-          else if (e.needs_clip(f)) clipm |= uint8_t(1u << q);  // SpaceOperator.cpp:3240-3273
+          for (int c = 0; c < 5; c++) f[c] = (q & 1) ? v[c] + T(0.5) * sg[c] : v[c] - T(0.5) * sg[c];
         }
-        if (cons) m = uint8_t(clipm | (uspace ? 0x40 : 0));
+        if (e.bad(f)) cons = false;
+        else if (e.needs_clip(f)) clipm |= uint8_t(1u << q);  // SpaceOperator.cpp:3240-3273
       }
-      if (!cons) {
-        slopes(p, lx, ly, 0, sx);
-        slopes(p, lx, ly, 1, sy);
-        slopes(p, lx, ly, 2, sz);
-        const int err2 = cell_faces(e, v, sx, sy, sz, m);
-        if (err2) err = err2;
-      }
+      if (cons) {
+        m = uint8_t(clipm | (uspace ? 0x40 : 0));
 #pragma unroll
-      for (int c = 0; c < 5; c++) {
-        sm.sig[ms][0][c][my][mx] = sx[c];
-        sm.sig[ms][1][c][my][mx] = sy[c];
-        sm.sig[ms][2][c][my][mx] = sz[c];
+        for (int c = 0; c < 5; c++) {
+          sm.sig[ms][0][c][my][mx] = sx[c];
+          sm.sig[ms][1][c][my][mx] = sy[c];
+          sm.sig[ms][2][c][my][mx] = sz[c];
+        }
       }
-      sm.mask[ms][my][mx] = m;
-      if (err) {
-        const int ia = wrap_index(i0 + mx - 1, g.nx), ja = wrap_index(j0 + my - 1, g.ny);
-        report(a.err, err, (int)(((long long)ka * g.ny + ja) * g.nx + ia), where + 1);
+    }
+    if (!cons) {
+      // primitive slopes direction by direction, each direction's faces in
+      // the reference's order (l, r, b, t, k, f)
+      const int dlo = (own || CONS) ? 0 : dh, dhi = (own || CONS) ? 2 : dh;
+      bool chain_done = false;
+#pragma unroll 1
+      for (int d = dlo; d <= dhi; d++) {
+        T sd[5];
+        slopes(p, lx, ly, d, sd);
+#pragma unroll
+        for (int c = 0; c < 5; c++) sm.sig[ms][d][c][my][mx] = sd[c];
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+          T f[5];
+#pragma unroll
+          for (int c = 0; c < 5; c++) f[c] = side ? v[c] + T(0.5) * sd[c] : v[c] - T(0.5) * sd[c];
+          const bool bad = e.bad(f);
+          bool reverted = false;
+          // Reconstructor.cpp:719-775: only the first non-physical face is reverted.
+          if (!chain_done && bad) { reverted = true; chain_done = true; }
+          // SpaceOperator.cpp:3240-3273: a face needing clipping reverts to the cell value.
+          if (!reverted && e.needs_clip(f)) reverted = true;
+          if (reverted) m |= uint8_t(1u << (2 * d + side));
+          // SpaceOperator.cpp:3275-3277: a face still non-physical is fatal.
+          else if (bad) err = ERR_STATE;
+        }
       }
+    }
+    sm.mask[ms][my][mx] = m;
+    if (err && (own || CONS)) {
+      const int ka = wrap_index(p, g.nz);
+      const int ia = wrap_index(i0 + mx - 1, g.nx), ja = wrap_index(j0 + my - 1, g.ny);
+      report(a.err, err, (int)(((long long)ka * g.ny + ja) * g.nx + ia), where + 1);
     }
   };
 
@@ -830,31 +831,68 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     if (err) report(a.err, err, -1, where + 2);
   };
 
-  // All faces needed by plane m: x and y faces of plane m (if do_xy) and the
-  // z faces m+1/2, one work item per face.
+  // (3a) the faces of plane m owned by this thread: the x face left of its
+  // cell, the y face below it (if do_xy) and the z face m+1/2 above it; one
+  // call site, so the flux code is inlined once.
   auto faces = [&](int m, bool do_xy) {
-    const int nxy = do_xy ? S::NFX + S::NFY : 0;
-    const int nall = nxy + S::NFZ;
     const int zs = (m + 1) & 1;
-    for (int q = tid; q < nall; q += NT) {
+#pragma unroll 1
+    for (int k = do_xy ? 0 : 2; k < 3; k++) {
+      const int d = k;
+      const int mxL = k == 0 ? tx : tx + 1, myL = k == 1 ? ty : ty + 1;
+      const int pR = k == 2 ? m + 1 : m;
+      T* dst = k == 0 ? &sm.fx[0][ty * (TX + 1) + tx] : (k == 1 ? &sm.fy[0][ty * TX + tx] : &sm.fz[zs][0][ty * TX + tx]);
+      const int stride = k == 0 ? S::NFX : (k == 1 ? S::NFY : S::NFZ);
       T F[5], F2[5];
-      if (q < S::NFX && do_xy) {              // x face left of (fxi, fyi)
-        const int fyi = q / (TX + 1), fxi = q - fyi * (TX + 1);
-        face_flux(0, m, fxi, fyi + 1, m, fxi + 1, fyi + 1, F, F2);
+      face_flux(d, m, mxL, myL, pR, tx + 1, ty + 1, F, F2);
 #pragma unroll
-        for (int c = 0; c < 5; c++) sm.fx[c][q] = F[c];
-      } else if (q < nxy) {                   // y face below (fxi, fyi)
-        const int r = q - S::NFX;
-        const int fyi = r / TX, fxi = r - fyi * TX;
-        face_flux(1, m, fxi + 1, fyi, m, fxi + 1, fyi + 1, F, F2);
+      for (int c = 0; c < 5; c++) dst[c * stride] = F[c];
+    }
+  };
+
+  // (2) + (3b) one phase: slopes and revert bits of plane p (do_mask): the
+  // tile's cells, one per thread, then the halo cells in their single
+  // direction; and the tile's right x faces and top y faces of plane mf
+  // (do_bf), whose cells' slopes are complete since the previous plane.
+  // Spreading the halo cells and those faces over the threads that have no
+  // second item keeps the phase at about one cell and a third per thread.
+  auto mask_and_edge_faces = [&](int p, bool do_mask, int mf, bool do_bf) {
+    constexpr int NH = CONS ? S::MX * S::MY - NT : 2 * (TX + TY);  // halo items
+    constexpr int NB = TX + TY;                                     // edge faces
+    for (int q = tid; q < NT + NH + NB; q += NT) {
+      if (q < NT + NH) {
+        if (!do_mask) continue;
+        const int r = q - NT;
+        int mx = tx + 1, my = ty + 1, dh = 0;
+        if (r < 0) {
+          // a cell of the tile
+        } else if (CONS) {  // the ring of the mask region: bottom row, top row, then the two side columns
+          if (r < S::MX) { mx = r; my = 0; }
+          else if (r < 2 * S::MX) { mx = r - S::MX; my = S::MY - 1; }
+          else { const int r2 = r - 2 * S::MX; mx = (r2 & 1) ? S::MX - 1 : 0; my = 1 + (r2 >> 1); }
+        } else if (r < 2 * TY) {  // x-halo columns (mx = 0, TX + 1)
+          mx = r < TY ? 0 : TX + 1;
+          my = (r < TY ? r : r - TY) + 1;
+        } else {                  // y-halo rows (my = 0, TY + 1)
+          const int r2 = r - 2 * TY;
+          mx = (r2 < TX ? r2 : r2 - TX) + 1;
+          my = r2 < TX ? 0 : TY + 1;
+          dh = 1;
+        }
+        mask_cell(p, mx, my, r < 0, dh);
+      } else {
+        if (!do_bf) continue;
+        const int r = q - NT - NH;
+        const bool xf = r < TY;  // x face right of the tile's last column (row r), else
+                                 // y face above its top row (column r - TY)
+        const int fx = r - TY;
+        T F[5], F2[5];
+        face_flux(xf ? 0 : 1, mf, xf ? TX : fx + 1, xf ? r + 1 : TY, mf, xf ? TX + 1 : fx + 1, xf ? r + 1 : TY + 1, F,
+                  F2);
+        T* dst = xf ? &sm.fx[0][r * (TX + 1) + TX] : &sm.fy[0][TY * TX + fx];
+        const int stride = xf ? S::NFX : S::NFY;
 #pragma unroll
-        for (int c = 0; c < 5; c++) sm.fy[c][r] = F[c];
-      } else {                                // z face m+1/2 of column (fxi, fyi)
-        const int r = q - nxy;
-        const int fyi = r / TX, fxi = r - fyi * TX;
-        face_flux(2, m, fxi + 1, fyi + 1, m + 1, fxi + 1, fyi + 1, F, F2);
-#pragma unroll
-        for (int c = 0; c < 5; c++) sm.fz[zs][c][r] = F[c];
+        for (int c = 0; c < 5; c++) dst[c * stride] = F[c];
       }
     }
   };
@@ -908,7 +946,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
           for (int c = 0; c < 5; c++) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.Us[c] + offp));
         }
       }
-      if (m + 1 >= kb - 1 && !plane_is_ghost(m + 1)) mask_plane(m + 1);
+      mask_and_edge_faces(m + 1, m + 1 >= kb - 1 && !plane_is_ghost(m + 1), m, m >= kb);
       __syncthreads();
       if (m >= kb - 1) faces(m, m >= kb);
       __syncthreads();

@@ -435,11 +435,12 @@ class Mlp:
 
 def mlp_features_pairs(mats, VL, VR, dirs):
     """Network input features of per-pair problems: X [n, 16] (float32),
-    base pressure pac [n], valid [n]."""
+    scale [n, 2] = (base B, shift S) of the target log((p* + S) / B),
+    valid [n]."""
     VL, VR, dirs = (np.ascontiguousarray(a, np.float64) for a in (VL, VR, dirs))
     n = len(VL)
     X = np.zeros((n, 16), np.float32)
-    P = np.zeros(n)
+    P = np.zeros((n, 2))
     valid = np.zeros(n, np.int32)
     check(lib().m2cg_mlp_features_pairs(abi.material_array(mats), n, abi.dptr(VL), abi.dptr(VR), abi.dptr(dirs),
                                         _fptr(X), abi.dptr(P), abi.iptr(valid)))

@@ -45,16 +45,16 @@ def solve(s, mats, VL, VR, dirs, warm=None, chunk=250_000):
 
 
 def training_set(n, seed, s=None):
-    """Features X [m, 16] and targets y = log(p*/pac) (pac: the acoustic
-    estimate returned as the features' base pressure) of the solvable
-    problems (solver OK, p* > 0, features valid) among n samples."""
+    """Features X [m, 16] and targets y = log((p* + S) / B) (B, S: the base
+    and shift the features return; B is the shifted acoustic estimate) of
+    the solvable problems (solver OK, features valid) among n samples."""
     s = s or abi.scheme()
     mats, VL, VR, dirs = sample_problems(n, seed)
     r = solve(s, mats, VL, VR, dirs)
     X, P, valid = gpu.mlp_features_pairs(mats, VL, VR, dirs)
-    ps = r["Vsm"][:, 4]
-    keep = (r["err"] == 0) & (ps > 0) & (valid != 0)
-    y = np.log(ps[keep] / P[keep]).astype(np.float32)
+    q = r["Vsm"][:, 4] + P[:, 1]
+    keep = (r["err"] == 0) & (q > 0) & (valid != 0)
+    y = np.log(q[keep] / P[keep, 0]).astype(np.float32)
     return X[keep], y, keep.mean()
 
 

@@ -67,6 +67,7 @@ extern "C" int host_riemann(const m2cg_scheme* s, const m2cg_material* mats, int
   P.failure_threshold = s->riem_failure_threshold;
   P.pressure_at_failure = s->riem_pressure_at_failure;
   P.warm_delta = s->riem_warm_delta;
+  P.warm_gate = s->riem_warm_gate;
   const int cap = 512;  // the device solver's path capacity (riemann_batch.h)
   std::vector<double> scratch(2 * 3 * cap);
   RiemannSolver rs;

@@ -103,10 +103,12 @@ def _warm_vs_cold(net):
     dp = np.abs(ph - pc) / P
     ev_c, ev_h = cold["evals"][both].mean(), hot["evals"][both].mean()
     it_c, it_h = cold["iters"][both].mean(), hot["iters"][both].mean()
-    ok = (cold["err"] == 0) & (cold["Vsm"][:, 4] > 0) & np.isfinite(warm)
-    rel = np.abs(np.log(warm[ok] / cold["Vsm"][ok, 4]))
+    # proposal error on the shifted scale p + min(pinf_l, pinf_r), as trained
+    sh = np.minimum(mats["p_c"][0::2], mats["p_c"][1::2])
+    ok = (cold["err"] == 0) & (cold["Vsm"][:, 4] + sh > 0) & np.isfinite(warm) & (warm + sh > 0)
+    rel = np.abs(np.log((warm[ok] + sh[ok]) / (cold["Vsm"][ok, 4] + sh[ok])))
     print(f"\nwarm start: evaluations {ev_c:.3f} -> {ev_h:.3f} ({ev_c / ev_h:.2f}x), "
-          f"secant iterations {it_c:.3f} -> {it_h:.3f}; |log(p/p*)| median {np.median(rel):.2e} "
+          f"secant iterations {it_c:.3f} -> {it_h:.3f}; |log((p+S)/(p*+S))| median {np.median(rel):.2e} "
           f"p90 {np.percentile(rel, 90):.2e}; |dp*|/P p99 {np.percentile(dp, 99):.2e} max {dp.max():.2e}")
     # the solver decides: both solves pass its stopping test (velocity
     # mismatch below tol_main x max sound speed, or a bracket narrower than
