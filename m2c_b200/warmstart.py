@@ -32,6 +32,42 @@ def sample_problems(n, seed):
     return mats, VL, VR, dirs
 
 
+def sample_cluster_problems(n, seed):
+    """n seeded interface problems of the bubble-cluster kind: water
+    (stiffened gas gamma 6.12, p_inf 3.43e8 Pa, density log-uniform in
+    990..1400 kg/m^3) against air (gamma 1.4, density log-uniform in
+    1..300 kg/m^3), on either side; both sides near one base state (pressure
+    log-uniform in 1e5..3e9 Pa, velocity uniform in +-700 m/s) with relative
+    pressure and velocity departures log-uniform in 1e-4..0.5, so that the
+    set runs from near-acoustic problems (most of the cluster's interface
+    faces) to strong waves (the collapse)."""
+    rng = np.random.default_rng(seed)
+    water_left = rng.uniform(size=n) < 0.5
+    gam = np.empty(2 * n)
+    pinf = np.empty(2 * n)
+    gam[0::2] = np.where(water_left, 6.12, 1.4)
+    gam[1::2] = np.where(water_left, 1.4, 6.12)
+    pinf[0::2] = np.where(water_left, 3.43e8, 0.0)
+    pinf[1::2] = np.where(water_left, 0.0, 3.43e8)
+    mats = abi.material_table(gam, pinf)
+    p0 = 10.0 ** rng.uniform(5.0, np.log10(3e9), n)
+    u0 = rng.uniform(-700.0, 700.0, n)
+    rw = 10.0 ** rng.uniform(np.log10(990.0), np.log10(1400.0), n)
+    ra = 10.0 ** rng.uniform(0.0, np.log10(300.0), n)
+    VL = np.zeros((n, 5))
+    VR = np.zeros((n, 5))
+    VL[:, 0] = np.where(water_left, rw, ra)
+    VR[:, 0] = np.where(water_left, ra, rw)
+    for V in (VL, VR):
+        dp = 10.0 ** rng.uniform(-4.0, np.log10(0.5), n) * rng.choice([-1.0, 1.0], n)
+        du = 10.0 ** rng.uniform(-4.0, np.log10(0.5), n) * rng.choice([-1.0, 1.0], n)
+        V[:, 4] = p0 * (1.0 + dp)
+        V[:, 1] = u0 + du * np.maximum(np.abs(u0), 10.0)
+    dirs = np.zeros((n, 3))
+    dirs[:, 0] = 1.0
+    return mats, VL, VR, dirs
+
+
 def solve(s, mats, VL, VR, dirs, warm=None, chunk=250_000):
     """Exact solves in chunks; returns dict of arrays (Vs, id, Vsm, Vsp, iters, evals, err)."""
     out = {k: [] for k in ("Vs", "id", "Vsm", "Vsp", "iters", "evals", "err")}
@@ -44,12 +80,18 @@ def solve(s, mats, VL, VR, dirs, warm=None, chunk=250_000):
     return {k: np.concatenate(v) for k, v in out.items()}
 
 
-def training_set(n, seed, s=None):
+def training_set(n, seed, s=None, cluster_fraction=0.25):
     """Features X [m, 16] and targets y = log((p* + S) / B) (B, S: the base
     and shift the features return; B is the shifted acoustic estimate) of
-    the solvable problems (solver OK, features valid) among n samples."""
+    the solvable problems (solver OK, features valid) among n samples, a
+    fraction cluster_fraction of them of the bubble-cluster kind."""
     s = s or abi.scheme()
-    mats, VL, VR, dirs = sample_problems(n, seed)
+    nc = int(round(n * cluster_fraction))
+    mats, VL, VR, dirs = sample_problems(n - nc, seed)
+    if nc:
+        parts = [(mats, VL, VR, dirs), sample_cluster_problems(nc, seed + 1)]
+        mats = np.concatenate([q[0] for q in parts])
+        VL, VR, dirs = (np.concatenate([q[k] for q in parts]) for k in (1, 2, 3))
     r = solve(s, mats, VL, VR, dirs)
     X, P, valid = gpu.mlp_features_pairs(mats, VL, VR, dirs)
     q = r["Vsm"][:, 4] + P[:, 1]
