@@ -76,6 +76,11 @@ typedef struct {
   double q;               /* NASG energyConstant */
   double rhomin, pmin, rhomax, pmax;
   double failsafe_density;
+  /* ViscosityModelData CONSTANT (ViscoFcnConstant, ViscoFcn.h): dynamic and
+   * bulk viscosity [Pa s]; both 0 = NONE (inviscid). With any material
+   * viscous, the stage adds the viscous fluxes of ViscosityOperator::
+   * AddDiffusionFluxes (ViscosityOperator.cpp:200-408) to the residual. */
+  double mu, mu_bulk;
 } m2cg_material;
 
 /* Numerical scheme (SchemeData, ReconstructionData, TsData, MultiPhaseData,

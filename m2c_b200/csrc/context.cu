@@ -21,6 +21,7 @@
 #include "../../include/m2c_gpu.h"
 #include "launch.h"
 #include "multiphase.h"
+#include "viscous.h"
 
 using namespace m2c;
 
@@ -166,6 +167,7 @@ struct m2cg_ctx {
   bool rs_valid = false;  // the multiphase star states stored by the last step match the resident state
   m2cg_counters counters = {};
   Multiphase* mp = nullptr;  // two-material machinery (nullptr for one material)
+  Viscous* visc = nullptr;   // viscous fluxes (nullptr when every material is inviscid)
   // probes (ProbeOutput): per probe the lower node (i, j, k), the trilinear
   // coordinates and the valid-corner mask; records sampled on the device
   int nprobe = 0, probe_every = 0, probe_cap = 0, probe_count = 0;
@@ -440,6 +442,12 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
     st = multiphase_create(c->stream, g, sk, *scheme, mats, nmat, *ls, xc, dxs, &c->mp);
     if (st) fail(st, "two-material setup refused or failed (status %d): interface options or level-set settings", (int)st);
   }
+  if (!st) {
+    const double* xc[3] = {c->hxc.data(), c->hyc.data(), c->hzc.data()};
+    const double* dxs[3] = {c->hdx.data(), c->hdy.data(), c->hdz.data()};
+    st = viscous_create(c->stream, g, mats, nmat, xc, dxs, &c->visc);
+    if (st) fail(st, "viscous-flux buffers could not be allocated");
+  }
   if (st) {
     m2cg_destroy(c);
     return st;
@@ -476,6 +484,7 @@ extern "C" m2cg_status m2cg_destroy(m2cg_ctx* c) {
   cudaFree(c->stage_buf);
   cudaFree(c->probe_ijk); cudaFree(c->probe_xi); cudaFree(c->probe_rec);
   if (c->mp) multiphase_destroy(c->mp);
+  if (c->visc) viscous_destroy(c->visc);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return M2CG_OK;
@@ -865,6 +874,10 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
       m2cg_status st = multiphase_stage(c->mp, c->stream, a);
       if (st) return st;
     }
+    if (c->visc) {
+      m2cg_status sv = viscous_faces(c->visc, c->stream, a, mixed);
+      if (sv) return fail(sv, "viscous-flux launch failed");
+    }
     m2cg_status st = launch_stage(c, a);
     if (st) return st;
   }
@@ -972,6 +985,10 @@ extern "C" m2cg_status m2cg_compute_residual(m2cg_ctx* c, double* R_host) {
     }
     st = multiphase_stage(c->mp, c->stream, a);
     if (st) return st;
+  }
+  if (c->visc) {
+    m2cg_status sv = viscous_faces(c->visc, c->stream, a, c->scheme.precision == M2CG_PREC_MIXED);
+    if (sv) return fail(sv, "viscous-flux launch failed");
   }
   m2cg_status st = launch_stage(c, a);
   if (st) return st;

@@ -115,6 +115,17 @@ struct IfaceView {
   double* faces_out;
 };
 
+// Viscous face fluxes (area-weighted; momentum x, y, z and energy, the mass
+// component being zero): fr[d] is added by the right cell of a face of axis
+// d, fl[d] subtracted by its left cell; [4][faces], faces of axis d indexed
+// x: (k ny + j)(nx + 1) + i, y: (k (ny + 1) + j) nx + i, z: (k ny + j) nx + i
+// with (i, j, k) the face's right cell. fr[0] == NULL: inviscid.
+struct ViscView {
+  const double* fr[3];
+  const double* fl[3];
+  long long nf[3];
+};
+
 struct StageArgs {
   Grid3 g;
   SchemeK s;
@@ -139,6 +150,7 @@ struct StageArgs {
   int nitems;            // CTAs that share the (tile, plane) units evenly
   double* Ro[5];         // if set: write the residual R only (no RK update)
   IfaceView iface;
+  ViscView visc;
   int use_tma;           // planes by tensor copy (x and y not periodic, maps built)
   CUtensorMap tin;       // 4D map of the stage input (Pin as one five-component buffer)
 };
@@ -1040,6 +1052,26 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
           // of two nearby FP32 fluxes is exact), one conversion per component
           f = double((sm.fx[c][fxl + 1] - fl) * axf + (sm.fy[c][fyl + TX] - gl) * ayf +
                      (sm.fz[zr][c][fzc] - hl) * azf);
+        }
+        if (a.visc.fr[0]) {
+          // viscous fluxes (ViscosityOperator::AddDiffusionFluxes), added to
+          // the flux sum in its cell order: this cell's low x, y, z faces,
+          // then the low faces of its +x, +y, +z neighbours
+          if (c == 0) {
+            f = f + 0.0; f = f + 0.0; f = f + 0.0;
+            f = f - 0.0; f = f - 0.0; f = f - 0.0;
+          } else {
+            const long long S = a.visc.nf[0], cc = (long long)(c - 1) * S;
+            const long long fxi = ((long long)m * g.ny + gj) * (g.nx + 1) + gi;
+            const long long fyi = ((long long)m * (g.ny + 1) + gj) * g.nx + gi;
+            const long long fzi = ((long long)m * g.ny + gj) * g.nx + gi;
+            f = f + a.visc.fr[0][cc + fxi];
+            f = f + a.visc.fr[1][cc + fyi];
+            f = f + a.visc.fr[2][cc + fzi];
+            f = f - a.visc.fl[0][cc + fxi + 1];
+            f = f - a.visc.fl[1][cc + fyi + g.nx];
+            f = f - a.visc.fl[2][cc + fzi + (long long)g.ny * g.nx];
+          }
         }
         const double R = f * inv_mvol;
         if (a.Ro[0]) a.Ro[c][off] = R;

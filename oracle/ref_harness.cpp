@@ -29,6 +29,8 @@
 #include <MultiPhaseOperator.h>
 #include <TimeIntegrator.h>
 #include <Utils.h>
+#include <Interpolator.h>
+#include <GradientCalculatorCentral.h>
 
 #include <chrono>
 #include <cmath>
@@ -66,6 +68,8 @@ struct RefCase {
   TimeIntegratorBase* integrator = nullptr;
   SpaceVariable3D* V = nullptr;
   SpaceVariable3D* ID = nullptr;
+  InterpolatorLinear* interp = nullptr;         // viscous fluxes (Main.cpp:195-205)
+  GradientCalculatorCentral* grad = nullptr;
   int NX = 0, NY = 0, NZ = 0;
   double t = 0.0;
   int time_step = 0;
@@ -88,6 +92,11 @@ void fill_material(MaterialModelData* d, const m2cg_material& m) {
   d->nasgModel.pressureConstant = m.p_c;
   d->nasgModel.volumeConstant = m.b;
   d->nasgModel.energyConstant = m.q;
+  if (m.mu != 0.0 || m.mu_bulk != 0.0) {
+    d->viscosity.type = ViscosityModelData::CONSTANT;
+    d->viscosity.dynamicViscosity = m.mu;
+    d->viscosity.bulkViscosity = m.mu_bulk;
+  }
 }
 
 void fill_scheme(IoData& iod, const m2cg_scheme& s) {
@@ -236,6 +245,14 @@ void* m2cref_create(const m2cg_grid* g, const m2cg_scheme* s, const m2cg_materia
   c->dms = new DataManagers3D(c->comm, c->NX, c->NY, c->NZ);
   c->gmi->GetSubdomainInfo(c->comm, *c->dms);
   c->spo = new SpaceOperator(c->comm, *c->dms, iod, c->vf, *c->ff, *c->riemann, *c->gmi, false);
+  bool viscous = false;
+  for (int m = 0; m < nmat; m++) viscous = viscous || mats[m].mu != 0.0 || mats[m].mu_bulk != 0.0;
+  if (viscous) {  // Main.cpp:195-205: linear interpolation + central differences for the viscous terms
+    c->interp = new InterpolatorLinear(c->comm, *c->dms, c->spo->GetMeshCoordinates(), c->spo->GetMeshDeltaXYZ());
+    c->grad = new GradientCalculatorCentral(c->comm, *c->dms, c->spo->GetMeshCoordinates(), c->spo->GetMeshDeltaXYZ(),
+                                            *c->interp);
+    c->spo->SetupViscosityOperator(c->interp, c->grad, false);
+  }
 
   c->V = new SpaceVariable3D(c->comm, &(c->dms->ghosted1_5dof));
   c->ID = new SpaceVariable3D(c->comm, &(c->dms->ghosted1_1dof));
@@ -375,6 +392,8 @@ void m2cref_destroy(void* h) {
   c->ID->Destroy(); delete c->ID;
   c->spo->Destroy();
   delete c->spo;
+  if (c->grad) { c->grad->Destroy(); delete c->grad; }
+  if (c->interp) { c->interp->Destroy(); delete c->interp; }
   c->dms->DestroyAllDataManagers();
   delete c->dms;
   delete c->gmi;
