@@ -949,7 +949,7 @@ static cudaError_t autotune(m2cg_batch* b, int fix_threads, int fix_cpb, int fix
 static int van_albada_k() {
   // uniform tube meshes: A = B = 1 (Reconstructor.cpp:103-121)
   for (int k = 2; k < 1000; k++) {
-    const double rhs = 2.0 / (1.0 + pow((k - 1.0) / k, k - 1) / k) * std::min(1.0, 1.0);
+    const double rhs = 2.0 / (1.0 + m2c::cr_pow_int((k - 1.0) / k, k - 1) / k) * std::min(1.0, 1.0);
     if (1.0 <= rhs) return k;
   }
   return -1;

@@ -262,7 +262,7 @@ static bool axis_limiter(const std::vector<double>& dx, bool periodic, int limit
     if (limiter == M2CG_LIM_VANALBADA) {
       int k;
       for (k = 2; k < 1000; k++) {
-        double rhs = 2.0 / (1.0 + pow((k - 1.0) / k, k - 1) / k) * std::min(A[i], 1.0);
+        double rhs = 2.0 / (1.0 + m2c::cr_pow_int((k - 1.0) / k, k - 1) / k) * std::min(A[i], 1.0);
         if (B[i] <= rhs) break;
       }
       if (k >= 999) return false;

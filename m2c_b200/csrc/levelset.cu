@@ -101,7 +101,7 @@ m2cg_status levelset_geom_create(cudaStream_t s, const Grid3& g, const m2cg_leve
       if (ls.solver == M2CG_LS_FINITE_VOLUME && ls.limiter == M2CG_LIM_VANALBADA) {
         int k;
         for (k = 2; k < 1000; k++) {
-          const double rhs = 2.0 / (1.0 + pow((k - 1.0) / k, k - 1) / k) * std::min(fA[a][i], 1.0);
+          const double rhs = 2.0 / (1.0 + m2c::cr_pow_int((k - 1.0) / k, k - 1) / k) * std::min(fA[a][i], 1.0);
           if (fB[a][i] <= rhs) break;
         }
         if (k >= 999) return M2CG_ERR_ARG;

@@ -171,13 +171,40 @@ M2C_HD T lim_genminmod(T A, T B, T alpha, T dq0, T dq1) {
   return T(0);
 }
 
-// x^k for a small positive integer k by repeated multiplication; for k = 2
-// (uniform meshes) this is the correctly rounded square, equal to pow(x, 2).
+// x^k, correctly rounded, for an integer k >= 1 (the van Albada limiter's
+// exponent and the setup of that exponent, Reconstructor.h:107-108,
+// Reconstructor.cpp:109). x^2 is the correctly rounded square; a higher
+// power is carried as a double-double product (each step an exact fma
+// product plus the low part's cross terms, relative error below k 2^-104)
+// and rounded once, so it is the correctly rounded value except within
+// ~k 2^-104 of a rounding midpoint. The reference takes these powers from
+// the C library's pow, which rounds the other way on about 1e-3 of
+// arguments (x^2 included); with these the host build, the oracle's
+// correctly rounded build and the GPU agree bit for bit.
+M2C_HD double cr_pow_int(double x, int k) {
+  if (k <= 1) return k == 1 ? x : 1.0;
+  if (k == 2) return x * x;
+  double h = x, l = 0.0;
+  for (int i = 1; i < k; i++) {
+    const double p = h * x;
+    const double e = fma(h, x, -p) + l * x;  // exact low part of h x, plus l x
+    h = p + e;                                // renormalise (|e| << |p|)
+    l = e - (h - p);
+  }
+  return h;
+}
+
+// x^k in the compute type: FP64 correctly rounded (cr_pow_int), FP32 by
+// repeated multiplication (the mixed path's flux half).
 template <typename T>
 M2C_HD T ipow(T x, int k) {
-  T r = x;
-  for (int i = 1; i < k; i++) r = r * x;
-  return r;
+  if constexpr (sizeof(T) == 8) {
+    return cr_pow_int(x, k);
+  } else {
+    T r = x;
+    for (int i = 1; i < k; i++) r = r * x;
+    return r;
+  }
 }
 
 template <typename T>
