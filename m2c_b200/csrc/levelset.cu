@@ -161,6 +161,7 @@ __device__ double ls_residual(const Grid3& g, const LsGeom& geo, const double* p
   const double pc = phi[off];
   const double vel[3] = {u, v, w};
   double term[3];
+#pragma unroll
   for (int a = 0; a < 3; a++) {
     const int c = a == 0 ? i : (a == 1 ? j : k);
     const bool per = g.bc[2 * a] == BC_PERIODIC;
@@ -223,7 +224,26 @@ __global__ void __launch_bounds__(256) k_ls_stage(LsStageArgs a) {
       const double inv = 1.0 / a.Us[0][off];
       u = a.Us[1][off] * inv; v = a.Us[2][off] * inv; w = a.Us[3][off] * inv;
     }
-    const double R = ls_residual(g, a.geo, a.in, i, j, k, u, v, w);
+    double R;
+    if (i >= 2 && i < g.nx - 2 && j >= 2 && j < g.ny - 2 && k >= 2 && k < g.nz - 2) {
+      // interior: every stencil point is a cell of the domain (the same
+      // arithmetic as ls_residual, without its boundary rules)
+      const double* ph = a.in + off;
+      const long long sy = g.px, sz = g.plane;
+      const double pc = ph[0];
+      const double tx = u >= 0 ? fd4(a.geo.cl[0] + 4 * i, ph[-2], ph[-1], pc, ph[1]) * u
+                               : fd4(a.geo.cr[0] + 4 * i, ph[-1], pc, ph[1], ph[2]) * u;
+      // the right-biased y derivative takes its first-order coefficients where
+      // i >= ny - 1 (the reference's index test, see ls_residual)
+      const double* cry = (g.bc[2] != BC_PERIODIC && !(i < g.ny - 1)) ? a.geo.cr1y : a.geo.cr[1];
+      const double ty = v >= 0 ? fd4(a.geo.cl[1] + 4 * j, ph[-2 * sy], ph[-sy], pc, ph[sy]) * v
+                               : fd4(cry + 4 * j, ph[-sy], pc, ph[sy], ph[2 * sy]) * v;
+      const double tz = w >= 0 ? fd4(a.geo.cl[2] + 4 * k, ph[-2 * sz], ph[-sz], pc, ph[sz]) * w
+                               : fd4(a.geo.cr[2] + 4 * k, ph[-sz], pc, ph[sz], ph[2 * sz]) * w;
+      R = (tx + ty + tz) * -1.0;
+    } else {
+      R = ls_residual(g, a.geo, a.in, i, j, k, u, v, w);
+    }
     double base;
     if (a.stage == 1)
       base = a.phin[off];

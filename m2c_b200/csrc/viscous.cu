@@ -108,23 +108,32 @@ __device__ void node_deriv(const ViscDev& d, const T* const* P, const int* c, in
   int cm[3] = {c[0], c[1], c[2]}, cp[3] = {c[0], c[1], c[2]};
   cm[t] = it - 1;
   cp[t] = it + 1;
+  // CalculateCoefficients zeroes the coefficients of every node that
+  // SpaceVariable3D::OutsidePhysicalDomainAndUnpopulated reports
+  // (SpaceVariable.h:150-158). Its x test reads (i < 0 || j >= NX), so a node
+  // with j >= NX that is a ghost in y or z counts as an unpopulated edge too
+  // (the top y-ghost row when NY >= NX): its derivative is zero.
+  const int cnt = int(c[0] < 0 || c[1] >= n[0]) + int(c[1] < 0 || c[1] >= n[1]) + int(c[2] < 0 || c[2] >= n[2]);
+  const bool zero = cnt > 1;
   double v0[3], vm[3], vp[3];
   node_vel(d, P, c[0], c[1], c[2], v0);
   if (it == 0 && ghost_other) {
-    const double coeff = 1.0 / (x[it + 1] - x[it]);
+    const double coeff = zero ? 0.0 : 1.0 / (x[it + 1] - x[it]);
+    const double cm1 = zero ? 0.0 : -coeff;
     node_vel(d, P, cp[0], cp[1], cp[2], vp);
-    for (int q = 0; q < 3; q++) out[q] = -coeff * v0[q] + coeff * vp[q];
+    for (int q = 0; q < 3; q++) out[q] = cm1 * v0[q] + coeff * vp[q];
   } else if (it == n[t] - 1 && ghost_other) {
-    const double coeff = 1.0 / (x[it] - x[it - 1]);
+    const double coeff = zero ? 0.0 : 1.0 / (x[it] - x[it - 1]);
+    const double cm1 = zero ? 0.0 : -coeff;
     node_vel(d, P, cm[0], cm[1], cm[2], vm);
-    for (int q = 0; q < 3; q++) out[q] = -coeff * vm[q] + coeff * v0[q];
+    for (int q = 0; q < 3; q++) out[q] = cm1 * vm[q] + coeff * v0[q];
   } else {
     const double dx0 = x[it] - x[it - 1];
     const double dx1 = x[it + 1] - x[it];
     const double dx2 = dx0 + dx1;
-    const double c0 = -dx1 / (dx0 * dx2);
-    const double c1 = 1.0 / dx0 - 1.0 / dx1;
-    const double c2 = dx0 / (dx1 * dx2);
+    const double c0 = zero ? 0.0 : -dx1 / (dx0 * dx2);
+    const double c1 = zero ? 0.0 : 1.0 / dx0 - 1.0 / dx1;
+    const double c2 = zero ? 0.0 : dx0 / (dx1 * dx2);
     node_vel(d, P, cm[0], cm[1], cm[2], vm);
     node_vel(d, P, cp[0], cp[1], cp[2], vp);
     for (int q = 0; q < 3; q++) out[q] = c0 * vm[q] + c1 * v0[q] + c2 * vp[q];

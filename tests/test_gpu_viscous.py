@@ -18,8 +18,8 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def viscous_box(bc, mesh=None, precision=abi.PREC_FP64, mu=2.0e-3, bulk=7.0e-4):
-    g, s, mats, V = cases.random_box(14, 11, 9, seed=5, bc=bc, rk=3, precision=precision, mesh=mesh)
+def viscous_box(bc, mesh=None, precision=abi.PREC_FP64, mu=2.0e-3, bulk=7.0e-4, dims=(14, 11, 9)):
+    g, s, mats, V = cases.random_box(*dims, seed=5, bc=bc, rk=3, precision=precision, mesh=mesh)
     mats = [abi.material(1.4, 0.0, mu=mu, mu_bulk=bulk)]
     return g, s, mats, V
 
@@ -31,11 +31,15 @@ BCS = {
 }
 
 
+@pytest.mark.parametrize("dims", [(14, 11, 9), (9, 14, 11)])
 @pytest.mark.parametrize("bcname", sorted(BCS))
-def test_viscous_residual_matches_reference(gpu, ref, bcname):
+def test_viscous_residual_matches_reference(gpu, ref, bcname, dims):
     """The residual of one stage (advective + viscous fluxes over -volume) on
-    a box with every boundary rule the viscous ghosts take."""
-    g, s, mats, V = viscous_box(BCS[bcname])
+    a box with every boundary rule the viscous ghosts take. With ny >= nx the
+    reference's ghost test (SpaceVariable.h:150-158, whose x clause reads
+    j >= NX) zeroes the velocity derivatives on the top y-ghost row and on the
+    z-ghost layers' rows j >= nx; the (9, 14, 11) box has both."""
+    g, s, mats, V = viscous_box(BCS[bcname], dims=dims)
     sol = gpu.Solver(g, s, mats)
     sol.upload(V)
     rc = ref.RefCase(g, s, mats)
@@ -43,7 +47,7 @@ def test_viscous_residual_matches_reference(gpu, ref, bcname):
     Rg, Rr = inner(sol.residual()), inner(rc.residual())
     assert rel_err(Rg, Rr) <= TOL
     # the viscous part is not negligible: the inviscid residual differs
-    g2, s2, _, _ = viscous_box(BCS[bcname])
+    g2, s2, _, _ = viscous_box(BCS[bcname], dims=dims)
     inv = gpu.Solver(g2, s2, [abi.material(1.4, 0.0)])
     inv.upload(V)
     assert rel_err(inner(inv.residual()), Rr) > 1e-6
@@ -119,8 +123,7 @@ def test_viscous_mixed_tracks_fp64(gpu):
         sol.run(10)
         out.append(inner(sol.download()[0]))
         sol.close()
-    for c in range(5):
-        assert l1_rel(out[1][..., c], out[0][..., c]) <= 1e-5, c
+    assert l1_rel(out[1], out[0]) <= 1e-5
 
 
 def test_batched_tubes_refuse_viscosity(gpu):
