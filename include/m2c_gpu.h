@@ -81,6 +81,14 @@ typedef struct {
    * viscous, the stage adds the viscous fluxes of ViscosityOperator::
    * AddDiffusionFluxes (ViscosityOperator.cpp:200-408) to the residual. */
   double mu, mu_bulk;
+  /* HeatDiffusionModelData CONSTANT (HeatDiffusionFcn.h): diffusivity;
+   * 0 = NONE. With any material diffusive, the stage adds the heat fluxes of
+   * HeatDiffusionOperator::AddDiffusionFluxes (HeatDiffusionOperator.cpp:
+   * 90-198). Temperature laws (VarFcnSG.h:70-78, VarFcnNASG.h:61): SG
+   * T = T0 + (e - e0)/cv, or T = T0 + (e + p/rho - h0)/cp where cp > 0 and
+   * cv <= 0; NASG T = (e - q - p_c (1/rho - b))/cv (1/0 read as 0). */
+  double heat_diffusivity;
+  double cv, T0, e0, cp, h0;
 } m2cg_material;
 
 /* Numerical scheme (SchemeData, ReconstructionData, TsData, MultiPhaseData,

@@ -47,6 +47,8 @@ class Material(C.Structure):
         ("eos", C.c_int), ("gamma", C.c_double), ("p_c", C.c_double), ("b", C.c_double), ("q", C.c_double),
         ("rhomin", C.c_double), ("pmin", C.c_double), ("rhomax", C.c_double), ("pmax", C.c_double),
         ("failsafe_density", C.c_double), ("mu", C.c_double), ("mu_bulk", C.c_double),
+        ("heat_diffusivity", C.c_double), ("cv", C.c_double), ("T0", C.c_double), ("e0", C.c_double),
+        ("cp", C.c_double), ("h0", C.c_double),
     ]
 
 
@@ -76,8 +78,10 @@ class LevelSet(C.Structure):
 
 
 def material(gamma=1.4, p_c=0.0, eos=EOS_SG, b=0.0, q=0.0, rhomin=0.0, pmin=-DBL_MAX,
-             rhomax=DBL_MAX, pmax=DBL_MAX, failsafe_density=1.0e-10, mu=0.0, mu_bulk=0.0):
-    return Material(eos, gamma, p_c, b, q, rhomin, pmin, rhomax, pmax, failsafe_density, mu, mu_bulk)
+             rhomax=DBL_MAX, pmax=DBL_MAX, failsafe_density=1.0e-10, mu=0.0, mu_bulk=0.0, heat_diffusivity=0.0,
+             cv=0.0, T0=0.0, e0=0.0, cp=0.0, h0=0.0):
+    return Material(eos, gamma, p_c, b, q, rhomin, pmin, rhomax, pmax, failsafe_density, mu, mu_bulk,
+                    heat_diffusivity, cv, T0, e0, cp, h0)
 
 
 def scheme(**kw):
@@ -196,7 +200,9 @@ def iptr(a):
 # numpy mirror of m2cg_material (C layout: int, padding, nine doubles)
 MATERIAL_DTYPE = np.dtype([("eos", "<i4"), ("gamma", "<f8"), ("p_c", "<f8"), ("b", "<f8"), ("q", "<f8"),
                            ("rhomin", "<f8"), ("pmin", "<f8"), ("rhomax", "<f8"), ("pmax", "<f8"),
-                           ("failsafe_density", "<f8"), ("mu", "<f8"), ("mu_bulk", "<f8")], align=True)
+                           ("failsafe_density", "<f8"), ("mu", "<f8"), ("mu_bulk", "<f8"),
+                           ("heat_diffusivity", "<f8"), ("cv", "<f8"), ("T0", "<f8"), ("e0", "<f8"), ("cp", "<f8"),
+                           ("h0", "<f8")], align=True)
 
 
 def material_table(gamma, p_c):

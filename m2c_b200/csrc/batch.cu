@@ -965,8 +965,8 @@ extern "C" m2cg_status m2cg_batch_create(const m2cg_scheme* scheme, int ntubes, 
     return bfail(M2CG_ERR_UNSUPPORTED, "only primitive-variable reconstruction is implemented");
   if (scheme->rk_order < 1 || scheme->rk_order > 3) return bfail(M2CG_ERR_ARG, "rk_order must be 1, 2 or 3");
   for (int q = 0; q < 2 * ntubes; q++)
-    if (mats[q].mu != 0.0 || mats[q].mu_bulk != 0.0)
-      return bfail(M2CG_ERR_UNSUPPORTED, "viscous materials are not implemented for the batched tubes");
+    if (mats[q].mu != 0.0 || mats[q].mu_bulk != 0.0 || mats[q].heat_diffusivity != 0.0)
+      return bfail(M2CG_ERR_UNSUPPORTED, "viscous or heat-diffusive materials are not implemented for the batched tubes");
   if (scheme->mp_recon != 0 || scheme->mp_phasechange_type != 0)
     return bfail(M2CG_ERR_UNSUPPORTED, "interface recon must be CONSTANT with the Riemann-solution update");
   long long N = 0;

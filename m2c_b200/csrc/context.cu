@@ -445,7 +445,7 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   if (!st) {
     const double* xc[3] = {c->hxc.data(), c->hyc.data(), c->hzc.data()};
     const double* dxs[3] = {c->hdx.data(), c->hdy.data(), c->hdz.data()};
-    st = viscous_create(c->stream, g, mats, nmat, xc, dxs, &c->visc);
+    st = viscous_create(c->stream, g, sk.ed, mats, nmat, xc, dxs, &c->visc);
     if (st) fail(st, "viscous-flux buffers could not be allocated");
   }
   if (st) {

@@ -123,6 +123,7 @@ struct IfaceView {
 struct ViscView {
   const double* fr[3];
   const double* fl[3];
+  const double* fh[3];  // heat-diffusion flux per face (energy only), same indexing; NULL: none
   long long nf[3];
 };
 
@@ -1072,6 +1073,19 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
             f = f - a.visc.fl[1][cc + fyi + g.nx];
             f = f - a.visc.fl[2][cc + fzi + (long long)g.ny * g.nx];
           }
+        }
+        if (c == 4 && a.visc.fh[0]) {
+          // heat fluxes (HeatDiffusionOperator::AddDiffusionFluxes, after the
+          // viscous ones), energy only, in the same cell order
+          const long long fxi = ((long long)m * g.ny + gj) * (g.nx + 1) + gi;
+          const long long fyi = ((long long)m * (g.ny + 1) + gj) * g.nx + gi;
+          const long long fzi = ((long long)m * g.ny + gj) * g.nx + gi;
+          f = f + a.visc.fh[0][fxi];
+          f = f + a.visc.fh[1][fyi];
+          f = f + a.visc.fh[2][fzi];
+          f = f - a.visc.fh[0][fxi + 1];
+          f = f - a.visc.fh[1][fyi + g.nx];
+          f = f - a.visc.fh[2][fzi + (long long)g.ny * g.nx];
         }
         const double R = f * inv_mvol;
         if (a.Ro[0]) a.Ro[c][off] = R;

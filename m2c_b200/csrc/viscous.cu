@@ -34,6 +34,13 @@ struct ViscDev {
   const double* wg[3];  // widths incl. one ghost per side
   double mu[MAXMAT];    // ViscoFcnConstant dyna (0 and bulk 0: NONE)
   double bulk[MAXMAT];
+  int viscous, heat;    // which fluxes are formed
+  // heat diffusion: HeatDiffusionFcnConstant diffusivity and the EOS's
+  // temperature law (VarFcnSG.h:70-78, VarFcnNASG.h:61)
+  double kappa[MAXMAT];
+  double invcv[MAXMAT], T0[MAXMAT], e0[MAXMAT], invcp[MAXMAT], h0[MAXMAT];
+  int use_cp[MAXMAT];
+  Eos<double> eos[MAXMAT];
   int nmat;
 };
 
@@ -42,6 +49,7 @@ struct Viscous {
   double* base = nullptr;  // coordinates and widths
   double* fr = nullptr;    // [3 axes][4][nf] (one allocation)
   double* fl = nullptr;
+  double* fh = nullptr;    // heat flux per face [3 axes][nf]
   long long stride = 0;    // faces per component block (the largest axis' face count)
 };
 
@@ -83,6 +91,48 @@ __device__ void node_vel(const ViscDev& d, const T* const* P, int i, int j, int 
   } else if (bc != BC_PERIODIC) {  // SYMMETRY / SLIPWALL: the normal velocity flips
     v[axis] = -v[axis];
   }
+}
+
+// Density and pressure of cell (i, j, k), interior or a face ghost (the
+// boundary rules keep the image's density and pressure except at INLET /
+// OUTLET ghosts).
+template <typename T>
+__device__ void node_rho_p(const ViscDev& d, const T* const* P, int i, int j, int k, double& rho, double& p) {
+  const Grid3& g = d.g;
+  int ix[3] = {i, j, k};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  int axis = -1, side = 0;
+  for (int a = 0; a < 3; a++) {
+    if (ix[a] < 0) { axis = a; side = 0; }
+    else if (ix[a] >= n[a]) { axis = a; side = 1; }
+  }
+  if (axis >= 0) {
+    const int bc = g.bc[2 * axis + side];
+    if (bc == BC_INLET || bc == BC_OUTLET) {
+      const double* st = bc == BC_INLET ? g.inlet : g.outlet;
+      rho = st[0];
+      p = st[4];
+      return;
+    }
+    if (bc == BC_PERIODIC) ix[axis] = side ? ix[axis] - n[axis] : ix[axis] + n[axis];
+    else ix[axis] = side ? n[axis] - 1 : 0;
+  }
+  const long long o = voff(g, ix[0], ix[1], ix[2]);
+  rho = double(P[0][o]);
+  p = double(P[4][o]);
+}
+
+// HeatDiffusionOperator::AddDiffusionFluxes step 1: the temperature of a cell
+// from its EOS (GetInternalEnergyPerUnitMass, then GetTemperature).
+__device__ __forceinline__ double temperature(const ViscDev& d, int id, double rho, double p) {
+  const Eos<double>& e = d.eos[id];
+  const double en = e.energy(rho, p);
+  if (e.kind != EOS_SG) return d.invcv[id] * (en - e.q - e.pstiff * (1.0 / rho - e.b));
+  if (d.use_cp[id]) {
+    const double pp = e.pressure(rho, en);
+    return d.T0[id] + d.invcp[id] * (en + pp / rho - d.h0[id]);
+  }
+  return d.T0[id] + d.invcv[id] * (en - d.e0[id]);
 }
 
 __device__ __forceinline__ uint8_t node_id(const Grid3& g, const uint8_t* id, int i, int j, int k) {
@@ -171,7 +221,7 @@ __device__ __forceinline__ void visc_flux(double mu, double bulk, int d, const d
 // One thread per cell (i, j, k) of [0, nx] x [0, ny] x [0, nz]: the faces of
 // the three axes whose right cell it is.
 template <typename T>
-__global__ void k_visc_faces(ViscDev d, StageArgs a, double* fr, double* fl, long long S) {
+__global__ void k_visc_faces(ViscDev d, StageArgs a, double* fr, double* fl, double* fh, long long S) {
   const Grid3& g = d.g;
   const T* P[5];
   for (int c = 0; c < 5; c++) P[c] = static_cast<const T*>(a.Pin[c]);
@@ -194,48 +244,76 @@ __global__ void k_visc_faces(ViscDev d, StageArgs a, double* fr, double* fl, lon
       const double* x = d.xg[ax] + 1;
       const double* w = d.wg[ax] + 1;
       const int iR = cR[ax];
-      // interpolation coefficients of the face (Interpolator.cpp:165-176)
-      const double xh = x[iR] - 0.5 * w[iR];
       const double dd = x[iR] - x[iR - 1];
-      const double cl = (x[iR] - xh) / dd, cr = (xh - x[iR - 1]) / dd;
-      double vL[3], vR[3];
-      node_vel(d, P, cL[0], cL[1], cL[2], vL);
-      node_vel(d, P, cR[0], cR[1], cR[2], vR);
-      double v3[3], D[3][3];  // D[t] = d(u, v, w)/d(axis t) at the face
-      for (int c = 0; c < 3; c++) v3[c] = cl * vL[c] + cr * vR[c];
-      for (int c = 0; c < 3; c++) D[ax][c] = (vR[c] - vL[c]) / dd;
-      // a cell is a ghost in another axis than t where it is a ghost of ax (L at the
-      // low boundary, R at the high one)
-      const bool gL = cL[ax] < 0, gR = cR[ax] >= n[ax];
-      for (int t = 0; t < 3; t++) {
-        if (t == ax) continue;
-        double dl[3], dr[3];
-        node_deriv(d, P, cL, t, gL, dl);
-        node_deriv(d, P, cR, t, gR, dr);
-        for (int c = 0; c < 3; c++) D[t][c] = cl * dl[c] + cr * dr[c];
-      }
-      // area of the right cell (ViscosityOperator.cpp:278-386): widths of its
-      // two other axes (a ghost has the width of its boundary cell)
+      // area of the right cell (ViscosityOperator.cpp:278-386, HeatDiffusionOperator.cpp:
+      // 157-181): widths of its two other axes (a ghost has its boundary cell's)
       const int b1 = ax == 0 ? 1 : 0, b2 = ax == 2 ? 1 : 2;
       const double area = (d.wg[b1] + 1)[cR[b1]] * (d.wg[b2] + 1)[cR[b2]];
       const uint8_t idR = node_id(g, a.id, cR[0], cR[1], cR[2]);
       const uint8_t idL = node_id(g, a.id, cL[0], cL[1], cL[2]);
-      double FR[4], FL[4];
-      visc_flux(d.mu[idR], d.bulk[idR], ax, D[0], D[1], D[2], v3, FR);
-      for (int c = 0; c < 4; c++) FR[c] = FR[c] * area;
-      if (idL == idR || ax == 2) {
-        for (int c = 0; c < 4; c++) FL[c] = FR[c];
-      } else {
-        visc_flux(d.mu[idL], d.bulk[idL], ax, D[0], D[1], D[2], v3, FL);
-        for (int c = 0; c < 4; c++) FL[c] = area * FL[c];
-      }
       long long fidx;
       if (ax == 0) fidx = ((long long)k * g.ny + j) * (g.nx + 1) + i;
       else if (ax == 1) fidx = ((long long)k * (g.ny + 1) + j) * g.nx + i;
       else fidx = ((long long)k * g.ny + j) * g.nx + i;
-      for (int c = 0; c < 4; c++) {
-        fr[(ax * 4 + c) * S + fidx] = FR[c];
-        fl[(ax * 4 + c) * S + fidx] = FL[c];
+      if (d.viscous) {
+        // interpolation coefficients of the face (Interpolator.cpp:165-176)
+        const double xh = x[iR] - 0.5 * w[iR];
+        const double cl = (x[iR] - xh) / dd, cr = (xh - x[iR - 1]) / dd;
+        double vL[3], vR[3];
+        node_vel(d, P, cL[0], cL[1], cL[2], vL);
+        node_vel(d, P, cR[0], cR[1], cR[2], vR);
+        double v3[3], D[3][3];  // D[t] = d(u, v, w)/d(axis t) at the face
+        for (int c = 0; c < 3; c++) v3[c] = cl * vL[c] + cr * vR[c];
+        for (int c = 0; c < 3; c++) D[ax][c] = (vR[c] - vL[c]) / dd;
+        // a cell is a ghost in another axis than t where it is a ghost of ax (L at the
+        // low boundary, R at the high one)
+        const bool gL = cL[ax] < 0, gR = cR[ax] >= n[ax];
+        for (int t = 0; t < 3; t++) {
+          if (t == ax) continue;
+          double dl[3], dr[3];
+          node_deriv(d, P, cL, t, gL, dl);
+          node_deriv(d, P, cR, t, gR, dr);
+          for (int c = 0; c < 3; c++) D[t][c] = cl * dl[c] + cr * dr[c];
+        }
+        double FR[4], FL[4];
+        visc_flux(d.mu[idR], d.bulk[idR], ax, D[0], D[1], D[2], v3, FR);
+        for (int c = 0; c < 4; c++) FR[c] = FR[c] * area;
+        if (idL == idR || ax == 2) {
+          for (int c = 0; c < 4; c++) FL[c] = FR[c];
+        } else {
+          visc_flux(d.mu[idL], d.bulk[idL], ax, D[0], D[1], D[2], v3, FL);
+          for (int c = 0; c < 4; c++) FL[c] = area * FL[c];
+        }
+        for (int c = 0; c < 4; c++) {
+          fr[(ax * 4 + c) * S + fidx] = FR[c];
+          fl[(ax * 4 + c) * S + fidx] = FL[c];
+        }
+      }
+      if (d.heat) {
+        // HeatDiffusionOperator::AddDiffusionFluxes (HeatDiffusionOperator.cpp:96-185):
+        // the harmonic mean of the two diffusivities times the central
+        // temperature difference across the face. Its y and z faces reuse the
+        // denominator of the cell's own x face; where the cell has no x face
+        // (the y-ghost row, the z-ghost plane) the denominator is the one the
+        // traversal computed last: the x face of cell (nx, ny - 1, k) resp.
+        // (nx, ny - 1, nz - 1).
+        double rL, pL, rR, pR;
+        node_rho_p(d, P, cL[0], cL[1], cL[2], rL, pL);
+        node_rho_p(d, P, cR[0], cR[1], cR[2], rR, pR);
+        const double dT = (temperature(d, idR, rR, pR) - temperature(d, idL, rL, pL)) / dd;
+        const double myk = d.kappa[idR], neighk = d.kappa[idL];
+        double denom;
+        if (ax == 0) {
+          denom = myk + neighk;
+        } else if (cR[1] < n[1] && cR[2] < n[2]) {
+          denom = myk + d.kappa[node_id(g, a.id, i - 1, j, k)];
+        } else {
+          const int kk = ax == 1 ? k : n[2] - 1;
+          denom = d.kappa[node_id(g, a.id, n[0], n[1] - 1, kk)] + d.kappa[node_id(g, a.id, n[0] - 1, n[1] - 1, kk)];
+        }
+        double f = (denom == 0) ? 0.0 : 2.0 * myk * neighk / denom * dT;
+        f = f * area;
+        fh[ax * S + fidx] = f;
       }
     }
   }
@@ -243,19 +321,34 @@ __global__ void k_visc_faces(ViscDev d, StageArgs a, double* fr, double* fl, lon
 
 }  // namespace
 
-m2cg_status viscous_create(cudaStream_t s, const Grid3& g, const m2cg_material* mats, int nmat,
-                           const double* const* xc, const double* const* dx, Viscous** out) {
+m2cg_status viscous_create(cudaStream_t s, const Grid3& g, const Eos<double>* eos, const m2cg_material* mats,
+                           int nmat, const double* const* xc, const double* const* dx, Viscous** out) {
   *out = nullptr;
-  bool any = false;
-  for (int m = 0; m < nmat; m++) any = any || mats[m].mu != 0.0 || mats[m].mu_bulk != 0.0;
-  if (!any) return M2CG_OK;
+  bool viscous = false, heat = false;
+  for (int m = 0; m < nmat; m++) {
+    viscous = viscous || mats[m].mu != 0.0 || mats[m].mu_bulk != 0.0;
+    heat = heat || mats[m].heat_diffusivity != 0.0;
+  }
+  if (!viscous && !heat) return M2CG_OK;
   Viscous* v = new Viscous;
   memset(&v->d, 0, sizeof v->d);
   v->d.g = g;
   v->d.nmat = nmat;
+  v->d.viscous = viscous ? 1 : 0;
+  v->d.heat = heat ? 1 : 0;
   for (int m = 0; m < nmat && m < MAXMAT; m++) {
     v->d.mu[m] = mats[m].mu;
     v->d.bulk[m] = mats[m].mu_bulk;
+    // VarFcnSG / VarFcnNASG constructors (VarFcnSG.h:130-142): 1/cv and 1/cp
+    // read as 0 where cv, cp are 0; cp is used where cp > 0 and cv <= 0
+    v->d.kappa[m] = mats[m].heat_diffusivity;
+    v->d.invcv[m] = mats[m].cv == 0.0 ? 0.0 : 1.0 / mats[m].cv;
+    v->d.invcp[m] = mats[m].cp == 0.0 ? 0.0 : 1.0 / mats[m].cp;
+    v->d.T0[m] = mats[m].T0;
+    v->d.e0[m] = mats[m].e0;
+    v->d.h0[m] = mats[m].h0;
+    v->d.use_cp[m] = (mats[m].cp > 0.0 && mats[m].cv <= 0.0) ? 1 : 0;
+    v->d.eos[m] = eos[m];
   }
   const int n[3] = {g.nx, g.ny, g.nz};
   // coordinates and widths with one ghost per side (SpaceOperator::
@@ -280,8 +373,11 @@ m2cg_status viscous_create(cudaStream_t s, const Grid3& g, const m2cg_material* 
   if (nf[2] > big) big = nf[2];
   v->stride = big;
   bool ok = cudaMalloc((void**)&v->base, host.size() * sizeof(double)) == cudaSuccess;
-  ok = ok && cudaMalloc((void**)&v->fr, 3 * 4 * big * sizeof(double)) == cudaSuccess;
-  ok = ok && cudaMalloc((void**)&v->fl, 3 * 4 * big * sizeof(double)) == cudaSuccess;
+  if (viscous) {
+    ok = ok && cudaMalloc((void**)&v->fr, 3 * 4 * big * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&v->fl, 3 * 4 * big * sizeof(double)) == cudaSuccess;
+  }
+  if (heat) ok = ok && cudaMalloc((void**)&v->fh, 3 * big * sizeof(double)) == cudaSuccess;
   if (!ok) {
     viscous_destroy(v);
     return M2CG_ERR_NOMEM;
@@ -300,6 +396,7 @@ void viscous_destroy(Viscous* v) {
   cudaFree(v->base);
   cudaFree(v->fr);
   cudaFree(v->fl);
+  cudaFree(v->fh);
   delete v;
 }
 
@@ -309,14 +406,16 @@ m2cg_status viscous_faces(Viscous* v, cudaStream_t s, StageArgs& a, bool mixed) 
   long long blocks = (total + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (mixed)
-    k_visc_faces<float><<<(int)blocks, 256, 0, s>>>(v->d, a, v->fr, v->fl, v->stride);
+    k_visc_faces<float><<<(int)blocks, 256, 0, s>>>(v->d, a, v->fr, v->fl, v->fh, v->stride);
   else
-    k_visc_faces<double><<<(int)blocks, 256, 0, s>>>(v->d, a, v->fr, v->fl, v->stride);
+    k_visc_faces<double><<<(int)blocks, 256, 0, s>>>(v->d, a, v->fr, v->fl, v->fh, v->stride);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
-  // axis ax's block starts at ax * 4 * stride; component c of face f at + c * stride + f
+  // viscous: axis ax's block starts at ax * 4 * stride, component c of face f
+  // at + c * stride + f; heat: axis ax's face f at ax * stride + f
   for (int ax = 0; ax < 3; ax++) {
-    a.visc.fr[ax] = v->fr + ax * 4 * v->stride;
-    a.visc.fl[ax] = v->fl + ax * 4 * v->stride;
+    a.visc.fr[ax] = v->fr ? v->fr + ax * 4 * v->stride : nullptr;
+    a.visc.fl[ax] = v->fl ? v->fl + ax * 4 * v->stride : nullptr;
+    a.visc.fh[ax] = v->fh ? v->fh + ax * v->stride : nullptr;
     a.visc.nf[ax] = v->stride;
   }
   return M2CG_OK;

@@ -18,10 +18,11 @@ namespace m2c {
 
 struct Viscous;
 
-// xc/dx: host cell centres and widths per axis. *out = NULL (and M2CG_OK)
-// when no material is viscous.
-m2cg_status viscous_create(cudaStream_t s, const Grid3& g, const m2cg_material* mats, int nmat,
-                           const double* const* xc, const double* const* dx, Viscous** out);
+// eos: the materials' FP64 EOS (temperature laws); xc/dx: host cell centres
+// and widths per axis. *out = NULL (and M2CG_OK) when no material is
+// viscous or heat-diffusive.
+m2cg_status viscous_create(cudaStream_t s, const Grid3& g, const Eos<double>* eos, const m2cg_material* mats,
+                           int nmat, const double* const* xc, const double* const* dx, Viscous** out);
 void viscous_destroy(Viscous* v);
 // Faces of the stage whose arguments are a (its input state a.Pin in the
 // compute type: float when mixed); fills a.visc.

@@ -92,6 +92,16 @@ void fill_material(MaterialModelData* d, const m2cg_material& m) {
   d->nasgModel.pressureConstant = m.p_c;
   d->nasgModel.volumeConstant = m.b;
   d->nasgModel.energyConstant = m.q;
+  d->sgModel.cv = m.cv;
+  d->sgModel.T0 = m.T0;
+  d->sgModel.e0 = m.e0;
+  d->sgModel.cp = m.cp;
+  d->sgModel.h0 = m.h0;
+  d->nasgModel.cv = m.cv;
+  if (m.heat_diffusivity != 0.0) {
+    d->heat_diffusion.type = HeatDiffusionModelData::CONSTANT;
+    d->heat_diffusion.diffusivity = m.heat_diffusivity;
+  }
   if (m.mu != 0.0 || m.mu_bulk != 0.0) {
     d->viscosity.type = ViscosityModelData::CONSTANT;
     d->viscosity.dynamicViscosity = m.mu;
@@ -245,13 +255,17 @@ void* m2cref_create(const m2cg_grid* g, const m2cg_scheme* s, const m2cg_materia
   c->dms = new DataManagers3D(c->comm, c->NX, c->NY, c->NZ);
   c->gmi->GetSubdomainInfo(c->comm, *c->dms);
   c->spo = new SpaceOperator(c->comm, *c->dms, iod, c->vf, *c->ff, *c->riemann, *c->gmi, false);
-  bool viscous = false;
-  for (int m = 0; m < nmat; m++) viscous = viscous || mats[m].mu != 0.0 || mats[m].mu_bulk != 0.0;
-  if (viscous) {  // Main.cpp:195-205: linear interpolation + central differences for the viscous terms
+  bool viscous = false, heat = false;
+  for (int m = 0; m < nmat; m++) {
+    viscous = viscous || mats[m].mu != 0.0 || mats[m].mu_bulk != 0.0;
+    heat = heat || mats[m].heat_diffusivity != 0.0;
+  }
+  if (viscous || heat) {  // Main.cpp:195-208: linear interpolation + central differences
     c->interp = new InterpolatorLinear(c->comm, *c->dms, c->spo->GetMeshCoordinates(), c->spo->GetMeshDeltaXYZ());
     c->grad = new GradientCalculatorCentral(c->comm, *c->dms, c->spo->GetMeshCoordinates(), c->spo->GetMeshDeltaXYZ(),
                                             *c->interp);
     c->spo->SetupViscosityOperator(c->interp, c->grad, false);
+    c->spo->SetupHeatDiffusionOperator(c->interp, c->grad);
   }
 
   c->V = new SpaceVariable3D(c->comm, &(c->dms->ghosted1_5dof));

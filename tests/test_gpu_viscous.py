@@ -132,3 +132,66 @@ def test_batched_tubes_refuse_viscosity(gpu):
     mats[0] = abi.material(mats[0].gamma, mats[0].p_c, mu=1e-3)
     with pytest.raises(gpu.M2CError):
         gpu.Batch(cases.tube_scheme(), lens, mats, VL, VR)
+
+
+HEAT_BC = (abi.BC_INLET, abi.BC_OUTLET, abi.BC_SYMMETRY, abi.BC_STICKWALL, abi.BC_SLIPWALL, abi.BC_SYMMETRY)
+
+
+@pytest.mark.parametrize("law", ["cv", "cp"])
+@pytest.mark.parametrize("dims", [(14, 11, 9), (9, 14, 11)])
+def test_heat_diffusion_matches_reference(gpu, ref, law, dims):
+    """HeatDiffusionOperator::AddDiffusionFluxes: the temperature from the
+    EOS's law (T0 + (e - e0)/cv, or T0 + (e + p/rho - h0)/cp), the central
+    temperature difference across each face times the harmonic mean of the
+    two diffusivities, energy only, added after the viscous fluxes; with and
+    without viscosity, residual and whole steps."""
+    g, s, _, V = cases.random_box(*dims, seed=5, bc=HEAT_BC, rk=3)
+    kw = dict(cv=2.5, T0=1.0, e0=0.5) if law == "cv" else dict(cp=3.5, T0=1.0, h0=0.7)
+    for mu in (0.0, 2.0e-3):
+        mats = [abi.material(1.4, 0.0, heat_diffusivity=0.2, mu=mu, **kw)]
+        sol = gpu.Solver(g, s, mats)
+        sol.upload(V)
+        rc = ref.RefCase(g, s, mats)
+        rc.set_state(V)
+        assert rel_err(inner(sol.residual()), inner(rc.residual())) <= TOL
+        sol.run(4)
+        rc.run(4)
+        assert rel_err(inner(sol.download()[0]), inner(rc.get_state()[0])) <= TOL
+        sol.close()
+
+
+def test_heat_diffusion_two_materials_matches_reference(gpu, ref):
+    """Different diffusivities on the two sides of the bubble (harmonic mean
+    at the interface, the y and z faces reusing the x face's denominator as
+    the reference does), with a NASG liquid's temperature law on one side."""
+    if not ref.available("crpow"):
+        pytest.skip("reference oracle with correctly rounded pow not built (make -C oracle refcr)")
+    g, s, mats, ls, V, ID, PHI = cases.bubble_case(20, reinit_frequency=-1, radius=4.0e-3)
+    mats = [abi.material(mats[0].gamma, mats[0].p_c, heat_diffusivity=0.6, cv=4180.0, T0=293.0, e0=0.0,
+                         mu=1.0e-3),
+            abi.material(mats[1].gamma, mats[1].p_c, heat_diffusivity=0.026, cv=718.0, T0=293.0, e0=2.1e5)]
+    sol = gpu.Solver(g, s, mats, ls)
+    sol.upload(V, ID, PHI)
+    rc = ref.RefCaseCR(g, s, mats, ls)
+    rc.set_state(V, ID, PHI)
+    assert rel_err(inner(sol.residual()), inner(rc.residual())) <= TOL
+    for _ in range(3):
+        sol.run(1)
+        rc.run(1)
+    Vg, IDg, _ = sol.download()
+    Vr, IDr, _ = rc.get_state()
+    assert np.array_equal(inner(IDg), inner(IDr))
+    assert rel_err(inner(Vg), inner(Vr)) <= TOL
+    sol.close()
+
+
+def test_heat_diffusion_nasg_matches_reference(gpu, ref):
+    g, s, _, V = cases.random_box(12, 10, 8, seed=9, bc=HEAT_BC, rk=3, nasg=True)
+    mats = [abi.material(1.19, 7.028e8, eos=abi.EOS_NASG, b=6.61e-4, q=-1.177788e6, heat_diffusivity=0.6,
+                         cv=3610.0)]
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V)
+    assert rel_err(inner(sol.residual()), inner(rc.residual())) <= TOL
+    sol.close()
