@@ -76,6 +76,25 @@ class TimeIntegratorGPU : public TimeIntegratorBase {
       m.q = nasg ? d.nasgModel.energyConstant : 0.0;
       m.rhomin = d.rhomin; m.pmin = d.pmin; m.rhomax = d.rhomax; m.pmax = d.pmax;
       m.failsafe_density = d.failsafe_density;
+      // viscosity and heat diffusion (ViscosityModelData / HeatDiffusionModelData
+      // CONSTANT) with the EOS's temperature law; other models are refused
+      if (d.viscosity.type == ViscosityModelData::CONSTANT) {
+        m.mu = d.viscosity.dynamicViscosity;
+        m.mu_bulk = d.viscosity.bulkViscosity;
+      } else if (d.viscosity.type != ViscosityModelData::NONE) {
+        print_error("*** Error: the GPU integrator implements the CONSTANT viscosity model only.\n");
+        exit_mpi();
+      }
+      if (d.heat_diffusion.type == HeatDiffusionModelData::CONSTANT) m.heat_diffusivity = d.heat_diffusion.diffusivity;
+      m.cv = nasg ? d.nasgModel.cv : d.sgModel.cv;
+      m.T0 = nasg ? 0.0 : d.sgModel.T0;
+      m.e0 = nasg ? 0.0 : d.sgModel.e0;
+      m.cp = nasg ? 0.0 : d.sgModel.cp;
+      m.h0 = nasg ? 0.0 : d.sgModel.h0;
+      if (m.heat_diffusivity != 0.0 && !nasg && d.sgModel.cv > 0 && d.sgModel.rho0 > 0) {
+        print_error("*** Error: the GPU integrator does not implement the rho0 temperature law.\n");
+        exit_mpi();
+      }
       mats.push_back(m);
     }
     // scheme (SchemeData, ReconstructionData, TsData, MultiPhaseData, ExactRiemannSolverData)
