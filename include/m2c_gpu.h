@@ -426,7 +426,10 @@ m2cg_status m2cg_batch_get_tuning(const m2cg_batch* b, m2cg_batch_tuning* t);
  * iterations and errors (as counted at SpaceOperator.cpp:2818), unresolved
  * cells of the post-step update, kernel launches. */
 m2cg_status m2cg_batch_get_counters(m2cg_batch* b, m2cg_counters* c);
-/* First device error code of each tube (0 = none), ntubes entries. */
+/* First device error code of each tube (0 = none), ntubes entries. A tube
+ * that reported an error is not advanced further (the reference aborts the
+ * run there); its downloaded state and time are those of the step where it
+ * failed, left part-way, and are not defined. The other tubes go on. */
 m2cg_status m2cg_batch_tube_errors(m2cg_batch* b, int* codes);
 /* Advance nsteps and return the device time of those steps (CUDA events on
  * the batch's stream). *ms is written even when a tube reported an error

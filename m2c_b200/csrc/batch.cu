@@ -96,6 +96,9 @@ __device__ __forceinline__ void tube_fail(const TubeArgs& A, int t, int code, in
 // SpaceOperator::ComputeTimeStepSize per tube (dy = dz = 1), the ID snapshot,
 // and the ordered list of interface faces (ID differs across the face).
 __device__ void tube_begin(const TubeArgs& A, int t, int cur, int lane) {
+  // a tube that reported an error stops where it failed (the reference
+  // aborts there); the warp decides from one read
+  if (__shfl_sync(0xffffffffu, lane == 0 ? A.terr[t] : 0, 0)) return;
   const long long o = A.off[t];
   const int n = (int)(A.off[t + 1] - o);
   const double h = 1.0 / n;
@@ -210,8 +213,10 @@ __global__ void k_tube_riemann(TubeArgs A, TubeStage S) {
   rs.path3.pt = rs.path1.pt + 3 * RIEMANN_PATH_CAP;
   rs.path3.cap = RIEMANN_PATH_CAP;
   // one thread per tube (tubes rarely hold more than one interface face)
-  for (long long tt = tid; tt < A.ntubes; tt += nth)
+  for (long long tt = tid; tt < A.ntubes; tt += nth) {
+    if (A.terr[tt]) continue;  // failed tubes stop
     for (int k = 0; k < A.nif[tt]; k++) tube_riemann(A, S, (int)tt, k, rs);
+  }
 }
 
 // Features of every interface problem of this stage (the states the Riemann
@@ -223,7 +228,7 @@ __global__ void k_tube_features(TubeArgs A, TubeStage S, float* X, double* P, in
        w += (long long)gridDim.x * blockDim.x) {
     const int t = (int)(w / TUBE_IFACE_CAP), k = (int)(w - (long long)t * TUBE_IFACE_CAP);
     int ok = 0;
-    if (k < A.nif[t]) {
+    if (k < A.nif[t] && !A.terr[t]) {
       const long long o = A.off[t];
       const int i = A.iface[w];
       const uint8_t idL = A.id[o + i - 1], idR = A.id[o + i];
@@ -518,8 +523,13 @@ __device__ __forceinline__ void tube_stage_item(const TubeArgs& A, const TubeSta
 __global__ void k_tube_stage(const __grid_constant__ TubeArgs A, const TubeStage S) {
   extern __shared__ __align__(16) unsigned char tube_smem_raw[];
   const TubeSmem sm = tube_smem(tube_smem_raw, A.cpb);
+  __shared__ int failed;
   for (int item = blockIdx.x; item < A.nitems; item += gridDim.x) {
     const int2 it = A.items[item];
+    __syncthreads();
+    if (threadIdx.x == 0) failed = A.terr[it.x];
+    __syncthreads();
+    if (failed) continue;  // the CTA skips a failed tube's chunk together
     tube_stage_item(A, S, sm, it.x, it.y);
   }
 }
@@ -578,6 +588,7 @@ __device__ int tube_local_update(const TubeArgs& A, double* const* V, int t, lon
 // Material ID from the sign change of phi and the ordered update of cells
 // whose ID changed (MultiPhaseOperator.cpp:127-332, 824-1027); one warp per tube.
 __device__ void tube_end(const TubeArgs& A, int t, int cur_new, int lane) {
+  if (__shfl_sync(0xffffffffu, lane == 0 ? A.terr[t] : 0, 0)) return;
   const long long o = A.off[t];
   const int n = (int)(A.off[t + 1] - o);
   const double* phnew = A.phi[cur_new];
@@ -659,7 +670,12 @@ __global__ void __launch_bounds__(128) k_tube_run(const __grid_constant__ TubeAr
     if (t < 0) return;
     const int n = (int)(A.off[t + 1] - A.off[t]);
     int cur = cur0;
+    __shared__ int failed;
     for (int step = 0; step < nsteps; step++) {
+      __syncthreads();
+      if (threadIdx.x == 0) failed = A.terr[t];
+      __syncthreads();
+      if (failed) break;  // a tube that reported an error stops where it failed
       if (warp == 0) tube_begin(A, t, cur, lane);
       __syncthreads();
       for (int st = 1; st <= A.rk; st++) {
