@@ -470,9 +470,13 @@ def extra_tubes(ntubes=4096, steps=200, mlp=None):
                        f"Riemann, RK2, CFL 0.5, {steps} steps", "cells": int(lens.sum()),
            "redrawn_at_t0": int(redrawn)}
     peak, _ = measured_peak()
-    for label, net in (("cold", None), ("warm_start", mlp)):
-        if label == "warm_start" and net is None:
+    # after the first steps most interface problems are near-acoustic, where
+    # the acoustic estimate already starts within one iteration; gate 0.03
+    # ignores proposals that close to it
+    for label, net, gate in (("cold", None, 0.0), ("warm_start", mlp, 0.0), ("warm_start_gate_0.03", mlp, 0.03)):
+        if label != "cold" and net is None:
             continue
+        s.riem_warm_gate = gate
         b = gpu.Batch(s, lens, mats, VL, VR)
         if net is not None:
             b.set_mlp(net)

@@ -991,6 +991,8 @@ extern "C" m2cg_status m2cg_batch_create(const m2cg_scheme* scheme, int ntubes, 
     N += len[t];
   }
   if (N > 0x7fffffffLL) return bfail(M2CG_ERR_ARG, "more than 2^31 cells in a batch");
+  if (tuning && tuning->use_graph == 2 && tuning->threads_per_block != 0 && tuning->threads_per_block != 128)
+    return bfail(M2CG_ERR_ARG, "the persistent launch (use_graph 2) runs 128 threads per block");
   m2cg_batch* b = new m2cg_batch;
   b->scheme = *scheme;
   b->ntubes = ntubes;

@@ -49,3 +49,24 @@ def test_defaults_match_reference_iodata():
     pm = abi.material()
     for name, _ in abi.Material._fields_:
         assert getattr(m, name) == getattr(pm, name), name
+
+
+def test_batch_create_rejects_bad_arguments_before_any_device_call():
+    """m2cg_batch_create validates its arguments on the host first: a tube
+    shorter than 4 cells, viscous materials, and a persistent launch asked
+    for with a block size other than its 128 threads are refused with
+    M2CG_ERR_ARG / M2CG_ERR_UNSUPPORTED and a message, without a GPU."""
+    import numpy as np
+    from m2c_b200 import abi, cases, gpu
+    s = cases.tube_scheme()
+    lens, mats, VL, VR, _ = cases.tubes(3, seed=2)
+    with pytest.raises(gpu.M2CError, match="128 threads"):
+        gpu.Batch(s, lens, mats, VL, VR, cells_per_block=256, threads_per_block=256, use_graph=2)
+    short = np.array(lens)
+    short[1] = 3
+    with pytest.raises(gpu.M2CError, match="at least 4 cells"):
+        gpu.Batch(s, short, mats, VL, VR)
+    visc = list(mats)
+    visc[2] = abi.material(visc[2].gamma, visc[2].p_c, mu=1e-3)
+    with pytest.raises(gpu.M2CError, match="viscous"):
+        gpu.Batch(s, lens, visc, VL, VR)
