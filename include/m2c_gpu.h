@@ -318,6 +318,25 @@ m2cg_status m2cg_riemann_batch_pairs(const m2cg_scheme* scheme, const m2cg_mater
                                      const double* warm, double* Vs, int* id, double* Vsm,
                                      double* Vsp, int* iters, int* evals, int* err);
 
+/* One-sided (wall) Riemann problems: the fluid state Vm[q] (material
+ * idm[q]) against a wall moving with velocity uwall[q] (3 components), dir[q]
+ * the unit normal pointing from the fluid towards the wall. Replaces
+ * ExactRiemannSolverBase::ComputeOneSidedRiemannSolution
+ * (ExactRiemannSolverBase.cpp:1931-2195), which the embedded-boundary branch
+ * of SpaceOperator::ComputeAdvectionFluxes calls on each side of a face the
+ * surface cuts (SpaceOperator.cpp:2438-2484). Outputs per problem: Vs, the
+ * state at the wall (xi = 0; zeros where id = -1, i.e. where the wall
+ * recedes from the fluid), id (idm[q] or -1), Vsm, the fluid's star state
+ * (normal velocity = the wall's), iters (optional; secant iterations of a
+ * shock), err: 0, or 1 where the reference reports a failure (it then
+ * returns the input state with the wall's normal velocity, or its best
+ * bracket point), | 2 integration-path capacity exhausted, | 4 a state the
+ * reference aborts on. Host pointers. */
+m2cg_status m2cg_riemann_wall_batch(const m2cg_scheme* scheme, const m2cg_material* mats, int nmat, int n,
+                                    const double* Vm, const int* idm, const double* uwall,
+                                    const double* dir, double* Vs, int* id, double* Vsm, int* iters,
+                                    int* err);
+
 /* The same batched Riemann solve for callers that cannot allocate device
  * memory: a host application whose memory pool owns the whole GPU, or a
  * runtime that forbids allocation on the path that calls it. No counterpart

@@ -196,6 +196,29 @@ def riemann_problems(n, seed=3, nmat_pairs=None):
     return mats, VL, idl, VR, idr, dirs
 
 
+def wall_problems(n, seed=7):
+    """Seeded one-sided (wall) Riemann problems: the riemann_problems state
+    distribution on the fluid side (material 0 or 1 of a stiffened-gas pair),
+    a wall velocity uniform in +-300 m/s per component, and a random unit
+    normal (so shocks, rarefactions, transonic fans and receding walls all
+    occur); about 2% of the problems have the wall's normal velocity equal
+    to the fluid's (the trivial branch). Returns (materials, Vm, idm, uwall,
+    dirs)."""
+    rng = np.random.default_rng(seed)
+    mats = [stiffened_gas_pair(rng), stiffened_gas_pair(rng)]
+    Vm = np.zeros((n, 5))
+    Vm[:, 0] = 10.0 ** rng.uniform(0.0, 3.0, n)
+    Vm[:, 1:4] = rng.uniform(-200.0, 200.0, (n, 3))
+    Vm[:, 4] = 10.0 ** rng.uniform(4.0, 9.0, n)
+    dirs = rng.normal(size=(n, 3))
+    dirs /= np.linalg.norm(dirs, axis=1)[:, None]
+    uwall = rng.uniform(-300.0, 300.0, (n, 3))
+    same = rng.random(n) < 0.02
+    uwall[same] = Vm[same, 1:4]
+    idm = rng.integers(0, 2, n).astype(np.int32)
+    return mats, Vm, idm, uwall, dirs
+
+
 def tube_states(n, rng):
     """Left/right primitive states of n tubes: densities log-uniform in
     1..1000 kg/m^3, velocities uniform in +-200 m/s (along the tube),

@@ -49,6 +49,54 @@ __global__ void k_riemann_batch(RiemannBatchArgs a) {
   }
 }
 
+// One-sided (wall) problems: the same thread-to-slot mapping, one path per
+// slot (the 1-wave's).
+struct RiemannWallArgs {
+  long long n;
+  RiemannParams P;
+  const Eos<double>* eos;
+  const double* Vm;     // [n][5]
+  const int* idm;
+  const double* uwall;  // [n][3]
+  const double* dir;    // [n][3]
+  double* Vs;           // [n][5] (zero where id = -1)
+  double* Vsm;          // [n][5]
+  int* id;
+  int* iters;           // or nullptr
+  int* err;
+  double* scratch;      // [slots][path_cap][3]
+  int path_cap;
+  long long scratch_slots;
+};
+
+__global__ void k_riemann_wall(RiemannWallArgs a) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.n; q += (long long)gridDim.x * blockDim.x) {
+    RiemannSolver rs;
+    rs.P = a.P;
+    rs.eos = a.eos;
+    rs.path1.pt = a.scratch + (q % a.scratch_slots) * 3 * (long long)a.path_cap;
+    rs.path1.cap = a.path_cap;
+    rs.path3.pt = nullptr;
+    rs.path3.cap = 0;
+    double Vm[5], uw[3], dir[3], Vs[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, Vsm[5];
+    for (int c = 0; c < 5; c++) Vm[c] = a.Vm[5 * q + c];
+    for (int c = 0; c < 3; c++) {
+      uw[c] = a.uwall[3 * q + c];
+      dir[c] = a.dir[3 * q + c];
+    }
+    int id = 0;
+    bool bad = false;
+    const int r = rs.solve_wall(dir, Vm, a.idm[q], uw, Vs, id, Vsm, bad);
+    for (int c = 0; c < 5; c++) {
+      a.Vs[5 * q + c] = Vs[c];
+      a.Vsm[5 * q + c] = Vsm[c];
+    }
+    a.id[q] = id;
+    if (a.iters) a.iters[q] = rs.iterations;
+    a.err[q] = r | (bad ? 4 : 0);
+  }
+}
+
 RiemannParams riemann_params(const m2cg_scheme& s) {
   RiemannParams P;
   P.maxIts_main = s.riem_maxits_main;
@@ -207,5 +255,93 @@ extern "C" m2cg_status m2cg_riemann_batch_pairs(const m2cg_scheme* scheme, const
                                 evals, err);
   if (st == M2CG_OK)
     for (int q = 0; q < n; q++) id[q] = id[q] & 1;
+  return st;
+}
+
+extern "C" m2cg_status m2cg_riemann_wall_batch(const m2cg_scheme* scheme, const m2cg_material* mats, int nmat, int n,
+                                               const double* Vm, const int* idm, const double* uwall,
+                                               const double* dir, double* Vs, int* id, double* Vsm, int* iters,
+                                               int* err) {
+  if (!scheme || !mats || nmat < 1 || nmat > MAXMAT_RIEMANN || n < 0 || !Vm || !idm || !uwall || !dir || !Vs || !id ||
+      !Vsm || !err) {
+    set_last_error("m2cg_riemann_wall_batch: null argument or material count outside 1..4");
+    return M2CG_ERR_ARG;
+  }
+  if (n == 0) return M2CG_OK;
+  for (int q = 0; q < n; q++)
+    if (idm[q] < 0 || idm[q] >= nmat) {
+      set_last_error("m2cg_riemann_wall_batch: material id outside 0..nmat-1");
+      return M2CG_ERR_ARG;
+    }
+  std::vector<Eos<double>> heos(MAXMAT_RIEMANN);
+  for (int m = 0; m < nmat; m++) heos[m] = eos_of_material(mats[m]);
+  cudaStream_t s;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+    set_last_error("m2cg_riemann_wall_batch: cudaStreamCreate failed (no CUDA device?)");
+    return M2CG_ERR_CUDA;
+  }
+  RiemannWallArgs a;
+  memset(&a, 0, sizeof a);
+  a.n = n;
+  a.P = riemann_params(*scheme);
+  a.path_cap = RIEMANN_PATH_CAP;
+  const long long max_slots = 148LL * 8 * 128;
+  a.scratch_slots = std::min<long long>(((long long)n + 127) / 128 * 128, max_slots);
+  auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t nn = (size_t)n;
+  const size_t eos_bytes = heos.size() * sizeof(Eos<double>);
+  const size_t total = 3 * rup(nn * 40) + 2 * rup(nn * 24) + 4 * rup(nn * 4) + rup(eos_bytes);
+  const size_t bytes_scratch = (size_t)a.scratch_slots * 3 * RIEMANN_PATH_CAP * sizeof(double);
+  char* buf = nullptr;
+  if (cudaMalloc((void**)&buf, total) != cudaSuccess || cudaMalloc((void**)&a.scratch, bytes_scratch) != cudaSuccess) {
+    cudaFree(buf);
+    cudaStreamDestroy(s);
+    set_last_error("m2cg_riemann_wall_batch: device allocation failed");
+    return M2CG_ERR_NOMEM;
+  }
+  char* p = buf;
+  auto take = [&](size_t b) { char* r = p; p += rup(b); return r; };
+  double* dVm = (double*)take(nn * 40);
+  double* duw = (double*)take(nn * 24);
+  double* ddir = (double*)take(nn * 24);
+  int* didm = (int*)take(nn * 4);
+  double* dVs = (double*)take(nn * 40);
+  double* dVsm = (double*)take(nn * 40);
+  int* did = (int*)take(nn * 4);
+  int* diters = (int*)take(nn * 4);
+  int* derr = (int*)take(nn * 4);
+  Eos<double>* deos = (Eos<double>*)take(eos_bytes);
+  cudaError_t e = cudaSuccess;
+  auto ck = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  ck(cudaMemcpyAsync(dVm, Vm, nn * 40, cudaMemcpyHostToDevice, s));
+  ck(cudaMemcpyAsync(duw, uwall, nn * 24, cudaMemcpyHostToDevice, s));
+  ck(cudaMemcpyAsync(ddir, dir, nn * 24, cudaMemcpyHostToDevice, s));
+  ck(cudaMemcpyAsync(didm, idm, nn * 4, cudaMemcpyHostToDevice, s));
+  ck(cudaMemcpyAsync(deos, heos.data(), eos_bytes, cudaMemcpyHostToDevice, s));
+  a.eos = deos; a.Vm = dVm; a.idm = didm; a.uwall = duw; a.dir = ddir;
+  a.Vs = dVs; a.Vsm = dVsm; a.id = did; a.iters = diters; a.err = derr;
+  if (e == cudaSuccess) {
+    // one thread per scratch slot (a multiple of 128 threads)
+    k_riemann_wall<<<(int)(a.scratch_slots / 128), 128, 0, s>>>(a);
+    ck(cudaGetLastError());
+  }
+  if (e == cudaSuccess) {
+    ck(cudaMemcpyAsync(Vs, dVs, nn * 40, cudaMemcpyDeviceToHost, s));
+    ck(cudaMemcpyAsync(Vsm, dVsm, nn * 40, cudaMemcpyDeviceToHost, s));
+    ck(cudaMemcpyAsync(id, did, nn * 4, cudaMemcpyDeviceToHost, s));
+    if (iters) ck(cudaMemcpyAsync(iters, diters, nn * 4, cudaMemcpyDeviceToHost, s));
+    ck(cudaMemcpyAsync(err, derr, nn * 4, cudaMemcpyDeviceToHost, s));
+  }
+  ck(cudaStreamSynchronize(s));
+  m2cg_status st = M2CG_OK;
+  if (e != cudaSuccess) {
+    char msg[200];
+    snprintf(msg, sizeof msg, "m2cg_riemann_wall_batch: %s", cudaGetErrorString(e));
+    set_last_error(msg);
+    st = M2CG_ERR_CUDA;
+  }
+  cudaFree(buf);
+  cudaFree(a.scratch);
+  cudaStreamDestroy(s);
   return st;
 }

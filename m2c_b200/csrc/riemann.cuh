@@ -935,6 +935,353 @@ struct RiemannSolver {
     if (iter == P.maxIts_main) return (nonadaptive ? RIEM_FAILED : RIEM_RETRY) | flags;
     return RIEM_OK | flags;
   }
+
+  // ---- one-sided (wall) problem: the fluid state on the minus side of a
+  // wall moving with normal velocity ustar (ExactRiemannSolverBase.cpp:
+  // 1931-2195 and its helpers). Only the 1-wave exists; its star velocity is
+  // the wall's.
+
+  // ComputeOneSidedRarefaction (1586-1728): integrate the 1-wave rarefaction
+  // in pressure from (rho, u, p) until its velocity reaches us > u. The step
+  // is sized by the velocity gained per step (target (us - u) / numSteps).
+  M2C_HD bool wall_rarefaction(double rho, double u, double p, double c, int id, double us, double& rhos, double& ps,
+                               bool* trans_rare, double* Vrare_x0) const {
+    const Eos<double>& e = eos[id];
+    rhos = rho;
+    ps = p;
+    const double du_goal = (us - u) / P.numSteps_rarefaction;
+    const double du_cap = du_goal * 1.25;
+    const double dp_lin = fabs(du_goal * c * rho);
+    const double dp_rel = (fabs(p) + 1.0e-6) / (P.numSteps_rarefaction * 2.5);
+    double dp = smin(dp_lin, dp_rel);
+    double r0 = rho, v0 = u, q0 = p, x0 = u - c;  // start of the step
+    double r1 = rho, v1 = u, q1 = p, x1;          // end of the step
+    const double utol = P.tol_rarefaction * smax(us - u, smax(fabs(us), fabs(u)));
+    double errU = 0, errR = 0;
+    for (int i = 0; i < P.numSteps_rarefaction * 5; i++) {
+      if (!rk_step(1, id, r0, v0, q0, dp, r1, v1, q1, x1, errU, errR)) {
+        dp /= 2.0;
+        continue;
+      }
+      const double dv = v1 - v0;
+      if (dv > du_cap) {
+        dp = dp / dv * du_goal;
+        continue;
+      }
+      if (v1 - us > utol) {  // overshot the wall velocity
+        if (dv != 0)
+          dp = dp / dv * (us - v0);
+        else
+          dp /= 2.0;
+        continue;
+      }
+      if (trans_rare && Vrare_x0 && x0 * x1 <= 0) {  // the fan crosses xi = 0
+        *trans_rare = true;
+        double w0 = fabs(x1), w1 = fabs(x0);
+        const double ww = w0 + w1;
+        w0 /= ww;
+        w1 /= ww;
+        Vrare_x0[0] = w0 * r0 + w1 * r1;
+        Vrare_x0[1] = w0 * v0 + w1 * v1;
+        Vrare_x0[2] = w0 * q0 + w1 * q1;
+      }
+      if (fabs(us - v1) <= utol) {
+        rhos = r1;
+        ps = q1;
+        return !e.bad(rhos, ps);
+      }
+      dp = smin(dp / dv * smin(du_goal, us - v1), dp * 5.0);
+      r0 = r1;
+      v0 = v1;
+      q0 = q1;
+      x0 = x1;
+    }
+    return false;  // did not reach us (the reference fails either way)
+  }
+
+  // FindInitialFeasiblePointsOneSidedByAcousticTheory (1119-1168): 0, 1 or 2
+  // points on the 1-wave curve, from the acoustic impedance.
+  M2C_HD int wall_acoustic_points(double rhol, double ul, double pl, double cl, int idl, double ustar, double& p0,
+                                  double& rhol0, double& ul0, double& p1, double& rhol1, double& ul1) {
+    const double Cl = rhol * cl;
+    p0 = pl + Cl * (ul - ustar);
+    bool ok = rho_u_star(1, path1, rhol, ul, pl, p0, idl, rhol, (p0 > pl) ? rhol * 1.1 : rhol * 0.9, rhol0, ul0,
+                         nullptr, nullptr);
+    if (!ok) {
+      p0 = 1.5 * pl;
+      ok = rho_u_star(1, path1, rhol, ul, pl, p0, idl, rhol, (p0 > pl) ? rhol * 1.1 : rhol * 0.9, rhol0, ul0,
+                      nullptr, nullptr);
+      if (!ok) return 0;
+    }
+    const double Clbar = (ul0 == ul) ? Cl : fabs(p0 - pl) / fabs(ul0 - ul);
+    p1 = pl + Clbar * (ul - ustar);
+    const double big = smax(fabs(p0), fabs(p1));
+    if (fabs(p1 - p0) / big < 1.0e-8) p1 = p0 + 1.0e-8 * big;
+    if (!rho_u_star(1, path1, rhol, ul, pl, p1, idl, rhol, rhol0, rhol1, ul1, nullptr, nullptr)) return 1;
+    return 2;
+  }
+
+  // FindInitialFeasiblePointsOneSided (2946-3016): the acoustic points, else
+  // a search at growing distances from pl.
+  M2C_HD bool wall_feasible_points(double rhol, double ul, double pl, double cl, int idl, double ustar, double& p0,
+                                   double& rhol0, double& ul0, double& p1, double& rhol1, double& ul1) {
+    const int found = wall_acoustic_points(rhol, ul, pl, cl, idl, ustar, p0, rhol0, ul0, p1, rhol1, ul1);
+    if (found == 2) return true;
+    bool ok = true;
+    if (found == 0) {
+      const double step = ul > ustar ? 0.5 * pl : -0.5 * pl;
+      for (int i = 0; i < P.maxIts_bracket; i++) {
+        p0 = pl + 0.01 * (i + 1) * (i + 1) * step;
+        if (p0 < P.min_pressure) p0 = P.pressure_at_failure;
+        ok = rho_u_star(1, path1, rhol, ul, pl, p0, idl, rhol, (p0 > pl) ? rhol * 1.1 : rhol * 0.9, rhol0, ul0,
+                        nullptr, nullptr);
+        if (ok) break;
+      }
+      if (!ok) return false;
+    }
+    const double step = p0 - pl;
+    for (int i = 0; i < P.maxIts_bracket; i++) {
+      p1 = p0 + 0.01 * (i + 1) * (i + 1) * step;
+      ok = rho_u_star(1, path1, rhol, ul, pl, p1, idl, rhol, rhol0, rhol1, ul1, nullptr, nullptr);
+      if (ok) break;
+    }
+    if (!ok) return false;
+    if (p0 > p1) {
+      swap_(p0, p1);
+      swap_(rhol0, rhol1);
+      swap_(ul0, ul1);
+    }
+    return true;
+  }
+
+  // FindInitialIntervalOneSided (800-958): from two feasible points, secant
+  // steps pushed 10% outward until ul(p) - ustar changes sign. On failure the
+  // point with the smallest |ul - ustar| (or pressure_at_failure, when that
+  // residual is not small) is returned as p0 = p1, and false.
+  M2C_HD bool wall_interval(double rhol, double ul, double pl, double cl, int idl, double ustar, double& p0,
+                            double& rhol0, double& ul0, double& p1, double& rhol1, double& ul1) {
+    if (!wall_feasible_points(rhol, ul, pl, cl, idl, ustar, p0, rhol0, ul0, p1, rhol1, ul1)) {
+      p0 = p1 = P.pressure_at_failure;
+      return false;
+    }
+    double p2, rhol2, ul2, f0, f1;
+    double best, p_best, rho_best, u_best;  // smallest |f| met (failsafe answer)
+    if (fabs(ul0 - ustar) < fabs(ul1 - ustar)) {
+      best = fabs(ul0 - ustar); p_best = p0; rho_best = rhol0; u_best = ul0;
+    } else {
+      best = fabs(ul1 - ustar); p_best = p1; rho_best = rhol1; u_best = ul1;
+    }
+    bool ok = true;
+    int i;
+    for (i = 0; i < P.maxIts_bracket; i++) {
+      f0 = ul0 - ustar;
+      f1 = ul1 - ustar;
+      if (f0 * f1 <= 0.0) return true;
+      if (fabs(f0 - f1) > 1e-9) {
+        p2 = p1 - f1 * (p1 - p0) / (f1 - f0);
+        if (p2 < p0)
+          p2 -= 0.1 * (p1 - p0);
+        else
+          p2 += 0.1 * (p1 - p0);
+      } else {
+        p2 = 1.1 * p1;
+      }
+      if (p2 < pl || i == int(P.maxIts_bracket / 2)) p2 = pl;
+      ok = rho_u_star(1, path1, rhol, ul, pl, p2, idl, rhol0, rhol1, rhol2, ul2, nullptr, nullptr);
+      if (!ok) {  // step back towards [p0, p1]
+        for (int j = 0; j < P.maxIts_bracket / 2; j++) {
+          if (p2 < p0)
+            p2 = p0 - 0.5 * (p0 - p2);
+          else
+            p2 = p1 + 0.5 * (p2 - p1);
+          if (p2 < pl) p2 = pl;
+          ok = rho_u_star(1, path1, rhol, ul, pl, p2, idl, rhol0, rhol1, rhol2, ul2, nullptr, nullptr);
+          if (ok) break;
+        }
+      }
+      if (!ok) break;
+      if (fabs(ul2 - ustar) < best) {
+        best = fabs(ul2 - ustar); p_best = p2; rho_best = rhol2; u_best = ul2;
+      }
+      if (p2 < p0) {
+        p1 = p0; rhol1 = rhol0; ul1 = ul0;
+        p0 = p2; rhol0 = rhol2; ul0 = ul2;
+      } else {
+        p0 = p1; rhol0 = rhol1; ul0 = ul1;
+        p1 = p2; rhol1 = rhol2; ul1 = ul2;
+      }
+    }
+    (void)i;
+    if (best < P.failure_threshold * fabs(ul - ustar)) {
+      p0 = p1 = p_best; rhol0 = rhol1 = rho_best; ul0 = ul1 = u_best;
+    } else {  // the problem may have no solution: the prescribed pressure
+      p2 = P.pressure_at_failure;
+      if (rho_u_star(1, path1, rhol, ul, pl, p2, idl, rhol0, rhol1, rhol2, ul2, nullptr, nullptr)) {
+        p0 = p1 = p2; rhol0 = rhol1 = rhol2; ul0 = ul1 = ul2;
+      } else {
+        p0 = p1 = p_best; rhol0 = rhol1 = rho_best; ul0 = ul1 = u_best;
+      }
+    }
+    return false;
+  }
+
+  // FinalizeOneSidedSolution (519-630): the state at xi = 0 (id = -1 where
+  // the wall moves away, ustar < 0, and the point lies beyond the fluid) and
+  // the star state Vsm with the tangential velocity of Vm.
+  M2C_HD void wall_finalize(const double* dir, const double* Vm, double rhol, double ul, double pl, int idl,
+                            double rhol2, double u2, double p2, bool trans_rare, const double* Vrare_x0, double* Vs,
+                            int& id, double* Vsm, bool& bad) const {
+    const double utanl[3] = {Vm[1] - ul * dir[0], Vm[2] - ul * dir[1], Vm[3] - ul * dir[2]};
+    id = u2 >= 0 ? idl : -1;
+    if (id != -1) {
+      Vs[0] = Vs[1] = Vs[2] = Vs[3] = Vs[4] = 0.0;
+      if (trans_rare) {
+        Vs[0] = Vrare_x0[0];
+        Vs[1] = Vrare_x0[1] * dir[0];
+        Vs[2] = Vrare_x0[1] * dir[1];
+        Vs[3] = Vrare_x0[1] * dir[2];
+        Vs[4] = Vrare_x0[2];
+      } else {
+        bool star = false;
+        if (pl >= p2) {  // rarefaction: is the tail left of xi = 0?
+          double el2 = eos[idl].energy(rhol2, p2);
+          double cl2 = eos[idl].c2(rhol2, el2);
+          if (rhol2 <= 0 || cl2 < 0) { bad = true; cl2 = 0; }  // the reference aborts
+          else cl2 = sqrt(cl2);
+          if (u2 - cl2 <= 0) star = true;
+        } else {  // shock: its speed
+          const double sh = (rhol2 * u2 - rhol * ul) / (rhol2 - rhol);
+          if (sh <= 0) star = true;
+        }
+        if (star) {
+          Vs[0] = rhol2; Vs[1] = u2 * dir[0]; Vs[2] = u2 * dir[1]; Vs[3] = u2 * dir[2]; Vs[4] = p2;
+        } else {
+          Vs[0] = rhol; Vs[1] = ul * dir[0]; Vs[2] = ul * dir[1]; Vs[3] = ul * dir[2]; Vs[4] = pl;
+        }
+      }
+      for (int i = 1; i <= 3; i++) Vs[i] += utanl[i - 1];
+    }
+    Vsm[0] = rhol2;
+    Vsm[1] = utanl[0] + u2 * dir[0];
+    Vsm[2] = utanl[1] + u2 * dir[1];
+    Vsm[3] = utanl[2] + u2 * dir[2];
+    Vsm[4] = p2;
+  }
+
+  // The input state with its normal velocity replaced by the wall's: the
+  // answer of a solve that failed (2022-2040, 2082-2100).
+  M2C_HD static void wall_fallback(const double* dir, const double* Vm, double ul, double ustar, int idl, double* Vs,
+                                   int& id, double* Vsm) {
+    const double utanl[3] = {Vm[1] - ul * dir[0], Vm[2] - ul * dir[1], Vm[3] - ul * dir[2]};
+    Vsm[0] = Vm[0];
+    Vsm[1] = utanl[0] + ustar * dir[0];
+    Vsm[2] = utanl[1] + ustar * dir[1];
+    Vsm[3] = utanl[2] + ustar * dir[2];
+    Vsm[4] = Vm[4];
+    if (ustar >= 0) {
+      id = idl;
+      for (int i = 0; i < 5; i++) Vs[i] = Vsm[i];
+    } else {
+      id = -1;
+    }
+  }
+
+  // ComputeOneSidedRiemannSolution (1931-2195): Vm (id idl) against a wall
+  // whose velocity is Ustar, dir the unit normal pointing from the fluid to
+  // the wall. Trivial when the normal velocities agree, a rarefaction when
+  // the fluid moves away from the wall, else a shock whose pressure is found
+  // by the safeguarded secant method. Returns RIEM_OK or RIEM_FAILED
+  // (| RIEM_PATH_OVERFLOW); bad_state is set where the reference aborts.
+  M2C_HD int solve_wall(const double* dir, const double* Vm, int idl, const double* Ustar, double* Vs, int& id,
+                        double* Vsm, bool& bad_state) {
+    bad_state = false;
+    iterations = 0;
+    evaluations = 0;
+    const double rhol = Vm[0];
+    const double ul = Vm[1] * dir[0] + Vm[2] * dir[1] + Vm[3] * dir[2];
+    const double pl = Vm[4];
+    const double ustar = Ustar[0] * dir[0] + Ustar[1] * dir[1] + Ustar[2] * dir[2];
+    const Eos<double>& e = eos[idl];
+    const double el = e.energy(rhol, pl);
+    double cl = e.c2(rhol, el);
+    if (rhol <= 0 || cl < 0) {  // the reference aborts here
+      bad_state = true;
+      wall_fallback(dir, Vm, ul, ustar, idl, Vs, id, Vsm);
+      return RIEM_FAILED;
+    }
+    cl = sqrt(cl);
+    path1.n = 0;
+    path1.overflow = false;
+    path1.push(pl, rhol, ul);
+    double p0 = DBL_MIN, ul0 = 0.0, rhol0 = DBL_MIN;
+    double p1 = DBL_MIN, ul1 = 0.0, rhol1 = DBL_MIN;
+    double p2 = DBL_MIN, ul2 = 0.0, rhol2 = DBL_MIN;
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    bool trans_rare = false;
+    double Vrare_x0[3] = {0.0, 0.0, 0.0};
+    auto flags = [&]() { return path1.overflow ? RIEM_PATH_OVERFLOW : 0; };
+    if (fabs(ul - ustar) < 1.0e-20) {
+      wall_finalize(dir, Vm, rhol, ul, pl, idl, rhol, ul, pl, trans_rare, Vrare_x0, Vs, id, Vsm, bad_state);
+      return RIEM_OK;
+    }
+    if (ul < ustar) {  // rarefaction
+      if (!wall_rarefaction(rhol, ul, pl, cl, idl, ustar, rhol2, p2, &trans_rare, Vrare_x0)) {
+        wall_fallback(dir, Vm, ul, ustar, idl, Vs, id, Vsm);
+        return RIEM_FAILED | flags();
+      }
+      wall_finalize(dir, Vm, rhol, ul, pl, idl, rhol2, ustar, p2, trans_rare, Vrare_x0, Vs, id, Vsm, bad_state);
+      return RIEM_OK | flags();
+    }
+    // shock
+    if (!wall_interval(rhol, ul, pl, cl, idl, ustar, p0, rhol0, ul0, p1, rhol1, ul1)) {
+      if (!rho_u_star(1, path1, rhol, ul, pl, p1, idl, rhol0, rhol0 * 1.1, rhol2, ul2, &trans_rare, Vrare_x0)) {
+        wall_fallback(dir, Vm, ul, ustar, idl, Vs, id, Vsm);
+        return RIEM_FAILED | flags();
+      }
+      wall_finalize(dir, Vm, rhol, ul, pl, idl, rhol2, ustar, p1, trans_rare, Vrare_x0, Vs, id, Vsm, bad_state);
+      return RIEM_FAILED | flags();
+    }
+    f0 = ul0 - ustar;
+    f1 = ul1 - ustar;
+    double denom = 0;
+    int iter = 0;
+    double err_p = 1.0, err_u = 1.0;
+    p2 = p1;
+    f2 = f1;
+    for (iter = 0; iter < P.maxIts_main; iter++) {
+      denom = f1 - f0;
+      if (denom == 0) {
+        p2 = 0.5 * (p0 + p1);
+      } else {
+        p2 = p2 - f2 * (p1 - p0) / denom;
+        if (p2 <= p0 || p2 >= p1) p2 = 0.5 * (p0 + p1);
+      }
+    retry_wall:
+      if (!rho_u_star(1, path1, rhol, ul, pl, p2, idl, rhol0, rhol1, rhol2, ul2, &trans_rare, Vrare_x0)) {
+        p2 = 0.5 * (p2 + p0);
+        iter++;
+        if (iter < P.maxIts_main)
+          goto retry_wall;
+        else
+          break;
+      }
+      f2 = ul2 - ustar;
+      if (f0 * f2 < 0.0) {
+        p1 = p2; f1 = f2; rhol1 = rhol2;
+      } else {
+        p0 = p2; f0 = f2; rhol0 = rhol2;
+      }
+      err_p = fabs(p1 - p0) / fabs(pl + 0.5 * rhol * ul * ul);
+      err_u = fabs(f2) / cl;
+      if ((err_p < P.tol_main && err_u < P.tol_main) || (err_p < P.tol_main * 1e-3) || (err_u < P.tol_main * 1e-3))
+        break;
+      trans_rare = false;
+    }
+    iterations = iter + 1;
+    wall_finalize(dir, Vm, rhol, ul, pl, idl, rhol2, ustar, p2, trans_rare, Vrare_x0, Vs, id, Vsm, bad_state);
+    if (iter == P.maxIts_main) return RIEM_FAILED | flags();
+    return RIEM_OK | flags();
+  }
 };
 
 }  // namespace m2c

@@ -66,6 +66,9 @@ def lib():
     L.m2cg_riemann_batch_pairs.argtypes = [C.POINTER(abi.Scheme), C.POINTER(abi.Material), C.c_int, dp, dp, dp, dp,
                                            dp, ip, dp, dp, ip, ip, ip]
     L.m2cg_riemann_batch_pairs.restype = C.c_int
+    L.m2cg_riemann_wall_batch.argtypes = [C.POINTER(abi.Scheme), C.POINTER(abi.Material), C.c_int, C.c_int, dp, ip,
+                                          dp, dp, dp, ip, dp, ip, ip]
+    L.m2cg_riemann_wall_batch.restype = C.c_int
     L.m2cg_batch_create.argtypes = [C.POINTER(abi.Scheme), C.c_int, ip, C.POINTER(abi.Material), dp, dp,
                                     C.POINTER(BatchTuning), C.POINTER(vp)]
     L.m2cg_batch_run.argtypes = [vp, C.c_int]
@@ -124,6 +127,24 @@ def riemann_batch(s, mats, VL, idl, VR, idr, dirs, warm=None):
                                    abi.iptr(idr), abi.dptr(dirs), abi.dptr(warm), abi.dptr(Vs), abi.iptr(mid),
                                    abi.dptr(Vsm), abi.dptr(Vsp), abi.iptr(it), abi.iptr(err)))
     return Vs, mid, Vsm, Vsp, it, err
+
+
+def riemann_wall_batch(s, mats, Vm, idm, uwall, dirs):
+    """One-sided (wall) Riemann problems on the GPU
+    (ExactRiemannSolverBase::ComputeOneSidedRiemannSolution): fluid state
+    Vm[q] of material idm[q] against a wall moving with velocity uwall[q],
+    dirs[q] the unit normal from the fluid to the wall. Returns Vs (zero
+    where id = -1), id, Vsm, iterations, err."""
+    n = len(idm)
+    Vm, uwall, dirs = (np.ascontiguousarray(a, np.float64) for a in (Vm, uwall, dirs))
+    idm = np.ascontiguousarray(idm, np.int32)
+    Vs, Vsm = np.zeros((n, 5)), np.zeros((n, 5))
+    mid, it, err = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    arr = (abi.Material * len(mats))(*mats)
+    check(lib().m2cg_riemann_wall_batch(C.byref(s), arr, len(mats), n, abi.dptr(Vm), abi.iptr(idm),
+                                        abi.dptr(uwall), abi.dptr(dirs), abi.dptr(Vs), abi.iptr(mid),
+                                        abi.dptr(Vsm), abi.iptr(it), abi.iptr(err)))
+    return Vs, mid, Vsm, it, err
 
 
 def riemann_batch_pairs(s, mats, VL, VR, dirs, warm=None):

@@ -63,6 +63,7 @@ def _load(path, prefix):
     f("point_p2c").argtypes = [vp, C.c_int, dp, ip, dp]
     f("point_riemann").restype = C.c_int
     f("point_riemann").argtypes = [vp, C.c_int, dp, dp, ip, dp, ip, dp, ip, dp, dp, ip]
+    f("point_riemann_wall").argtypes = [vp, C.c_int, dp, dp, ip, dp, dp, ip, dp, ip]
     f("point_destroy").argtypes = [vp]
     _libs[path] = lib
     return lib
@@ -176,6 +177,18 @@ class _Point:
                                  abi.iptr(idr), abi.dptr(Vs), abi.iptr(mid), abi.dptr(Vsm), abi.dptr(Vsp),
                                  abi.iptr(err))
         return Vs, mid, Vsm, Vsp, err
+
+    def riemann_wall(self, dirs, Vm, idm, uwall):
+        """ExactRiemannSolverBase::ComputeOneSidedRiemannSolution per problem:
+        returns (Vs, id, Vsm, err); Vs is zero where id = -1."""
+        n = len(idm)
+        dirs, Vm, uwall = (np.ascontiguousarray(a, np.float64) for a in (dirs, Vm, uwall))
+        idm = np.ascontiguousarray(idm, np.int32)
+        Vs, Vsm = np.zeros((n, 5)), np.zeros((n, 5))
+        mid, err = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        self._f("point_riemann_wall")(self.h, n, abi.dptr(dirs), abi.dptr(Vm), abi.iptr(idm), abi.dptr(uwall),
+                                      abi.dptr(Vs), abi.iptr(mid), abi.dptr(Vsm), abi.iptr(err))
+        return Vs, mid, Vsm, err
 
     def close(self):
         if self.h:

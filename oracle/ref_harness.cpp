@@ -498,6 +498,26 @@ int m2cref_point_riemann(void* h, int n, const double* dir, const double* VL, co
   return nerr;
 }
 
+// ExactRiemannSolverBase::ComputeOneSidedRiemannSolution on each problem;
+// Vs is zeroed first (the reference leaves it untouched where id = -1).
+int m2cref_point_riemann_wall(void* h, int n, const double* dir, const double* Vm, const int* idm,
+                              const double* uwall, double* Vs, int* id, double* Vsm, int* err) {
+  RefPoint* p = (RefPoint*)h;
+  int nerr = 0;
+  for (int q = 0; q < n; q++) {
+    double d[3], a[5], w[3];
+    memcpy(d, dir + 3 * q, sizeof d);
+    memcpy(a, Vm + 5 * q, sizeof a);
+    memcpy(w, uwall + 3 * q, sizeof w);
+    for (int c = 0; c < 5; c++) Vs[5 * q + c] = 0.0;
+    int midid = 0;
+    err[q] = p->riemann->ComputeOneSidedRiemannSolution(d, a, idm[q], w, Vs + 5 * q, midid, Vsm + 5 * q);
+    id[q] = midid;
+    nerr += err[q] != 0;
+  }
+  return nerr;
+}
+
 void m2cref_point_destroy(void* h) {
   RefPoint* p = (RefPoint*)h;
   delete p->ff;

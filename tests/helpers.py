@@ -53,3 +53,19 @@ def host_riemann(lib, s, mats, VL, idl, VR, idr, dirs, libm=True):
     lib.host_riemann(C.byref(s), table, len(mats), n, *[p(a) for a in args], p(Vs), p(mid), p(Vsm), p(Vsp),
                      p(err), p(retried), int(bool(libm)), p(mis))
     return Vs, mid, Vsm, Vsp, err, retried, mis
+
+
+def host_riemann_wall(lib, s, mats, Vm, idm, uwall, dirs, libm=True):
+    """One-sided (wall) problems with the host build of the library's solver
+    (RiemannSolver::solve_wall); pow chosen as in host_riemann. Returns (Vs,
+    id, Vsm, err, misrounded)."""
+    n = len(Vm)
+    table = (abi.Material * len(mats))(*mats)
+    Vs, Vsm = np.zeros((n, 5)), np.zeros((n, 5))
+    mid, err, mis = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    args = [np.ascontiguousarray(a) for a in (dirs, np.asarray(Vm, np.float64), np.asarray(idm, np.int32),
+                                              np.asarray(uwall, np.float64))]
+    lib.host_riemann_wall(C.byref(s), table, len(mats), n, *[p(a) for a in args], p(Vs), p(mid), p(Vsm), p(err),
+                          int(bool(libm)), p(mis))
+    return Vs, mid, Vsm, err, mis

@@ -90,3 +90,60 @@ extern "C" int host_riemann(const m2cg_scheme* s, const m2cg_material* mats, int
   }
   return 0;
 }
+
+// One-sided (wall) problems, RiemannSolver::solve_wall, with the same pow
+// selection; Vs is zeroed first (the solver leaves it untouched where the
+// state at the wall is undefined, id = -1).
+extern "C" int host_riemann_wall(const m2cg_scheme* s, const m2cg_material* mats, int nmat, int n, const double* dir,
+                                 const double* Vm, const int* idm, const double* uwall, double* Vs, int* id,
+                                 double* Vsm, int* err, int libm, int* misrounded) {
+  g_libm = libm;
+  std::vector<Eos<double>> eos(nmat);
+  for (int m = 0; m < nmat; m++) {
+    MatParams p;
+    p.kind = mats[m].eos;
+    p.gam = mats[m].gamma;
+    p.pc = mats[m].p_c;
+    p.b = mats[m].b;
+    p.q = mats[m].q;
+    p.rhomin = mats[m].rhomin;
+    p.pmin = mats[m].pmin;
+    p.rhomax = mats[m].rhomax;
+    p.pmax = mats[m].pmax;
+    p.failsafe_density = mats[m].failsafe_density;
+    eos[m] = make_eos<double>(p);
+  }
+  RiemannParams P;
+  P.maxIts_main = s->riem_maxits_main;
+  P.maxIts_bracket = s->riem_maxits_bracket;
+  P.maxIts_shock = s->riem_maxits_shock;
+  P.numSteps_rarefaction = s->riem_nsteps_rarefaction;
+  P.tol_main = s->riem_tol_main;
+  P.tol_shock = s->riem_tol_shock;
+  P.tol_rarefaction = s->riem_tol_rarefaction;
+  P.min_pressure = s->riem_min_pressure;
+  P.failure_threshold = s->riem_failure_threshold;
+  P.pressure_at_failure = s->riem_pressure_at_failure;
+  P.warm_delta = s->riem_warm_delta;
+  P.warm_gate = s->riem_warm_gate;
+  const int cap = 512;
+  std::vector<double> scratch(3 * cap);
+  RiemannSolver rs;
+  rs.P = P;
+  rs.eos = eos.data();
+  rs.path1.pt = scratch.data();
+  rs.path1.cap = cap;
+  rs.path3.pt = nullptr;
+  rs.path3.cap = 0;
+  for (int q = 0; q < n; q++) {
+    bool bad = false;
+    int mid = 0;
+    g_misrounded = 0;
+    for (int c = 0; c < 5; c++) Vs[5 * q + c] = 0.0;
+    const int r = rs.solve_wall(dir + 3 * q, Vm + 5 * q, idm[q], uwall + 3 * q, Vs + 5 * q, mid, Vsm + 5 * q, bad);
+    id[q] = mid;
+    err[q] = r | (bad ? 4 : 0);
+    if (misrounded) misrounded[q] = g_misrounded;
+  }
+  return 0;
+}

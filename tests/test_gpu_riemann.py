@@ -92,3 +92,40 @@ def test_riemann_trivial_and_symmetric(gpu):
     assert err[1] == 0 and err2[0] == 0
     assert abs(Vsm[1, 4] - Vsp2[0, 4]) <= 1e-4 * Vsm[1, 4]
     assert abs(Vsm[1, 0] - Vsp2[0, 0]) <= 1e-4 * Vsm[1, 0]
+
+
+@pytest.mark.parametrize("seed", [7, 8])
+def test_wall_riemann_batch_bit_identical_to_reference(gpu, ref, seed):
+    """One-sided (wall) problems (ExactRiemannSolverBase::
+    ComputeOneSidedRiemannSolution, ExactRiemannSolverBase.cpp:1931-2195)
+    against the unmodified reference: every output of every problem
+    bit-identical, the failures (seed 8: rarefactions that cannot reach the
+    wall's velocity, answered with the input state) included. The path calls
+    no step-control pow on these problems (the host build counts them), so
+    the unmodified reference is the bar."""
+    n = 4000
+    mats, Vm, idm, uwall, dirs = cases.wall_problems(n, seed=seed)
+    s = abi.scheme()
+    Vs, mid, Vsm, err = ref.RefPoint(s, mats).riemann_wall(dirs, Vm, idm, uwall)
+    gVs, gid, gVsm, it, gerr = gpu.riemann_wall_batch(s, mats, Vm, idm, uwall, dirs)
+    for a, b in ((gVs, Vs), (gVsm, Vsm)):
+        bad = ~_same_rows(a, b)
+        assert not bad.any(), (bad.sum(), np.nonzero(bad)[0][:5])
+    assert np.array_equal(gid, mid)
+    assert np.array_equal((gerr & 1) != 0, err != 0)
+    assert not (gerr & 6).any()
+    un = np.einsum("ij,ij->i", Vm[:, 1:4], dirs)
+    uw = np.einsum("ij,ij->i", uwall, dirs)
+    shock = un > uw
+    assert it[shock & (gerr == 0)].min() >= 1 and it[~shock].max() == 0
+    # the star state carries the wall's normal velocity wherever the solve succeeded
+    ok = gerr == 0
+    assert np.allclose(np.einsum("ij,ij->i", gVsm[ok, 1:4], dirs[ok]), uw[ok], rtol=1e-9, atol=1e-9)
+
+
+def test_wall_riemann_batch_rejects_bad_material_id(gpu):
+    mats, Vm, idm, uwall, dirs = cases.wall_problems(8, seed=7)
+    idm = idm.copy()
+    idm[3] = 2
+    with pytest.raises(gpu.M2CError):
+        gpu.riemann_wall_batch(abi.scheme(), mats, Vm, idm, uwall, dirs)

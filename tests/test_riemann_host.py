@@ -153,3 +153,38 @@ extern "C" long check(long n, unsigned long long seed, long* libm_sq_diff) {
     assert bad == 0, bad
     # the C library's x^2 differs from the correctly rounded square on ~1e-3 of arguments
     assert 0 < diff.value < n * 3e-3, diff.value
+
+
+@pytest.mark.parametrize("seed", [7, 8])
+def test_host_wall_solver_bit_identical_to_reference(ref, host_riemann_lib, seed):
+    """One-sided (wall) problems (ExactRiemannSolverBase::
+    ComputeOneSidedRiemannSolution, ExactRiemannSolverBase.cpp:1931-2195):
+    with the C library's pow every output equals the reference's bit for bit;
+    with the correctly rounded pow, against the reference built with it
+    (refcr), too. The seeded set holds every branch: trivial, rarefaction
+    (with transonic fans and receding walls, id = -1) and shock."""
+    from tests.helpers import host_riemann_wall
+    n = 3000
+    mats, Vm, idm, uwall, dirs = cases.wall_problems(n, seed=seed)
+    s = abi.scheme()
+    Vs, mid, Vsm, err = ref.RefPoint(s, mats).riemann_wall(dirs, Vm, idm, uwall)
+    hVs, hmid, hVsm, herr, mis = host_riemann_wall(host_riemann_lib, s, mats, Vm, idm, uwall, dirs)
+    assert np.array_equal(hVs, Vs) and np.array_equal(hVsm, Vsm)
+    assert np.array_equal(hmid, mid)
+    assert np.array_equal((herr & 1) != 0, err != 0)
+    assert not (herr & 6).any()
+    un = np.einsum("ij,ij->i", Vm[:, 1:4], dirs)
+    uw = np.einsum("ij,ij->i", uwall, dirs)
+    assert (un < uw).sum() > n // 4 and (un > uw).sum() > n // 4  # rarefactions and shocks
+    assert (mid == -1).sum() > 0 and (un == uw).sum() > 0
+    if seed == 8:  # rarefactions that cannot reach the wall's velocity: the failure answer
+        assert (err != 0).sum() > 20
+    # the one-sided path reaches the step-control pow only through a trial
+    # pressure below the fluid's (a rarefaction in ComputeRhoUStar), which
+    # these problems never take
+    assert not mis.any()
+    if ref.available("crpow"):
+        Vs2, mid2, Vsm2, err2 = ref.RefPointCR(s, mats).riemann_wall(dirs, Vm, idm, uwall)
+        cVs, cmid, cVsm, cerr, _ = host_riemann_wall(host_riemann_lib, s, mats, Vm, idm, uwall, dirs, libm=False)
+        assert np.array_equal(cVs, Vs2) and np.array_equal(cVsm, Vsm2) and np.array_equal(cmid, mid2)
+        assert np.array_equal((cerr & 1) != 0, err2 != 0)
