@@ -137,6 +137,12 @@ typedef struct {
    * estimate already starts within the network's own error. 0 (default):
    * every proposal departing by more than riem_warm_delta is used. */
   double riem_warm_gate;
+  /* EmbeddedBoundaryMethodData (IoData.h:1340-1360), for faces cut by an
+   * embedded surface (m2cg_set_wall_faces): direction of the one-sided
+   * Riemann problems, 0 EMBEDDED_SURFACE, 1 MESH (default), 2 AVERAGE; state
+   * reconstruction at the surface, 0 CONSTANT (default; LINEAR is refused). */
+  int ebm_riemann_normal;
+  int ebm_recon;
 } m2cg_scheme;
 
 /* One level set (LevelSetSchemeData, IoData.h:653-679; reinit
@@ -229,8 +235,33 @@ typedef struct {
                                     within 10 layers, MultiPhaseOperator.cpp:1352-1369) */
   long long riemann_nontrivial;  /* interface Riemann problems not answered by the trivial branch
                                     (equal normal velocity and pressure, ExactRiemannSolverBase.cpp:129-134) */
+  long long wall_riemann_calls;  /* one-sided Riemann problems at faces cut by an embedded surface (their
+                                    failures are counted in riemann_errors, as the reference does) */
 } m2cg_counters;
 m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
+
+/* Faces cut by embedded surfaces (walls), for every following stage until
+ * replaced; n = 0 removes them. Replaces the embedded-boundary branch of
+ * SpaceOperator::ComputeAdvectionFluxes (SpaceOperator.cpp:2438-2484, and the
+ * y/z faces at 2568-2612, 2695-2739): on a cut face each side gets its
+ * numerical flux against its own one-sided Riemann star state
+ * (ExactRiemannSolverBase::ComputeOneSidedRiemannSolution on its cell-centred
+ * stage state, the star state clipped), solved on the device each stage.
+ * faces [n][4] = (axis d: 0 x, 1 y, 2 z; i, j, k): the face between interior
+ * cell (i, j, k) and its low neighbour along d, which must be interior too
+ * (index along d >= 1). What the reference's intersector data yields for
+ * that face through SpaceOperator::FindEdgeSurfaceIntersections
+ * (SpaceOperator.cpp:3435-3501), [n][3] each: nwall_fwd / uwall_fwd, the
+ * surface's unit normal and velocity at the intersection nearest the low
+ * cell; nwall_bwd / uwall_bwd, those nearest the high cell. The normals are
+ * used by scheme->ebm_riemann_normal EMBEDDED_SURFACE and AVERAGE. Refused
+ * (M2CG_ERR_UNSUPPORTED): LINEAR reconstruction at the surface, viscous or
+ * heat-diffusive materials (the diffusion operators' own wall branches are
+ * not built), faces on the subdomain boundary. Every cell stays active (the
+ * reference's INACTIVE_MATERIAL_ID regions enclosed by a surface are not
+ * represented). Host pointers. */
+m2cg_status m2cg_set_wall_faces(m2cg_ctx* ctx, int n, const int* faces, const double* nwall_fwd,
+                                const double* uwall_fwd, const double* nwall_bwd, const double* uwall_bwd);
 
 /* MultiPhaseOperator::UpdateStateVariablesAfterInterfaceMotion
  * (MultiPhaseOperator.cpp:823-1400) on the context's resident state: every
@@ -437,7 +468,10 @@ m2cg_status m2cg_batch_create(const m2cg_scheme* scheme, int ntubes, const int* 
                               const m2cg_batch_tuning* tuning, m2cg_batch** out);
 /* Advance every tube by nsteps steps with a per-tube CFL dt. */
 m2cg_status m2cg_batch_run(m2cg_batch* b, int nsteps);
-/* Download tube states: V (5 doubles per cell, tubes concatenated), ID per cell. */
+/* Download tube states: V (5 doubles per cell, tubes concatenated), ID per
+ * cell, time per tube. After a tube reported an error the arrays are still
+ * written (the other tubes' states are valid) and the status names the
+ * error. */
 m2cg_status m2cg_batch_download(m2cg_batch* b, double* V, int* ID, double* t_per_tube);
 /* The tuning in use (the autotuner's choice where the caller passed 0). */
 m2cg_status m2cg_batch_get_tuning(const m2cg_batch* b, m2cg_batch_tuning* t);

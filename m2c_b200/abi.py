@@ -65,6 +65,7 @@ class Scheme(C.Structure):
         ("riem_min_pressure", C.c_double), ("riem_failure_threshold", C.c_double),
         ("riem_pressure_at_failure", C.c_double), ("riem_warm_delta", C.c_double),
         ("mp_riemann_normal", C.c_int), ("riem_warm_gate", C.c_double),
+        ("ebm_riemann_normal", C.c_int), ("ebm_recon", C.c_int),
     ]
 
 
@@ -82,6 +83,10 @@ def material(gamma=1.4, p_c=0.0, eos=EOS_SG, b=0.0, q=0.0, rhomin=0.0, pmin=-DBL
              cv=0.0, T0=0.0, e0=0.0, cp=0.0, h0=0.0):
     return Material(eos, gamma, p_c, b, q, rhomin, pmin, rhomax, pmax, failsafe_density, mu, mu_bulk,
                     heat_diffusivity, cv, T0, e0, cp, h0)
+
+
+# EmbeddedBoundaryMethodData::RiemannNormal (IoData.h:1345)
+EBM_NORMAL_SURFACE, EBM_NORMAL_MESH, EBM_NORMAL_AVERAGE = 0, 1, 2
 
 
 def scheme(**kw):
@@ -113,6 +118,8 @@ def scheme(**kw):
     s.riem_pressure_at_failure = 1.0e-8
     s.riem_warm_delta = 3.0e-4
     s.mp_riemann_normal = RIEMANN_NORMAL_MESH
+    s.ebm_riemann_normal = EBM_NORMAL_MESH
+    s.ebm_recon = 0
     for k, v in kw.items():
         if not hasattr(s, k):
             raise AttributeError(k)

@@ -24,7 +24,7 @@ COMMON = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcom
 # --use_fast_math changes only single-precision arithmetic (approximate
 # division/sqrt, flush to zero): the FP32 flux half of the mixed path.
 FAST_FP32 = {"kernels_mixed.cu"}
-NO_FMA = {"kernels_fp64.cu", "context.cu", "viscous.cu", "multiphase.cu", "riemann.cu", "levelset.cu", "batch.cu",
+NO_FMA = {"kernels_fp64.cu", "context.cu", "viscous.cu", "walls.cu", "multiphase.cu", "riemann.cu", "levelset.cu", "batch.cu",
           "noalloc.cu"}
 
 

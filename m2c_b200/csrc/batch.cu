@@ -1186,8 +1186,10 @@ extern "C" m2cg_status m2cg_batch_run(m2cg_batch* b, int nsteps) {
 
 extern "C" m2cg_status m2cg_batch_download(m2cg_batch* b, double* V, int* ID, double* t_per_tube) {
   if (!b) return bfail(M2CG_ERR_ARG, "null argument");
-  m2cg_status st = batch_check(b);
-  if (st) return st;
+  // a tube's error stops that tube only: the states are still copied (the
+  // failed tubes' are not defined) and the status names the error
+  const m2cg_status st = batch_check(b);
+  if (st == M2CG_ERR_CUDA) return st;
   const long long N = b->ncell;
   if (V) {
     std::vector<double> tmp(N);
@@ -1209,7 +1211,7 @@ extern "C" m2cg_status m2cg_batch_download(m2cg_batch* b, double* V, int* ID, do
       return bfail(M2CG_ERR_CUDA, "download failed");
     for (int t = 0; t < b->ntubes; t++) t_per_tube[t] = clk[2 * t];
   }
-  return M2CG_OK;
+  return st;
 }
 
 extern "C" m2cg_status m2cg_batch_get_tuning(const m2cg_batch* b, m2cg_batch_tuning* t) {

@@ -22,6 +22,7 @@
 #include "launch.h"
 #include "multiphase.h"
 #include "viscous.h"
+#include "walls.h"
 
 using namespace m2c;
 
@@ -87,6 +88,8 @@ extern "C" void m2cg_default_scheme(m2cg_scheme* s) {
   s->riem_warm_gate = 0.0;
   s->riem_warm_delta = 3.0e-4;  // measured: the narrowest bracket that keeps the evaluations low
   s->mp_riemann_normal = 1;  // MultiPhaseData::MESH (IoData.cpp:1408)
+  s->ebm_riemann_normal = 1; // EmbeddedBoundaryMethodData::MESH (IoData.cpp:2937-2938)
+  s->ebm_recon = 0;          // CONSTANT
 }
 
 extern "C" void m2cg_default_material(m2cg_material* m) {
@@ -168,6 +171,7 @@ struct m2cg_ctx {
   m2cg_counters counters = {};
   Multiphase* mp = nullptr;  // two-material machinery (nullptr for one material)
   Viscous* visc = nullptr;   // viscous fluxes (nullptr when every material is inviscid)
+  Walls* walls = nullptr;    // faces cut by embedded surfaces (nullptr: none)
   // probes (ProbeOutput): per probe the lower node (i, j, k), the trilinear
   // coordinates and the valid-corner mask; records sampled on the device
   int nprobe = 0, probe_every = 0, probe_cap = 0, probe_count = 0;
@@ -311,6 +315,8 @@ static MatParams to_params(const m2cg_material& m) {
   p.failsafe_density = m.failsafe_density;
   return p;
 }
+
+static void set_stage_items(m2cg_ctx* c, bool multi);
 
 extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* scheme, const m2cg_material* mats,
                                    int nmat, const m2cg_levelset* ls, int nls, m2cg_ctx** out) {
@@ -460,13 +466,7 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
                      : (nls == 1 ? StageTY<double, true>::value : StageTY<double, false>::value);
   c->ntx = (c->nx + TX - 1) / TX;
   c->nty = (c->ny + ty - 1) / ty;
-  {
-    const int resident = scheme->precision == M2CG_PREC_MIXED ? stage_resident_mixed(scheme->flux, nls == 1)
-                                                              : stage_resident_fp64(scheme->flux, nls == 1);
-    const long long units = (long long)c->ntx * c->nty * c->nz;
-    const long long by_len = (units + 7) / 8;
-    c->nitems = (int)std::max<long long>(1, std::min<long long>(resident, by_len));
-  }
+  set_stage_items(c, nls == 1);
   CK(cudaStreamSynchronize(c->stream));
   *out = c;
   return M2CG_OK;
@@ -484,6 +484,7 @@ extern "C" m2cg_status m2cg_destroy(m2cg_ctx* c) {
   cudaFree(c->stage_buf);
   cudaFree(c->probe_ijk); cudaFree(c->probe_xi); cudaFree(c->probe_rec);
   if (c->mp) multiphase_destroy(c->mp);
+  if (c->walls) walls_destroy(c->walls);
   if (c->visc) viscous_destroy(c->visc);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -799,6 +800,44 @@ static void rk_coeffs(int r, int s, double& a_prev, double& a_un, double& b) {
   a_prev = 2.0 / 3.0; a_un = 1.0 / 3.0; b = 2.0 / 3.0;
 }
 
+// Persistent grid size of the stage kernel variant (two-material or not).
+static void set_stage_items(m2cg_ctx* c, bool multi) {
+  const int resident = c->scheme.precision == M2CG_PREC_MIXED ? stage_resident_mixed(c->scheme.flux, multi)
+                                                               : stage_resident_fp64(c->scheme.flux, multi);
+  const long long units = (long long)c->ntx * c->nty * c->nz;
+  const long long by_len = (units + 7) / 8;
+  c->nitems = (int)std::max<long long>(1, std::min<long long>(resident, by_len));
+}
+
+extern "C" m2cg_status m2cg_set_wall_faces(m2cg_ctx* c, int n, const int* faces, const double* nwall_fwd,
+                                           const double* uwall_fwd, const double* nwall_bwd,
+                                           const double* uwall_bwd) {
+  if (!c || n < 0) return fail(M2CG_ERR_ARG, "bad argument");
+  CK(cudaStreamSynchronize(c->stream));
+  if (n == 0) {
+    walls_destroy(c->walls);
+    c->walls = nullptr;
+    set_stage_items(c, c->mp != nullptr);
+    return M2CG_OK;
+  }
+  if (c->visc)
+    return fail(M2CG_ERR_UNSUPPORTED,
+                "cut faces with viscous or heat-diffusive materials (the diffusion operators' wall branches) are not implemented");
+  const size_t smem = c->scheme.precision == M2CG_PREC_MIXED ? stage_smem_mixed(true) : stage_smem_fp64(true);
+  int maxsm = 0;
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  if ((size_t)maxsm < smem) return fail(M2CG_ERR_CUDA, "stage kernel needs %zu B shared memory, device has %d", smem, maxsm);
+  Walls* w = nullptr;
+  char msg[200] = {0};
+  const m2cg_status st = walls_create(c->stream, c->g, c->nalloc, c->scheme, n, faces, nwall_fwd, uwall_fwd, nwall_bwd,
+                                      uwall_bwd, &w, msg, sizeof msg);
+  if (st) return fail(st, "cut faces refused: %s", msg);
+  walls_destroy(c->walls);
+  c->walls = w;
+  set_stage_items(c, true);
+  return M2CG_OK;
+}
+
 static m2cg_status launch_stage(m2cg_ctx* c, StageArgs& a) {
   a.ntx = c->ntx;
   a.nty = c->nty;
@@ -810,8 +849,10 @@ static m2cg_status launch_stage(m2cg_ctx* c, StageArgs& a) {
     cudaEventCreate(&e1);
     cudaEventRecord(e0, c->stream);
   }
-  cudaError_t e = c->scheme.precision == M2CG_PREC_MIXED ? launch_stage_mixed(a, c->stream, c->mp != nullptr, &grid)
-                                                          : launch_stage_fp64(a, c->stream, c->mp != nullptr, &grid);
+  // the two-material kernel variant also carries the branch of cut faces
+  const bool multi = c->mp != nullptr || c->walls != nullptr;
+  cudaError_t e = c->scheme.precision == M2CG_PREC_MIXED ? launch_stage_mixed(a, c->stream, multi, &grid)
+                                                          : launch_stage_fp64(a, c->stream, multi, &grid);
   if (c->profile) {
     cudaEventRecord(e1, c->stream);
     c->ev.push_back(e0);
@@ -878,6 +919,7 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
       m2cg_status sv = viscous_faces(c->visc, c->stream, a, mixed);
       if (sv) return fail(sv, "viscous-flux launch failed");
     }
+    if (c->walls && walls_stage(c->walls, c->stream, a)) return fail(M2CG_ERR_CUDA, "cut-face pre-pass launch failed");
     m2cg_status st = launch_stage(c, a);
     if (st) return st;
   }
@@ -990,6 +1032,7 @@ extern "C" m2cg_status m2cg_compute_residual(m2cg_ctx* c, double* R_host) {
     m2cg_status sv = viscous_faces(c->visc, c->stream, a, c->scheme.precision == M2CG_PREC_MIXED);
     if (sv) return fail(sv, "viscous-flux launch failed");
   }
+  if (c->walls && walls_stage(c->walls, c->stream, a)) return fail(M2CG_ERR_CUDA, "cut-face pre-pass launch failed");
   m2cg_status st = launch_stage(c, a);
   if (st) return st;
   // pack R (interior) into the ghosted AoS layout
@@ -1012,6 +1055,12 @@ extern "C" m2cg_status m2cg_get_counters(const m2cg_ctx* c, m2cg_counters* out) 
   if (!c || !out) return fail(M2CG_ERR_ARG, "null argument");
   *out = c->counters;
   if (c->mp) multiphase_counters(c->mp, out);
+  if (c->walls) {
+    long long solves = 0, failures = 0;
+    walls_counters(c->walls, c->stream, &solves, &failures);
+    out->wall_riemann_calls += solves;
+    out->riemann_errors += failures;
+  }
   return M2CG_OK;
 }
 

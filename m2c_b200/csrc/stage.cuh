@@ -127,6 +127,16 @@ struct ViscView {
   long long nf[3];
 };
 
+// Faces cut by an embedded surface (walls) and the one-sided Riemann star
+// states of their two sides for this stage, from the wall pre-pass
+// (SpaceOperator.cpp:2438-2484 and the y/z analogues). mask == NULL: no walls.
+struct WallView {
+  const uint8_t* mask;  // per cell: bit d set where the low face along axis d is a wall
+  const int* slot;      // per cell; valid only where mask != 0
+  const double* Vsm;    // [slot][3 faces][5]: the low neighbour's star state (its flux against it)
+  const double* Vsp;    // [slot][3 faces][5]: this cell's star state
+};
+
 struct StageArgs {
   Grid3 g;
   SchemeK s;
@@ -152,6 +162,7 @@ struct StageArgs {
   double* Ro[5];         // if set: write the residual R only (no RK update)
   IfaceView iface;
   ViscView visc;
+  WallView wall;
   int use_tma;           // planes by tensor copy (x and y not periodic, maps built)
   CUtensorMap tin;       // 4D map of the stage input (Pin as one five-component buffer)
 };
@@ -791,12 +802,23 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       }
       return;
     }
-    if (MULTI && idL != idR) {
+    // a face cut by an embedded surface (interior faces only) takes the wall
+    // branch, which the reference tests before the material-interface one
+    bool wall = false;
+    long long offW = 0;
+    if (MULTI && a.wall.mask && rL && rR) {
+      const int gi = wrap_index(i0 + mxR - 1, g.nx), gj = wrap_index(j0 + myR - 1, g.ny);
+      offW = (long long)wrap_index(pR, g.nz) * g.plane + (long long)gj * g.px + gi;
+      wall = (a.wall.mask[offW] >> d) & 1;
+    }
+    if (MULTI && (wall || idL != idR)) {
       // Material interface (SpaceOperator.cpp:2486-2542): two one-sided fluxes
       // against the exact Riemann star states, or LLF across the interface.
+      // Wall (2438-2484, CONSTANT reconstruction at the wall): the left
+      // cell's flux against its one-sided star state.
       const IfaceView& iv = a.iface;
       T WL[5], WR[5];
-      if (iv.mp_recon == 0) {  // constant reconstruction: cell-centred states
+      if (wall || iv.mp_recon == 0) {  // constant reconstruction: cell-centred states
 #pragma unroll
         for (int c = 0; c < 5; c++) {
           WL[c] = M2C_VV(sL, c, myL + 1, mxL + 1);
@@ -806,7 +828,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
 #pragma unroll
         for (int c = 0; c < 5; c++) { WL[c] = VL[c]; WR[c] = VR[c]; }
       }
-      if (iv.mp_flux == 2) {
+      if (!wall && iv.mp_flux == 2) {
         err = flux_llf2(eos_of<T, MULTI>(a.s, idL), eos_of<T, MULTI>(a.s, idR), d, WL, WR, F);
 #pragma unroll
         for (int c = 0; c < 5; c++) F2[c] = F[c];
@@ -814,9 +836,9 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
         // the right cell's index carries the slot of its low faces
         const int gi = wrap_index(i0 + mxR - 1, g.nx), gj = wrap_index(j0 + myR - 1, g.ny);
         const int gk = wrap_index(pR, g.nz);
-        const int slot = iv.slot[(long long)gk * g.plane + (long long)gj * g.px + gi];
+        const int slot = wall ? a.wall.slot[offW] : iv.slot[(long long)gk * g.plane + (long long)gj * g.px + gi];
         const long long base = ((long long)slot * 3 + d) * 5;
-        if (iv.mp_flux == 0) {  // Godunov flux of the state at xi = 0
+        if (!wall && iv.mp_flux == 0) {  // Godunov flux of the state at xi = 0
           T Vm[5];
 #pragma unroll
           for (int c = 0; c < 5; c++) Vm[c] = T(iv.Vmid[base + c]);
@@ -824,14 +846,12 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
 #pragma unroll
           for (int c = 0; c < 5; c++) F2[c] = F[c];
         } else {
-          T Sm[5], Sp[5];
+          const double* src = wall ? a.wall.Vsm : iv.Vsm;
+          T Sm[5];
 #pragma unroll
-          for (int c = 0; c < 5; c++) {
-            Sm[c] = T(iv.Vsm[base + c]);
-            Sp[c] = T(iv.Vsp[base + c]);
-          }
+          for (int c = 0; c < 5; c++) Sm[c] = T(src[base + c]);
+          // the right cell's flux against its own star state is formed in its update
           err = flux_of<T, FLUX>(eos_of<T, MULTI>(a.s, idL), d, WL, Sm, delta, F);
-          (void)Sp;  // the right cell's flux against Sp is formed in its update
         }
       }
     } else {
@@ -999,32 +1019,40 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       // Low faces that are material interfaces under the NUMERICAL interface
       // flux: this cell's flux is its EOS's numerical flux between the right
       // star state and its own cell-centred state (SpaceOperator.cpp:2499-2542).
+      // Low faces cut by an embedded surface likewise take this cell's flux
+      // against its one-sided star state (SpaceOperator.cpp:2462-2478).
       T F2[3][5];
       bool ifc[3] = {false, false, false};
       if constexpr (MULTI) {
-        if (a.iface.mp_flux == 1) {
+        const uint8_t wm = a.wall.mask ? a.wall.mask[off] : 0;
+        const bool num = a.iface.mp_flux == 1 && a.iface.slot;  // interface slots exist
+        if (num || wm) {
           const int sc = slot4(m), lx = tx + 2, ly = ty + 2;
           const uint8_t me = sm.ids[sc][ly][lx];
-          ifc[0] = me != sm.ids[sc][ly][lx - 1];
-          ifc[1] = me != sm.ids[sc][ly - 1][lx];
-          ifc[2] = me != sm.ids[slot4(m - 1)][ly][lx];
+          ifc[0] = (wm & 1) || (num && me != sm.ids[sc][ly][lx - 1]);
+          ifc[1] = (wm & 2) || (num && me != sm.ids[sc][ly - 1][lx]);
+          ifc[2] = (wm & 4) || (num && me != sm.ids[slot4(m - 1)][ly][lx]);
           if (ifc[0] || ifc[1] || ifc[2]) {
-            const int slot = a.iface.slot[off];
+            const int islot = num ? a.iface.slot[off] : 0;
+            const int wslot = wm ? a.wall.slot[off] : 0;
             for (int d = 0; d < 3; d++) {
               if (!ifc[d]) continue;
+              const bool w = (wm >> d) & 1;
               // this cell's side of the face: its cell-centred state, or its
-              // reconstructed state on that face (vl) under LINEAR
+              // reconstructed state on that face (vl) under LINEAR interface
+              // reconstruction
               T W[5];
-              if (a.iface.mp_recon) {
+              if (!w && a.iface.mp_recon) {
                 cell_face(m, tx + 1, ty + 1, d, 0, W);
               } else {
 #pragma unroll
                 for (int c = 0; c < 5; c++) W[c] = M2C_VV(sc, c, ly, lx);
               }
-              const long long base = ((long long)slot * 3 + d) * 5;
+              const long long base = ((long long)(w ? wslot : islot) * 3 + d) * 5;
+              const double* src = w ? a.wall.Vsp : a.iface.Vsp;
               T Sp[5];
 #pragma unroll
-              for (int c = 0; c < 5; c++) Sp[c] = T(a.iface.Vsp[base + c]);
+              for (int c = 0; c < 5; c++) Sp[c] = T(src[base + c]);
               const int err2 = flux_of<T, FLUX>(eos_of<T, MULTI>(a.s, me), d, Sp, W, delta, F2[d]);
               if (err2) report(a.err, err2, -1, where + 2);
             }

@@ -30,7 +30,7 @@ class Counters(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in (
         "steps", "cells_updated", "riemann_calls", "riemann_iterations", "riemann_errors",
         "clipped_cells", "reinit_calls", "kernel_launches", "unresolved_cells", "riemann_evaluations",
-        "failsafe_cells", "riemann_nontrivial")]
+        "failsafe_cells", "riemann_nontrivial", "wall_riemann_calls")]
 
 
 class BatchTuning(C.Structure):
@@ -69,6 +69,7 @@ def lib():
     L.m2cg_riemann_wall_batch.argtypes = [C.POINTER(abi.Scheme), C.POINTER(abi.Material), C.c_int, C.c_int, dp, ip,
                                           dp, dp, dp, ip, dp, ip, ip]
     L.m2cg_riemann_wall_batch.restype = C.c_int
+    L.m2cg_set_wall_faces.argtypes = [vp, C.c_int, ip, dp, dp, dp, dp]
     L.m2cg_batch_create.argtypes = [C.POINTER(abi.Scheme), C.c_int, ip, C.POINTER(abi.Material), dp, dp,
                                     C.POINTER(BatchTuning), C.POINTER(vp)]
     L.m2cg_batch_run.argtypes = [vp, C.c_int]
@@ -283,6 +284,24 @@ class Solver:
         check(lib().m2cg_read_probes(self.h, abi.dptr(out), C.byref(cnt)))
         return out[:cnt.value]
 
+    def set_wall_faces(self, faces, nwall_fwd=None, uwall_fwd=None, nwall_bwd=None, uwall_bwd=None):
+        """Faces cut by an embedded surface for the following stages
+        (m2cg_set_wall_faces): faces [n][4] = (axis, i, j, k), the face
+        between cell (i, j, k) and its low neighbour; the surface's unit
+        normal and velocity seen from the low cell (fwd) and from the high
+        cell (bwd), [n][3] each (velocities default to zero, normals to the
+        face normal). An empty list removes the walls."""
+        faces = np.ascontiguousarray(np.asarray(faces, np.int32).reshape(-1, 4))
+        n = len(faces)
+        def arr(a, default):
+            return np.ascontiguousarray(default if a is None else np.asarray(a, np.float64).reshape(n, 3))
+        en = np.zeros((n, 3))
+        en[np.arange(n), faces[:, 0]] = 1.0
+        nf, uf = arr(nwall_fwd, en), arr(uwall_fwd, np.zeros((n, 3)))
+        nb, ub = arr(nwall_bwd, en), arr(uwall_bwd, np.zeros((n, 3)))
+        check(lib().m2cg_set_wall_faces(self.h, n, abi.iptr(faces), abi.dptr(nf), abi.dptr(uf), abi.dptr(nb),
+                                        abi.dptr(ub)))
+
     def set_mlp(self, mlp):
         """Start every interface Riemann solve of the steps from the
         network's proposal (None detaches; two materials only)."""
@@ -340,12 +359,16 @@ class Batch:
             check(st)
         return ms.value
 
-    def download(self):
-        """Returns (list of per-tube V arrays [len, 5], list of ID arrays, t per tube)."""
+    def download(self, check_errors=True):
+        """Returns (list of per-tube V arrays [len, 5], list of ID arrays, t per
+        tube). With check_errors=False a tube error does not raise (the
+        failed tubes' states are not defined; tube_errors() tells which)."""
         V = np.empty((self.ncell, 5))
         ID = np.empty(self.ncell, np.int32)
         t = np.empty(self.ntubes)
-        check(lib().m2cg_batch_download(self.h, abi.dptr(V), abi.iptr(ID), abi.dptr(t)))
+        st = lib().m2cg_batch_download(self.h, abi.dptr(V), abi.iptr(ID), abi.dptr(t))
+        if st and (check_errors or st == 2):  # 2: CUDA error (nothing copied)
+            check(st)
         cuts = np.cumsum(self.lens)[:-1]
         return np.split(V, cuts), np.split(ID, cuts), t
 

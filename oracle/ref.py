@@ -50,6 +50,7 @@ def _load(path, prefix):
     f("compute_dt").restype = C.c_double
     f("compute_dt").argtypes = [vp]
     f("compute_residual").argtypes = [vp, dp]
+    f("compute_residual_walls").argtypes = [vp, C.c_int, ip, dp, dp, dp, dp, dp]
     f("advance").argtypes = [vp, C.c_double]
     f("run").restype = C.c_int
     f("run").argtypes = [vp, C.c_int, C.c_double, dp]
@@ -112,6 +113,17 @@ class _Case:
     def residual(self):
         R = np.zeros(abi.ghosted_shape(self.g, 5))
         self._f("compute_residual")(self.h, abi.dptr(R))
+        return R
+
+    def residual_walls(self, faces, nwall_fwd, uwall_fwd, nwall_bwd, uwall_bwd):
+        """SpaceOperator::ComputeResidual with an embedded surface cutting the
+        listed faces (the arguments of Solver.set_wall_faces, all given)."""
+        faces = np.ascontiguousarray(np.asarray(faces, np.int32).reshape(-1, 4))
+        arrs = [np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1, 3))
+                for a in (nwall_fwd, uwall_fwd, nwall_bwd, uwall_bwd)]
+        R = np.zeros(abi.ghosted_shape(self.g, 5))
+        self._f("compute_residual_walls")(self.h, len(faces), abi.iptr(faces), *[abi.dptr(a) for a in arrs],
+                                          abi.dptr(R))
         return R
 
     def advance(self, dt):

@@ -31,6 +31,8 @@
 #include <Utils.h>
 #include <Interpolator.h>
 #include <GradientCalculatorCentral.h>
+#include <EmbeddedBoundaryDataSet.h>
+#include <TriangulatedSurface.h>
 
 #include <chrono>
 #include <cmath>
@@ -127,6 +129,8 @@ void fill_scheme(IoData& iod, const m2cg_scheme& s) {
   iod.multiphase.phasechange_dir = (MultiPhaseData::PhaseChangeDirection)s.mp_phasechange_dir;
   iod.multiphase.apply_failsafe_density = (MultiPhaseData::OnOff)s.mp_apply_failsafe_density;
   iod.multiphase.riemann_normal = (MultiPhaseData::RiemannNormal)s.mp_riemann_normal;
+  iod.ebm.riemann_normal = (EmbeddedBoundaryMethodData::RiemannNormal)s.ebm_riemann_normal;
+  iod.ebm.recon = (EmbeddedBoundaryMethodData::ReconstructionAtInterface)s.ebm_recon;
   ExactRiemannSolverData& r = iod.exact_riemann;
   r.maxIts_main = s.riem_maxits_main;
   r.maxIts_bracket = s.riem_maxits_bracket;
@@ -350,6 +354,60 @@ double m2cref_compute_dt(void* h) {
   double dt = 0.0, cfl = 0.0;
   c->spo->ComputeTimeStepSize(*c->V, *c->ID, dt, cfl);
   return dt;
+}
+
+// R for the current state with faces cut by an embedded surface: one
+// EmbeddedBoundaryDataSet whose intersector results are written directly, so
+// that SpaceOperator::FindEdgeSurfaceIntersections (SpaceOperator.cpp:
+// 3435-3501) yields the given normal and velocity on each listed face. Face q
+// = (axis d, i, j, k) gets two triangles, 2q (forward: normal nf, node
+// velocity uf) and 2q+1 (backward), each met at barycentric coordinates
+// (1, 0, 0), so the interpolated surface velocity is the given one exactly;
+// XForward / XBackward of node (i, j, k), component d, hold 2q and 2q+1.
+void m2cref_compute_residual_walls(void* h, int n, const int* faces, const double* nf, const double* uf,
+                                   const double* nb, const double* ub, double* R) {
+  RefCase* c = (RefCase*)h;
+  TriangulatedSurface surf;
+  std::vector<IntersectionPoint> xs;
+  SpaceVariable3D xf(c->comm, &(c->dms->ghosted1_3dof)), xb(c->comm, &(c->dms->ghosted1_3dof));
+  xf.SetConstantValue(-1.0, true);
+  xb.SetConstantValue(-1.0, true);
+  Vec3D*** f = (Vec3D***)xf.GetDataPointer();
+  Vec3D*** b = (Vec3D***)xb.GetDataPointer();
+  double xi[3] = {1.0, 0.0, 0.0};
+  for (int q = 0; q < n; q++) {
+    const int d = faces[4 * q], i = faces[4 * q + 1], j = faces[4 * q + 2], k = faces[4 * q + 3];
+    for (int side = 0; side < 2; side++) {
+      const double* nw = side == 0 ? nf + 3 * q : nb + 3 * q;
+      const double* uw = side == 0 ? uf + 3 * q : ub + 3 * q;
+      const int base = (int)surf.Udot.size();
+      surf.X.push_back(Vec3D(0.0, 0.0, 0.0));
+      surf.X.push_back(Vec3D(0.0, 0.0, 0.0));
+      surf.X.push_back(Vec3D(0.0, 0.0, 0.0));
+      surf.Udot.push_back(Vec3D(uw[0], uw[1], uw[2]));
+      surf.Udot.push_back(Vec3D(0.0, 0.0, 0.0));
+      surf.Udot.push_back(Vec3D(0.0, 0.0, 0.0));
+      surf.elems.push_back(Int3(base, base + 1, base + 2));
+      surf.elemNorm.push_back(Vec3D(nw[0], nw[1], nw[2]));
+      const int tid = 2 * q + side;
+      xs.push_back(IntersectionPoint(i, j, k, d, side == 0 ? 0.25 : 0.75, tid, xi));
+      (side == 0 ? f : b)[k][j][i][d] = (double)tid;
+    }
+  }
+  xf.RestoreDataPointerAndInsert();
+  xb.RestoreDataPointerAndInsert();
+  std::vector<std::unique_ptr<EmbeddedBoundaryDataSet>> ebds;
+  ebds.push_back(std::make_unique<EmbeddedBoundaryDataSet>());
+  ebds[0]->surface_ptr = &surf;
+  ebds[0]->XForward_ptr = &xf;
+  ebds[0]->XBackward_ptr = &xb;
+  ebds[0]->intersections_ptr = &xs;
+  SpaceVariable3D Rv(c->comm, &(c->dms->ghosted1_5dof));
+  c->spo->ComputeResidual(*c->V, *c->ID, Rv, nullptr, nullptr, nullptr, &ebds);
+  copy_out(Rv, R, 5, c->NX, c->NY, c->NZ);
+  Rv.Destroy();
+  xf.Destroy();
+  xb.Destroy();
 }
 
 // R for the current state (ghosted layout, 5 dof).

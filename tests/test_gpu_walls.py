@@ -1,0 +1,154 @@
+"""Faces cut by an embedded surface (walls) against the reference's
+embedded-boundary branch of SpaceOperator::ComputeAdvectionFluxes
+(SpaceOperator.cpp:2438-2484 and the y/z analogues): on each cut face the low
+cell's flux against its one-sided Riemann star state
+(ExactRiemannSolverBase::ComputeOneSidedRiemannSolution, the surface seen
+forward) and the high cell's against its own (seen backward).
+
+The reference side runs SpaceOperator::ComputeResidual with one
+EmbeddedBoundaryDataSet whose intersector results are written so that
+FindEdgeSurfaceIntersections yields the same normal and velocity on the same
+faces (oracle/ref_harness.cpp, m2cref_compute_residual_walls). Bar: the FP64
+residual within 1e-12 relative (max norm per variable); the mixed path
+tracks FP64 in L1.
+"""
+import numpy as np
+import pytest
+
+from m2c_b200 import abi, cases
+from tests.helpers import inner, l1_rel, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def wall_faces(g, n, seed, speed=0.4):
+    """n distinct interior faces of every axis (the low neighbour interior
+    too), unit normals near each face normal, velocities uniform in
+    +-speed per component."""
+    rng = np.random.default_rng(seed)
+    dims = (g.nx, g.ny, g.nz)
+    out = set()
+    while len(out) < n:
+        d = int(rng.integers(0, 3))
+        ijk = [int(rng.integers(0, m)) for m in dims]
+        ijk[d] = int(rng.integers(1, dims[d]))
+        out.add((d, *ijk))
+    faces = np.array(sorted(out), np.int32)
+    def normals():
+        v = rng.normal(scale=0.4, size=(n, 3))
+        v[np.arange(n), faces[:, 0]] += rng.choice([-1.0, 1.0], n)
+        return v / np.linalg.norm(v, axis=1)[:, None]
+    nf, nb = normals(), normals()
+    uf = rng.uniform(-speed, speed, (n, 3))
+    ub = rng.uniform(-speed, speed, (n, 3))
+    return faces, nf, uf, nb, ub
+
+
+@pytest.mark.parametrize("normal", [abi.EBM_NORMAL_MESH, abi.EBM_NORMAL_SURFACE, abi.EBM_NORMAL_AVERAGE])
+@pytest.mark.parametrize("flux", [abi.FLUX_HLLC, abi.FLUX_ROE])
+def test_wall_residual_matches_reference(gpu, ref, normal, flux):
+    g, s, mats, V = cases.random_box(14, 11, 9, seed=5, flux=flux)
+    s.ebm_riemann_normal = normal
+    W = wall_faces(g, 120, seed=normal)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    sol.set_wall_faces(*W)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V)
+    Rg, Rr = inner(sol.residual()), inner(rc.residual_walls(*W))
+    assert rel_err(Rg, Rr) <= TOL
+    # the walls matter: the residual without them differs
+    assert rel_err(inner(rc.residual()), Rr) > 1e-6
+    # each residual evaluation solves two one-sided problems per cut face
+    c = sol.counters()
+    assert c["wall_riemann_calls"] == 2 * len(W[0])
+    # removing the walls restores the plain residual
+    sol.set_wall_faces(np.zeros((0, 4), np.int32))
+    assert rel_err(inner(sol.residual()), inner(rc.residual())) <= TOL
+    sol.close()
+
+
+def test_wall_residual_of_receding_and_fast_walls_matches_reference(gpu, ref):
+    """Walls moving away faster than the fluid can follow (the one-sided
+    rarefaction reports failure and the reference keeps the input state
+    with the wall's normal velocity) and walls driven into the fluid
+    (strong shocks)."""
+    g, s, mats, V = cases.random_box(12, 10, 8, seed=9)
+    W = wall_faces(g, 90, seed=4, speed=12.0)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    sol.set_wall_faces(*W)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V)
+    assert rel_err(inner(sol.residual()), inner(rc.residual_walls(*W))) <= TOL
+    assert sol.counters()["riemann_errors"] > 0
+    sol.close()
+
+
+def test_wall_residual_two_materials_matches_reference(gpu, ref):
+    """A surface through the bubble case: cut faces between two cells of the
+    same material and across the material interface (the wall branch is
+    taken there, as in the reference), water and air."""
+    if not ref.available("crpow"):
+        pytest.skip("reference oracle with correctly rounded pow not built (make -C oracle refcr)")
+    g, s, mats, ls, V, ID, PHI = cases.bubble_case(16, reinit_frequency=-1, radius=4.0e-3)
+    V[1:-1, 1:-1, 1:-1, 1:4] += np.array([20.0, -10.0, 5.0])
+    faces = [(0, 8, j, k) for j in range(3, 13) for k in range(3, 13)]
+    faces += [(1, i, 8, k) for i in range(5, 11) for k in range(5, 11)]
+    faces = np.array(faces, np.int32)
+    n = len(faces)
+    rng = np.random.default_rng(3)
+    en = np.zeros((n, 3))
+    en[np.arange(n), faces[:, 0]] = 1.0
+    uf = rng.uniform(-30.0, 30.0, (n, 3))
+    W = (faces, en, uf, en, uf)
+    sol = gpu.Solver(g, s, mats, ls)
+    sol.upload(V, ID, PHI)
+    sol.set_wall_faces(*W)
+    rc = ref.RefCaseCR(g, s, mats, ls)
+    rc.set_state(V, ID, PHI)
+    idg = inner(ID)
+    lo = np.array([idg[k, j, i - 1] if d == 0 else idg[k, j - 1, i] for d, i, j, k in faces])
+    hi = np.array([idg[k, j, i] for d, i, j, k in faces])
+    assert (lo != hi).sum() > 0 and (lo == hi).sum() > 0
+    assert rel_err(inner(sol.residual()), inner(rc.residual_walls(*W))) <= TOL
+    sol.close()
+
+
+def test_wall_steps_mixed_track_fp64(gpu):
+    out = []
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        g, s, mats, V = cases.random_box(14, 11, 9, seed=5, precision=prec)
+        W = wall_faces(g, 120, seed=1)
+        sol = gpu.Solver(g, s, mats)
+        sol.upload(V)
+        sol.set_wall_faces(*W)
+        sol.run(8)
+        out.append(inner(sol.download()[0]))
+        assert sol.counters()["wall_riemann_calls"] == 8 * 3 * 2 * len(W[0])
+        sol.close()
+    assert l1_rel(out[1], out[0]) <= 1e-5
+
+
+def test_wall_faces_refused(gpu):
+    g, s, mats, V = cases.random_box(10, 8, 6, seed=5)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    with pytest.raises(gpu.M2CError, match="inside the subdomain"):
+        sol.set_wall_faces([(0, 0, 3, 3)])  # the face on the x0 boundary
+    with pytest.raises(gpu.M2CError, match="twice"):
+        sol.set_wall_faces([(1, 2, 3, 3), (1, 2, 3, 3)])
+    with pytest.raises(gpu.M2CError, match="outside"):
+        sol.set_wall_faces([(2, 2, 3, 6)])
+    sol.close()
+    s.ebm_recon = 1
+    sol = gpu.Solver(g, s, mats)
+    with pytest.raises(gpu.M2CError, match="CONSTANT"):
+        sol.set_wall_faces([(0, 3, 3, 3)])
+    sol.close()
+    visc = gpu.Solver(g, abi.scheme(), [abi.material(1.4, 0.0, mu=1e-3)])
+    with pytest.raises(gpu.M2CError, match="viscous"):
+        visc.set_wall_faces([(0, 3, 3, 3)])
+    visc.close()
