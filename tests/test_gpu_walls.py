@@ -95,7 +95,7 @@ def test_wall_residual_two_materials_matches_reference(gpu, ref):
         pytest.skip("reference oracle with correctly rounded pow not built (make -C oracle refcr)")
     g, s, mats, ls, V, ID, PHI = cases.bubble_case(16, reinit_frequency=-1, radius=4.0e-3)
     V[1:-1, 1:-1, 1:-1, 1:4] += np.array([20.0, -10.0, 5.0])
-    faces = [(0, 8, j, k) for j in range(3, 13) for k in range(3, 13)]
+    faces = [(0, 10, j, k) for j in range(3, 13) for k in range(3, 13)]
     faces += [(1, i, 8, k) for i in range(5, 11) for k in range(5, 11)]
     faces = np.array(faces, np.int32)
     n = len(faces)
