@@ -419,6 +419,42 @@ def extra_box(n=256, steps=20, warmup=3, cpu=True):
     return out
 
 
+def extra_walls(n=192, steps=20, warmup=3):
+    """A flat surface across the periodic box (ideal gas, Roe + generalized
+    minmod, RK3): every x face of the plane i = n/2 cut, the surface at rest
+    (m2cg_set_wall_faces; per stage two one-sided exact Riemann problems per
+    cut face, then the wall branch of the face fluxes). Time per step with
+    and without the surface, mixed and FP64."""
+    import numpy as np
+    from m2c_b200 import abi, cases, gpu
+    jj, kk = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    faces = np.stack([np.zeros(n * n, np.int32), np.full(n * n, n // 2, np.int32), jj.ravel().astype(np.int32),
+                      kk.ravel().astype(np.int32)], axis=1)
+    out = {"workload": f"periodic box {n}^3 cut by a resting plane (x faces at i = {n // 2}, {n * n} cut faces), "
+                       f"Roe + generalized minmod, RK3"}
+    for prec, name in ((abi.PREC_MIXED, "mixed"), (abi.PREC_FP64, "fp64")):
+        g, s, mats, V = cases.fourier_box(n, precision=prec, seed=2024)
+        r = {}
+        for walls in (False, True):
+            sol = gpu.Solver(g, s, mats)
+            sol.upload(V)
+            if walls:
+                sol.set_wall_faces(faces)
+            sol.time_steps(warmup)
+            c0 = sol.counters()
+            ms, _ = sol.time_steps(steps)
+            c1 = sol.counters()
+            sol.close()
+            key = "with_plane" if walls else "without"
+            r[key] = {"ms_per_step": ms / steps, "cell_updates_per_s": n ** 3 * steps / (ms / 1e3)}
+            if walls:
+                r[key]["wall_riemann_calls_per_step"] = (c1["wall_riemann_calls"] - c0["wall_riemann_calls"]) / steps
+                r[key]["wall_riemann_errors"] = c1["riemann_errors"] - c0["riemann_errors"]
+        r["plane_cost_ms_per_step"] = r["with_plane"]["ms_per_step"] - r["without"]["ms_per_step"]
+        out[name] = r
+    return out
+
+
 def extra_bubble(n=192, nbubbles=1, steps=500, warmup=3):
     """Single bubble (192^3, 500 steps), mixed vs FP64: cell-updates/s, HBM
     fraction of the algorithmic bytes, and the mixed path's error against the
@@ -700,6 +736,7 @@ def main():
         for name, fn in (("periodic_box_256", lambda: extra_box(cpu=not args.no_cpu_baseline)),
                          ("single_bubble_192", lambda: extra_bubble()),
                          ("batched_tubes", lambda: extra_tubes(mlp=net)),
+                         ("embedded_plane_192", lambda: extra_walls()),
                          ("learned_warm_start", lambda: extra_warm_start(net) if net is not None else
                           {"unavailable": "m2c_b200/data/warmstart_mlp.npz not present"}),
                          ("learned_warm_start_cluster", lambda: extra_cluster_warm_start(net) if net is not None else

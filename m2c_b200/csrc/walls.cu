@@ -24,6 +24,8 @@ struct Walls {
   double* Vsm = nullptr;    // [slot][3][5]
   double* Vsp = nullptr;
   unsigned long long* cnt = nullptr;  // [0] solves, [1] failed solves
+  int* work = nullptr;                // one-sided problems: (slot * 3 + d) * 2 + side
+  int nwork = 0;
   double* scratch = nullptr;          // per thread: one integration path
   int threads = 0;
 };
@@ -39,8 +41,9 @@ struct WallPassArgs {
   double* Vsm;
   double* Vsp;
   unsigned long long* cnt;
+  const int* work;
   double* scratch;
-  int nslot;
+  int nwork;
   int normal_mode;
 };
 
@@ -77,7 +80,11 @@ __device__ __forceinline__ void wall_direction(int mode, int d, int fb, const do
   }
 }
 
-__global__ void k_wall_riemann(WallPassArgs a) {
+// One thread per one-sided problem (a side of a cut face): the two sides of
+// a face are independent solves, so splitting them doubles the resident
+// warps that hide the FP64 latency of the rarefaction integration (4 CTAs
+// per SM at 128 registers: more resident warps beat the few spills).
+__global__ void __launch_bounds__(128, 4) k_wall_riemann(WallPassArgs a) {
   const Grid3& g = a.st.g;
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   RiemannSolver rs;
@@ -88,38 +95,31 @@ __global__ void k_wall_riemann(WallPassArgs a) {
   rs.path3.pt = nullptr;
   rs.path3.cap = 0;
   unsigned long long solves = 0, failed = 0;
-  for (long long w = tid; w < 3LL * a.nslot; w += (long long)gridDim.x * blockDim.x) {
-    const int sl = (int)(w / 3), d = (int)(w - 3LL * sl);
+  for (long long w = tid; w < a.nwork; w += (long long)gridDim.x * blockDim.x) {
+    const int item = a.work[w];
+    const int side = item & 1, sl = (item >> 1) / 3, d = (item >> 1) - 3 * sl;
     const int i = a.cell[3 * sl], j = a.cell[3 * sl + 1], k = a.cell[3 * sl + 2];
     const long long offR = (long long)k * g.plane + (long long)j * g.px + i;
-    if (!((a.mask[offR] >> d) & 1)) continue;
-    const long long offL = offR - (d == 0 ? 1LL : (d == 1 ? g.px : g.plane));
-    const uint8_t idL = a.st.id[offL], idR = a.st.id[offR];
-    double VL[5], VR[5];
-    wall_stage_state(a.st, offL, idL, VL);
-    wall_stage_state(a.st, offR, idR, VR);
-    const double* gm = a.geo + (3LL * sl + d) * 12;
-    double dir[3], Vs[5], Vsm[5], Vsp[5];
+    // side 0: the low cell against the surface seen forward; side 1: the high
+    // cell against it seen backward (SpaceOperator.cpp:2440-2479)
+    const long long off = side ? offR : offR - (d == 0 ? 1LL : (d == 1 ? g.px : g.plane));
+    const uint8_t id = a.st.id[off];
+    double V[5];
+    wall_stage_state(a.st, off, id, V);
+    const double* gm = a.geo + (3LL * sl + d) * 12 + 6 * side;
+    double dir[3], Vs[5], Vst[5];
     int mid = 0;
-    bool bad1 = false, bad2 = false;
-    // the low cell against the surface seen forward, then the high cell
-    // against it seen backward (SpaceOperator.cpp:2440-2479)
-    wall_direction(a.normal_mode, d, 1, gm, dir);
-    const int r1 = rs.solve_wall(dir, VL, idL, gm + 3, Vs, mid, Vsm, bad1);
-    a.st.s.ed[idL].clip(Vsm);
-    wall_direction(a.normal_mode, d, -1, gm + 6, dir);
-    const int r2 = rs.solve_wall(dir, VR, idR, gm + 9, Vs, mid, Vsp, bad2);
-    a.st.s.ed[idR].clip(Vsp);
-    const long long b = (3LL * sl + d) * 5;
-    for (int c = 0; c < 5; c++) {
-      a.Vsm[b + c] = Vsm[c];
-      a.Vsp[b + c] = Vsp[c];
-    }
-    solves += 2;
-    failed += (r1 & RIEM_FAILED ? 1 : 0) + (r2 & RIEM_FAILED ? 1 : 0);
+    bool bad = false;
+    wall_direction(a.normal_mode, d, side ? -1 : 1, gm, dir);
+    const int r = rs.solve_wall(dir, V, id, gm + 3, Vs, mid, Vst, bad);
+    a.st.s.ed[id < a.st.s.nmat ? id : 0].clip(Vst);
+    double* out = (side ? a.Vsp : a.Vsm) + (3LL * sl + d) * 5;
+    for (int c = 0; c < 5; c++) out[c] = Vst[c];
+    solves += 1;
+    failed += (r & RIEM_FAILED) ? 1 : 0;
     const int cellR = (int)(((long long)k * g.ny + j) * g.nx + i);
-    if ((r1 | r2) & RIEM_PATH_OVERFLOW) report(a.st.err, ERR_ITER_CAP, cellR, 9);
-    if (bad1 || bad2) report(a.st.err, ERR_STATE, cellR, 10);
+    if (r & RIEM_PATH_OVERFLOW) report(a.st.err, ERR_ITER_CAP, cellR, 9);
+    if (bad) report(a.st.err, ERR_STATE, cellR, 10);
   }
   if (solves) atomicAdd(&a.cnt[0], solves);
   if (failed) atomicAdd(&a.cnt[1], failed);
@@ -184,9 +184,18 @@ m2cg_status walls_create(cudaStream_t s, const Grid3& g, size_t nalloc, const m2
   w->nslot = (int)bits.size();
   w->normal_mode = scheme.ebm_riemann_normal;
   w->P = riemann_params(scheme);
-  // one integration path per thread; at most 2 resident 128-thread CTAs per SM
-  const long long work = 3LL * w->nslot;
-  w->threads = (int)std::min<long long>((work + 127) / 128 * 128, 148LL * 2 * 128);
+  // the one-sided problems, both sides of every cut face
+  std::vector<int> work;
+  for (int sl = 0; sl < w->nslot; sl++)
+    for (int d = 0; d < 3; d++)
+      if (bits[sl] & (1 << d)) {
+        work.push_back((sl * 3 + d) * 2);
+        work.push_back((sl * 3 + d) * 2 + 1);
+      }
+  w->nwork = (int)work.size();
+  // one integration path (12 KiB) per thread, at most 4 resident 128-thread
+  // CTAs per SM
+  w->threads = (int)std::min<long long>((w->nwork + 127) / 128 * 128, 148LL * 4 * 128);
   bool ok = cudaMalloc((void**)&w->mask, nalloc) == cudaSuccess &&
             cudaMalloc((void**)&w->slot, nalloc * sizeof(int)) == cudaSuccess &&
             cudaMalloc((void**)&w->cell, cells.size() * sizeof(int)) == cudaSuccess &&
@@ -194,6 +203,7 @@ m2cg_status walls_create(cudaStream_t s, const Grid3& g, size_t nalloc, const m2
             cudaMalloc((void**)&w->Vsm, (size_t)w->nslot * 15 * sizeof(double)) == cudaSuccess &&
             cudaMalloc((void**)&w->Vsp, (size_t)w->nslot * 15 * sizeof(double)) == cudaSuccess &&
             cudaMalloc((void**)&w->cnt, 2 * sizeof(unsigned long long)) == cudaSuccess &&
+            cudaMalloc((void**)&w->work, work.size() * sizeof(int)) == cudaSuccess &&
             cudaMalloc((void**)&w->scratch, (size_t)w->threads * 3 * RIEMANN_PATH_CAP * sizeof(double)) == cudaSuccess;
   if (!ok) {
     walls_destroy(w);
@@ -213,6 +223,7 @@ m2cg_status walls_create(cudaStream_t s, const Grid3& g, size_t nalloc, const m2
     e = cudaMemcpyAsync(w->cell, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(w->geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w->work, work.data(), work.size() * sizeof(int), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(w->cnt, 0, 2 * sizeof(unsigned long long), s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host vectors go out of scope
   if (e != cudaSuccess) {
@@ -232,6 +243,7 @@ void walls_destroy(Walls* w) {
   cudaFree(w->Vsm);
   cudaFree(w->Vsp);
   cudaFree(w->cnt);
+  cudaFree(w->work);
   cudaFree(w->scratch);
   delete w;
 }
@@ -246,8 +258,9 @@ m2cg_status walls_stage(Walls* w, cudaStream_t s, StageArgs& a) {
   p.Vsm = w->Vsm;
   p.Vsp = w->Vsp;
   p.cnt = w->cnt;
+  p.work = w->work;
   p.scratch = w->scratch;
-  p.nslot = w->nslot;
+  p.nwork = w->nwork;
   p.normal_mode = w->normal_mode;
   k_wall_riemann<<<w->threads / 128, 128, 0, s>>>(p);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
