@@ -116,6 +116,8 @@ class TimeIntegratorGPU : public TimeIntegratorBase {
     s.mp_phasechange_dir = (int)iod.multiphase.phasechange_dir;
     s.mp_apply_failsafe_density = (int)iod.multiphase.apply_failsafe_density;
     s.mp_riemann_normal = (int)iod.multiphase.riemann_normal;
+    s.ebm_riemann_normal = (int)iod.ebm.riemann_normal;  // EmbeddedBoundaryMethodData
+    s.ebm_recon = (int)iod.ebm.recon;
     const ExactRiemannSolverData& r = iod.exact_riemann;
     s.riem_maxits_main = r.maxIts_main;
     s.riem_maxits_bracket = r.maxIts_bracket;
