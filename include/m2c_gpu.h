@@ -140,7 +140,8 @@ typedef struct {
   /* EmbeddedBoundaryMethodData (IoData.h:1340-1360), for faces cut by an
    * embedded surface (m2cg_set_wall_faces): direction of the one-sided
    * Riemann problems, 0 EMBEDDED_SURFACE, 1 MESH (default), 2 AVERAGE; state
-   * reconstruction at the surface, 0 CONSTANT (default; LINEAR is refused). */
+   * reconstruction at the surface, 0 CONSTANT (default: cell-centred states)
+   * or 1 LINEAR (the limited face states; a face pass writes them). */
   int ebm_riemann_normal;
   int ebm_recon;
 } m2cg_scheme;
@@ -254,8 +255,11 @@ m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
  * (SpaceOperator.cpp:3435-3501), [n][3] each: nwall_fwd / uwall_fwd, the
  * surface's unit normal and velocity at the intersection nearest the low
  * cell; nwall_bwd / uwall_bwd, those nearest the high cell. The normals are
- * used by scheme->ebm_riemann_normal EMBEDDED_SURFACE and AVERAGE. Refused
- * (M2CG_ERR_UNSUPPORTED): LINEAR reconstruction at the surface, viscous or
+ * used by scheme->ebm_riemann_normal EMBEDDED_SURFACE and AVERAGE; with
+ * scheme->ebm_recon LINEAR the one-sided problems and fluxes take the face
+ * states of the linear reconstruction. A cut face that also separates two
+ * materials takes the wall branch and stores no interface Riemann solution,
+ * as in the reference. Refused (M2CG_ERR_UNSUPPORTED): viscous or
  * heat-diffusive materials (the diffusion operators' own wall branches are
  * not built), faces on the subdomain boundary. Every cell stays active (the
  * reference's INACTIVE_MATERIAL_ID regions enclosed by a surface are not

@@ -906,12 +906,17 @@ static m2cg_status rk_step(m2cg_ctx* c, bool want_dtmin) {
     a.us_clipped = s > 1 ? c->clipflags + (s - 2) : nullptr;
     a.clipped_out = c->clipflags + (s - 1);
     a.dtmin_bits = (a.final_stage && want_dtmin && !c->mp) ? c->dtmin : nullptr;
-    if (c->mp) {
+    {  // face pass: reconstructed states of the interface / cut faces (LINEAR)
       StageArgs fa = a;
-      if (multiphase_face_pass(c->mp, fa)) {
+      bool fp = c->mp && multiphase_face_pass(c->mp, fa);
+      if (c->walls && walls_face_pass(c->walls, fa)) fp = true;
+      if (fp) {
         m2cg_status st = launch_stage(c, fa);
         if (st) return st;
       }
+    }
+    if (c->walls) walls_view(c->walls, a);  // the interface pre-pass skips cut faces
+    if (c->mp) {
       m2cg_status st = multiphase_stage(c->mp, c->stream, a);
       if (st) return st;
     }
@@ -1020,12 +1025,19 @@ extern "C" m2cg_status m2cg_compute_residual(m2cg_ctx* c, double* R_host) {
     c->rs_valid = false;  // the interface slots are reassigned
     m2cg_status st = multiphase_begin_step(c->mp, c->stream, Vn, c->id);
     if (st) return st;
+  }
+  {  // face pass: reconstructed states of the interface / cut faces (LINEAR)
     StageArgs fa = a;
-    if (multiphase_face_pass(c->mp, fa)) {
-      st = launch_stage(c, fa);
+    bool fp = c->mp && multiphase_face_pass(c->mp, fa);
+    if (c->walls && walls_face_pass(c->walls, fa)) fp = true;
+    if (fp) {
+      m2cg_status st = launch_stage(c, fa);
       if (st) return st;
     }
-    st = multiphase_stage(c->mp, c->stream, a);
+  }
+  if (c->walls) walls_view(c->walls, a);  // the interface pre-pass skips cut faces
+  if (c->mp) {
+    m2cg_status st = multiphase_stage(c->mp, c->stream, a);
     if (st) return st;
   }
   if (c->visc) {

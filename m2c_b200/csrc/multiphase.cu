@@ -328,6 +328,12 @@ __global__ void __launch_bounds__(128, M2C_IFACE_MINB) k_iface_riemann(IfaceRiem
     int ni, nj, nk;
     low_neighbour(g, i, j, k, d, ni, nj, nk);
     const long long offR = offset_of(g, i, j, k), offL = offset_of(g, ni, nj, nk);
+    if (a.st.wall.mask && ((a.st.wall.mask[offR] >> d) & 1)) {
+      // a face cut by an embedded surface takes the wall branch: no interface
+      // problem and no stored Riemann solution there (SpaceOperator.cpp:2438)
+      if (a.rsValid) a.rsValid[s * 3 + d] = 0;
+      continue;
+    }
     const uint8_t idR = a.st.id[offR], idL = a.st.id[offL];
     double VL[5], VR[5];
     iface_states(a, s, d, offL, idL, offR, idR, VL, VR);

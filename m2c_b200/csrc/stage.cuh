@@ -135,6 +135,11 @@ struct WallView {
   const int* slot;      // per cell; valid only where mask != 0
   const double* Vsm;    // [slot][3 faces][5]: the low neighbour's star state (its flux against it)
   const double* Vsp;    // [slot][3 faces][5]: this cell's star state
+  int linear;           // EmbeddedBoundaryMethodData::recon LINEAR: reconstructed face states
+  // Face pass (LINEAR): if set, the kernel writes the reconstructed states
+  // on both sides of every cut face, [slot][3 faces][low, high][5], for the
+  // one-sided problems solved before the stage proper; no flux, no update.
+  double* faces_out;
 };
 
 struct StageArgs {
@@ -768,7 +773,19 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     }
     T VL[5], VR[5];
     const uint8_t idL = sm.ids[sL][myL + 1][mxL + 1], idR = sm.ids[sR][myR + 1][mxR + 1];
-    if (MULTI && a.iface.faces_out && idL == idR) {
+    // a face cut by an embedded surface (interior faces only) takes the wall
+    // branch, which the reference tests before the material-interface one
+    bool wall = false;
+    long long offW = 0;
+    if (MULTI && a.wall.mask && rL && rR) {
+      const int gi = wrap_index(i0 + mxR - 1, g.nx), gj = wrap_index(j0 + myR - 1, g.ny);
+      offW = (long long)wrap_index(pR, g.nz) * g.plane + (long long)gj * g.px + gi;
+      wall = (a.wall.mask[offW] >> d) & 1;
+    }
+    // face pass: only the faces whose states a pre-pass solves from
+    const bool fp_iface = MULTI && a.iface.faces_out && idL != idR;
+    const bool fp_wall = MULTI && a.wall.faces_out && wall;
+    if (MULTI && (a.iface.faces_out || a.wall.faces_out) && !fp_iface && !fp_wall) {
 #pragma unroll
       for (int c = 0; c < 5; c++) { F[c] = T(0); F2[c] = T(0); }
       return;
@@ -788,28 +805,23 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       ghost_face(g.bc[2 * d + 1], d, VL, gc, eos_of<T, MULTI>(a.s, idR), VR);
     }
     int err = ERR_NONE;
-    if (MULTI && a.iface.faces_out) {  // face pass: the interface faces' states only
+    if (fp_iface || fp_wall) {  // face pass: the interface or cut faces' states only
 #pragma unroll
       for (int c = 0; c < 5; c++) { F[c] = T(0); F2[c] = T(0); }
       const int gi = wrap_index(i0 + mxR - 1, g.nx), gj = wrap_index(j0 + myR - 1, g.ny);
       const int gk = wrap_index(pR, g.nz);
-      const int slot = a.iface.slot[(long long)gk * g.plane + (long long)gj * g.px + gi];
-      double* o = a.iface.faces_out + ((long long)slot * 3 + d) * 10;
+      const long long offR = (long long)gk * g.plane + (long long)gj * g.px + gi;
+      for (int q = 0; q < 2; q++) {
+        if (q == 0 ? !fp_iface : !fp_wall) continue;
+        const int slot = q == 0 ? a.iface.slot[offR] : a.wall.slot[offR];
+        double* o = (q == 0 ? a.iface.faces_out : a.wall.faces_out) + ((long long)slot * 3 + d) * 10;
 #pragma unroll
-      for (int c = 0; c < 5; c++) {
-        o[c] = double(VL[c]);
-        o[5 + c] = double(VR[c]);
+        for (int c = 0; c < 5; c++) {
+          o[c] = double(VL[c]);
+          o[5 + c] = double(VR[c]);
+        }
       }
       return;
-    }
-    // a face cut by an embedded surface (interior faces only) takes the wall
-    // branch, which the reference tests before the material-interface one
-    bool wall = false;
-    long long offW = 0;
-    if (MULTI && a.wall.mask && rL && rR) {
-      const int gi = wrap_index(i0 + mxR - 1, g.nx), gj = wrap_index(j0 + myR - 1, g.ny);
-      offW = (long long)wrap_index(pR, g.nz) * g.plane + (long long)gj * g.px + gi;
-      wall = (a.wall.mask[offW] >> d) & 1;
     }
     if (MULTI && (wall || idL != idR)) {
       // Material interface (SpaceOperator.cpp:2486-2542): two one-sided fluxes
@@ -818,7 +830,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       // cell's flux against its one-sided star state.
       const IfaceView& iv = a.iface;
       T WL[5], WR[5];
-      if (wall || iv.mp_recon == 0) {  // constant reconstruction: cell-centred states
+      if (wall ? !a.wall.linear : iv.mp_recon == 0) {  // constant reconstruction: cell-centred states
 #pragma unroll
         for (int c = 0; c < 5; c++) {
           WL[c] = M2C_VV(sL, c, myL + 1, mxL + 1);
@@ -983,7 +995,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       __syncthreads();
       if (m >= kb - 1) faces(m, m >= kb);
       __syncthreads();
-      if (m < kb || !own || (MULTI && a.iface.faces_out)) continue;
+      if (m < kb || !own || (MULTI && (a.iface.faces_out || a.wall.faces_out))) continue;
       // (4) residual + RK update of plane m
       const double dzk = g.dz[m];
       const double ax = dyj * dzk, ay = dxi * dzk, az = dxi * dyj;
@@ -1042,7 +1054,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
               // reconstructed state on that face (vl) under LINEAR interface
               // reconstruction
               T W[5];
-              if (!w && a.iface.mp_recon) {
+              if (w ? a.wall.linear : a.iface.mp_recon) {
                 cell_face(m, tx + 1, ty + 1, d, 0, W);
               } else {
 #pragma unroll

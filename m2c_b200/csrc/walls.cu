@@ -25,6 +25,8 @@ struct Walls {
   double* Vsp = nullptr;
   unsigned long long* cnt = nullptr;  // [0] solves, [1] failed solves
   int* work = nullptr;                // one-sided problems: (slot * 3 + d) * 2 + side
+  int linear = 0;                     // LINEAR reconstruction at the surface
+  double* faceV = nullptr;            // LINEAR: the face pass's states, [slot][3][low, high][5]
   int nwork = 0;
   double* scratch = nullptr;          // per thread: one integration path
   int threads = 0;
@@ -42,6 +44,7 @@ struct WallPassArgs {
   double* Vsp;
   unsigned long long* cnt;
   const int* work;
+  const double* faceV;
   double* scratch;
   int nwork;
   int normal_mode;
@@ -105,7 +108,12 @@ __global__ void __launch_bounds__(128, 4) k_wall_riemann(WallPassArgs a) {
     const long long off = side ? offR : offR - (d == 0 ? 1LL : (d == 1 ? g.px : g.plane));
     const uint8_t id = a.st.id[off];
     double V[5];
-    wall_stage_state(a.st, off, id, V);
+    if (a.faceV) {  // LINEAR: vr of the low cell, vl of the high cell (SpaceOperator.cpp:2452, 2474)
+      const double* fv = a.faceV + (3LL * sl + d) * 10 + 5 * side;
+      for (int c = 0; c < 5; c++) V[c] = fv[c];
+    } else {
+      wall_stage_state(a.st, off, id, V);
+    }
     const double* gm = a.geo + (3LL * sl + d) * 12 + 6 * side;
     double dir[3], Vs[5], Vst[5];
     int mid = 0;
@@ -136,8 +144,8 @@ m2cg_status walls_create(cudaStream_t s, const Grid3& g, size_t nalloc, const m2
     return st;
   };
   if (n < 1 || !faces || !nf || !uf || !nb || !ub) return refuse(M2CG_ERR_ARG, "no faces or a null array");
-  if (scheme.ebm_recon != 0)
-    return refuse(M2CG_ERR_UNSUPPORTED, "only CONSTANT reconstruction at embedded surfaces is implemented");
+  if (scheme.ebm_recon != 0 && scheme.ebm_recon != 1)
+    return refuse(M2CG_ERR_ARG, "ebm_recon must be 0 (CONSTANT) or 1 (LINEAR)");
   if (scheme.ebm_riemann_normal < 0 || scheme.ebm_riemann_normal > 2)
     return refuse(M2CG_ERR_ARG, "ebm_riemann_normal must be 0 (EMBEDDED_SURFACE), 1 (MESH) or 2 (AVERAGE)");
   const int nn[3] = {g.nx, g.ny, g.nz};
@@ -183,6 +191,7 @@ m2cg_status walls_create(cudaStream_t s, const Grid3& g, size_t nalloc, const m2
   Walls* w = new Walls;
   w->nslot = (int)bits.size();
   w->normal_mode = scheme.ebm_riemann_normal;
+  w->linear = scheme.ebm_recon == 1 && scheme.rec_type == M2CG_REC_LINEAR;
   w->P = riemann_params(scheme);
   // the one-sided problems, both sides of every cut face
   std::vector<int> work;
@@ -204,6 +213,7 @@ m2cg_status walls_create(cudaStream_t s, const Grid3& g, size_t nalloc, const m2
             cudaMalloc((void**)&w->Vsp, (size_t)w->nslot * 15 * sizeof(double)) == cudaSuccess &&
             cudaMalloc((void**)&w->cnt, 2 * sizeof(unsigned long long)) == cudaSuccess &&
             cudaMalloc((void**)&w->work, work.size() * sizeof(int)) == cudaSuccess &&
+            (!w->linear || cudaMalloc((void**)&w->faceV, (size_t)w->nslot * 30 * sizeof(double)) == cudaSuccess) &&
             cudaMalloc((void**)&w->scratch, (size_t)w->threads * 3 * RIEMANN_PATH_CAP * sizeof(double)) == cudaSuccess;
   if (!ok) {
     walls_destroy(w);
@@ -244,6 +254,7 @@ void walls_destroy(Walls* w) {
   cudaFree(w->Vsp);
   cudaFree(w->cnt);
   cudaFree(w->work);
+  cudaFree(w->faceV);
   cudaFree(w->scratch);
   delete w;
 }
@@ -259,16 +270,40 @@ m2cg_status walls_stage(Walls* w, cudaStream_t s, StageArgs& a) {
   p.Vsp = w->Vsp;
   p.cnt = w->cnt;
   p.work = w->work;
+  p.faceV = w->faceV;
   p.scratch = w->scratch;
   p.nwork = w->nwork;
   p.normal_mode = w->normal_mode;
   k_wall_riemann<<<w->threads / 128, 128, 0, s>>>(p);
   if (cudaGetLastError() != cudaSuccess) return M2CG_ERR_CUDA;
+  walls_view(w, a);
+  return M2CG_OK;
+}
+
+void walls_view(const Walls* w, StageArgs& a) {
   a.wall.mask = w->mask;
   a.wall.slot = w->slot;
   a.wall.Vsm = w->Vsm;
   a.wall.Vsp = w->Vsp;
-  return M2CG_OK;
+  a.wall.linear = w->linear;
+  a.wall.faces_out = nullptr;
+}
+
+bool walls_face_pass(const Walls* w, StageArgs& a) {
+  if (!w->linear) return false;
+  walls_view(w, a);
+  a.wall.faces_out = w->faceV;
+  for (int p = 0; p < 5; p++) {
+    a.Po[p] = nullptr;
+    a.Uo[p] = nullptr;
+    a.Vo[p] = nullptr;
+    a.Vfo[p] = nullptr;
+    a.Ro[p] = nullptr;
+  }
+  a.final_stage = 0;
+  a.clipped_out = nullptr;
+  a.dtmin_bits = nullptr;
+  return true;
 }
 
 void walls_counters(Walls* w, cudaStream_t s, long long* solves, long long* failures) {

@@ -30,6 +30,11 @@ m2cg_status walls_create(cudaStream_t s, const Grid3& g, size_t nalloc, const m2
 void walls_destroy(Walls* w);
 // The one-sided solves of the stage whose arguments are a; fills a.wall.
 m2cg_status walls_stage(Walls* w, cudaStream_t s, StageArgs& a);
+// The cut faces' view without solving (the interface pre-pass skips them).
+void walls_view(const Walls* w, StageArgs& a);
+// LINEAR reconstruction at the surface: makes a the arguments of the face
+// pass that writes the cut faces' reconstructed states (false: none needed).
+bool walls_face_pass(const Walls* w, StageArgs& a);
 // One-sided solves so far and how many of them the solver reported as
 // failed (the reference's riemann_errors, SpaceOperator.cpp:2446-2447).
 void walls_counters(Walls* w, cudaStream_t s, long long* solves, long long* failures);

@@ -70,6 +70,31 @@ def test_wall_residual_matches_reference(gpu, ref, normal, flux):
     sol.close()
 
 
+@pytest.mark.parametrize("normal", [abi.EBM_NORMAL_MESH, abi.EBM_NORMAL_AVERAGE])
+def test_wall_residual_linear_reconstruction_matches_reference(gpu, ref, normal):
+    """EmbeddedBoundaryMethodData::recon LINEAR: the one-sided problems and
+    the fluxes take the limited face states (vr of the low cell, vl of the
+    high cell, SpaceOperator.cpp:2452-2456, 2474-2478), which a face pass of
+    the stage kernel writes; every limiter branch of the random box."""
+    g, s, mats, V = cases.random_box(14, 11, 9, seed=5)
+    s.ebm_recon = 1
+    s.ebm_riemann_normal = normal
+    W = wall_faces(g, 120, seed=7)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    sol.set_wall_faces(*W)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V)
+    Rr = inner(rc.residual_walls(*W))
+    assert rel_err(inner(sol.residual()), Rr) <= TOL
+    s0 = abi.scheme(**{f: getattr(s, f) for f, _ in abi.Scheme._fields_})
+    s0.ebm_recon = 0
+    rc0 = ref.RefCase(g, s0, mats)
+    rc0.set_state(V)
+    assert rel_err(inner(rc0.residual_walls(*W)), Rr) > 1e-8  # LINEAR differs from CONSTANT
+    sol.close()
+
+
 def test_wall_residual_of_receding_and_fast_walls_matches_reference(gpu, ref):
     """Walls moving away faster than the fluid can follow (the one-sided
     rarefaction reports failure and the reference keeps the input state
@@ -87,10 +112,13 @@ def test_wall_residual_of_receding_and_fast_walls_matches_reference(gpu, ref):
     sol.close()
 
 
-def test_wall_residual_two_materials_matches_reference(gpu, ref):
+@pytest.mark.parametrize("linear", [False, True])
+def test_wall_residual_two_materials_matches_reference(gpu, ref, linear):
     """A surface through the bubble case: cut faces between two cells of the
     same material and across the material interface (the wall branch is
-    taken there, as in the reference), water and air."""
+    taken there, as in the reference), water and air; with linear=True LINEAR
+    reconstruction at both the material interface and the surface (one face
+    pass writes both sets of face states)."""
     if not ref.available("crpow"):
         pytest.skip("reference oracle with correctly rounded pow not built (make -C oracle refcr)")
     g, s, mats, ls, V, ID, PHI = cases.bubble_case(16, reinit_frequency=-1, radius=4.0e-3)
@@ -104,6 +132,9 @@ def test_wall_residual_two_materials_matches_reference(gpu, ref):
     en[np.arange(n), faces[:, 0]] = 1.0
     uf = rng.uniform(-30.0, 30.0, (n, 3))
     W = (faces, en, uf, en, uf)
+    if linear:
+        s.mp_recon = 1
+        s.ebm_recon = 1
     sol = gpu.Solver(g, s, mats, ls)
     sol.upload(V, ID, PHI)
     sol.set_wall_faces(*W)
@@ -143,9 +174,9 @@ def test_wall_faces_refused(gpu):
     with pytest.raises(gpu.M2CError, match="outside"):
         sol.set_wall_faces([(2, 2, 3, 6)])
     sol.close()
-    s.ebm_recon = 1
+    s.ebm_recon = 2
     sol = gpu.Solver(g, s, mats)
-    with pytest.raises(gpu.M2CError, match="CONSTANT"):
+    with pytest.raises(gpu.M2CError, match="ebm_recon"):
         sol.set_wall_faces([(0, 3, 3, 3)])
     sol.close()
     visc = gpu.Solver(g, abi.scheme(), [abi.material(1.4, 0.0, mu=1e-3)])
