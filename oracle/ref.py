@@ -51,6 +51,8 @@ def _load(path, prefix):
     f("compute_dt").argtypes = [vp]
     f("compute_residual").argtypes = [vp, dp]
     f("compute_residual_walls").argtypes = [vp, C.c_int, ip, dp, dp, dp, dp, dp]
+    f("run_walls").argtypes = [vp, C.c_int, ip, dp, dp, dp, dp, C.c_int, dp]
+    f("run_walls").restype = C.c_int
     f("advance").argtypes = [vp, C.c_double]
     f("run").restype = C.c_int
     f("run").argtypes = [vp, C.c_int, C.c_double, dp]
@@ -125,6 +127,20 @@ class _Case:
         self._f("compute_residual_walls")(self.h, len(faces), abi.iptr(faces), *[abi.dptr(a) for a in arrs],
                                           abi.dptr(R))
         return R
+
+    def run_walls(self, faces, nwall_fwd, uwall_fwd, nwall_bwd, uwall_bwd, nsteps):
+        """nsteps CFL steps of one material (RK2 / RK3 as the reference's
+        integrator takes them) with an embedded surface cutting the listed
+        faces; returns (steps, t)."""
+        faces = np.ascontiguousarray(np.asarray(faces, np.int32).reshape(-1, 4))
+        arrs = [np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1, 3))
+                for a in (nwall_fwd, uwall_fwd, nwall_bwd, uwall_bwd)]
+        t = C.c_double(0.0)
+        n = self._f("run_walls")(self.h, len(faces), abi.iptr(faces), *[abi.dptr(a) for a in arrs], nsteps,
+                                 C.byref(t))
+        if n < 0:
+            raise ValueError("run_walls: one material without level sets only")
+        return n, t.value
 
     def advance(self, dt):
         self._f("advance")(self.h, dt)

@@ -356,58 +356,130 @@ double m2cref_compute_dt(void* h) {
   return dt;
 }
 
-// R for the current state with faces cut by an embedded surface: one
-// EmbeddedBoundaryDataSet whose intersector results are written directly, so
-// that SpaceOperator::FindEdgeSurfaceIntersections (SpaceOperator.cpp:
-// 3435-3501) yields the given normal and velocity on each listed face. Face q
-// = (axis d, i, j, k) gets two triangles, 2q (forward: normal nf, node
-// velocity uf) and 2q+1 (backward), each met at barycentric coordinates
-// (1, 0, 0), so the interpolated surface velocity is the given one exactly;
-// XForward / XBackward of node (i, j, k), component d, hold 2q and 2q+1.
+// An embedded surface cutting the listed faces: one EmbeddedBoundaryDataSet
+// whose intersector results are written directly, so that
+// SpaceOperator::FindEdgeSurfaceIntersections (SpaceOperator.cpp:3435-3501)
+// yields the given normal and velocity on each face. Face q = (axis d, i, j,
+// k) gets two triangles, 2q (forward: normal nf, node velocity uf) and 2q+1
+// (backward), each met at barycentric coordinates (1, 0, 0), so the
+// interpolated surface velocity is the given one exactly; XForward /
+// XBackward of node (i, j, k), component d, hold 2q and 2q+1.
+struct HandSurface {
+  TriangulatedSurface surf;
+  std::vector<IntersectionPoint> xs;
+  SpaceVariable3D* xf = nullptr;
+  SpaceVariable3D* xb = nullptr;
+  std::vector<std::unique_ptr<EmbeddedBoundaryDataSet>> ebds;
+  HandSurface(RefCase* c, int n, const int* faces, const double* nf, const double* uf, const double* nb,
+              const double* ub) {
+    xf = new SpaceVariable3D(c->comm, &(c->dms->ghosted1_3dof));
+    xb = new SpaceVariable3D(c->comm, &(c->dms->ghosted1_3dof));
+    xf->SetConstantValue(-1.0, true);
+    xb->SetConstantValue(-1.0, true);
+    Vec3D*** f = (Vec3D***)xf->GetDataPointer();
+    Vec3D*** b = (Vec3D***)xb->GetDataPointer();
+    double xi[3] = {1.0, 0.0, 0.0};
+    for (int q = 0; q < n; q++) {
+      const int d = faces[4 * q], i = faces[4 * q + 1], j = faces[4 * q + 2], k = faces[4 * q + 3];
+      for (int side = 0; side < 2; side++) {
+        const double* nw = side == 0 ? nf + 3 * q : nb + 3 * q;
+        const double* uw = side == 0 ? uf + 3 * q : ub + 3 * q;
+        const int base = (int)surf.Udot.size();
+        for (int v = 0; v < 3; v++) surf.X.push_back(Vec3D(0.0, 0.0, 0.0));
+        surf.Udot.push_back(Vec3D(uw[0], uw[1], uw[2]));
+        surf.Udot.push_back(Vec3D(0.0, 0.0, 0.0));
+        surf.Udot.push_back(Vec3D(0.0, 0.0, 0.0));
+        surf.elems.push_back(Int3(base, base + 1, base + 2));
+        surf.elemNorm.push_back(Vec3D(nw[0], nw[1], nw[2]));
+        const int tid = 2 * q + side;
+        xs.push_back(IntersectionPoint(i, j, k, d, side == 0 ? 0.25 : 0.75, tid, xi));
+        (side == 0 ? f : b)[k][j][i][d] = (double)tid;
+      }
+    }
+    xf->RestoreDataPointerAndInsert();
+    xb->RestoreDataPointerAndInsert();
+    ebds.push_back(std::make_unique<EmbeddedBoundaryDataSet>());
+    ebds[0]->surface_ptr = &surf;
+    ebds[0]->XForward_ptr = xf;
+    ebds[0]->XBackward_ptr = xb;
+    ebds[0]->intersections_ptr = &xs;
+  }
+  ~HandSurface() {
+    xf->Destroy();
+    xb->Destroy();
+    delete xf;
+    delete xb;
+  }
+};
+
+// R for the current state with an embedded surface cutting the listed faces.
 void m2cref_compute_residual_walls(void* h, int n, const int* faces, const double* nf, const double* uf,
                                    const double* nb, const double* ub, double* R) {
   RefCase* c = (RefCase*)h;
-  TriangulatedSurface surf;
-  std::vector<IntersectionPoint> xs;
-  SpaceVariable3D xf(c->comm, &(c->dms->ghosted1_3dof)), xb(c->comm, &(c->dms->ghosted1_3dof));
-  xf.SetConstantValue(-1.0, true);
-  xb.SetConstantValue(-1.0, true);
-  Vec3D*** f = (Vec3D***)xf.GetDataPointer();
-  Vec3D*** b = (Vec3D***)xb.GetDataPointer();
-  double xi[3] = {1.0, 0.0, 0.0};
-  for (int q = 0; q < n; q++) {
-    const int d = faces[4 * q], i = faces[4 * q + 1], j = faces[4 * q + 2], k = faces[4 * q + 3];
-    for (int side = 0; side < 2; side++) {
-      const double* nw = side == 0 ? nf + 3 * q : nb + 3 * q;
-      const double* uw = side == 0 ? uf + 3 * q : ub + 3 * q;
-      const int base = (int)surf.Udot.size();
-      surf.X.push_back(Vec3D(0.0, 0.0, 0.0));
-      surf.X.push_back(Vec3D(0.0, 0.0, 0.0));
-      surf.X.push_back(Vec3D(0.0, 0.0, 0.0));
-      surf.Udot.push_back(Vec3D(uw[0], uw[1], uw[2]));
-      surf.Udot.push_back(Vec3D(0.0, 0.0, 0.0));
-      surf.Udot.push_back(Vec3D(0.0, 0.0, 0.0));
-      surf.elems.push_back(Int3(base, base + 1, base + 2));
-      surf.elemNorm.push_back(Vec3D(nw[0], nw[1], nw[2]));
-      const int tid = 2 * q + side;
-      xs.push_back(IntersectionPoint(i, j, k, d, side == 0 ? 0.25 : 0.75, tid, xi));
-      (side == 0 ? f : b)[k][j][i][d] = (double)tid;
-    }
-  }
-  xf.RestoreDataPointerAndInsert();
-  xb.RestoreDataPointerAndInsert();
-  std::vector<std::unique_ptr<EmbeddedBoundaryDataSet>> ebds;
-  ebds.push_back(std::make_unique<EmbeddedBoundaryDataSet>());
-  ebds[0]->surface_ptr = &surf;
-  ebds[0]->XForward_ptr = &xf;
-  ebds[0]->XBackward_ptr = &xb;
-  ebds[0]->intersections_ptr = &xs;
+  HandSurface hs(c, n, faces, nf, uf, nb, ub);
   SpaceVariable3D Rv(c->comm, &(c->dms->ghosted1_5dof));
-  c->spo->ComputeResidual(*c->V, *c->ID, Rv, nullptr, nullptr, nullptr, &ebds);
+  c->spo->ComputeResidual(*c->V, *c->ID, Rv, nullptr, nullptr, nullptr, &hs.ebds);
   copy_out(Rv, R, 5, c->NX, c->NY, c->NZ);
   Rv.Destroy();
-  xf.Destroy();
-  xb.Destroy();
+}
+
+// nsteps CFL steps of one material with an embedded surface cutting the
+// listed faces: the statements of TimeIntegratorRK2 / RK3::
+// AdvanceOneTimeStep (TimeIntegrator.cpp:291-428, 496-690) without level
+// sets (UpdateSolutionAfterTimeStepping then does nothing), with the
+// surface's data set passed to every ComputeResidual, as the reference's
+// integrator does with its EmbeddedBoundaryOperator's. Returns steps taken.
+int m2cref_run_walls(void* h, int n, const int* faces, const double* nf, const double* uf, const double* nb,
+                     const double* ub, int nsteps, double* t_out) {
+  RefCase* c = (RefCase*)h;
+  if (!c->Phi.empty()) return -1;
+  const int rk = c->iod.ts.expl.type == ExplicitData::RUNGE_KUTTA_3 ? 3 : 2;
+  HandSurface hs(c, n, faces, nf, uf, nb, ub);
+  auto* E = &hs.ebds;
+  SpaceVariable3D R(c->comm, &(c->dms->ghosted1_5dof)), Un(c->comm, &(c->dms->ghosted1_5dof)),
+      U1(c->comm, &(c->dms->ghosted1_5dof)), V1(c->comm, &(c->dms->ghosted1_5dof)),
+      V2(c->comm, &(c->dms->ghosted1_5dof));
+  SpaceVariable3D& V = *c->V;
+  SpaceVariable3D& ID = *c->ID;
+  SpaceOperator& spo = *c->spo;
+  int done = 0;
+  for (; done < nsteps; done++) {
+    double dt = 0.0, cfl = 0.0;
+    spo.ComputeTimeStepSize(V, ID, dt, cfl);
+    c->time_step++;
+    c->t += dt;
+    spo.ComputeResidual(V, ID, R, nullptr, nullptr, nullptr, E);
+    spo.PrimitiveToConservative(V, ID, Un);
+    U1.AXPlusBY(0.0, 1.0, Un);
+    U1.AXPlusBY(1.0, dt, R);
+    spo.ConservativeToPrimitive(U1, ID, V1);
+    if (spo.ClipDensityAndPressure(V1, ID)) spo.PrimitiveToConservative(V1, ID, U1);
+    spo.ApplyBoundaryConditions(V1);
+    spo.ComputeResidual(V1, ID, R, nullptr, nullptr, nullptr, E);
+    if (rk == 2) {
+      U1.AXPlusBY(0.5, 0.5, Un);
+      U1.AXPlusBY(1.0, 0.5 * dt, R);
+    } else {
+      U1.AXPlusBY(0.25, 0.75, Un);
+      U1.AXPlusBY(1.0, 0.25 * dt, R);
+      spo.ConservativeToPrimitive(U1, ID, V2);
+      if (spo.ClipDensityAndPressure(V2, ID)) spo.PrimitiveToConservative(V2, ID, U1);
+      spo.ApplyBoundaryConditions(V2);
+      spo.ComputeResidual(V2, ID, R, nullptr, nullptr, nullptr, E);
+      U1.AXPlusBY(2.0 / 3.0, 1.0 / 3.0, Un);
+      U1.AXPlusBY(1.0, 2.0 / 3.0 * dt, R);
+    }
+    spo.ConservativeToPrimitive(U1, ID, V);
+    spo.ClipDensityAndPressure(V, ID);
+    spo.ApplyBoundaryConditions(V);
+  }
+  R.Destroy();
+  Un.Destroy();
+  U1.Destroy();
+  V1.Destroy();
+  V2.Destroy();
+  if (t_out) *t_out = c->t;
+  return done;
 }
 
 // R for the current state (ghosted layout, 5 dof).

@@ -148,6 +148,27 @@ def test_wall_residual_two_materials_matches_reference(gpu, ref, linear):
     sol.close()
 
 
+@pytest.mark.parametrize("rk,linear", [(3, False), (2, False), (3, True)])
+def test_wall_steps_match_reference(gpu, ref, rk, linear):
+    """Whole CFL steps with cut faces: the reference side takes the
+    statements of TimeIntegratorRK2 / RK3::AdvanceOneTimeStep with the
+    surface's data set in every ComputeResidual (oracle/ref_harness.cpp,
+    m2cref_run_walls)."""
+    g, s, mats, V = cases.random_box(14, 11, 9, seed=5, rk=rk)
+    s.ebm_recon = int(linear)
+    W = wall_faces(g, 120, seed=2)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    sol.set_wall_faces(*W)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V)
+    n, t = sol.run(6)
+    nr, tr = rc.run_walls(*W, 6)
+    assert n == nr == 6 and t == tr
+    assert rel_err(inner(sol.download()[0]), inner(rc.get_state()[0])) <= TOL
+    sol.close()
+
+
 def test_wall_steps_mixed_track_fp64(gpu):
     out = []
     for prec in (abi.PREC_FP64, abi.PREC_MIXED):
