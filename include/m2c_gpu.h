@@ -259,9 +259,11 @@ m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
  * scheme->ebm_recon LINEAR the one-sided problems and fluxes take the face
  * states of the linear reconstruction. A cut face that also separates two
  * materials takes the wall branch and stores no interface Riemann solution,
- * as in the reference. Refused (M2CG_ERR_UNSUPPORTED): viscous or
- * heat-diffusive materials (the diffusion operators' own wall branches are
- * not built), faces on the subdomain boundary. Every cell stays active (the
+ * as in the reference. Heat diffusion is unaffected by the surface, as in
+ * the reference (HeatDiffusionOperator::AddDiffusionFluxes does not use it).
+ * Refused (M2CG_ERR_UNSUPPORTED): viscous materials (the viscosity
+ * operator's ghost-fluid population at cut faces is not built), faces on
+ * the subdomain boundary. Every cell stays active (the
  * reference's INACTIVE_MATERIAL_ID regions enclosed by a surface are not
  * represented). Host pointers. */
 m2cg_status m2cg_set_wall_faces(m2cg_ctx* ctx, int n, const int* faces, const double* nwall_fwd,

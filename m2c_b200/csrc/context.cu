@@ -820,9 +820,12 @@ extern "C" m2cg_status m2cg_set_wall_faces(m2cg_ctx* c, int n, const int* faces,
     set_stage_items(c, c->mp != nullptr);
     return M2CG_OK;
   }
-  if (c->visc)
+  // HeatDiffusionOperator::AddDiffusionFluxes leaves cut faces alone (its
+  // EBDS argument is unused); ViscosityOperator's ghost-fluid population at
+  // cut faces (ViscosityOperator.cpp:208-213) is not built
+  if (viscous_has_viscosity(c->visc))
     return fail(M2CG_ERR_UNSUPPORTED,
-                "cut faces with viscous or heat-diffusive materials (the diffusion operators' wall branches) are not implemented");
+                "cut faces with viscous materials (the viscosity operator's ghost-fluid branch) are not implemented");
   const size_t smem = c->scheme.precision == M2CG_PREC_MIXED ? stage_smem_mixed(true) : stage_smem_fp64(true);
   int maxsm = 0;
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);

@@ -391,6 +391,8 @@ m2cg_status viscous_create(cudaStream_t s, const Grid3& g, const Eos<double>* eo
   return cudaGetLastError() == cudaSuccess ? M2CG_OK : M2CG_ERR_CUDA;
 }
 
+bool viscous_has_viscosity(const Viscous* v) { return v && v->d.viscous; }
+
 void viscous_destroy(Viscous* v) {
   if (!v) return;
   cudaFree(v->base);

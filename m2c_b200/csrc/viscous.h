@@ -24,6 +24,8 @@ struct Viscous;
 m2cg_status viscous_create(cudaStream_t s, const Grid3& g, const Eos<double>* eos, const m2cg_material* mats,
                            int nmat, const double* const* xc, const double* const* dx, Viscous** out);
 void viscous_destroy(Viscous* v);
+// Whether any material is viscous (heat diffusion alone: false).
+bool viscous_has_viscosity(const Viscous* v);
 // Faces of the stage whose arguments are a (its input state a.Pin in the
 // compute type: float when mixed); fills a.visc.
 m2cg_status viscous_faces(Viscous* v, cudaStream_t s, StageArgs& a, bool mixed);
@@ -33,4 +35,5 @@ m2cg_status viscous_faces(Viscous* v, cudaStream_t s, StageArgs& a, bool mixed);
 using m2c::Viscous;
 using m2c::viscous_create;
 using m2c::viscous_destroy;
+using m2c::viscous_has_viscosity;
 using m2c::viscous_faces;

@@ -169,6 +169,22 @@ def test_wall_steps_match_reference(gpu, ref, rk, linear):
     sol.close()
 
 
+def test_wall_residual_with_heat_diffusion_matches_reference(gpu, ref):
+    """Heat diffusion ignores the surface in the reference
+    (HeatDiffusionOperator::AddDiffusionFluxes takes the data set but does
+    not use it): the heat fluxes are added as without cut faces."""
+    g, s, _, V = cases.random_box(14, 11, 9, seed=5)
+    mats = [abi.material(1.4, 0.0, heat_diffusivity=0.02, cv=2.5, T0=1.0, e0=0.5)]
+    W = wall_faces(g, 120, seed=3)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V)
+    sol.set_wall_faces(*W)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V)
+    assert rel_err(inner(sol.residual()), inner(rc.residual_walls(*W))) <= TOL
+    sol.close()
+
+
 def test_wall_steps_mixed_track_fp64(gpu):
     out = []
     for prec in (abi.PREC_FP64, abi.PREC_MIXED):
