@@ -36,9 +36,10 @@ Extras (rank 0 at N = 1, skipped by --only-headline), under "extras": the
 256^3 single-material periodic box (mixed vs FP64, with its own roofline,
 CPU figure and end-to-end figure), the 192^3 single bubble over 500 steps,
 the 4096 batched two-material tubes (CUDA-graph replay, autotuned tiles,
-with and without the learned warm start), and the learned warm start's
-evaluations and iterations saved on held-out interface problems (network in
-m2c_b200/data/warmstart_mlp.npz).
+with and without the learned warm start), a 192^3 box cut by a resting
+plane (one-sided Riemann problems at the cut faces), and the learned warm
+start's evaluations and iterations saved on held-out interface problems and
+on the cluster (network in m2c_b200/data/warmstart_mlp.npz).
 """
 import argparse
 import json
@@ -93,6 +94,8 @@ def parse():
                    help="run only the cluster workload at N^3, mixed then FP64, and print its JSON (profiling)")
     p.add_argument("--box", type=int, default=0, metavar="N",
                    help="run only the periodic-box workload at N^3 and print its JSON (profiling)")
+    p.add_argument("--plane", type=int, default=0, metavar="N",
+                   help="run only the box cut by a resting plane at N^3 and print its JSON (profiling)")
     return p.parse_args()
 
 
@@ -666,6 +669,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         print(json.dumps(extra_box(n=args.box, steps=args.steps, warmup=args.warmup, cpu=False)))
+        return
+    if args.plane:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(extra_walls(n=args.plane, steps=args.steps, warmup=args.warmup)))
         return
 
     # CPU baseline first (spawned processes, before any GPU work), rank 0, N=1 only
