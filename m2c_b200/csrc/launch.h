@@ -29,10 +29,10 @@ cudaError_t launch_stage_mixed(const StageArgs& a, cudaStream_t s, bool multi, i
 int stage_resident_fp64(int flux, bool multi);
 int stage_resident_mixed(int flux, bool multi);
 
-template <typename T, int FLUX, bool MULTI, bool CONS = false>
+template <typename T, int FLUX, bool MULTI, bool CONS = false, bool WALLS = false>
 cudaError_t stage_occupancy(int* per_sm, int* nsm) {
   constexpr int TY = StageTY<T, MULTI>::value;
-  auto k = stage_kernel<T, TY, FLUX, MULTI, CONS>;
+  auto k = stage_kernel<T, TY, FLUX, MULTI, CONS, WALLS>;
   const size_t smem = sizeof(StageSmemAll<T, TY, MULTI>);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -45,13 +45,13 @@ cudaError_t stage_occupancy(int* per_sm, int* nsm) {
   return e;
 }
 
-template <typename T, int FLUX, bool MULTI, bool CONS>
+template <typename T, int FLUX, bool MULTI, bool CONS, bool WALLS = false>
 cudaError_t launch_stage_one(const StageArgs& a, cudaStream_t s, int* grid_out) {
   constexpr int TY = StageTY<T, MULTI>::value;
-  auto k = stage_kernel<T, TY, FLUX, MULTI, CONS>;
+  auto k = stage_kernel<T, TY, FLUX, MULTI, CONS, WALLS>;
   const size_t smem = sizeof(StageSmemAll<T, TY, MULTI>);
   int per_sm = 1, nsm = 148;
-  cudaError_t e = stage_occupancy<T, FLUX, MULTI, CONS>(&per_sm, &nsm);
+  cudaError_t e = stage_occupancy<T, FLUX, MULTI, CONS, WALLS>(&per_sm, &nsm);
   if (e != cudaSuccess) return e;
   int grid = a.nitems < per_sm * nsm ? a.nitems : per_sm * nsm;
   if (grid_out) *grid_out = grid;
@@ -62,6 +62,9 @@ cudaError_t launch_stage_one(const StageArgs& a, cudaStream_t s, int* grid_out) 
 template <typename T, int FLUX>
 cudaError_t launch_stage_f(const StageArgs& a, cudaStream_t s, bool multi, int* g) {
   const bool cons = a.s.rec_var != 0 && a.s.rec_linear;
+  if (multi && a.wall.mask)  // faces cut by an embedded surface attached
+    return cons ? launch_stage_one<T, FLUX, true, true, true>(a, s, g)
+                : launch_stage_one<T, FLUX, true, false, true>(a, s, g);
   if (multi)
     return cons ? launch_stage_one<T, FLUX, true, true>(a, s, g) : launch_stage_one<T, FLUX, true, false>(a, s, g);
   return cons ? launch_stage_one<T, FLUX, false, true>(a, s, g) : launch_stage_one<T, FLUX, false, false>(a, s, g);

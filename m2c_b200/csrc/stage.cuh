@@ -315,7 +315,9 @@ template <> struct StageOcc<float> { static constexpr int value = M2C_STAGE_OCC_
 
 // CONS: reconstruction in conservative or characteristic variables (a
 // separate instantiation so the primitive-variable kernels carry none of it).
-template <typename T, int TY, int FLUX, bool MULTI, bool CONS>
+// WALLS (two-material variant only): the branch of faces cut by an embedded
+// surface is compiled in; without it the kernel carries none of its tests.
+template <typename T, int TY, int FLUX, bool MULTI, bool CONS, bool WALLS = false>
 __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(const __grid_constant__ StageArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   typedef StageSmem<T, TY> S;
@@ -777,15 +779,15 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
     // branch, which the reference tests before the material-interface one
     bool wall = false;
     long long offW = 0;
-    if (MULTI && a.wall.mask && rL && rR) {
+    if (WALLS && rL && rR) {
       const int gi = wrap_index(i0 + mxR - 1, g.nx), gj = wrap_index(j0 + myR - 1, g.ny);
       offW = (long long)wrap_index(pR, g.nz) * g.plane + (long long)gj * g.px + gi;
       wall = (a.wall.mask[offW] >> d) & 1;
     }
     // face pass: only the faces whose states a pre-pass solves from
     const bool fp_iface = MULTI && a.iface.faces_out && idL != idR;
-    const bool fp_wall = MULTI && a.wall.faces_out && wall;
-    if (MULTI && (a.iface.faces_out || a.wall.faces_out) && !fp_iface && !fp_wall) {
+    const bool fp_wall = WALLS && a.wall.faces_out && wall;
+    if (MULTI && (a.iface.faces_out || (WALLS && a.wall.faces_out)) && !fp_iface && !fp_wall) {
 #pragma unroll
       for (int c = 0; c < 5; c++) { F[c] = T(0); F2[c] = T(0); }
       return;
@@ -995,7 +997,7 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       __syncthreads();
       if (m >= kb - 1) faces(m, m >= kb);
       __syncthreads();
-      if (m < kb || !own || (MULTI && (a.iface.faces_out || a.wall.faces_out))) continue;
+      if (m < kb || !own || (MULTI && (a.iface.faces_out || (WALLS && a.wall.faces_out)))) continue;
       // (4) residual + RK update of plane m
       const double dzk = g.dz[m];
       const double ax = dyj * dzk, ay = dxi * dzk, az = dxi * dyj;
@@ -1036,8 +1038,8 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       T F2[3][5];
       bool ifc[3] = {false, false, false};
       if constexpr (MULTI) {
-        const uint8_t wm = a.wall.mask ? a.wall.mask[off] : 0;
-        const bool num = a.iface.mp_flux == 1 && a.iface.slot;  // interface slots exist
+        const uint8_t wm = WALLS ? a.wall.mask[off] : 0;
+        const bool num = a.iface.mp_flux == 1;  // set only with interface slots (two-material contexts)
         if (num || wm) {
           const int sc = slot4(m), lx = tx + 2, ly = ty + 2;
           const uint8_t me = sm.ids[sc][ly][lx];
