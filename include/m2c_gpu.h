@@ -144,6 +144,11 @@ typedef struct {
    * or 1 LINEAR (the limited face states; a face pass writes them). */
   int ebm_riemann_normal;
   int ebm_recon;
+  /* EquationsData::dummy_state (VarFcnDummy): the fixed state of inactive
+   * cells, those with material ID = nmat (regions enclosed by an embedded
+   * surface; contexts without a level set): density, pressure, internal
+   * energy per unit mass (defaults 1e-6, 0, 0, IoData.cpp:30-42). */
+  double inactive_density, inactive_pressure, inactive_energy;
 } m2cg_scheme;
 
 /* One level set (LevelSetSchemeData, IoData.h:653-679; reinit

@@ -66,6 +66,7 @@ class Scheme(C.Structure):
         ("riem_pressure_at_failure", C.c_double), ("riem_warm_delta", C.c_double),
         ("mp_riemann_normal", C.c_int), ("riem_warm_gate", C.c_double),
         ("ebm_riemann_normal", C.c_int), ("ebm_recon", C.c_int),
+        ("inactive_density", C.c_double), ("inactive_pressure", C.c_double), ("inactive_energy", C.c_double),
     ]
 
 
@@ -120,6 +121,9 @@ def scheme(**kw):
     s.mp_riemann_normal = RIEMANN_NORMAL_MESH
     s.ebm_riemann_normal = EBM_NORMAL_MESH
     s.ebm_recon = 0
+    s.inactive_density = 1.0e-6
+    s.inactive_pressure = 0.0
+    s.inactive_energy = 0.0
     for k, v in kw.items():
         if not hasattr(s, k):
             raise AttributeError(k)

@@ -118,6 +118,9 @@ class TimeIntegratorGPU : public TimeIntegratorBase {
     s.mp_riemann_normal = (int)iod.multiphase.riemann_normal;
     s.ebm_riemann_normal = (int)iod.ebm.riemann_normal;  // EmbeddedBoundaryMethodData
     s.ebm_recon = (int)iod.ebm.recon;
+    s.inactive_density = iod.eqs.dummy_state.density;  // VarFcnDummy (Main.cpp:137)
+    s.inactive_pressure = iod.eqs.dummy_state.pressure;
+    s.inactive_energy = iod.eqs.dummy_state.internal_energy_per_mass;
     const ExactRiemannSolverData& r = iod.exact_riemann;
     s.riem_maxits_main = r.maxIts_main;
     s.riem_maxits_bracket = r.maxIts_bracket;

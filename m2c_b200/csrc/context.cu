@@ -90,6 +90,9 @@ extern "C" void m2cg_default_scheme(m2cg_scheme* s) {
   s->mp_riemann_normal = 1;  // MultiPhaseData::MESH (IoData.cpp:1408)
   s->ebm_riemann_normal = 1; // EmbeddedBoundaryMethodData::MESH (IoData.cpp:2937-2938)
   s->ebm_recon = 0;          // CONSTANT
+  s->inactive_density = 1.0e-6;  // StateVariable::StateVariable (IoData.cpp:30-42)
+  s->inactive_pressure = 0.0;
+  s->inactive_energy = 0.0;
 }
 
 extern "C" void m2cg_default_material(m2cg_material* m) {
@@ -433,6 +436,9 @@ extern "C" m2cg_status m2cg_create(const m2cg_grid* grid, const m2cg_scheme* sch
   sk.alpha = scheme->minmod_coeff;
   sk.delta = scheme->roe_delta;
   sk.nmat = nmat;
+  sk.dummy[0] = scheme->inactive_density;  // EquationsData::dummy_state (VarFcnDummy)
+  sk.dummy[1] = scheme->inactive_pressure;
+  sk.dummy[2] = scheme->inactive_energy;
   for (int m = 0; m < MAXMAT; m++) {
     MatParams p = to_params(mats[m < nmat ? m : 0]);
     sk.ed[m] = make_eos<double>(p);
@@ -520,9 +526,13 @@ __global__ void k_clip_state(Grid3 g, SchemeK sk, double* v0, double* v1, double
     int k = (int)(q / ((long long)g.nx * g.ny));
     long long o = (long long)k * g.plane + (long long)j * g.px + i;
     double V[5] = {v0[o], v1[o], v2[o], v3[o], v4[o]};
-    const Eos<double>& e = sk.ed[id[o] < sk.nmat ? id[o] : 0];
-    e.clip(V);
-    if (e.bad(V)) report(err, ERR_STATE, (int)q, 0);
+    if (id[o] >= sk.nmat) {  // inactive: VarFcnDummy::ClipDensityAndPressure sets its fixed state
+      V[0] = sk.dummy[0]; V[1] = V[2] = V[3] = 0.0; V[4] = sk.dummy[1];
+    } else {
+      const Eos<double>& e = sk.ed[id[o]];
+      e.clip(V);
+      if (e.bad(V)) report(err, ERR_STATE, (int)q, 0);
+    }
     v0[o] = V[0]; v1[o] = V[1]; v2[o] = V[2]; v3[o] = V[3]; v4[o] = V[4];
   }
 }
@@ -545,14 +555,21 @@ __global__ void k_to_float(Grid3 g, const double* v0, const double* v1, const do
   }
 }
 
-__global__ void k_unpack_id(const double* aos, int nx, int ny, int nz, long long px, long long plane, uint8_t* id) {
+// IDs 0..nmat-1, or nmat (inactive) where the context allows it (no level
+// set, no diffusive material); anything else is reported and stored as 0.
+__global__ void k_unpack_id(const double* aos, int nx, int ny, int nz, long long px, long long plane, uint8_t* id,
+                            int nmat, int allow_inactive, DevError* err) {
   long long n = (long long)nx * ny * nz;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     int i = (int)(q % nx);
     int j = (int)((q / nx) % ny);
     int k = (int)(q / ((long long)nx * ny));
     long long h = ((long long)(k + 1) * (ny + 2) + (j + 1)) * (nx + 2) + (i + 1);
-    id[(long long)k * plane + (long long)j * px + i] = (uint8_t)aos[h];
+    const double v = aos[h];
+    const int top = allow_inactive ? nmat : nmat - 1;
+    const bool ok = v >= 0.0 && v <= (double)top;
+    if (!ok) report(err, ERR_MATERIAL_ID, (int)q, 0);
+    id[(long long)k * plane + (long long)j * px + i] = ok ? (uint8_t)v : (uint8_t)0;
   }
 }
 
@@ -612,7 +629,8 @@ __global__ void __launch_bounds__(256) k_cfl(Grid3 g, SchemeK sk, const double* 
   for (int k = blockIdx.z; i < g.nx && j < g.ny && k < g.nz; k += gridDim.z) {
     const long long q = ((long long)k * g.ny + j) * g.nx + i;
     long long o = (long long)k * g.plane + (long long)j * g.px + i;
-    const Eos<double>& e = sk.ed[id && id[o] < sk.nmat ? id[o] : 0];
+    if (id && id[o] >= sk.nmat) continue;  // inactive cells do not limit the step (SpaceOperator.cpp:2154)
+    const Eos<double>& e = sk.ed[id ? id[o] : 0];
     double rho = v0[o], p = v4[o];
     double c2 = e.c2(rho, e.energy(rho, p));
     if (c2 < 0.0) report(err, ERR_SOUND, (int)q, 5);
@@ -674,6 +692,10 @@ static m2cg_status check_device_error(m2cg_ctx* c) {
     if (e.code == ERR_UNSUPPORTED)
       return fail(st, "unresolved background cells with apply_failsafe_density Off need the level-set "
                       "correction of unresolved cells, which is not supported");
+    if (e.code == ERR_MATERIAL_ID)
+      return fail(M2CG_ERR_ARG, "material ID out of range at cell %d: 0..nmat-1, or nmat (inactive, enclosed by "
+                                "an embedded surface) in a context without a level set or diffusive materials",
+                  e.cell);
     return fail(st, "device error code %d at cell %d (site %d)", e.code, e.cell, e.where);
   }
   return M2CG_OK;
@@ -710,7 +732,10 @@ extern "C" m2cg_status m2cg_upload_state(m2cg_ctx* c, const double* V, const dou
   double** D = c->V[c->cur];
   if (ID) {
     CK(cudaMemcpyAsync(c->stage_buf, ID, ng * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    k_unpack_id<<<grid1d(n), 256, 0, c->stream>>>(c->stage_buf, c->nx, c->ny, c->nz, c->px, c->plane, c->id);
+    // inactive cells (ID = nmat): one material without a level set, no diffusive material
+    const int allow_inactive = (!c->mp && !c->visc) ? 1 : 0;
+    k_unpack_id<<<grid1d(n), 256, 0, c->stream>>>(c->stage_buf, c->nx, c->ny, c->nz, c->px, c->plane, c->id,
+                                                  c->sk.nmat, allow_inactive, c->err);
   }
   CK(cudaMemcpyAsync(c->stage_buf, V, ng * 5 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   k_unpack_state<<<grid1d(n), 256, 0, c->stream>>>(c->stage_buf, c->nx, c->ny, c->nz, c->px, c->plane, 5, nullptr,

@@ -41,7 +41,8 @@ enum {
   ERR_HLLC = 10,      // NaN S* in HLLC (FluxFcnHLLC.h:235-241)
   ERR_RIEMANN = 4,
   ERR_ITER_CAP = 6,
-  ERR_UNSUPPORTED = 8  // a path the library does not implement was reached (state update)
+  ERR_UNSUPPORTED = 8,  // a path the library does not implement was reached (state update)
+  ERR_MATERIAL_ID = 11  // an uploaded material ID beyond the materials (or inactive where not allowed)
 };
 
 // std::min / std::max semantics (not fmin/fmax): min(a,b) = (b<a)?b:a.

@@ -92,7 +92,8 @@ struct SchemeK {
   int rec_var;             // ReconstructionData::VariableType: 0 primitive, 1 conservative,
                            // 2 primitive characteristic, 3 conservative characteristic
   double alpha, delta;
-  int nmat;
+  int nmat;               // material IDs 0..nmat-1; nmat = inactive (enclosed by an embedded surface)
+  double dummy[3];         // the inactive cells' fixed state: density, pressure, internal energy per mass
   Eos<double> ed[MAXMAT];  // per-material EOS, FP64 (built on the host)
   Eos<float> ef[MAXMAT];   // the same in FP32 for the mixed path's flux half
 };
@@ -546,10 +547,15 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       const uint8_t id = sm.ids[s0][ly][lx];
       zero = id != sm.ids[sm1][lym][lxm] || id != sm.ids[sp1][lyp][lxp];
     }
+    // no difference toward an inactive neighbour (Reconstructor.cpp:475-502)
+    const bool offm = WALLS && sm.ids[sm1][lym][lxm] == a.s.nmat;
+    const bool offp = WALLS && sm.ids[sp1][lyp][lxp] == a.s.nmat;
 #pragma unroll
     for (int c = 0; c < 5; c++) {
       const T vc = M2C_VV(s0, c, ly, lx);
-      T sl = limited_slope_c(limiter, A, B, K, alpha, vc - M2C_VV(sm1, c, lym, lxm), M2C_VV(sp1, c, lyp, lxp) - vc);
+      const T dm = offm ? T(0) : vc - M2C_VV(sm1, c, lym, lxm);
+      const T dp = offp ? T(0) : M2C_VV(sp1, c, lyp, lxp) - vc;
+      T sl = limited_slope_c(limiter, A, B, K, alpha, dm, dp);
       sd[c] = zero ? T(0) : sl;
     }
   };
@@ -594,10 +600,11 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       for (int c = 0; c < 5; c++) qp[c] = t[c];
     }
     const T* q0 = uspace ? u : v;
+    const bool offm = WALLS && idm == a.s.nmat, offp = WALLS && idp == a.s.nmat;  // Reconstructor.cpp:529-556
 #pragma unroll
     for (int c = 0; c < 5; c++) {
-      dl[c] = q0[c] - qm[c];
-      dr[c] = qp[c] - q0[c];
+      dl[c] = offm ? T(0) : q0[c] - qm[c];
+      dr[c] = offp ? T(0) : qp[c] - q0[c];
     }
     bool ok = true;
     if (rv == 1) {
@@ -644,6 +651,15 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       return;
     }
     const uint8_t id = sm.ids[s0][ly][lx];
+    if (WALLS && id == a.s.nmat) {
+      // inactive: constant reconstruction, no checks (Reconstructor.cpp:452-462,
+      // SpaceOperator.cpp:3236-3237)
+      for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int c = 0; c < 5; c++) sm.sig[ms][d][c][my][mx] = T(0);
+      sm.mask[ms][my][mx] = 0;
+      return;
+    }
     const Eos<T>& e = eos_of<T, MULTI>(a.s, id);
     T v[5];
 #pragma unroll
@@ -823,6 +839,14 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
           o[5 + c] = double(VR[c]);
         }
       }
+      return;
+    }
+    if (WALLS && (idL == a.s.nmat || idR == a.s.nmat) && !(wall && idL != a.s.nmat)) {
+      // an inactive side gets no flux, and a face with an inactive cell that
+      // no surface cuts carries none (SpaceOperator.cpp:2441-2483, 2537-2551);
+      // the right cell of a cut face forms its own flux in its update
+#pragma unroll
+      for (int c = 0; c < 5; c++) { F[c] = T(0); F2[c] = T(0); }
       return;
     }
     if (MULTI && (wall || idL != idR)) {
@@ -1007,6 +1031,32 @@ __global__ void __launch_bounds__(TX * TY, StageOcc<T>::value) stage_kernel(cons
       const double inv_mvol = 1.0 / (-vol);
       const long long off = (long long)m * g.plane + (long long)gj * g.px + gi;
       const uint8_t id = MULTI ? a.id[off] : 0;
+      if (WALLS && id == a.s.nmat) {
+        // inactive: no residual (every face gives it a zero flux), and
+        // VarFcnDummy's fixed states after every stage (VarFcnDummy.h:44-57)
+        if (a.Ro[0]) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) a.Ro[c][off] = 0.0 * inv_mvol;
+          continue;
+        }
+        const double Vd[5] = {a.s.dummy[0], 0.0, 0.0, 0.0, a.s.dummy[1]};
+        if (a.final_stage) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) a.Vo[c][off] = Vd[c];
+          if (a.Vfo[0]) {
+#pragma unroll
+            for (int c = 0; c < 5; c++) a.Vfo[c][off] = float(Vd[c]);
+          }
+        } else {
+          const double Ud[5] = {a.s.dummy[0], 0.0, 0.0, 0.0, a.s.dummy[0] * a.s.dummy[2]};
+#pragma unroll
+          for (int c = 0; c < 5; c++) {
+            a.Uo[c][off] = Ud[c];
+            static_cast<T*>(a.Po[c])[off] = T(Vd[c]);
+          }
+        }
+        continue;
+      }
       const Eos<double>& e = eos_of<double, MULTI>(a.s, id);
       double Un[5], Unew[5], Vn[5];
 #pragma unroll

@@ -107,6 +107,7 @@ __global__ void __launch_bounds__(128, 4) k_wall_riemann(WallPassArgs a) {
     // cell against it seen backward (SpaceOperator.cpp:2440-2479)
     const long long off = side ? offR : offR - (d == 0 ? 1LL : (d == 1 ? g.px : g.plane));
     const uint8_t id = a.st.id[off];
+    if (id >= a.st.s.nmat) continue;  // an inactive side gets no flux and no problem
     double V[5];
     if (a.faceV) {  // LINEAR: vr of the low cell, vl of the high cell (SpaceOperator.cpp:2452, 2474)
       const double* fv = a.faceV + (3LL * sl + d) * 10 + 5 * side;

@@ -131,6 +131,9 @@ void fill_scheme(IoData& iod, const m2cg_scheme& s) {
   iod.multiphase.riemann_normal = (MultiPhaseData::RiemannNormal)s.mp_riemann_normal;
   iod.ebm.riemann_normal = (EmbeddedBoundaryMethodData::RiemannNormal)s.ebm_riemann_normal;
   iod.ebm.recon = (EmbeddedBoundaryMethodData::ReconstructionAtInterface)s.ebm_recon;
+  iod.eqs.dummy_state.density = s.inactive_density;
+  iod.eqs.dummy_state.pressure = s.inactive_pressure;
+  iod.eqs.dummy_state.internal_energy_per_mass = s.inactive_energy;
   ExactRiemannSolverData& r = iod.exact_riemann;
   r.maxIts_main = s.riem_maxits_main;
   r.maxIts_bracket = s.riem_maxits_bracket;

@@ -220,3 +220,79 @@ def test_wall_faces_refused(gpu):
     with pytest.raises(gpu.M2CError, match="viscous"):
         visc.set_wall_faces([(0, 3, 3, 3)])
     visc.close()
+
+
+def enclosed_block(g, V, lo=(4, 3, 3), hi=(9, 8, 6), speed=0.0, seed=0):
+    """A closed box-shaped surface around the cells lo <= (i, j, k) < hi:
+    those cells become inactive (material ID = nmat = 1, the dummy state),
+    and the faces of the block's boundary are cut, each seen from outside
+    with the outward normal and from inside with the inward one."""
+    rng = np.random.default_rng(seed)
+    ID = np.zeros(V.shape[:3])
+    V = V.copy()
+    sl = np.s_[lo[2] + 1:hi[2] + 1, lo[1] + 1:hi[1] + 1, lo[0] + 1:hi[0] + 1]
+    ID[sl] = 1
+    V[sl] = (1.0e-6, 0.0, 0.0, 0.0, 0.0)
+    faces, nf, nb = [], [], []
+    for d in range(3):
+        for side, plane in ((0, lo[d]), (1, hi[d])):
+            ranges = [range(lo[a], hi[a]) if a != d else [plane] for a in range(3)]
+            for i in ranges[0]:
+                for j in ranges[1]:
+                    for k in ranges[2]:
+                        faces.append((d, i, j, k))
+                        n = np.zeros(3)
+                        n[d] = -1.0 if side == 0 else 1.0  # the block's outward normal
+                        nf.append(n)  # seen from the low cell
+                        nb.append(n)
+    faces = np.array(faces, np.int32)
+    u = rng.uniform(-speed, speed, (len(faces), 3))
+    return ID, V, (faces, np.array(nf), u, np.array(nb), u)
+
+
+@pytest.mark.parametrize("linear,normal", [(False, abi.EBM_NORMAL_MESH), (True, abi.EBM_NORMAL_SURFACE)])
+def test_enclosed_inactive_region_matches_reference(gpu, ref, linear, normal):
+    """A closed surface around a block of inactive cells (the reference's
+    INACTIVE_MATERIAL_ID with VarFcnDummy's fixed state): no slope toward an
+    inactive neighbour, constant reconstruction and no checks inside, zero
+    fluxes on the inactive side of every cut face, no CFL contribution;
+    residual and 6 whole steps."""
+    g, s, mats, V = cases.random_box(14, 11, 9, seed=5, rk=3)
+    s.ebm_recon = int(linear)
+    s.ebm_riemann_normal = normal
+    ID, V, W = enclosed_block(g, V, speed=0.2, seed=1)
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V, ID)
+    sol.set_wall_faces(*W)
+    rc = ref.RefCase(g, s, mats)
+    rc.set_state(V, ID)
+    Rr = inner(rc.residual_walls(*W))
+    assert rel_err(inner(sol.residual()), Rr) <= TOL
+    n, t = sol.run(6)
+    nr, tr = rc.run_walls(*W, 6)
+    assert n == nr == 6 and t == tr
+    Vg, IDg, _ = sol.download()
+    Vr, IDr, _ = rc.get_state()
+    assert rel_err(inner(Vg), inner(Vr)) <= TOL
+    inside = inner(ID) == 1
+    assert np.array_equal(inner(Vg)[inside], np.tile([1.0e-6, 0.0, 0.0, 0.0, 0.0], (inside.sum(), 1)))
+    sol.close()
+
+
+def test_inactive_ids_allowed_only_where_supported(gpu):
+    """ID = nmat marks an inactive cell in a context of one material without
+    diffusion; elsewhere, and beyond nmat anywhere, the upload is refused."""
+    g, s, mats, V = cases.random_box(10, 8, 6, seed=5)
+    ID = np.zeros(V.shape[:3])
+    ID[3, 3, 3] = 1
+    sol = gpu.Solver(g, s, mats)
+    sol.upload(V, ID)  # accepted
+    ID[3, 3, 4] = 2
+    with pytest.raises(gpu.M2CError, match="material ID"):
+        sol.upload(V, ID)
+    sol.close()
+    heat = gpu.Solver(g, s, [abi.material(1.4, 0.0, heat_diffusivity=0.02, cv=2.5)])
+    ID[3, 3, 4] = 0
+    with pytest.raises(gpu.M2CError, match="material ID"):
+        heat.upload(V, ID)
+    heat.close()
