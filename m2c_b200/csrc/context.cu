@@ -770,7 +770,7 @@ extern "C" m2cg_status m2cg_update_states_after_interface_motion(m2cg_ctx* c, co
   long long n = (long long)c->nx * c->ny * c->nz;
   CK(cudaMemcpyAsync(c->stage_buf, IDn, ng * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   k_unpack_id<<<grid1d(n), 256, 0, c->stream>>>(c->stage_buf, c->nx, c->ny, c->nz, c->px, c->plane,
-                                                 multiphase_idn(c->mp));
+                                                 multiphase_idn(c->mp), c->sk.nmat, 0, c->err);
   CK(cudaGetLastError());
   const bool mixed = c->scheme.precision == M2CG_PREC_MIXED;
   st = multiphase_update_states(c->mp, c->stream, c->V[c->cur], mixed ? c->Vf[c->cur] : nullptr, c->id, c->err,
