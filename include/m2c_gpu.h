@@ -268,9 +268,11 @@ m2cg_status m2cg_get_counters(const m2cg_ctx* ctx, m2cg_counters* c);
  * the reference (HeatDiffusionOperator::AddDiffusionFluxes does not use it).
  * Refused (M2CG_ERR_UNSUPPORTED): viscous materials (the viscosity
  * operator's ghost-fluid population at cut faces is not built), faces on
- * the subdomain boundary. Every cell stays active (the
- * reference's INACTIVE_MATERIAL_ID regions enclosed by a surface are not
- * represented). Host pointers. */
+ * the subdomain boundary. Regions enclosed by a surface: upload their
+ * cells with material ID nmat (the reference's INACTIVE_MATERIAL_ID; one
+ * material, no level set, no diffusion); they keep the scheme's inactive
+ * state, take no slope from or flux across their side, and do not limit
+ * the time step. Host pointers. */
 m2cg_status m2cg_set_wall_faces(m2cg_ctx* ctx, int n, const int* faces, const double* nwall_fwd,
                                 const double* uwall_fwd, const double* nwall_bwd, const double* uwall_bwd);
 
