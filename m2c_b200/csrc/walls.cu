@@ -38,7 +38,6 @@ struct WallPassArgs {
   StageArgs st;
   RiemannParams P;
   const int* cell;
-  const uint8_t* mask;
   const double* geo;
   double* Vsm;
   double* Vsp;
@@ -265,7 +264,6 @@ m2cg_status walls_stage(Walls* w, cudaStream_t s, StageArgs& a) {
   p.st = a;
   p.P = w->P;
   p.cell = w->cell;
-  p.mask = w->mask;
   p.geo = w->geo;
   p.Vsm = w->Vsm;
   p.Vsp = w->Vsp;
