@@ -590,10 +590,10 @@ __device__ __forceinline__ double reinit_local(const Grid3& g, const LsGeom& geo
 //   stage 2: out = 0.25*in + 0.75*phi + 0.25*R(in)  (in = phi1, out = phi2)
 //   stage 3: phi = 1/3*phi + 2/3*in + 2/3*R(in)     (in = phi2, out = phi)
 // Thread (x, y) of CTA (bx, by, bz) owns cell (32 bx + x, 8 by + y, bz): no
-// index division, rows of 32 consecutive cells per warp. Five CTAs per SM (48
-// registers) rather than four (64): the stage waits on loads, and the extra
-// resident warps made it about 10 % faster at 384^3.
-__global__ void __launch_bounds__(256, 5) k_reinit_stage(Grid3 g, LsGeom geo, ReinitBuf b, int stage, double cfl,
+// index division, rows of 32 consecutive cells per warp. Six CTAs per SM (40
+// registers, a few spills) rather than four (64): the stage waits on loads,
+// and the extra resident warps made it about 13 % faster at 384^3.
+__global__ void __launch_bounds__(256, 6) k_reinit_stage(Grid3 g, LsGeom geo, ReinitBuf b, int stage, double cfl,
                                                       double tol, const double* in, double* phi, double* out,
                                                       int fix_first) {
   if (b.red[4] || (stage > 1 && b.red[3])) return;  // attempt finished, or converged on the residual in stage 1
