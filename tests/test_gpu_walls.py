@@ -185,10 +185,12 @@ def test_wall_residual_with_heat_diffusion_matches_reference(gpu, ref):
     sol.close()
 
 
-def test_wall_steps_mixed_track_fp64(gpu):
+@pytest.mark.parametrize("linear", [False, True])
+def test_wall_steps_mixed_track_fp64(gpu, linear):
     out = []
     for prec in (abi.PREC_FP64, abi.PREC_MIXED):
         g, s, mats, V = cases.random_box(14, 11, 9, seed=5, precision=prec)
+        s.ebm_recon = int(linear)
         W = wall_faces(g, 120, seed=1)
         sol = gpu.Solver(g, s, mats)
         sol.upload(V)
